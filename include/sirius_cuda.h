@@ -1,0 +1,297 @@
+/*
+ * sirius_cuda.h — C ABI of the B200 geodesic engine.
+ *
+ * This is the drop-in boundary for Sirius's per-pixel null-geodesic hot path.
+ * It replaces, for the CUDA backend slot the reference reserves:
+ *   - the OptiX C entry points  sirius_optix_*      (src/Sirius.Render/Acceleration/OptiX/RDOP006A.h:10-39)
+ *   - the per-ray CPU tracer    GeodesicTracer::trace (src/Sirius.Render/Integration/GTRC001A.h:220, GTRC001A.cpp:139-592)
+ *   - the integrator step       Geodesic::integrateStepRK45 (src/Sirius.Core/Geodesic/PHGD001A.h:120)
+ *   - the metric evaluation     IMetric::evaluate (src/Sirius.Core/Metric/PHMT000A.h:38)
+ *
+ * Conventions (all entry points):
+ *   - plain C types only; every struct below is POD with a fixed layout (static
+ *     asserts in the implementation pin the sizes);
+ *   - every call returns an int status (SIRIUS_OK == 0); no C++ exception ever
+ *     crosses this boundary; the last error message of a handle is available
+ *     from sirius_cuda_get_last_error();
+ *   - "host" entry points take caller-owned HOST buffers, copy in, run, copy out
+ *     and synchronise before returning (like sirius_optix_launch, RDOP001A.cu:1044);
+ *   - "_device" entry points take caller-owned DEVICE buffers and a CUDA stream
+ *     (cudaStream_t passed as void*), and are stream-ordered and asynchronous;
+ *   - one handle per host thread; a handle owns its device scratch memory;
+ *   - there is no CPU fallback: if the CUDA kernels cannot run the call fails
+ *     with SIRIUS_ERR_CUDA / SIRIUS_ERR_NO_DEVICE.
+ */
+#ifndef SIRIUS_CUDA_H
+#define SIRIUS_CUDA_H
+
+#include <stdint.h>
+#include <stddef.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+#define SIRIUS_CUDA_ABI_VERSION 1
+
+/* ---- status codes --------------------------------------------------------- */
+enum sirius_status {
+    SIRIUS_OK = 0,
+    SIRIUS_ERR_INVALID_ARGUMENT = 1,
+    SIRIUS_ERR_CUDA = 2,
+    SIRIUS_ERR_NO_DEVICE = 3,
+    SIRIUS_ERR_NOT_CONFIGURED = 4,
+    SIRIUS_ERR_TIMEOUT = 5,
+    SIRIUS_ERR_OUT_OF_MEMORY = 6,
+    SIRIUS_ERR_UNSUPPORTED = 7
+};
+
+/* ---- metric families (IMetric implementations) ---------------------------- */
+enum sirius_metric_family {
+    SIRIUS_METRIC_KERR_SCHILD = 0,   /* KerrSchildFamily (M,a,Q,Lambda), PHMT100A.h:72   */
+    SIRIUS_METRIC_MORRIS_THORNE = 1, /* MorrisThorneFamily, PHMT101A.h:111               */
+    SIRIUS_METRIC_ALCUBIERRE = 2     /* WarpDriveFamily, PHMT102A.h:71                   */
+};
+
+/* Morris-Thorne shape functions (WormholeShapeType, PHMT101A.h) */
+enum sirius_wormhole_shape {
+    SIRIUS_WORMHOLE_ELLIS = 0,
+    SIRIUS_WORMHOLE_ZERO_TIDAL = 1,
+    SIRIUS_WORMHOLE_ABSURDLY_BENIGN = 2
+};
+
+/* ---- ray outcomes ---------------------------------------------------------
+ * The first five keep the order of TraceResult::Outcome (GTRC001A.h:46-52);
+ * the rest split the reference's catch-all MAX_STEPS into explicit causes. */
+enum sirius_outcome {
+    SIRIUS_ESCAPED = 0,
+    SIRIUS_HORIZON = 1,
+    SIRIUS_DISK_HIT = 2,
+    SIRIUS_MAX_STEPS = 3,
+    SIRIUS_SPIRALING = 4,
+    SIRIUS_NUMERICAL_FAILURE = 5, /* NaN/Inf in the state (reference terminated = 3) */
+    SIRIUS_STEP_UNDERFLOW = 6,    /* h <= min_step after a reject (reference terminated = 5) */
+    SIRIUS_THROAT = 7,            /* reached the Morris-Thorne throat clamp */
+    SIRIUS_REJECTED = 8           /* reference-compatible mode only: a rejected step ends the ray
+                                     (GTRC001A.cpp:272-277 reports it as MAX_STEPS) */
+};
+
+/* ---- precision modes ------------------------------------------------------ */
+enum sirius_precision {
+    SIRIUS_PRECISION_FP64 = 0,  /* every operation in FP64 (the plain FP64 GPU integrator) */
+    SIRIUS_PRECISION_MIXED = 1  /* FP32 dual-number RHS, FP64 state accumulation, FP64
+                                   constraint re-projection, FP64 RHS and error control inside
+                                   the photon region and near the horizon */
+};
+
+enum sirius_integrator {
+    SIRIUS_INTEGRATOR_DP45 = 0,       /* Dormand-Prince RK45, PHGD001A.cpp:530-641 */
+    SIRIUS_INTEGRATOR_SYMPLECTIC = 1  /* Yoshida-composed kick-drift-kick, PHSI001A.h:136-215 */
+};
+
+enum sirius_projection {
+    SIRIUS_CAMERA_PINHOLE = 0,        /* PinholeCamera, CMBS001A.h:113-205 */
+    SIRIUS_CAMERA_EQUIRECTANGULAR = 1 /* 360x180 sky map (LensType::Panoramic has no
+                                         implementation in the reference, CMBS001A.h:68,351-362) */
+};
+
+/* ---- metric parameters ---------------------------------------------------- */
+typedef struct sirius_metric {
+    int32_t family;   /* enum sirius_metric_family */
+    int32_t shape;    /* enum sirius_wormhole_shape (Morris-Thorne only) */
+    double M, a, Q, Lambda;      /* Kerr-Schild family; a is the spin length a = a_* M */
+    double b0, Phi0;             /* Morris-Thorne throat radius and constant redshift */
+    double vs, sigma, R;         /* Alcubierre bubble velocity, wall steepness, radius */
+} sirius_metric;
+
+/* ---- camera (CameraConfig, CMBS001A.h:37-58) -------------------------------- */
+typedef struct sirius_camera {
+    double t, r, theta, phi;     /* observer position (Boyer-Lindquist / spherical) */
+    float yaw, pitch, roll;      /* radians */
+    float fov;                   /* degrees (pinhole) */
+    int32_t width, height;
+    int32_t projection;          /* enum sirius_projection */
+    int32_t reserved;            /* must be 0 (one sample per pixel, at the pixel centre) */
+} sirius_camera;
+
+/* ---- one frame of a (possibly heterogeneous) batch ------------------------ */
+typedef struct sirius_frame {
+    sirius_metric metric;
+    sirius_camera camera;
+    double disk_inner;           /* <= 0: use the prograde ISCO of the frame's (M,a) */
+    double disk_outer;
+    int64_t ray_offset;          /* first ray/pixel index of this frame in the batch outputs */
+} sirius_frame;
+
+/* ---- a host-generated camera ray (CameraRay, CMBS001A.h:26-32) -------------- */
+typedef struct sirius_camera_ray {
+    double origin[4];            /* (t, r, theta, phi) Boyer-Lindquist */
+    double direction[4];         /* (0, v_r, r v_theta, r sin(theta) v_phi) */
+} sirius_camera_ray;
+
+/* ---- tracer + integrator configuration -------------------------------------
+ * Mirrors IntegratorConfig (PHGD001A.h:48-58), TracerConfig (GTRC001A.h:162-196)
+ * and the precision / batching knobs of the B200 engine. */
+typedef struct sirius_trace_config {
+    /* IntegratorConfig */
+    double abs_tolerance;
+    double rel_tolerance;
+    double min_step;
+    double max_step;
+    double initial_step;
+    double safety_factor;
+    double step_grow_max;
+    double step_shrink_min;
+    /* TracerConfig */
+    double escape_radius;        /* coordinate radius sqrt(x^2+y^2+z^2) beyond which an outgoing ray escapes */
+    double horizon_factor;       /* terminate at r_BL < horizon_factor * r_+ */
+    int32_t max_steps;           /* accepted steps per ray */
+    int32_t enable_disk;         /* thin Novikov-Thorne disk crossings */
+    double disk_temperature_inner;
+    double crossing_weight_decay;/* image intensity weight exp(-decay * n) for crossing n */
+    /* volumetric radiative transfer */
+    int32_t enable_volumetric;
+    int32_t n_bins;              /* frequency bins, <= SIRIUS_MAX_BINS */
+    double nu_min, nu_max;       /* log-spaced bin centres, in units of the reference frequency */
+    double vol_j0;               /* emissivity normalisation: j = vol_j0 r^-2 exp(-z^2/(2 (h r)^2)) (nu_em)^-s */
+    double vol_alpha_over_j;     /* absorption alpha_nu = vol_alpha_over_j * j_nu */
+    double vol_height_ratio;     /* h in the Gaussian scale height h*r */
+    double vol_spectral_index;   /* s */
+    int32_t vol_substeps;        /* midpoint samples per step segment inside the emitting volume */
+    /* engine knobs */
+    int32_t integrator;          /* enum sirius_integrator */
+    int32_t precision;           /* enum sirius_precision */
+    int32_t compat;              /* 1: reference-compatible semantics (float roundings, stop on reject,
+                                    E-changing normalizeNull, Euclidean horizon/disk radii) */
+    int32_t projection_period;   /* FP64 constraint re-projection every N accepted steps (0 = never) */
+    int32_t spiral_check;        /* 1: the reference's spiral early-out (GTRC001A.cpp:322-352) */
+    double island_factor;        /* FP64 island: r_BL < island_factor * r_ph(retrograde) or r_BL < 2 r_+ */
+    double symplectic_step;      /* fixed d-lambda of the symplectic integrator */
+    int32_t symplectic_order;    /* 4, 6 or 8 (Yoshida) */
+    int32_t block_size;          /* threads per block (0 = autotuned / default) */
+    int32_t refill_threshold;    /* refill a warp when fewer than this many lanes are live (1..32) */
+    int32_t blocks_per_sm;       /* persistent grid = SMs * blocks_per_sm (0 = occupancy based) */
+    int32_t watchdog_ms;         /* bound on any spin-wait inside the kernels */
+    int32_t reserved[5];
+} sirius_trace_config;
+
+#define SIRIUS_MAX_BINS 32
+#define SIRIUS_FLAG_NUMERICAL_FAILURE 1  /* TraceResult::numerical_failure */
+#define SIRIUS_FLAG_PHOTON_RING 2        /* TraceResult::photon_ring */
+#define SIRIUS_MAX_CROSSINGS 4
+
+/* ---- per-ray result (TraceResult, GTRC001A.h:44-157) ------------------------ */
+typedef struct sirius_ray_result {
+    int32_t outcome;             /* enum sirius_outcome */
+    int32_t steps;               /* accepted steps */
+    int32_t rejected;            /* rejected step attempts */
+    int32_t n_crossings;         /* valid disk crossings (<= 4) */
+    double final_x[4];           /* KS Cartesian (t,x,y,z) (spherical for Morris-Thorne) */
+    double final_p[4];           /* covariant momentum p_mu at termination */
+    float final_k[4];            /* contravariant k^mu = g^{mu nu} p_nu at termination */
+    float disk_r[SIRIUS_MAX_CROSSINGS];      /* radius at crossing (BL r; Euclidean cylindrical in compat) */
+    float disk_phi[SIRIUS_MAX_CROSSINGS];
+    float disk_g[SIRIUS_MAX_CROSSINGS];      /* redshift factor g at crossing */
+    float disk_flux[SIRIUS_MAX_CROSSINGS];   /* Novikov-Thorne/Page-Thorne flux F(r) */
+    int32_t equatorial_crossings;
+    int32_t image_order;
+    float total_phi_change;
+    float min_radius;
+    float intensity;             /* bolometric: sum_n exp(-decay n) g_n^4 F(r_n) (+ volumetric) */
+    float E, Lz, Carter;         /* conserved quantities at termination (p_t, KS azimuthal, Carter Q) */
+    float E0, Lz0, Carter0;      /* ... at initialisation */
+    float null_drift_max;        /* max over accepted steps of |g^{mu nu} p_mu p_nu| before re-projection */
+    float null_final;            /* |g^{mu nu} p_mu p_nu| of the returned state */
+    float impact_parameter;
+    float magnification;
+    float optical_depth;
+    int32_t fp64_steps;          /* accepted steps taken on the FP64 island path (mixed precision) */
+    int32_t flags;               /* SIRIUS_FLAG_* bits */
+} sirius_ray_result;
+
+/* ---- launch statistics ------------------------------------------------------ */
+typedef struct sirius_launch_stats {
+    double kernel_ms;            /* device time of the trace kernel(s), CUDA events on the launch stream */
+    double total_ms;             /* device time of the whole call including copies */
+    int64_t rays;
+    int64_t accepted_steps;
+    int64_t rejected_steps;
+    int64_t fp64_steps;
+    int32_t kernel_launches;     /* kernels this engine launched for the call */
+    int32_t grid_blocks;
+    int32_t block_size;
+    int32_t status_flags;        /* bit 0: watchdog expired in a spin-wait */
+} sirius_launch_stats;
+
+typedef void* sirius_cuda_handle;
+
+/* ---- lifecycle (sirius_optix_create/destroy/initialize, RDOP006A.h:14-19) ---- */
+int sirius_cuda_create(int device, sirius_cuda_handle* out_handle);
+int sirius_cuda_destroy(sirius_cuda_handle handle);
+const char* sirius_cuda_get_last_error(sirius_cuda_handle handle);
+int sirius_cuda_abi_version(void);
+
+/* The defaults of TracerConfig/IntegratorConfig as set by RenderSession
+ * (SNRS001A.cpp:103-129) with the engine knobs at their defaults. */
+int sirius_cuda_default_config(sirius_trace_config* out_config);
+int sirius_cuda_configure(sirius_cuda_handle handle, const sirius_trace_config* config);
+
+/* ---- frame rendering (IAccelerator::launch + getFrameBuffer, ACIB001A.h:166-170;
+ *      sirius_optix_launch + sirius_optix_get_frame_buffer, RDOP006A.h:22,28) ---------
+ * Camera rays are generated on the device. Outputs are indexed by
+ * frame.ray_offset + y * width + x. Any output pointer may be NULL.
+ *   image:   one float per pixel (bolometric intensity)
+ *   spectra: n_bins floats per pixel (volumetric transfer), pixel-major
+ * Host variant: host buffers, synchronous. */
+int sirius_cuda_trace_frames(sirius_cuda_handle handle,
+                             const sirius_frame* frames, int32_t n_frames,
+                             sirius_ray_result* results, float* image, float* spectra);
+
+/* Device variant: frames/results/image/spectra are device pointers; stream-ordered. */
+int sirius_cuda_trace_frames_device(sirius_cuda_handle handle,
+                                    const sirius_frame* d_frames, int32_t n_frames,
+                                    int64_t total_rays,
+                                    sirius_ray_result* d_results, float* d_image, float* d_spectra,
+                                    void* stream);
+
+/* ---- batch form of GeodesicTracer::trace(const CameraRay&) (GTRC001A.h:220) ----
+ * Host-generated rays through one metric; disk_inner <= 0 selects the ISCO. */
+int sirius_cuda_trace_rays(sirius_cuda_handle handle, const sirius_metric* metric,
+                           double disk_inner, double disk_outer,
+                           const sirius_camera_ray* rays, int64_t n_rays,
+                           sirius_ray_result* results);
+
+/* ---- IMetric::evaluate on the device for a batch of points (PHMT000A.h:38) -------
+ * positions: n x 4; g: n x 16; dg: n x 64 with dg[l*16 + m*4 + n] = d_l g_mn.
+ * precision selects the FP64 or FP32 dual-number path. Host buffers. */
+int sirius_cuda_metric_evaluate(sirius_cuda_handle handle, const sirius_metric* metric,
+                                const double* positions, int64_t n, int32_t precision,
+                                double* g, double* dg);
+
+/* ---- one Dormand-Prince step for a batch of states (Geodesic::integrateStepRK45,
+ *      PHGD001A.cpp:530-641, without termination logic) ---------------------------
+ * state: n x 8 (x^mu, p_mu), h: n step sizes. On return state holds the accepted
+ * state (or the input if rejected), h the next step size, accepted[i] 0/1 and
+ * err[i] the scaled error norm. Host buffers. */
+int sirius_cuda_dp45_step(sirius_cuda_handle handle, const sirius_metric* metric,
+                          double* state, double* h, int32_t* accepted, double* err,
+                          int64_t n);
+
+/* ---- statistics of the last trace call ---------------------------------------- */
+int sirius_cuda_last_stats(sirius_cuda_handle handle, sirius_launch_stats* out_stats);
+
+/* ---- autotuner: times block size x refill threshold x blocks/SM on the given
+ * frames and stores the best setting in the handle's configuration.
+ * The chosen values are written to *out_config (may be NULL). ---------------- */
+int sirius_cuda_autotune(sirius_cuda_handle handle, const sirius_frame* frames, int32_t n_frames,
+                         sirius_trace_config* out_config);
+
+/* ---- SIMT peak microbenchmark: FMA-chain throughput of the device in FLOP/s
+ * (one FMA = 2 FLOP); precision 0 = FP64, 1 = FP32. ------------------------- */
+int sirius_cuda_measure_fma_peak(sirius_cuda_handle handle, int32_t precision, double* flops_per_s);
+
+#ifdef __cplusplus
+}
+#endif
+
+#endif /* SIRIUS_CUDA_H */

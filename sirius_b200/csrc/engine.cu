@@ -1,0 +1,1051 @@
+// engine.cu — the B200 geodesic engine: kernels and the C ABI (include/sirius_cuda.h).
+//
+// Kernels
+//   trace_kernel<MIXED>   persistent ray tracer. Each warp keeps 32 live rays;
+//                         when the live count falls below a threshold the
+//                         dead lanes are refilled from a global ray queue with
+//                         one atomicAdd per warp (ballot + popc prefix), so
+//                         rays with wildly different step counts do not idle
+//                         lanes. MIXED=false is the all-FP64 integrator (also
+//                         launched non-persistently as the plain baseline).
+//   metric_kernel         IMetric::evaluate for a batch of points.
+//   dp45_step_kernel      one Geodesic::integrateStepRK45 attempt per state.
+//   fma_peak_kernel       FP32/FP64 FMA-chain microbenchmark (roofline peak).
+#include <cuda_runtime.h>
+
+#include <algorithm>
+#include <chrono>
+#include <cmath>
+#include <cstdio>
+#include <cstring>
+#include <new>
+#include <string>
+#include <vector>
+
+#include "trace.cuh"
+
+using namespace sirius;
+
+static_assert(sizeof(sirius_metric) == 80, "sirius_metric layout");
+static_assert(sizeof(sirius_camera) == 64, "sirius_camera layout");
+static_assert(sizeof(sirius_frame) == 168, "sirius_frame layout");
+static_assert(sizeof(sirius_camera_ray) == 64, "sirius_camera_ray layout");
+
+namespace {
+
+constexpr unsigned kFull = 0xffffffffu;
+
+struct Params {
+    const FrameDev* frames;
+    int n_frames;
+    long long total;
+    sirius_ray_result* results;
+    float* image;
+    float* spectra;
+    const sirius_camera_ray* host_rays;  // optional: explicit camera rays (device copy)
+    unsigned long long* queue;            // [0] ray cursor
+    unsigned long long* counters;         // [0] accepted, [1] rejected, [2] fp64 steps
+    int* status;                          // [0] watchdog flag
+    int persistent;
+    int refill_threshold;
+    unsigned long long watchdog_ns;       // globaltimer bound for the whole launch, per warp
+    CfgDev c;
+};
+
+__device__ __forceinline__ unsigned long long globaltimer() {
+    unsigned long long t;
+    asm volatile("mov.u64 %0, %globaltimer;" : "=l"(t));
+    return t;
+}
+
+__device__ __forceinline__ int find_frame(const FrameDev* frames, int n, long long idx) {
+    int lo = 0, hi = n - 1;
+    while (lo < hi) {
+        const int mid = (lo + hi + 1) >> 1;
+        if (frames[mid].ray_offset <= idx) lo = mid; else hi = mid - 1;
+    }
+    return lo;
+}
+
+// Per-ray state held in registers between steps.
+struct Ray {
+    double x[4], p[4], kx[4], kp[4];
+    double h;
+    double intensity;
+    float min_r, null_max, tphi, prev_z;
+    int steps, rejected, attempts, ncross, eq, fp64_steps;
+    int frame;
+    long long idx;
+};
+
+__device__ __forceinline__ void write_default_crossings(sirius_ray_result* R) {
+#pragma unroll
+    for (int i = 0; i < SIRIUS_MAX_CROSSINGS; ++i) {
+        R->disk_r[i] = 0.f; R->disk_phi[i] = 0.f; R->disk_g[i] = 1.f; R->disk_flux[i] = 0.f;
+    }
+}
+
+__device__ __forceinline__ void invariants(const MetricDev& m, const InvForm& F, const double x[4], const double p[4],
+                                           float& E, float& Lz, float& Q) {
+    E = float(-p[0]);
+    if (m.family == SIRIUS_METRIC_MORRIS_THORNE) {
+        const double s = sin(x[2]), c = cos(x[2]);
+        Lz = float(p[3]);
+        Q = float(p[2] * p[2] + c * c * p[3] * p[3] / (s * s));
+        return;
+    }
+    const double L = x[1] * p[2] - x[2] * p[1];
+    Lz = float(L);
+    const double r = F.r;
+    const double ct = fmin(fmax(x[3] / r, -1.0), 1.0);
+    const double st = sqrt(fmax(1.0 - ct * ct, 1e-30));
+    const double pth = (ct / st) * (x[1] * p[1] + x[2] * p[2]) - r * st * p[3];
+    const double e = -p[0];
+    Q = float(pth * pth + ct * ct * (-m.a2 * e * e + L * L / (st * st)));
+}
+
+__device__ void begin_ray(const Params& P, Ray& s, long long idx, float* vol) {
+    s.idx = idx;
+    s.frame = P.n_frames > 1 ? find_frame(P.frames, P.n_frames, idx) : 0;
+    const FrameDev& F = P.frames[s.frame];
+    double dir[4];
+    if (P.host_rays) {
+        const sirius_camera_ray& cr = P.host_rays[idx];
+        for (int i = 0; i < 4; ++i) dir[i] = cr.direction[i];
+    } else {
+        const long long pix = idx - F.ray_offset;
+        camera_dir(F, int(pix % F.width), int(pix / F.width), dir);
+    }
+    init_state(F, dir, s.x, s.p);
+    rhs<double>(F.m, s.x, s.p, s.kx, s.kp);
+    s.h = P.c.h0;
+    s.intensity = 0.0;
+    s.min_r = 1e10f;
+    s.null_max = 0.f;
+    s.tphi = 0.f;
+    s.prev_z = float(s.x[3]);
+    s.steps = s.rejected = s.attempts = s.ncross = s.eq = s.fp64_steps = 0;
+    if (P.results) {
+        sirius_ray_result* R = P.results + idx;
+        write_default_crossings(R);
+        InvForm IF;
+        inv_form(F.m, s.x, IF);
+        float E, L, Q;
+        invariants(F.m, IF, s.x, s.p, E, L, Q);
+        R->E0 = E; R->Lz0 = L; R->Carter0 = Q;
+        // impact parameter heuristic (GTRC001A.cpp:208-233)
+        double k[4];
+        for (int i = 0; i < 4; ++i) k[i] = s.kx[i];
+        float b = 0.f;
+        if (F.m.family != SIRIUS_METRIC_MORRIS_THORNE) {
+            const double R0 = sqrt(s.x[1] * s.x[1] + s.x[2] * s.x[2] + s.x[3] * s.x[3]);
+            const double vm = sqrt(k[1] * k[1] + k[2] * k[2] + k[3] * k[3]);
+            const double vrad = (k[1] * s.x[1] + k[2] * s.x[2] + k[3] * s.x[3]) / R0;
+            b = float(R0 * sqrt(fmax(vm * vm - vrad * vrad, 0.0)) / fmax(vm, 1e-10));
+        }
+        R->impact_parameter = b;
+    }
+    if (vol)
+        for (int b = 0; b < P.c.nbins; ++b) { vol[2 * b * blockDim.x] = 0.f; vol[(2 * b + 1) * blockDim.x] = 0.f; }
+}
+
+__device__ void end_ray(const Params& P, Ray& s, int outcome, float magnification, int flags, float* vol) {
+    const FrameDev& F = P.frames[s.frame];
+    if (P.image) P.image[s.idx] = float(s.intensity);
+    if (P.spectra && vol)
+        for (int b = 0; b < P.c.nbins; ++b) P.spectra[s.idx * P.c.nbins + b] = vol[2 * b * blockDim.x];
+    if (!P.results) return;
+    sirius_ray_result* R = P.results + s.idx;
+    InvForm IF;
+    inv_form(F.m, s.x, IF);
+    float E, L, Q;
+    invariants(F.m, IF, s.x, s.p, E, L, Q);
+    R->outcome = outcome;
+    R->steps = s.steps;
+    R->rejected = s.rejected;
+    R->n_crossings = s.ncross;
+    for (int i = 0; i < 4; ++i) {
+        R->final_x[i] = s.x[i];
+        R->final_p[i] = s.p[i];
+        R->final_k[i] = float(s.kx[i]);
+    }
+    R->equatorial_crossings = s.eq;
+    R->image_order = s.eq >= 1 ? (s.eq + 1) / 2 : 0;
+    R->total_phi_change = s.tphi;
+    R->min_radius = s.min_r;
+    R->intensity = float(s.intensity);
+    R->E = E; R->Lz = L; R->Carter = Q;
+    R->null_drift_max = s.null_max;
+    R->null_final = float(fabs(inv_apply(F.m, IF, s.p, s.p)));
+    R->magnification = magnification;
+    float tau = 0.f;
+    if (vol)
+        for (int b = 0; b < P.c.nbins; ++b) tau = fmaxf(tau, vol[(2 * b + 1) * blockDim.x]);
+    R->optical_depth = tau;
+    R->fp64_steps = s.fp64_steps;
+    R->flags = flags;
+}
+
+// Volumetric transfer over the accepted segment x0 -> x1 (affine length h):
+// midpoint samples on the straight segment (GTRC001A.cpp:943-958), camera-first
+// accumulation per bin: I_b += T_b S (1 - e^-dtau), T_b = e^-tau_b,
+//   j = j0 r^-2 exp(-z^2/(2 (h_z r)^2)) nu_em^-s, alpha = c_a j,
+//   dtau = alpha (nu_cam/g) dl, S = g^3 / c_a.  (vol: [2b] = I_b, [2b+1] = tau_b, stride blockDim)
+__device__ void volumetric_segment(const Params& P, const FrameDev& F, const double x0[4], const double x1[4],
+                                   const double p[4], double h, float* vol) {
+    const CfgDev& c = P.c;
+    const int ns = c.vol_sub > 0 ? c.vol_sub : 1;
+    const float E = float(-p[0]);
+    const float Lz = float(x1[1] * p[2] - x1[2] * p[1]);
+    const float nu_cam = E / float(F.sqrt_m_gtt_cam);
+    const float dl = float(h) / float(ns);
+    for (int s = 0; s < ns; ++s) {
+        const double f = (s + 0.5) / ns;
+        const float xs = float(x0[1] + f * (x1[1] - x0[1]));
+        const float ys = float(x0[2] + f * (x1[2] - x0[2]));
+        const float zs = float(x0[3] + f * (x1[3] - x0[3]));
+        KSPieces<float> KP;
+        ks_pieces(F.m, xs, ys, zs, KP);
+        const float r = KP.r;
+        if (r < float(F.disk_in) || r > float(F.disk_out)) continue;
+        const float zr = zs / (float(c.vol_hz) * r);
+        if (fabsf(zr) > 4.f) continue;
+        const float g = kepler_g<float>(F.m, xs, ys, zs, r, E, Lz, float(F.sqrt_m_gtt_cam));
+        if (!(g > 0.f)) continue;
+        const float jsp = float(c.vol_j0) / (r * r) * __expf(-0.5f * zr * zr);
+        const float gs = __powf(g, float(c.vol_s));          // nu_em^-s = (g/nu_b)^s
+        const float dt0 = float(c.vol_aoj) * jsp * gs * (nu_cam / g) * dl;
+        const float S = g * g * g / float(c.vol_aoj);
+        for (int b = 0; b < c.nbins; ++b) {
+            const float dtau = dt0 * c.nu_pow[b];
+            float& I = vol[2 * b * blockDim.x];
+            float& tau = vol[(2 * b + 1) * blockDim.x];
+            I += __expf(-tau) * S * (1.f - __expf(-dtau));
+            tau += dtau;
+        }
+    }
+}
+
+// One iteration of the ray state machine: a DP45 attempt, and on acceptance
+// the termination checks. Returns -1 while the ray continues, else its outcome.
+template <bool MIXED>
+__device__ int advance(const Params& P, Ray& s, float& magnification, int& flags, float* vol) {
+    const FrameDev& F = P.frames[s.frame];
+    const MetricDev& m = F.m;
+    const CfgDev& c = P.c;
+    double xn[4], pn[4], k7x[4], k7p[4];
+    bool island = true;
+    if (MIXED) {
+        // FP64 island: inside island_factor * r_ph (retrograde) or near the horizon
+        const double R2 = s.x[1] * s.x[1] + s.x[2] * s.x[2] + s.x[3] * s.x[3];
+        island = (m.family == SIRIUS_METRIC_MORRIS_THORNE) ? (s.x[1] < F.island_r) : (R2 < F.island_r * F.island_r);
+    }
+    double err;
+    if (island) err = dp45_attempt<double>(m, c, s.x, s.p, s.h, s.kx, s.kp, xn, pn, k7x, k7p);
+    else err = dp45_attempt<float>(m, c, s.x, s.p, s.h, s.kx, s.kp, xn, pn, k7x, k7p);
+    ++s.attempts;
+    if (!(err <= 1.0)) {
+        ++s.rejected;
+        s.h = optimal_step(s.h, isfinite(err) ? err : 1e10, c);
+        if (s.h <= c.hmin) { ++s.steps; return SIRIUS_STEP_UNDERFLOW; }
+        if (s.attempts > c.max_steps * 64 + 1024) return SIRIUS_STEP_UNDERFLOW;
+        return -1;
+    }
+    // accepted
+    double x0[4], k0[4];
+#pragma unroll
+    for (int i = 0; i < 4; ++i) { x0[i] = s.x[i]; k0[i] = s.kx[i]; }
+    const double hstep = s.h;
+    s.h = optimal_step(s.h, err, c);
+    ++s.steps;
+    if (island && MIXED) ++s.fp64_steps;
+    bool bad = false;
+#pragma unroll
+    for (int i = 0; i < 4; ++i) {
+        bad |= !isfinite(xn[i]) || !isfinite(pn[i]) || !isfinite(k7x[i]);
+        s.x[i] = xn[i]; s.p[i] = pn[i]; s.kx[i] = k7x[i]; s.kp[i] = k7p[i];
+    }
+    if (bad) { flags |= SIRIUS_FLAG_NUMERICAL_FAILURE; return SIRIUS_NUMERICAL_FAILURE; }
+
+    // FP64 constraint re-projection (E, L_z and Carter preserving)
+    InvForm IF;
+    inv_form(m, s.x, IF);
+    if (c.proj_period > 0 && (s.steps % c.proj_period) == 0) {
+        const double before = project_null(m, IF, s.p);
+        s.null_max = fmaxf(s.null_max, float(fabs(before)));
+    }
+    const double rr = IF.r;
+    if (float(rr) < s.min_r) s.min_r = float(rr);
+    const bool mt = m.family == SIRIUS_METRIC_MORRIS_THORNE;
+
+    // winding: equatorial crossings and |d phi| (GTRC001A.cpp:294-309)
+    if (!mt) {
+        const float cz = float(s.x[3]);
+        if (s.prev_z * cz < 0.f) ++s.eq;
+        s.prev_z = cz;
+        const float cr = float(x0[1] * s.x[2] - x0[2] * s.x[1]);
+        const float dt = float(x0[1] * s.x[1] + x0[2] * s.x[2]);
+        s.tphi += fabsf(atan2f(cr, dt));
+    }
+    // spiral early-out (GTRC001A.cpp:322-352)
+    const int sidx = s.steps - 1;
+    if (c.spiral && !mt && (sidx % 100) == 0 && sidx > 100) {
+        const float ratio = s.min_r / float(F.r_ph_pro);
+        if (ratio < 1.5f && ratio > 0.9f && s.tphi > 2.f * float(kPi)) {
+            const double Reu = sqrt(s.x[1] * s.x[1] + s.x[2] * s.x[2] + s.x[3] * s.x[3]);
+            const double vrad = (s.x[1] * s.kx[1] + s.x[2] * s.kx[2] + s.x[3] * s.kx[3]) / Reu;
+            const double vt = sqrt(s.kx[1] * s.kx[1] + s.kx[2] * s.kx[2] + s.kx[3] * s.kx[3]);
+            if (fabs(vrad) / fmax(vt, 1e-10) < 0.3) return s.ncross > 0 ? SIRIUS_DISK_HIT : SIRIUS_SPIRALING;
+        }
+    }
+    // horizon
+    if (F.r_hor > 0.0 && rr < F.r_hor) return SIRIUS_HORIZON;
+    // throat
+    if (mt && s.x[1] <= 1.001 * m.b0 * 1.0001) return SIRIUS_THROAT;
+    // escape
+    {
+        const double Resc = mt ? s.x[1] : sqrt(s.x[1] * s.x[1] + s.x[2] * s.x[2] + s.x[3] * s.x[3]);
+        if (Resc > c.escape_r) {
+            const double vrad = mt ? s.kx[1] : (s.x[1] * s.kx[1] + s.x[2] * s.kx[2] + s.x[3] * s.kx[3]);
+            if (vrad > 0.0) {
+                const float ratio = s.min_r / float(F.r_ph_pro);
+                if (ratio < 1.5f) {
+                    flags |= SIRIUS_FLAG_PHOTON_RING;
+                    magnification = ratio > 1.f ? fminf(1.f + 2.f / fmaxf(ratio - 1.f, 0.1f), 20.f) : 20.f;
+                }
+                return s.ncross > 0 ? SIRIUS_DISK_HIT : SIRIUS_ESCAPED;
+            }
+        }
+    }
+    if (m.family != SIRIUS_METRIC_KERR_SCHILD || !c.enable_disk || !F.has_horizon) {
+        return s.steps >= c.max_steps ? (s.ncross > 0 ? SIRIUS_DISK_HIT : SIRIUS_MAX_STEPS) : -1;
+    }
+    if (c.enable_vol && vol) volumetric_segment(P, F, x0, s.x, s.p, hstep, vol);
+
+    // thin-disk crossing (GTRC001A.h:404-431, GTRC001A.cpp:468-555): cubic
+    // Hermite location of z = 0 inside the step, BL radius, exact redshift
+    if (x0[3] * s.x[3] < 0.0) {
+        const double sc = hermite_root(x0[3], s.x[3], k0[3], s.kx[3], hstep);
+        const double q2 = sc * sc, q3 = q2 * sc;
+        const double h00 = 2.0 * q3 - 3.0 * q2 + 1.0, h10 = q3 - 2.0 * q2 + sc, h01 = -2.0 * q3 + 3.0 * q2,
+                     h11 = q3 - q2;
+        double xc[4];
+#pragma unroll
+        for (int i = 0; i < 4; ++i) xc[i] = h00 * x0[i] + h10 * hstep * k0[i] + h01 * s.x[i] + h11 * hstep * s.kx[i];
+        xc[3] = 0.0;
+        InvForm CF;
+        inv_form(m, xc, CF);
+        const double rc = CF.r;
+        if (rc >= F.disk_in && rc <= F.disk_out && s.ncross < SIRIUS_MAX_CROSSINGS) {
+            const int n = s.ncross;
+            const double E = -s.p[0], Lz = xc[1] * s.p[2] - xc[2] * s.p[1];
+            const double g = kepler_g<double>(m, xc[1], xc[2], 0.0, rc, E, Lz, F.sqrt_m_gtt_cam);
+            const double Fl = nt_flux(rc, F.a_star, F.isco, F.disk_in, F.disk_out);
+            s.intensity += exp(-c.decay * n) * g * g * g * g * Fl;
+            if (P.results) {
+                sirius_ray_result* R = P.results + s.idx;
+                R->disk_r[n] = float(rc);
+                R->disk_phi[n] = float(atan2(xc[2], xc[1]));
+                R->disk_g[n] = float(g);
+                R->disk_flux[n] = float(Fl);
+            }
+            s.ncross = n + 1;
+            const float ratio = s.min_r / float(F.r_ph_pro);
+            if (ratio < 1.5f) {
+                flags |= SIRIUS_FLAG_PHOTON_RING;
+                magnification = ratio > 1.f ? fminf(1.f + 2.f / fmaxf(ratio - 1.f, 0.05f), 100.f) : 100.f;
+            }
+            if (s.ncross >= SIRIUS_MAX_CROSSINGS) return SIRIUS_DISK_HIT;
+        }
+    }
+    if (s.steps >= c.max_steps) return s.ncross > 0 ? SIRIUS_DISK_HIT : SIRIUS_MAX_STEPS;
+    return -1;
+}
+
+// Persistent tracer. Dynamic shared memory: 2 * nbins floats per thread (volumetric bins).
+template <bool MIXED>
+__global__ void __launch_bounds__(128) trace_kernel(Params P) {
+    extern __shared__ float smem[];
+    float* vol = (P.c.enable_vol && P.c.nbins > 0) ? smem + threadIdx.x : nullptr;
+    const int lane = threadIdx.x & 31;
+    const unsigned lt_mask = (1u << lane) - 1u;
+    Ray s;
+    bool alive = false;
+    float magnification = 1.f;
+    int flags = 0;
+    unsigned long long acc = 0, rej0 = 0, f64 = 0;
+    bool exhausted = false;
+    const unsigned long long t_start = globaltimer();
+
+    if (!P.persistent) {
+        const long long idx = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+        if (idx < P.total) { begin_ray(P, s, idx, vol); alive = true; }
+        exhausted = true;
+    }
+    for (unsigned iter = 0;; ++iter) {
+        if (P.persistent && !exhausted) {
+            const unsigned dead = __ballot_sync(kFull, !alive);
+            const int nlive = 32 - __popc(dead);
+            if (dead && nlive < P.refill_threshold) {
+                unsigned long long base = 0;
+                if (lane == 0) base = atomicAdd(P.queue, (unsigned long long)__popc(dead));
+                base = __shfl_sync(kFull, base, 0);
+                if (base >= (unsigned long long)P.total) exhausted = true;
+                if (!alive) {
+                    const unsigned long long idx = base + __popc(dead & lt_mask);
+                    if (idx < (unsigned long long)P.total) {
+                        begin_ray(P, s, (long long)idx, vol);
+                        alive = true;
+                        magnification = 1.f;
+                        flags = 0;
+                    }
+                }
+            }
+            if ((iter & 255u) == 0) {
+                int stop = 0;
+                if (lane == 0) {
+                    if (globaltimer() - t_start > P.watchdog_ns) atomicOr(P.status, 1);
+                    stop = *((volatile int*)P.status) & 1;
+                }
+                stop = __shfl_sync(kFull, stop, 0);
+                if (stop) {
+                    // watchdog: abandon the remaining queue and close the live rays
+                    exhausted = true;
+                    if (alive) { end_ray(P, s, SIRIUS_MAX_STEPS, magnification, flags, vol); alive = false; }
+                }
+            }
+        }
+        if (__ballot_sync(kFull, alive) == 0) {
+            if (!P.persistent || exhausted) break;
+            continue;
+        }
+        if (alive) {
+            const int out = advance<MIXED>(P, s, magnification, flags, vol);
+            if (out >= 0) {
+                end_ray(P, s, out, magnification, flags, vol);
+                acc += s.steps;
+                rej0 += s.rejected;
+                f64 += s.fp64_steps;
+                alive = false;
+            }
+        }
+    }
+    // warp-aggregated counters
+    for (int o = 16; o > 0; o >>= 1) {
+        acc += __shfl_down_sync(kFull, acc, o);
+        rej0 += __shfl_down_sync(kFull, rej0, o);
+        f64 += __shfl_down_sync(kFull, f64, o);
+    }
+    if (lane == 0) {
+        atomicAdd(&P.counters[0], acc);
+        atomicAdd(&P.counters[1], rej0);
+        atomicAdd(&P.counters[2], f64);
+    }
+}
+
+__global__ void metric_kernel(MetricDev m, const double* pos, long long n, int fp32, double* g, double* dg) {
+    const long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= n) return;
+    if (fp32) {
+        float x[4], gg[16], dd[64];
+        for (int j = 0; j < 4; ++j) x[j] = float(pos[4 * i + j]);
+        metric_full<float>(m, x, gg, dd);
+        for (int j = 0; j < 16; ++j) g[16 * i + j] = gg[j];
+        for (int j = 0; j < 64; ++j) dg[64 * i + j] = dd[j];
+    } else {
+        double x[4], gg[16], dd[64];
+        for (int j = 0; j < 4; ++j) x[j] = pos[4 * i + j];
+        metric_full<double>(m, x, gg, dd);
+        for (int j = 0; j < 16; ++j) g[16 * i + j] = gg[j];
+        for (int j = 0; j < 64; ++j) dg[64 * i + j] = dd[j];
+    }
+}
+
+__global__ void dp45_step_kernel(MetricDev m, CfgDev c, double* state, double* h, int* accepted, double* err,
+                                 long long n) {
+    const long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= n) return;
+    double x[4], p[4], kx[4], kp[4], xn[4], pn[4], k7x[4], k7p[4];
+    for (int j = 0; j < 4; ++j) { x[j] = state[8 * i + j]; p[j] = state[8 * i + 4 + j]; }
+    rhs<double>(m, x, p, kx, kp);
+    const double e = dp45_attempt<double>(m, c, x, p, h[i], kx, kp, xn, pn, k7x, k7p);
+    err[i] = e;
+    accepted[i] = e <= 1.0 ? 1 : 0;
+    if (e <= 1.0)
+        for (int j = 0; j < 4; ++j) { state[8 * i + j] = xn[j]; state[8 * i + 4 + j] = pn[j]; }
+    h[i] = optimal_step(h[i], e, c);
+}
+
+// FMA-chain peak: 8 independent chains per thread, ITER iterations each.
+template <class T>
+__global__ void fma_peak_kernel(T* out, int iters, T seed) {
+    T a0 = seed + T(threadIdx.x), a1 = a0 + T(1), a2 = a0 + T(2), a3 = a0 + T(3);
+    T a4 = a0 + T(4), a5 = a0 + T(5), a6 = a0 + T(6), a7 = a0 + T(7);
+    const T b = T(0.9999), c = T(1e-7);
+    for (int i = 0; i < iters; ++i) {
+#pragma unroll
+        for (int j = 0; j < 16; ++j) {
+            a0 = fma(a0, b, c); a1 = fma(a1, b, c); a2 = fma(a2, b, c); a3 = fma(a3, b, c);
+            a4 = fma(a4, b, c); a5 = fma(a5, b, c); a6 = fma(a6, b, c); a7 = fma(a7, b, c);
+        }
+    }
+    const T s = a0 + a1 + a2 + a3 + a4 + a5 + a6 + a7;
+    if (s == T(-12345.678)) out[0] = s;  // keeps the chains alive
+}
+
+// ---------------------------------------------------------------------------
+// Host side
+// ---------------------------------------------------------------------------
+struct Handle {
+    int device = 0;
+    int num_sms = 0;
+    cudaStream_t stream = nullptr;
+    sirius_trace_config cfg{};
+    bool configured = false;
+    std::string last_error;
+    FrameDev* d_frames = nullptr;
+    size_t frames_cap = 0;
+    sirius_ray_result* d_results = nullptr;
+    size_t results_cap = 0;
+    float* d_image = nullptr;
+    size_t image_cap = 0;
+    float* d_spectra = nullptr;
+    size_t spectra_cap = 0;
+    sirius_camera_ray* d_rays = nullptr;
+    size_t rays_cap = 0;
+    unsigned long long* d_queue = nullptr;  // [0] cursor, [1..3] counters
+    int* d_status = nullptr;
+    cudaEvent_t ev[4] = {};
+    sirius_launch_stats stats{};
+};
+
+int fail(Handle* h, int code, const std::string& msg) {
+    if (h) h->last_error = msg;
+    return code;
+}
+
+#define CK(call)                                                                              \
+    do {                                                                                      \
+        cudaError_t e_ = (call);                                                              \
+        if (e_ != cudaSuccess)                                                                \
+            return fail(H, e_ == cudaErrorMemoryAllocation ? SIRIUS_ERR_OUT_OF_MEMORY : SIRIUS_ERR_CUDA, \
+                        std::string(#call) + ": " + cudaGetErrorString(e_));                  \
+    } while (0)
+
+template <class T>
+int ensure(Handle* H, T*& ptr, size_t& cap, size_t count) {
+    if (count <= cap && ptr) return SIRIUS_OK;
+    if (ptr) CK(cudaFree(ptr));
+    ptr = nullptr;
+    cap = 0;
+    size_t n = std::max<size_t>(count, 1);
+    CK(cudaMalloc((void**)&ptr, n * sizeof(T)));
+    cap = n;
+    return SIRIUS_OK;
+}
+
+double isco_host(double a_star) {
+    const double a = std::min(std::fabs(a_star), 1.0);
+    const double Z1 = 1 + std::cbrt(1 - a * a) * (std::cbrt(1 + a) + std::cbrt(1 - a));
+    const double Z2 = std::sqrt(3 * a * a + Z1 * Z1);
+    return a_star >= 0 ? 3 + Z2 - std::sqrt((3 - Z1) * (3 + Z1 + 2 * Z2))
+                       : 3 + Z2 + std::sqrt((3 - Z1) * (3 + Z1 + 2 * Z2));
+}
+
+MetricDev make_metric(const sirius_metric& s) {
+    MetricDev m{};
+    m.family = s.family;
+    m.shape = s.shape;
+    m.M = s.M; m.a = s.a; m.Q = s.Q; m.Lambda = s.Lambda;
+    m.a2 = s.a * s.a; m.Q2 = s.Q * s.Q; m.lam3 = s.Lambda / 3.0; m.sqrtM = std::sqrt(std::max(s.M, 0.0));
+    m.has_lambda = std::fabs(s.Lambda) > 1e-15;
+    m.b0 = s.b0; m.Phi0 = s.Phi0; m.gtt_mt = -std::exp(2.0 * s.Phi0);
+    m.vs = s.vs; m.sigma = s.sigma; m.Rb = s.R;
+    m.inv_2tanhsR = (s.sigma * s.R != 0.0) ? 1.0 / (2.0 * std::tanh(s.sigma * s.R)) : 0.0;
+    return m;
+}
+
+int validate_metric(Handle* H, const sirius_metric& m) {
+    if (m.family < 0 || m.family > 2) return fail(H, SIRIUS_ERR_INVALID_ARGUMENT, "unknown metric family");
+    if (!std::isfinite(m.M) || !std::isfinite(m.a) || !std::isfinite(m.Q) || !std::isfinite(m.Lambda))
+        return fail(H, SIRIUS_ERR_INVALID_ARGUMENT, "non-finite metric parameter");
+    if (m.family == SIRIUS_METRIC_MORRIS_THORNE && !(m.b0 > 0))
+        return fail(H, SIRIUS_ERR_INVALID_ARGUMENT, "Morris-Thorne throat radius must be > 0");
+    if (m.family == SIRIUS_METRIC_ALCUBIERRE && !(m.sigma > 0 && m.R > 0))
+        return fail(H, SIRIUS_ERR_INVALID_ARGUMENT, "Alcubierre sigma and R must be > 0");
+    return SIRIUS_OK;
+}
+
+FrameDev make_frame(const sirius_frame& f, const sirius_trace_config& c) {
+    FrameDev F{};
+    F.m = make_metric(f.metric);
+    F.ray_offset = f.ray_offset;
+    F.width = f.camera.width;
+    F.height = f.camera.height;
+    F.n_rays = (long long)f.camera.width * f.camera.height;
+    F.projection = f.camera.projection;
+    // camera (CameraConfig, CMBS001A.h:37-58); theta clamp of initializeLightray (GTRC001A.cpp:25)
+    const double th = std::clamp(f.camera.theta, 0.01, kPi - 0.01);
+    F.cam_t = f.camera.t; F.cam_r = f.camera.r; F.cam_th = th; F.cam_ph = f.camera.phi;
+    F.cam_st = std::sin(th); F.cam_ct = std::cos(th); F.cam_sp = std::sin(f.camera.phi); F.cam_cp = std::cos(f.camera.phi);
+    F.aspect = float(f.camera.width) / float(f.camera.height);
+    F.tan_half_fov = std::tan(f.camera.fov * float(kPi) / 360.0f);
+    F.cY = std::cos(f.camera.yaw); F.sY = std::sin(f.camera.yaw);
+    F.cP = std::cos(f.camera.pitch); F.sP = std::sin(f.camera.pitch);
+    F.cR = std::cos(f.camera.roll); F.sR = std::sin(f.camera.roll);
+    const sirius_metric& m = f.metric;
+    const double a_star = m.M != 0 ? m.a / m.M : 0.0;
+    F.a_star = a_star;
+    F.isco = isco_host(a_star) * m.M;
+    F.disk_in = f.disk_inner > 0 ? f.disk_inner : F.isco;
+    F.disk_out = f.disk_outer;
+    const double d = m.M * m.M - m.a * m.a - m.Q * m.Q;
+    F.has_horizon = (m.family == SIRIUS_METRIC_KERR_SCHILD && d >= 0 && m.M > 0) ? 1 : 0;
+    const double rp = F.has_horizon ? m.M + std::sqrt(d) : -1.0;
+    F.r_hor = F.has_horizon ? rp * c.horizon_factor : -1.0;
+    const double aM = std::clamp(a_star, -0.998, 0.998);
+    F.r_ph_pro = 2.0 * m.M * (1.0 + std::cos((2.0 / 3.0) * std::acos(std::clamp(-aM, -1.0, 1.0))));
+    const double r_ph_retro = 2.0 * m.M * (1.0 + std::cos((2.0 / 3.0) * std::acos(std::clamp(std::fabs(a_star), -1.0, 1.0))));
+    if (m.family == SIRIUS_METRIC_KERR_SCHILD)
+        F.island_r = std::max(c.island_factor * r_ph_retro, 2.0 * std::max(rp, 0.0));
+    else if (m.family == SIRIUS_METRIC_MORRIS_THORNE)
+        F.island_r = c.island_factor * 3.0 * m.b0;
+    else
+        F.island_r = c.island_factor * (m.R + 3.0 / std::max(m.sigma, 1e-6));
+    // static observer at the camera: sqrt(-g_tt) (KS family g_tt = -1 + H - Lambda R^2/3)
+    double gtt = -1.0;
+    if (m.family == SIRIUS_METRIC_KERR_SCHILD) {
+        const double x = f.camera.r * F.cam_st * F.cam_cp, y = f.camera.r * F.cam_st * F.cam_sp, z = f.camera.r * F.cam_ct;
+        const double R2 = x * x + y * y + z * z, Rm2 = R2 - m.a * m.a;
+        const double sd = std::sqrt(std::max(Rm2 * Rm2 + 4.0 * m.a * m.a * z * z, 1e-20));
+        const double r2 = std::max(0.5 * (Rm2 + sd), 1e-10), r = std::sqrt(r2);
+        const double H = (2.0 * m.M * r - m.Q * m.Q) * r2 / (r2 * r2 + m.a * m.a * z * z);
+        gtt = -1.0 + H - (std::fabs(m.Lambda) > 1e-15 ? m.Lambda * R2 / 3.0 : 0.0);
+    } else if (m.family == SIRIUS_METRIC_MORRIS_THORNE) {
+        gtt = -std::exp(2.0 * m.Phi0);
+    } else {
+        const double rs = std::max(f.camera.r, 1e-10);
+        const double fs = (std::tanh(m.sigma * (rs + m.R)) - std::tanh(m.sigma * (rs - m.R))) / (2.0 * std::tanh(m.sigma * m.R));
+        gtt = -(1.0 - m.vs * m.vs * fs * fs);
+    }
+    F.sqrt_m_gtt_cam = std::sqrt(std::max(-gtt, 1e-30));
+    return F;
+}
+
+CfgDev make_cfg(const sirius_trace_config& c) {
+    CfgDev d{};
+    d.atol = c.abs_tolerance; d.rtol = c.rel_tolerance; d.hmin = c.min_step; d.hmax = c.max_step;
+    d.h0 = c.initial_step; d.safety = c.safety_factor; d.grow = c.step_grow_max; d.shrink = c.step_shrink_min;
+    d.escape_r = c.escape_radius; d.decay = c.crossing_weight_decay;
+    d.max_steps = c.max_steps; d.enable_disk = c.enable_disk; d.enable_vol = c.enable_volumetric;
+    d.nbins = c.enable_volumetric ? std::min(c.n_bins, SIRIUS_MAX_BINS) : 0;
+    d.vol_sub = c.vol_substeps; d.proj_period = c.projection_period; d.spiral = c.spiral_check; d.compat = c.compat;
+    d.vol_j0 = c.vol_j0; d.vol_aoj = c.vol_alpha_over_j; d.vol_hz = c.vol_height_ratio; d.vol_s = c.vol_spectral_index;
+    for (int b = 0; b < d.nbins; ++b) {
+        const double nu = d.nbins == 1 ? c.nu_min : c.nu_min * std::pow(c.nu_max / c.nu_min, double(b) / (d.nbins - 1));
+        d.nu[b] = float(nu);
+        d.nu_pow[b] = float(std::pow(nu, -c.vol_spectral_index));
+    }
+    return d;
+}
+
+int validate_config(Handle* H, const sirius_trace_config& c) {
+    if (!(c.abs_tolerance > 0) || !(c.rel_tolerance >= 0)) return fail(H, SIRIUS_ERR_INVALID_ARGUMENT, "tolerances must be > 0");
+    if (!(c.min_step > 0) || !(c.max_step >= c.min_step) || !(c.initial_step > 0))
+        return fail(H, SIRIUS_ERR_INVALID_ARGUMENT, "step limits must satisfy 0 < min_step <= max_step, initial_step > 0");
+    if (c.max_steps <= 0) return fail(H, SIRIUS_ERR_INVALID_ARGUMENT, "max_steps must be > 0");
+    if (c.enable_volumetric && (c.n_bins <= 0 || c.n_bins > SIRIUS_MAX_BINS))
+        return fail(H, SIRIUS_ERR_INVALID_ARGUMENT, "n_bins must be in 1..32 when volumetric transfer is on");
+    if (c.enable_volumetric && !(c.nu_min > 0 && c.nu_max >= c.nu_min && c.vol_alpha_over_j > 0 && c.vol_height_ratio > 0))
+        return fail(H, SIRIUS_ERR_INVALID_ARGUMENT, "invalid volumetric parameters");
+    if (c.precision != SIRIUS_PRECISION_FP64 && c.precision != SIRIUS_PRECISION_MIXED)
+        return fail(H, SIRIUS_ERR_INVALID_ARGUMENT, "unknown precision mode");
+    if (c.integrator != SIRIUS_INTEGRATOR_DP45)
+        return fail(H, SIRIUS_ERR_UNSUPPORTED, "only the DP45 integrator is available in this build");
+    if (c.compat) return fail(H, SIRIUS_ERR_UNSUPPORTED, "reference-compatible mode is not available on the GPU path");
+    if (c.block_size < 0 || c.block_size > 1024 || (c.block_size % 32) != 0)
+        return fail(H, SIRIUS_ERR_INVALID_ARGUMENT, "block_size must be a multiple of 32 in 0..1024");
+    if (c.refill_threshold < 0 || c.refill_threshold > 32)
+        return fail(H, SIRIUS_ERR_INVALID_ARGUMENT, "refill_threshold must be in 0..32");
+    return SIRIUS_OK;
+}
+
+// Launch the tracer over [0, total) of already-uploaded frames.
+int launch_trace(Handle* H, int n_frames, long long total, sirius_ray_result* d_results, float* d_image,
+                 float* d_spectra, const sirius_camera_ray* d_rays, cudaStream_t st, bool timed) {
+    const sirius_trace_config& c = H->cfg;
+    Params P{};
+    P.frames = H->d_frames;
+    P.n_frames = n_frames;
+    P.total = total;
+    P.results = d_results;
+    P.image = d_image;
+    P.spectra = d_spectra;
+    P.host_rays = d_rays;
+    P.queue = H->d_queue;
+    P.counters = H->d_queue + 1;
+    P.status = H->d_status;
+    P.c = make_cfg(c);
+    const bool mixed = c.precision == SIRIUS_PRECISION_MIXED;
+    // persistent unless blocks_per_sm < 0 (plain one-thread-per-ray launch)
+    P.persistent = c.blocks_per_sm >= 0 ? 1 : 0;
+    P.refill_threshold = c.refill_threshold > 0 ? c.refill_threshold : 24;
+    const int block = 128;  // matches __launch_bounds__
+    const size_t shmem = size_t(2) * P.c.nbins * block * sizeof(float);
+    int grid;
+    if (P.persistent) {
+        int per_sm = c.blocks_per_sm;
+        if (per_sm <= 0) {
+            int occ = 0;
+            if (mixed)
+                CK(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, trace_kernel<true>, block, shmem));
+            else
+                CK(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, trace_kernel<false>, block, shmem));
+            per_sm = std::max(occ, 1);
+        }
+        grid = H->num_sms * per_sm;
+        const long long need = (total + block - 1) / block;
+        if (grid > need) grid = int(std::max<long long>(need, 1));
+    } else {
+        grid = int((total + block - 1) / block);
+    }
+    CK(cudaMemsetAsync(H->d_queue, 0, 4 * sizeof(unsigned long long), st));
+    CK(cudaMemsetAsync(H->d_status, 0, sizeof(int), st));
+    // whole-launch bound on the device clock (each warp measures from its own start)
+    P.watchdog_ns = c.watchdog_ms > 0 ? (unsigned long long)c.watchdog_ms * 1000000ull : ~0ull;
+    if (timed) CK(cudaEventRecord(H->ev[1], st));
+    if (mixed) trace_kernel<true><<<grid, block, shmem, st>>>(P);
+    else trace_kernel<false><<<grid, block, shmem, st>>>(P);
+    CK(cudaGetLastError());
+    if (timed) CK(cudaEventRecord(H->ev[2], st));
+    H->stats.grid_blocks = grid;
+    H->stats.block_size = block;
+    H->stats.kernel_launches = 1;
+    return SIRIUS_OK;
+}
+
+int finish_stats(Handle* H, cudaStream_t st, long long total, bool timed) {
+    unsigned long long cnt[4] = {};
+    int status = 0;
+    CK(cudaMemcpyAsync(cnt, H->d_queue, sizeof(cnt), cudaMemcpyDeviceToHost, st));
+    CK(cudaMemcpyAsync(&status, H->d_status, sizeof(int), cudaMemcpyDeviceToHost, st));
+    CK(cudaStreamSynchronize(st));
+    H->stats.rays = total;
+    H->stats.accepted_steps = (long long)cnt[1];
+    H->stats.rejected_steps = (long long)cnt[2];
+    H->stats.fp64_steps = (long long)cnt[3];
+    H->stats.status_flags = status;
+    if (timed) {
+        float k = 0, t = 0;
+        CK(cudaEventElapsedTime(&k, H->ev[1], H->ev[2]));
+        CK(cudaEventElapsedTime(&t, H->ev[0], H->ev[3]));
+        H->stats.kernel_ms = k;
+        H->stats.total_ms = t;
+    }
+    if (status & 1) return fail(H, SIRIUS_ERR_TIMEOUT, "trace kernel stopped by its watchdog");
+    return SIRIUS_OK;
+}
+
+}  // namespace
+
+// ---------------------------------------------------------------------------
+// C ABI
+// ---------------------------------------------------------------------------
+extern "C" {
+
+int sirius_cuda_abi_version(void) { return SIRIUS_CUDA_ABI_VERSION; }
+
+int sirius_cuda_default_config(sirius_trace_config* c) {
+    if (!c) return SIRIUS_ERR_INVALID_ARGUMENT;
+    std::memset(c, 0, sizeof(*c));
+    // IntegratorConfig / TracerConfig as RenderSession sets them (SNRS001A.cpp:103-129)
+    c->abs_tolerance = 5e-6; c->rel_tolerance = 5e-6; c->min_step = 1e-5; c->max_step = 2.0; c->initial_step = 0.1;
+    c->safety_factor = 0.9; c->step_grow_max = 2.0; c->step_shrink_min = 0.1;
+    c->escape_radius = 200.0; c->horizon_factor = 1.05; c->max_steps = 20000; c->enable_disk = 1;
+    c->disk_temperature_inner = 1.0; c->crossing_weight_decay = kPi;
+    c->enable_volumetric = 0; c->n_bins = 0; c->nu_min = 1e-2; c->nu_max = 1e2; c->vol_j0 = 1.0;
+    c->vol_alpha_over_j = 0.1; c->vol_height_ratio = 0.1; c->vol_spectral_index = 0.7; c->vol_substeps = 4;
+    c->integrator = SIRIUS_INTEGRATOR_DP45; c->precision = SIRIUS_PRECISION_FP64; c->compat = 0;
+    c->projection_period = 1; c->spiral_check = 0; c->island_factor = 1.5; c->symplectic_step = 0.01;
+    c->symplectic_order = 4; c->block_size = 0; c->refill_threshold = 0; c->blocks_per_sm = 0; c->watchdog_ms = 30000;
+    return SIRIUS_OK;
+}
+
+int sirius_cuda_create(int device, sirius_cuda_handle* out) {
+    if (!out) return SIRIUS_ERR_INVALID_ARGUMENT;
+    *out = nullptr;
+    int n = 0;
+    if (cudaGetDeviceCount(&n) != cudaSuccess || n <= 0) { cudaGetLastError(); return SIRIUS_ERR_NO_DEVICE; }
+    if (device < 0 || device >= n) return SIRIUS_ERR_INVALID_ARGUMENT;
+    Handle* H = new (std::nothrow) Handle();
+    if (!H) return SIRIUS_ERR_OUT_OF_MEMORY;
+    H->device = device;
+    auto bail = [&](int code) { delete H; return code; };
+    if (cudaSetDevice(device) != cudaSuccess) return bail(SIRIUS_ERR_CUDA);
+    cudaDeviceProp prop;
+    if (cudaGetDeviceProperties(&prop, device) != cudaSuccess) return bail(SIRIUS_ERR_CUDA);
+    if (prop.major < 10) return bail(SIRIUS_ERR_UNSUPPORTED);
+    H->num_sms = prop.multiProcessorCount;
+    if (cudaStreamCreateWithFlags(&H->stream, cudaStreamNonBlocking) != cudaSuccess) return bail(SIRIUS_ERR_CUDA);
+    for (auto& e : H->ev)
+        if (cudaEventCreate(&e) != cudaSuccess) return bail(SIRIUS_ERR_CUDA);
+    if (cudaMalloc((void**)&H->d_queue, 8 * sizeof(unsigned long long)) != cudaSuccess) return bail(SIRIUS_ERR_OUT_OF_MEMORY);
+    if (cudaMalloc((void**)&H->d_status, sizeof(int)) != cudaSuccess) return bail(SIRIUS_ERR_OUT_OF_MEMORY);
+    sirius_cuda_default_config(&H->cfg);
+    H->configured = true;
+    *out = H;
+    return SIRIUS_OK;
+}
+
+int sirius_cuda_destroy(sirius_cuda_handle h) {
+    Handle* H = static_cast<Handle*>(h);
+    if (!H) return SIRIUS_ERR_INVALID_ARGUMENT;
+    cudaSetDevice(H->device);
+    if (H->stream) cudaStreamSynchronize(H->stream);
+    cudaFree(H->d_frames); cudaFree(H->d_results); cudaFree(H->d_image); cudaFree(H->d_spectra);
+    cudaFree(H->d_rays); cudaFree(H->d_queue); cudaFree(H->d_status);
+    for (auto& e : H->ev) if (e) cudaEventDestroy(e);
+    if (H->stream) cudaStreamDestroy(H->stream);
+    delete H;
+    return SIRIUS_OK;
+}
+
+const char* sirius_cuda_get_last_error(sirius_cuda_handle h) {
+    Handle* H = static_cast<Handle*>(h);
+    return H ? H->last_error.c_str() : "invalid handle";
+}
+
+int sirius_cuda_configure(sirius_cuda_handle h, const sirius_trace_config* c) {
+    Handle* H = static_cast<Handle*>(h);
+    if (!H || !c) return SIRIUS_ERR_INVALID_ARGUMENT;
+    const int rc = validate_config(H, *c);
+    if (rc != SIRIUS_OK) return rc;
+    H->cfg = *c;
+    H->configured = true;
+    return SIRIUS_OK;
+}
+
+static int upload_frames(Handle* H, const sirius_frame* frames, int n, long long* total_out) {
+    std::vector<FrameDev> fd(n);
+    long long total = 0;
+    for (int i = 0; i < n; ++i) {
+        const sirius_frame& f = frames[i];
+        int rc = validate_metric(H, f.metric);
+        if (rc != SIRIUS_OK) return rc;
+        if (f.camera.width <= 0 || f.camera.height <= 0 || !(f.camera.r > 0))
+            return fail(H, SIRIUS_ERR_INVALID_ARGUMENT, "camera needs width, height > 0 and r > 0");
+        if (f.camera.projection != SIRIUS_CAMERA_PINHOLE && f.camera.projection != SIRIUS_CAMERA_EQUIRECTANGULAR)
+            return fail(H, SIRIUS_ERR_INVALID_ARGUMENT, "unknown camera projection");
+        if (f.ray_offset != total)
+            return fail(H, SIRIUS_ERR_INVALID_ARGUMENT, "frames must be contiguous: ray_offset[i] = sum of previous pixel counts");
+        fd[i] = make_frame(f, H->cfg);
+        total += fd[i].n_rays;
+    }
+    int rc = ensure(H, H->d_frames, H->frames_cap, size_t(n));
+    if (rc != SIRIUS_OK) return rc;
+    CK(cudaMemcpyAsync(H->d_frames, fd.data(), n * sizeof(FrameDev), cudaMemcpyHostToDevice, H->stream));
+    *total_out = total;
+    return SIRIUS_OK;
+}
+
+int sirius_cuda_trace_frames(sirius_cuda_handle h, const sirius_frame* frames, int32_t n_frames,
+                             sirius_ray_result* results, float* image, float* spectra) {
+    Handle* H = static_cast<Handle*>(h);
+    if (!H || !frames || n_frames <= 0) return SIRIUS_ERR_INVALID_ARGUMENT;
+    CK(cudaSetDevice(H->device));
+    cudaStream_t st = H->stream;
+    CK(cudaEventRecord(H->ev[0], st));
+    long long total = 0;
+    int rc = upload_frames(H, frames, n_frames, &total);
+    if (rc != SIRIUS_OK) return rc;
+    const int nb = H->cfg.enable_volumetric ? std::min(H->cfg.n_bins, SIRIUS_MAX_BINS) : 0;
+    if (results && (rc = ensure(H, H->d_results, H->results_cap, size_t(total))) != SIRIUS_OK) return rc;
+    if (image && (rc = ensure(H, H->d_image, H->image_cap, size_t(total))) != SIRIUS_OK) return rc;
+    if (spectra && nb && (rc = ensure(H, H->d_spectra, H->spectra_cap, size_t(total) * nb)) != SIRIUS_OK) return rc;
+    rc = launch_trace(H, n_frames, total, results ? H->d_results : nullptr, image ? H->d_image : nullptr,
+                      (spectra && nb) ? H->d_spectra : nullptr, nullptr, st, true);
+    if (rc != SIRIUS_OK) return rc;
+    if (results) CK(cudaMemcpyAsync(results, H->d_results, size_t(total) * sizeof(sirius_ray_result), cudaMemcpyDeviceToHost, st));
+    if (image) CK(cudaMemcpyAsync(image, H->d_image, size_t(total) * sizeof(float), cudaMemcpyDeviceToHost, st));
+    if (spectra && nb) CK(cudaMemcpyAsync(spectra, H->d_spectra, size_t(total) * nb * sizeof(float), cudaMemcpyDeviceToHost, st));
+    CK(cudaEventRecord(H->ev[3], st));
+    return finish_stats(H, st, total, true);
+}
+
+int sirius_cuda_trace_frames_device(sirius_cuda_handle h, const sirius_frame* d_frames_user, int32_t n_frames,
+                                    int64_t total_rays, sirius_ray_result* d_results, float* d_image, float* d_spectra,
+                                    void* stream) {
+    Handle* H = static_cast<Handle*>(h);
+    if (!H || !d_frames_user || n_frames <= 0 || total_rays <= 0) return SIRIUS_ERR_INVALID_ARGUMENT;
+    CK(cudaSetDevice(H->device));
+    cudaStream_t st = stream ? static_cast<cudaStream_t>(stream) : H->stream;
+    // frames arrive in device memory: bring the small descriptors to the host to derive constants
+    std::vector<sirius_frame> hf(n_frames);
+    CK(cudaMemcpyAsync(hf.data(), d_frames_user, n_frames * sizeof(sirius_frame), cudaMemcpyDeviceToHost, st));
+    CK(cudaStreamSynchronize(st));
+    long long total = 0;
+    cudaStream_t keep = H->stream;
+    H->stream = st;
+    int rc = upload_frames(H, hf.data(), n_frames, &total);
+    H->stream = keep;
+    if (rc != SIRIUS_OK) return rc;
+    if (total != total_rays) return fail(H, SIRIUS_ERR_INVALID_ARGUMENT, "total_rays does not match the frames");
+    CK(cudaEventRecord(H->ev[0], st));
+    rc = launch_trace(H, n_frames, total, d_results, d_image, d_spectra, nullptr, st, true);
+    if (rc != SIRIUS_OK) return rc;
+    CK(cudaEventRecord(H->ev[3], st));
+    return SIRIUS_OK;
+}
+
+int sirius_cuda_trace_rays(sirius_cuda_handle h, const sirius_metric* metric, double disk_inner, double disk_outer,
+                           const sirius_camera_ray* rays, int64_t n_rays, sirius_ray_result* results) {
+    Handle* H = static_cast<Handle*>(h);
+    if (!H || !metric || !rays || !results || n_rays <= 0) return SIRIUS_ERR_INVALID_ARGUMENT;
+    CK(cudaSetDevice(H->device));
+    // All rays of one call share the camera origin of the first ray (the CameraRay batch of a frame).
+    for (int64_t i = 1; i < n_rays; ++i)
+        for (int j = 0; j < 4; ++j)
+            if (rays[i].origin[j] != rays[0].origin[j])
+                return fail(H, SIRIUS_ERR_INVALID_ARGUMENT, "all rays of one call must share the camera origin");
+    sirius_frame f{};
+    f.metric = *metric;
+    f.camera.t = rays[0].origin[0];
+    f.camera.r = rays[0].origin[1];
+    f.camera.theta = rays[0].origin[2];
+    f.camera.phi = rays[0].origin[3];
+    f.camera.width = 1;
+    f.camera.height = 1;
+    f.camera.fov = 30.f;
+    f.disk_inner = disk_inner;
+    f.disk_outer = disk_outer;
+    f.ray_offset = 0;
+    cudaStream_t st = H->stream;
+    CK(cudaEventRecord(H->ev[0], st));
+    long long dummy = 0;
+    int rc = upload_frames(H, &f, 1, &dummy);
+    if (rc != SIRIUS_OK) return rc;
+    if ((rc = ensure(H, H->d_rays, H->rays_cap, size_t(n_rays))) != SIRIUS_OK) return rc;
+    if ((rc = ensure(H, H->d_results, H->results_cap, size_t(n_rays))) != SIRIUS_OK) return rc;
+    CK(cudaMemcpyAsync(H->d_rays, rays, size_t(n_rays) * sizeof(sirius_camera_ray), cudaMemcpyHostToDevice, st));
+    rc = launch_trace(H, 1, n_rays, H->d_results, nullptr, nullptr, H->d_rays, st, true);
+    if (rc != SIRIUS_OK) return rc;
+    CK(cudaMemcpyAsync(results, H->d_results, size_t(n_rays) * sizeof(sirius_ray_result), cudaMemcpyDeviceToHost, st));
+    CK(cudaEventRecord(H->ev[3], st));
+    return finish_stats(H, st, n_rays, true);
+}
+
+int sirius_cuda_metric_evaluate(sirius_cuda_handle h, const sirius_metric* metric, const double* positions, int64_t n,
+                                int32_t precision, double* g, double* dg) {
+    Handle* H = static_cast<Handle*>(h);
+    if (!H || !metric || !positions || !g || !dg || n <= 0) return SIRIUS_ERR_INVALID_ARGUMENT;
+    int rc = validate_metric(H, *metric);
+    if (rc != SIRIUS_OK) return rc;
+    CK(cudaSetDevice(H->device));
+    double *dp = nullptr, *dgp = nullptr, *ddg = nullptr;
+    CK(cudaMalloc((void**)&dp, size_t(n) * 4 * sizeof(double)));
+    CK(cudaMalloc((void**)&dgp, size_t(n) * 16 * sizeof(double)));
+    CK(cudaMalloc((void**)&ddg, size_t(n) * 64 * sizeof(double)));
+    cudaStream_t st = H->stream;
+    CK(cudaMemcpyAsync(dp, positions, size_t(n) * 4 * sizeof(double), cudaMemcpyHostToDevice, st));
+    metric_kernel<<<unsigned((n + 127) / 128), 128, 0, st>>>(make_metric(*metric), dp, n, precision == SIRIUS_PRECISION_MIXED,
+                                                               dgp, ddg);
+    CK(cudaGetLastError());
+    CK(cudaMemcpyAsync(g, dgp, size_t(n) * 16 * sizeof(double), cudaMemcpyDeviceToHost, st));
+    CK(cudaMemcpyAsync(dg, ddg, size_t(n) * 64 * sizeof(double), cudaMemcpyDeviceToHost, st));
+    CK(cudaStreamSynchronize(st));
+    cudaFree(dp); cudaFree(dgp); cudaFree(ddg);
+    return SIRIUS_OK;
+}
+
+int sirius_cuda_dp45_step(sirius_cuda_handle h, const sirius_metric* metric, double* state, double* hh, int32_t* accepted,
+                          double* err, int64_t n) {
+    Handle* H = static_cast<Handle*>(h);
+    if (!H || !metric || !state || !hh || !accepted || !err || n <= 0) return SIRIUS_ERR_INVALID_ARGUMENT;
+    int rc = validate_metric(H, *metric);
+    if (rc != SIRIUS_OK) return rc;
+    CK(cudaSetDevice(H->device));
+    double *ds = nullptr, *dh = nullptr, *de = nullptr;
+    int* da = nullptr;
+    CK(cudaMalloc((void**)&ds, size_t(n) * 8 * sizeof(double)));
+    CK(cudaMalloc((void**)&dh, size_t(n) * sizeof(double)));
+    CK(cudaMalloc((void**)&de, size_t(n) * sizeof(double)));
+    CK(cudaMalloc((void**)&da, size_t(n) * sizeof(int)));
+    cudaStream_t st = H->stream;
+    CK(cudaMemcpyAsync(ds, state, size_t(n) * 8 * sizeof(double), cudaMemcpyHostToDevice, st));
+    CK(cudaMemcpyAsync(dh, hh, size_t(n) * sizeof(double), cudaMemcpyHostToDevice, st));
+    dp45_step_kernel<<<unsigned((n + 127) / 128), 128, 0, st>>>(make_metric(*metric), make_cfg(H->cfg), ds, dh, da, de, n);
+    CK(cudaGetLastError());
+    CK(cudaMemcpyAsync(state, ds, size_t(n) * 8 * sizeof(double), cudaMemcpyDeviceToHost, st));
+    CK(cudaMemcpyAsync(hh, dh, size_t(n) * sizeof(double), cudaMemcpyDeviceToHost, st));
+    CK(cudaMemcpyAsync(err, de, size_t(n) * sizeof(double), cudaMemcpyDeviceToHost, st));
+    CK(cudaMemcpyAsync(accepted, da, size_t(n) * sizeof(int), cudaMemcpyDeviceToHost, st));
+    CK(cudaStreamSynchronize(st));
+    cudaFree(ds); cudaFree(dh); cudaFree(de); cudaFree(da);
+    return SIRIUS_OK;
+}
+
+int sirius_cuda_last_stats(sirius_cuda_handle h, sirius_launch_stats* out) {
+    Handle* H = static_cast<Handle*>(h);
+    if (!H || !out) return SIRIUS_ERR_INVALID_ARGUMENT;
+    *out = H->stats;
+    return SIRIUS_OK;
+}
+
+int sirius_cuda_autotune(sirius_cuda_handle h, const sirius_frame* frames, int32_t n_frames, sirius_trace_config* out) {
+    Handle* H = static_cast<Handle*>(h);
+    if (!H || !frames || n_frames <= 0) return SIRIUS_ERR_INVALID_ARGUMENT;
+    CK(cudaSetDevice(H->device));
+    long long total = 0;
+    int rc = upload_frames(H, frames, n_frames, &total);
+    if (rc != SIRIUS_OK) return rc;
+    if ((rc = ensure(H, H->d_image, H->image_cap, size_t(total))) != SIRIUS_OK) return rc;
+    const sirius_trace_config base = H->cfg;
+    const int thresholds[] = {8, 16, 24, 28, 32};
+    const int per_sm[] = {1, 2, 3, 4};
+    double best = 1e300;
+    sirius_trace_config best_cfg = base;
+    for (int t : thresholds)
+        for (int b : per_sm) {
+            H->cfg = base;
+            H->cfg.refill_threshold = t;
+            H->cfg.blocks_per_sm = b;
+            CK(cudaEventRecord(H->ev[0], H->stream));
+            rc = launch_trace(H, n_frames, total, nullptr, H->d_image, nullptr, nullptr, H->stream, true);
+            if (rc != SIRIUS_OK) { H->cfg = base; return rc; }
+            CK(cudaEventRecord(H->ev[3], H->stream));
+            rc = finish_stats(H, H->stream, total, true);
+            if (rc != SIRIUS_OK) { H->cfg = base; return rc; }
+            if (H->stats.kernel_ms < best) { best = H->stats.kernel_ms; best_cfg = H->cfg; }
+        }
+    H->cfg = best_cfg;
+    if (out) *out = best_cfg;
+    return SIRIUS_OK;
+}
+
+int sirius_cuda_measure_fma_peak(sirius_cuda_handle h, int32_t precision, double* flops_per_s) {
+    Handle* H = static_cast<Handle*>(h);
+    if (!H || !flops_per_s) return SIRIUS_ERR_INVALID_ARGUMENT;
+    CK(cudaSetDevice(H->device));
+    const int block = 256, iters = 2048;
+    const int grid = H->num_sms * 8;
+    double* dout = nullptr;
+    CK(cudaMalloc((void**)&dout, sizeof(double)));
+    float best = 1e30f;
+    for (int rep = 0; rep < 4; ++rep) {
+        CK(cudaEventRecord(H->ev[0], H->stream));
+        if (precision == 0) fma_peak_kernel<double><<<grid, block, 0, H->stream>>>(dout, iters, 1.0);
+        else fma_peak_kernel<float><<<grid, block, 0, H->stream>>>((float*)dout, iters, 1.0f);
+        CK(cudaGetLastError());
+        CK(cudaEventRecord(H->ev[1], H->stream));
+        CK(cudaEventSynchronize(H->ev[1]));
+        float ms = 0;
+        CK(cudaEventElapsedTime(&ms, H->ev[0], H->ev[1]));
+        if (rep > 0) best = std::min(best, ms);
+    }
+    cudaFree(dout);
+    const double flops = 2.0 * 8.0 * 16.0 * double(iters) * double(grid) * double(block);
+    *flops_per_s = flops / (double(best) * 1e-3);
+    return SIRIUS_OK;
+}
+
+}  // extern "C"

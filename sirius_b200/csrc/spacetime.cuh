@@ -1,0 +1,313 @@
+// spacetime.cuh — metric families on the device.
+//
+// Each family supplies, in any precision T:
+//   rhs()          Hamilton's equations  dx^mu/dl = g^{mu nu} p_nu,
+//                  dp_mu/dl = 1/2 d_mu g_{rs} k^r k^s  (PHGD001A.cpp:159-202),
+//                  with d_mu g from register-resident dual numbers (dual.cuh);
+//   ginv()         the inverse metric as a bilinear form (for the FP64
+//                  constraint re-projection and the null value);
+//   radial()       the radial coordinate of the family and its gradient dr;
+//   metric_full()  g_{mu nu} and d_l g_{mu nu} (IMetric::evaluate, PHMT000A.h:38).
+// The Kerr-Schild family never forms a 4x4 inverse: with the null covector
+// l_mu = (1, (rx+ay)/(r^2+a^2), (ry-ax)/(r^2+a^2), z/r) (eta-null),
+// g = eta + H l l  has  g^{-1} = eta - H l# l#  (l# = eta l), and the
+// reference's "simplified" Lambda term -Lambda R^2/3 on g_tt
+// (PHMT100A.h:362-369) is folded in exactly by a Sherman-Morrison update.
+#pragma once
+
+#include "dual.cuh"
+#include "../../include/sirius_cuda.h"
+
+namespace sirius {
+
+struct MetricDev {
+    int family;
+    int shape;
+    double M, a, Q, Lambda;
+    double a2, Q2, lam3, sqrtM;   // a^2, Q^2, Lambda/3
+    int has_lambda;        // |Lambda| > 1e-15 (PHMT100A.h:365)
+    double b0, Phi0, gtt_mt;  // Morris-Thorne: g_tt = -exp(2 Phi0)
+    double vs, sigma, Rb, inv_2tanhsR;  // Alcubierre
+};
+
+template <class T>
+__device__ __forceinline__ T tmax(T a, T b) { return a > b ? a : b; }
+
+// ---------------------------------------------------------------------------
+// Kerr-Schild family (PHMT100A.h:198-396): H and l_i as dual numbers.
+// r solves r^4 - (R^2 - a^2) r^2 - a^2 z^2 = 0; its gradient enters as the
+// implicit-function seed  dr = (r x, r y, z (r^2 + a^2) / r) / sqrt(disc).
+// ---------------------------------------------------------------------------
+template <class T>
+struct KSPieces {
+    D3<T> H, l1, l2, l3;
+    T r;
+};
+
+template <class T>
+__device__ __forceinline__ void ks_pieces(const MetricDev& m, T x, T y, T z, KSPieces<T>& o) {
+    const T a = T(m.a), a2 = T(m.a2);
+    const T R2 = x * x + y * y + z * z;
+    const T Rm2 = R2 - a2;
+    const T disc = tmax(Rm2 * Rm2 + T(4) * a2 * z * z, T(1e-20));
+    const T sd = sqrt_(disc);
+    const T r2 = tmax((Rm2 + sd) * T(0.5), T(1e-10));
+    const T r = sqrt_(r2);
+    const T isd = rcp_(sd);
+    const T ir = rcp_(r);
+    const D3<T> rd = dwith(r, r * x * isd, r * y * isd, z * (r2 + a2) * isd * ir);
+    const D3<T> X = dvar(x, 0), Y = dvar(y, 1), Z = dvar(z, 2);
+    const D3<T> rr2 = rd * rd;
+    const D3<T> iden = inv(rr2 + a2);
+    o.l1 = (rd * X + Y * a) * iden;
+    o.l2 = (rd * Y - X * a) * iden;
+    o.l3 = Z * dwith(ir, -ir * ir * rd.d[0], -ir * ir * rd.d[1], -ir * ir * rd.d[2]);
+    const D3<T> num = (rd * T(2.0 * m.M) - T(m.Q2)) * rr2;
+    const D3<T> fden = rr2 * rr2 + Z * Z * a2;
+    o.H = num * inv(fden);
+    o.r = r;
+}
+
+template <class T>
+__device__ __forceinline__ void ks_rhs(const MetricDev& m, const T x[4], const T p[4], T k[4], T f[4]) {
+    KSPieces<T> P;
+    ks_pieces(m, x[1], x[2], x[3], P);
+    const T H = P.H.v, l1 = P.l1.v, l2 = P.l2.v, l3 = P.l3.v;
+    // g^{-1} p = eta p - H l# (l# . p), l# = (-1, l1, l2, l3)
+    const T lp = -p[0] + l1 * p[1] + l2 * p[2] + l3 * p[3];
+    k[0] = -p[0] + H * lp;
+    k[1] = p[1] - H * l1 * lp;
+    k[2] = p[2] - H * l2 * lp;
+    k[3] = p[3] - H * l3 * lp;
+    if (m.has_lambda) {
+        const T c = T(m.lam3) * (x[1] * x[1] + x[2] * x[2] + x[3] * x[3]);
+        const T w0 = -T(1) - H, w1 = H * l1, w2 = H * l2, w3 = H * l3;
+        const T s = c * (w0 * p[0] + w1 * p[1] + w2 * p[2] + w3 * p[3]) * rcp_(T(1) + c * (T(1) + H));
+        k[0] += s * w0; k[1] += s * w1; k[2] += s * w2; k[3] += s * w3;
+    }
+    // dp_lambda = 1/2 dH (l.k)^2 + H (l.k)(dl.k) [- Lambda x_lambda (k^0)^2 / 3]
+    const T lk = k[0] + l1 * k[1] + l2 * k[2] + l3 * k[3];
+    f[0] = T(0);
+#pragma unroll
+    for (int i = 0; i < 3; ++i) {
+        const T dlk = P.l1.d[i] * k[1] + P.l2.d[i] * k[2] + P.l3.d[i] * k[3];
+        f[i + 1] = lk * (T(0.5) * P.H.d[i] * lk + H * dlk);
+    }
+    if (m.has_lambda) {
+        const T q = T(m.lam3) * k[0] * k[0];
+        f[1] -= q * x[1]; f[2] -= q * x[2]; f[3] -= q * x[3];
+    }
+}
+
+// ---------------------------------------------------------------------------
+// Morris-Thorne (PHMT101A.h:195-345), chart (t, r, theta, phi); r clamped to
+// >= 1.001 b0 as the reference does (:293); g diagonal.
+// ---------------------------------------------------------------------------
+template <class T>
+__device__ __forceinline__ D3<T> mt_grr(const MetricDev& m, T r) {
+    const T b0 = T(m.b0);
+    const D3<T> R = dvar(tmax(r, b0 * T(1.001)), 0);
+    D3<T> b;
+    if (m.shape == SIRIUS_WORMHOLE_ZERO_TIDAL) b = dconst(b0);
+    else if (m.shape == SIRIUS_WORMHOLE_ABSURDLY_BENIGN) b = (dconst(T(2)) - inv(R) * b0) * b0;
+    else b = inv(R) * (b0 * b0);  // Ellis
+    D3<T> f = dconst(T(1)) - b * inv(R);
+    if (f.v < T(1e-10)) f = dconst(T(1e-10));
+    return inv(f);
+}
+
+template <class T>
+__device__ __forceinline__ void mt_rhs(const MetricDev& m, const T x[4], const T p[4], T k[4], T f[4]) {
+    const T r = tmax(x[1], T(m.b0) * T(1.001));
+    const T s = sin(x[2]), c = cos(x[2]);
+    const T s2 = tmax(s * s, T(1e-24));
+    const D3<T> grr = mt_grr(m, x[1]);
+    const T r2 = r * r;
+    k[0] = p[0] * rcp_(T(m.gtt_mt));
+    k[1] = p[1] * rcp_(grr.v);
+    k[2] = p[2] * rcp_(r2);
+    k[3] = p[3] * rcp_(r2 * s2);
+    f[0] = T(0);
+    f[1] = T(0.5) * grr.d[0] * k[1] * k[1] + r * (k[2] * k[2] + s2 * k[3] * k[3]);
+    f[2] = r2 * s * c * k[3] * k[3];
+    f[3] = T(0);
+}
+
+// ---------------------------------------------------------------------------
+// Alcubierre (PHMT102A.h:136-229), Cartesian, static bubble at the origin:
+// g_tt = -(1 - v^2 f^2), g_tx = -v f;  g^{tt} = -1, g^{tx} = -v f, g^{xx} = 1 - v^2 f^2.
+// ---------------------------------------------------------------------------
+template <class T>
+__device__ __forceinline__ D3<T> alc_f(const MetricDev& m, T x, T y, T z) {
+    const T rs = tmax(sqrt_(x * x + y * y + z * z), T(1e-10));
+    const T irs = rcp_(rs);
+    const D3<T> R = dwith(rs, x * irs, y * irs, z * irs);
+    const T sg = T(m.sigma), Rb = T(m.Rb);
+    return (dtanh((R + Rb) * sg) - dtanh((R - Rb) * sg)) * T(m.inv_2tanhsR);
+}
+
+template <class T>
+__device__ __forceinline__ void alc_rhs(const MetricDev& m, const T x[4], const T p[4], T k[4], T f[4]) {
+    const D3<T> F = alc_f(m, x[1], x[2], x[3]);
+    const T v = T(m.vs), vf = v * F.v;
+    k[0] = -p[0] - vf * p[1];
+    k[1] = -vf * p[0] + (T(1) - vf * vf) * p[1];
+    k[2] = p[2];
+    k[3] = p[3];
+    // dp = v df (v f (k^t)^2 - k^t k^x)
+    const T q = v * (vf * k[0] * k[0] - k[0] * k[1]);
+    f[0] = T(0);
+    f[1] = q * F.d[0];
+    f[2] = q * F.d[1];
+    f[3] = q * F.d[2];
+}
+
+template <class T>
+__device__ __forceinline__ void rhs(const MetricDev& m, const T x[4], const T p[4], T k[4], T f[4]) {
+    if (m.family == SIRIUS_METRIC_KERR_SCHILD) ks_rhs(m, x, p, k, f);
+    else if (m.family == SIRIUS_METRIC_MORRIS_THORNE) mt_rhs(m, x, p, k, f);
+    else alc_rhs(m, x, p, k, f);
+}
+
+// ---------------------------------------------------------------------------
+// Inverse metric as a bilinear form, evaluated once at x for up to three
+// covectors: out = {g^{-1}(u,u), g^{-1}(u,v), g^{-1}(v,v)}. Also returns the
+// family's radial coordinate r and its gradient d (the projection direction).
+// ---------------------------------------------------------------------------
+struct InvForm {
+    double r;      // radial coordinate (KS: Boyer-Lindquist r; MT: r; Alcubierre: R)
+    double d[4];   // dr
+    double H, l[4], c, w[4], sm;  // KS pieces
+    double diag[4];               // MT
+    double vf;                    // Alcubierre
+};
+
+__device__ __forceinline__ void inv_form(const MetricDev& m, const double x[4], InvForm& F) {
+    F.d[0] = 0.0;
+    if (m.family == SIRIUS_METRIC_MORRIS_THORNE) {
+        const double r = fmax(x[1], m.b0 * 1.001);
+        const double s = sin(x[2]);
+        const double s2 = fmax(s * s, 1e-24);
+        const D3<double> grr = mt_grr<double>(m, x[1]);
+        F.r = x[1];
+        F.d[1] = 1.0; F.d[2] = 0.0; F.d[3] = 0.0;
+        F.diag[0] = 1.0 / m.gtt_mt; F.diag[1] = 1.0 / grr.v; F.diag[2] = 1.0 / (r * r); F.diag[3] = 1.0 / (r * r * s2);
+        return;
+    }
+    const double X = x[1], Y = x[2], Z = x[3];
+    const double R2 = X * X + Y * Y + Z * Z;
+    if (m.family == SIRIUS_METRIC_ALCUBIERRE) {
+        const double Rr = sqrt(R2);
+        F.r = Rr;
+        F.d[1] = X / Rr; F.d[2] = Y / Rr; F.d[3] = Z / Rr;
+        const D3<double> f = alc_f<double>(m, X, Y, Z);
+        F.vf = m.vs * f.v;
+        return;
+    }
+    const double a2 = m.a2, Rm2 = R2 - a2;
+    const double sd = sqrt(fmax(Rm2 * Rm2 + 4.0 * a2 * Z * Z, 1e-20));
+    const double r2 = fmax(0.5 * (Rm2 + sd), 1e-10);
+    const double r = sqrt(r2);
+    F.r = r;
+    if (m.a == 0.0) {
+        const double Rr = sqrt(R2);
+        F.d[1] = X / Rr; F.d[2] = Y / Rr; F.d[3] = Z / Rr;
+    } else {
+        F.d[1] = r * X / sd; F.d[2] = r * Y / sd; F.d[3] = Z * (r2 + a2) / (r * sd);
+    }
+    const double den = r2 + a2;
+    F.l[0] = -1.0;  // l# = eta l
+    F.l[1] = (r * X + m.a * Y) / den;
+    F.l[2] = (r * Y - m.a * X) / den;
+    F.l[3] = Z / r;
+    F.H = (2.0 * m.M * r - m.Q2) * r2 / (r2 * r2 + a2 * Z * Z);
+    F.c = m.has_lambda ? m.lam3 * R2 : 0.0;
+    F.w[0] = -1.0 - F.H; F.w[1] = F.H * F.l[1]; F.w[2] = F.H * F.l[2]; F.w[3] = F.H * F.l[3];
+    F.sm = F.c / (1.0 + F.c * (1.0 + F.H));
+}
+
+__device__ __forceinline__ double inv_apply(const MetricDev& m, const InvForm& F, const double u[4], const double v[4]) {
+    if (m.family == SIRIUS_METRIC_MORRIS_THORNE)
+        return F.diag[0] * u[0] * v[0] + F.diag[1] * u[1] * v[1] + F.diag[2] * u[2] * v[2] + F.diag[3] * u[3] * v[3];
+    if (m.family == SIRIUS_METRIC_ALCUBIERRE)
+        return -u[0] * v[0] - F.vf * (u[0] * v[1] + u[1] * v[0]) + (1.0 - F.vf * F.vf) * u[1] * v[1] + u[2] * v[2] +
+               u[3] * v[3];
+    const double eta = -u[0] * v[0] + u[1] * v[1] + u[2] * v[2] + u[3] * v[3];
+    const double lu = F.l[0] * u[0] + F.l[1] * u[1] + F.l[2] * u[2] + F.l[3] * u[3];
+    const double lv = F.l[0] * v[0] + F.l[1] * v[1] + F.l[2] * v[2] + F.l[3] * v[3];
+    double s = eta - F.H * lu * lv;
+    if (m.has_lambda) {
+        const double wu = F.w[0] * u[0] + F.w[1] * u[1] + F.w[2] * u[2] + F.w[3] * u[3];
+        const double wv = F.w[0] * v[0] + F.w[1] * v[1] + F.w[2] * v[2] + F.w[3] * v[3];
+        s += F.sm * wu * wv;
+    }
+    return s;
+}
+
+// E/L_z/Carter-preserving constraint re-projection: p <- p + alpha dr with the
+// root alpha of g^{-1}(p + a dr, p + a dr) = 0 of smallest magnitude — the
+// chart-independent form of SymplecticIntegratorD::renormalizeNull's p_r
+// solve (PHSI001A.h:366-418). Returns the null value before projection.
+__device__ __forceinline__ double project_null(const MetricDev& m, const InvForm& F, double p[4]) {
+    const double A = inv_apply(m, F, F.d, F.d);
+    const double B = 2.0 * inv_apply(m, F, p, F.d);
+    const double C = inv_apply(m, F, p, p);
+    const double disc = B * B - 4.0 * A * C;
+    if (disc < 0.0 || fabs(A) < 1e-15) return C;
+    const double q = -0.5 * (B + (B >= 0.0 ? sqrt(disc) : -sqrt(disc)));
+    if (q == 0.0) return C;
+    const double alpha = C / q;
+#pragma unroll
+    for (int i = 0; i < 4; ++i) p[i] += alpha * F.d[i];
+    return C;
+}
+
+// ---------------------------------------------------------------------------
+// Full metric and derivatives (IMetric::evaluate): g[16], dg[64], dg[l*16+m*4+n].
+// ---------------------------------------------------------------------------
+template <class T>
+__device__ void metric_full(const MetricDev& m, const T x[4], T g[16], T dg[64]) {
+    for (int i = 0; i < 16; ++i) g[i] = T(0);
+    for (int i = 0; i < 64; ++i) dg[i] = T(0);
+    if (m.family == SIRIUS_METRIC_KERR_SCHILD) {
+        KSPieces<T> P;
+        ks_pieces(m, x[1], x[2], x[3], P);
+        const D3<T> one = dconst(T(1));
+        const D3<T> l[4] = {one, P.l1, P.l2, P.l3};
+        for (int a = 0; a < 4; ++a)
+            for (int b = 0; b < 4; ++b) {
+                const D3<T> h = P.H * l[a] * l[b];
+                const T eta = (a == b) ? (a == 0 ? T(-1) : T(1)) : T(0);
+                g[4 * a + b] = eta + h.v;
+                for (int q = 0; q < 3; ++q) dg[16 * (q + 1) + 4 * a + b] = h.d[q];
+            }
+        if (m.has_lambda) {
+            g[0] -= T(m.lam3) * (x[1] * x[1] + x[2] * x[2] + x[3] * x[3]);
+            for (int q = 0; q < 3; ++q) dg[16 * (q + 1)] -= T(2) * T(m.lam3) * x[q + 1];
+        }
+    } else if (m.family == SIRIUS_METRIC_MORRIS_THORNE) {
+        const T r = tmax(x[1], T(m.b0) * T(1.001));
+        const T s = sin(x[2]), c = cos(x[2]);
+        const D3<T> grr = mt_grr(m, x[1]);
+        g[0] = T(m.gtt_mt);
+        g[5] = grr.v;
+        g[10] = r * r;
+        g[15] = r * r * s * s;
+        dg[16 + 5] = grr.d[0];
+        dg[16 + 10] = T(2) * r;
+        dg[16 + 15] = T(2) * r * s * s;
+        dg[32 + 15] = T(2) * r * r * s * c;
+    } else {
+        const D3<T> F = alc_f(m, x[1], x[2], x[3]);
+        const T v = T(m.vs), vf = v * F.v;
+        g[0] = -(T(1) - vf * vf);
+        g[1] = g[4] = -vf;
+        g[5] = g[10] = g[15] = T(1);
+        for (int q = 0; q < 3; ++q) {
+            dg[16 * (q + 1)] = T(2) * v * v * F.v * F.d[q];
+            dg[16 * (q + 1) + 1] = dg[16 * (q + 1) + 4] = -v * F.d[q];
+        }
+    }
+}
+
+}  // namespace sirius

@@ -1,0 +1,301 @@
+// trace.cuh — the per-ray state machine of the geodesic engine (device code).
+//
+// One thread owns one ray at a time. A ray is initialised from its pixel
+// (PinholeCamera::generateRay + GeodesicTracer::initializeLightray,
+// CMBS001A.h:120-185, GTRC001A.cpp:15-134), advanced by Dormand-Prince 5(4)
+// steps on (x^mu, p_mu) (Geodesic::integrateStepRK45, PHGD001A.cpp:530-641)
+// with retry-on-reject, re-projected onto the null cone in FP64 after
+// accepted steps, and checked for the reference's terminations in its order
+// (GeodesicTracer::trace, GTRC001A.cpp:264-556): failure, spiral, horizon,
+// escape, volumetric segment, thin-disk crossing.
+#pragma once
+
+#include <stdint.h>
+
+#include "spacetime.cuh"
+
+namespace sirius {
+
+constexpr double kPi = 3.14159265358979323846;
+
+// Per-frame constants prepared on the host (double precision, host libm).
+struct FrameDev {
+    MetricDev m;
+    long long ray_offset, n_rays;
+    int width, height, projection, has_horizon;
+    // camera
+    double cam_t, cam_r, cam_st, cam_ct, cam_sp, cam_cp, cam_th, cam_ph;
+    float aspect, tan_half_fov, cY, sY, cP, sP, cR, sR;
+    // radii
+    double disk_in, disk_out, r_hor, island_r, a_star, isco, r_ph_pro;
+    double sqrt_m_gtt_cam;
+};
+
+struct CfgDev {
+    double atol, rtol, hmin, hmax, h0, safety, grow, shrink;
+    double escape_r, decay;
+    int max_steps, enable_disk, enable_vol, nbins, vol_sub, proj_period, spiral, compat;
+    double vol_j0, vol_aoj, vol_hz, vol_s;
+    float nu[SIRIUS_MAX_BINS];       // bin frequencies
+    float nu_pow[SIRIUS_MAX_BINS];   // nu^-s
+};
+
+// ---------------------------------------------------------------------------
+// Page-Thorne flux (AccretionDiskD::flux / fullPageThorneFlux, PHAD001A.h:112-361)
+// in geometric units F = 3/(8 pi r^3) Q(r); 16-point Gauss-Legendre on [r_isco, r]
+// (nodes/weights: Abramowitz & Stegun table 25.4).
+// ---------------------------------------------------------------------------
+__device__ __forceinline__ double pt_E(double r, double a) {
+    const double s = sqrt(r), d = r * sqrt(r * r - 3.0 * r + 2.0 * a * s);
+    return fabs(d) < 1e-15 ? 1.0 : (r * r - 2.0 * r + a * s) / d;
+}
+__device__ __forceinline__ double pt_L(double r, double a) {
+    const double s = sqrt(r), d = r * sqrt(r * r - 3.0 * r + 2.0 * a * s);
+    return fabs(d) < 1e-15 ? 0.0 : (r * r - 2.0 * a * s + a * a) / d;
+}
+__device__ __forceinline__ double pt_Om(double r, double a) { return 1.0 / (r * sqrt(r) + a); }
+__device__ __forceinline__ double pt_dLdr(double r, double a) {
+    if (r <= 0) return 0;
+    const double sr = sqrt(r);
+    const double N = r * r - 2.0 * a * sr + a * a, D = r * r - 3.0 * r + 2.0 * a * sr;
+    if (D <= 1e-15) return 0;
+    const double sD = sqrt(D), q = a / sr;
+    const double dN = 2.0 * r - q, dD = 2.0 * r - 3.0 + q;
+    const double drsD = (2.0 * D + r * dD) / (2.0 * sD), rsD = r * sD, den = rsD * rsD;
+    if (fabs(den) < 1e-30) return 0;
+    return (dN * rsD - N * drsD) / den;
+}
+__device__ __forceinline__ double pt_dOm(double r, double a) {
+    if (r <= 0) return 0;
+    const double den = r * sqrt(r) + a;
+    return -3.0 * sqrt(r) / (2.0 * den * den);
+}
+
+__device__ double nt_flux(double r, double a, double isco, double r_in, double r_out) {
+    const double gx[8] = {0.0950125098376374, 0.2816035507792589, 0.4580167776572274, 0.6178762444026438,
+                          0.7554044083550030, 0.8656312023878318, 0.9445750230732326, 0.9894009349916499};
+    const double gw[8] = {0.1894506104550685, 0.1826034150449236, 0.1691565193950025, 0.1495959888165767,
+                          0.1246289712555339, 0.0951585116824928, 0.0622535239386479, 0.0271524594117541};
+    if (r < r_in || r > r_out || r <= isco) return 0.0;
+    const double Fn = 3.0 / (8.0 * kPi * r * r * r);
+    if (r > 1.5 * isco) {
+        const double hw = 0.5 * (r - isco), mid = 0.5 * (r + isco);
+        double I = 0;
+        for (int sgn = -1; sgn <= 1; sgn += 2)
+            for (int i = 0; i < 8; ++i) {
+                const double rr = mid + hw * sgn * gx[i];
+                I += gw[i] * (pt_E(rr, a) - pt_Om(rr, a) * pt_L(rr, a)) * pt_dLdr(rr, a);
+            }
+        I *= hw;
+        const double EmOL = pt_E(r, a) - pt_Om(r, a) * pt_L(r, a);
+        if (fabs(EmOL) >= 1e-15) {
+            const double F = Fn * (-pt_dOm(r, a) / (EmOL * EmOL)) * I;
+            if (isfinite(F) && F > 0) return F;
+        }
+    }
+    const double it = 1.0 - sqrt(isco / r);
+    if (it <= 0) return 0.0;
+    const double y = sqrt(r), den = y * y * y * (y - 3.0 / y + 2.0 * a / (y * y));
+    double Q = fabs(den) > 1e-10 ? 1.0 / den : 1.0;
+    if (!isfinite(Q) || Q <= 0) Q = 1.0;
+    Q = fmin(fmax(Q, 0.1), 10.0);
+    return Fn * it * Q;
+}
+
+// ---------------------------------------------------------------------------
+// Camera ray for pixel (px, py). The pinhole arithmetic is the reference's
+// float arithmetic (CMBS001A.h:130-181) with every operation rounded
+// individually (no contraction), the trigonometric constants taken from the host.
+// ---------------------------------------------------------------------------
+__device__ __forceinline__ void camera_dir(const FrameDev& F, int px, int py, double dir[4]) {
+    dir[0] = 0.0;
+    if (F.projection == SIRIUS_CAMERA_EQUIRECTANGULAR) {
+        const double psi = (2.0 * (px + 0.5) / F.width - 1.0) * kPi;
+        const double chi = (1.0 - 2.0 * (py + 0.5) / F.height) * (0.5 * kPi);
+        double sc, cc, sps, cps;
+        sincos(chi, &sc, &cc);
+        sincos(psi, &sps, &cps);
+        dir[1] = -cc * cps;
+        dir[2] = -sc;
+        dir[3] = cc * sps;
+        return;
+    }
+    const float w = float(F.width), hgt = float(F.height);
+    const float pxn = __fmul_rn(__fsub_rn(__fdiv_rn(__fmul_rn(2.0f, __fadd_rn(float(px), 0.5f)), w), 1.0f), F.aspect);
+    const float pyn = __fsub_rn(1.0f, __fdiv_rn(__fmul_rn(2.0f, __fadd_rn(float(py), 0.5f)), hgt));
+    const float dx = __fmul_rn(pxn, F.tan_half_fov), dy = __fmul_rn(pyn, F.tan_half_fov), dz = -1.0f;
+    const float rx = __fsub_rn(__fmul_rn(dx, F.cR), __fmul_rn(dy, F.sR));
+    const float ry = __fadd_rn(__fmul_rn(dx, F.sR), __fmul_rn(dy, F.cR));
+    const float ry2 = __fsub_rn(__fmul_rn(ry, F.cP), __fmul_rn(dz, F.sP));
+    const float rz = __fadd_rn(__fmul_rn(ry, F.sP), __fmul_rn(dz, F.cP));
+    const float rx2 = __fadd_rn(__fmul_rn(rx, F.cY), __fmul_rn(rz, F.sY));
+    const float rz2 = __fadd_rn(__fmul_rn(-rx, F.sY), __fmul_rn(rz, F.cY));
+    const float len = __fsqrt_rn(__fadd_rn(__fadd_rn(__fmul_rn(rx2, rx2), __fmul_rn(ry2, ry2)), __fmul_rn(rz2, rz2)));
+    dir[1] = double(__fdiv_rn(rz2, len));
+    dir[2] = double(__fdiv_rn(-ry2, len));
+    dir[3] = double(__fdiv_rn(rx2, len));
+}
+
+// TensorOps::normalizeNull (MTTN001A.cpp:171-237) for k^0, given g_0mu, g_ij.
+__device__ __forceinline__ double null_k0(const double g[16], const double k[4]) {
+    const double A = g[0];
+    double B = 0, C = 0;
+    for (int i = 1; i < 4; ++i) B += 2.0 * g[i] * k[i];
+    for (int i = 1; i < 4; ++i)
+        for (int j = 1; j < 4; ++j) C += g[4 * i + j] * k[i] * k[j];
+    if (fabs(A) < 1e-15) return fabs(B) > 1e-15 ? -C / B : 1.0;
+    const double d = B * B - 4.0 * A * C;
+    if (d < 0.0) return 1.0;
+    const double sd = sqrt(d);
+    const double kp = (-B + sd) / (2.0 * A), km = (-B - sd) / (2.0 * A);
+    if (kp > 0.0) return kp;
+    if (km > 0.0) return km;
+    return fmax(kp, km);
+}
+
+// Initial state from a camera ray (GTRC001A.cpp:15-134 without float roundings).
+__device__ __forceinline__ void init_state(const FrameDev& F, const double dir[4], double x[4], double p[4]) {
+    const double r = F.cam_r, st = F.cam_st, ct = F.cam_ct, sp = F.cam_sp, cp = F.cam_cp;
+    const double vr = dir[1], vth = dir[2] / r;
+    double vph = dir[3] / (r * st);
+    if (fabs(st) < 1e-10) vph = 0.0;
+    double k[4];
+    double g[16], dg[64];
+    if (F.m.family == SIRIUS_METRIC_MORRIS_THORNE) {
+        x[0] = F.cam_t; x[1] = r; x[2] = F.cam_th; x[3] = F.cam_ph;
+        metric_full<double>(F.m, x, g, dg);
+        k[1] = vr / sqrt(g[5]); k[2] = vth; k[3] = vph;
+    } else {
+        x[0] = F.cam_t; x[1] = r * st * cp; x[2] = r * st * sp; x[3] = r * ct;
+        k[1] = vr * st * cp + r * vth * ct * cp - r * vph * st * sp;
+        k[2] = vr * st * sp + r * vth * ct * sp + r * vph * st * cp;
+        k[3] = vr * ct - r * vth * st;
+        metric_full<double>(F.m, x, g, dg);
+    }
+    k[0] = 0.0;
+    k[0] = null_k0(g, k);
+    for (int mu = 0; mu < 4; ++mu) {
+        double s = 0;
+        for (int nu = 0; nu < 4; ++nu) s += g[4 * mu + nu] * k[nu];
+        p[mu] = s;
+    }
+}
+
+// ---------------------------------------------------------------------------
+// Dormand-Prince 5(4) attempt (tableau: Dormand & Prince 1980; PHGD001A.cpp:16-79).
+// T is the stage precision: float for the FP32 bulk, double for FP64.
+// The state (x, p) stays in FP64; stage points are x + h sum a_ij k_j in T;
+// the update is accumulated in FP64 from the T-precision weighted sum.
+// On entry (kx, kp) = f(x, p). Returns the scaled RMS position error
+// (computeRK45ErrorNorm, PHGD001A.cpp:508-517).
+// ---------------------------------------------------------------------------
+template <class T>
+__device__ __forceinline__ double dp45_attempt(const MetricDev& m, const CfgDev& c, const double x[4], const double p[4],
+                                               double h, const double kx[4], const double kp[4], double xn[4],
+                                               double pn[4], double k7x[4], double k7p[4]) {
+    const T a21 = T(1.0 / 5.0);
+    const T a31 = T(3.0 / 40.0), a32 = T(9.0 / 40.0);
+    const T a41 = T(44.0 / 45.0), a42 = T(-56.0 / 15.0), a43 = T(32.0 / 9.0);
+    const T a51 = T(19372.0 / 6561.0), a52 = T(-25360.0 / 2187.0), a53 = T(64448.0 / 6561.0), a54 = T(-212.0 / 729.0);
+    const T a61 = T(9017.0 / 3168.0), a62 = T(-355.0 / 33.0), a63 = T(46732.0 / 5247.0), a64 = T(49.0 / 176.0),
+            a65 = T(-5103.0 / 18656.0);
+    const T b1 = T(35.0 / 384.0), b3 = T(500.0 / 1113.0), b4 = T(125.0 / 192.0), b5 = T(-2187.0 / 6784.0),
+            b6 = T(11.0 / 84.0);
+    const T e1 = T(35.0 / 384.0 - 5179.0 / 57600.0), e3 = T(500.0 / 1113.0 - 7571.0 / 16695.0),
+            e4 = T(125.0 / 192.0 - 393.0 / 640.0), e5 = T(-2187.0 / 6784.0 + 92097.0 / 339200.0),
+            e6 = T(11.0 / 84.0 - 187.0 / 2100.0), e7 = T(-1.0 / 40.0);
+    const T ht = T(h);
+    T X[4], P[4], k1x[4], k1p[4], k2x[4], k2p[4], k3x[4], k3p[4], k4x[4], k4p[4], k5x[4], k5p[4], k6x[4], k6p[4];
+    T xs[4], ps[4];
+#pragma unroll
+    for (int i = 0; i < 4; ++i) { X[i] = T(x[i]); P[i] = T(p[i]); k1x[i] = T(kx[i]); k1p[i] = T(kp[i]); }
+#pragma unroll
+    for (int i = 0; i < 4; ++i) { xs[i] = X[i] + ht * (a21 * k1x[i]); ps[i] = P[i] + ht * (a21 * k1p[i]); }
+    rhs(m, xs, ps, k2x, k2p);
+#pragma unroll
+    for (int i = 0; i < 4; ++i) {
+        xs[i] = X[i] + ht * (a31 * k1x[i] + a32 * k2x[i]);
+        ps[i] = P[i] + ht * (a31 * k1p[i] + a32 * k2p[i]);
+    }
+    rhs(m, xs, ps, k3x, k3p);
+#pragma unroll
+    for (int i = 0; i < 4; ++i) {
+        xs[i] = X[i] + ht * (a41 * k1x[i] + a42 * k2x[i] + a43 * k3x[i]);
+        ps[i] = P[i] + ht * (a41 * k1p[i] + a42 * k2p[i] + a43 * k3p[i]);
+    }
+    rhs(m, xs, ps, k4x, k4p);
+#pragma unroll
+    for (int i = 0; i < 4; ++i) {
+        xs[i] = X[i] + ht * (a51 * k1x[i] + a52 * k2x[i] + a53 * k3x[i] + a54 * k4x[i]);
+        ps[i] = P[i] + ht * (a51 * k1p[i] + a52 * k2p[i] + a53 * k3p[i] + a54 * k4p[i]);
+    }
+    rhs(m, xs, ps, k5x, k5p);
+#pragma unroll
+    for (int i = 0; i < 4; ++i) {
+        xs[i] = X[i] + ht * (a61 * k1x[i] + a62 * k2x[i] + a63 * k3x[i] + a64 * k4x[i] + a65 * k5x[i]);
+        ps[i] = P[i] + ht * (a61 * k1p[i] + a62 * k2p[i] + a63 * k3p[i] + a64 * k4p[i] + a65 * k5p[i]);
+    }
+    rhs(m, xs, ps, k6x, k6p);
+#pragma unroll
+    for (int i = 0; i < 4; ++i) {
+        const T sx = b1 * k1x[i] + b3 * k3x[i] + b4 * k4x[i] + b5 * k5x[i] + b6 * k6x[i];
+        const T sp = b1 * k1p[i] + b3 * k3p[i] + b4 * k4p[i] + b5 * k5p[i] + b6 * k6p[i];
+        xn[i] = x[i] + h * double(sx);
+        pn[i] = p[i] + h * double(sp);
+        xs[i] = T(xn[i]);
+        ps[i] = T(pn[i]);
+    }
+    T q7x[4], q7p[4];
+    rhs(m, xs, ps, q7x, q7p);
+    double en = 0.0;
+#pragma unroll
+    for (int i = 0; i < 4; ++i) {
+        k7x[i] = double(q7x[i]);
+        k7p[i] = double(q7p[i]);
+        const T ex = e1 * k1x[i] + e3 * k3x[i] + e4 * k4x[i] + e5 * k5x[i] + e6 * k6x[i] + e7 * q7x[i];
+        const double e = h * double(ex) / (c.atol + c.rtol * fabs(xn[i]));
+        en += e * e;
+    }
+    return sqrt(0.25 * en);
+}
+
+// Geodesic::computeOptimalStep (PHGD001A.cpp:471-483).
+__device__ __forceinline__ double optimal_step(double h, double err, const CfgDev& c) {
+    if (err < 1e-15) return fmin(h * c.grow, c.hmax);
+    double fac = c.safety * pow(1.0 / err, 0.2);
+    fac = fmax(c.shrink, fmin(c.grow, fac));
+    return fmax(c.hmin, fmin(c.hmax, h * fac));
+}
+
+// Cubic Hermite interpolation of z over the accepted step; bisection for z = 0.
+__device__ __forceinline__ double hermite_root(double z0, double z1, double dz0, double dz1, double h) {
+    double lo = 0.0, hi = 1.0, flo = z0;
+    for (int it = 0; it < 60; ++it) {
+        const double s = 0.5 * (lo + hi), s2 = s * s, s3 = s2 * s;
+        const double f = (2.0 * s3 - 3.0 * s2 + 1.0) * z0 + (s3 - 2.0 * s2 + s) * h * dz0 +
+                         (-2.0 * s3 + 3.0 * s2) * z1 + (s3 - s2) * h * dz1;
+        if ((f < 0.0) == (flo < 0.0)) { lo = s; flo = f; } else { hi = s; }
+    }
+    return 0.5 * (lo + hi);
+}
+
+// Keplerian emitter at BL radius rbl seen from the camera: g = (p.u_obs)/(p.u_em),
+// u_em = u^t (d_t + Omega d_phi) with u^t from the Killing norms at the point
+// (g_tt = -1 + H, g_t,phi = H (l.xi), g_phi,phi = x^2 + y^2 + H (l.xi)^2 in KS).
+template <class T>
+__device__ __forceinline__ T kepler_g(const MetricDev& m, T x, T y, T z, T rbl, T E, T Lz, T sqrt_m_gtt_cam) {
+    KSPieces<T> P;
+    ks_pieces(m, x, y, z, P);
+    const T H = P.H.v, lxi = -y * P.l1.v + x * P.l2.v;
+    T gtt = -T(1) + H;
+    if (m.has_lambda) gtt -= T(m.lam3) * (x * x + y * y + z * z);
+    const T gtp = H * lxi, gpp = x * x + y * y + H * lxi * lxi;
+    const T Om = T(m.sqrtM) * rcp_(rbl * sqrt_(rbl) + T(m.a) * T(m.sqrtM));
+    const T n = -(gtt + T(2) * Om * gtp + Om * Om * gpp);
+    if (!(n > T(0))) return T(0);
+    const T ut = rsqrt_(n);
+    const T den = sqrt_m_gtt_cam * ut * (T(1) - Om * Lz * rcp_(E));
+    return den > T(0) ? rcp_(den) : T(0);
+}
+
+}  // namespace sirius

@@ -1,0 +1,164 @@
+"""Python binding of the C ABI (include/sirius_cuda.h) via ctypes.
+
+This is a thin host-side mirror for scripts and tests; the product boundary is
+the C ABI itself. The library must have been built (sirius_b200.build.build());
+there is no fallback of any kind when it is missing or no CUDA device exists.
+"""
+import ctypes as C
+import os
+
+import numpy as np
+
+from . import abi
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+LIB_PATH = os.path.join(HERE, "libsirius_b200.so")
+
+_P = C.POINTER
+
+# Every symbol include/sirius_cuda.h declares (checked by tests/test_abi.py).
+EXPORTS = [
+    "sirius_cuda_abi_version", "sirius_cuda_default_config", "sirius_cuda_create", "sirius_cuda_destroy",
+    "sirius_cuda_get_last_error", "sirius_cuda_configure", "sirius_cuda_trace_frames",
+    "sirius_cuda_trace_frames_device", "sirius_cuda_trace_rays", "sirius_cuda_metric_evaluate",
+    "sirius_cuda_dp45_step", "sirius_cuda_last_stats", "sirius_cuda_autotune", "sirius_cuda_measure_fma_peak",
+]
+
+
+class SiriusError(RuntimeError):
+    def __init__(self, code, msg):
+        super().__init__(f"sirius_cuda error {code}: {msg}")
+        self.code = code
+
+
+def load_library(path=LIB_PATH):
+    if not os.path.exists(path):
+        raise FileNotFoundError(f"{path} is missing: build it with `python -c 'import __graft_entry__ as g; g.build()'`")
+    L = C.CDLL(path)
+    L.sirius_cuda_abi_version.restype = C.c_int
+    L.sirius_cuda_default_config.argtypes = [_P(abi.TraceConfig)]
+    L.sirius_cuda_create.argtypes = [C.c_int, _P(C.c_void_p)]
+    L.sirius_cuda_destroy.argtypes = [C.c_void_p]
+    L.sirius_cuda_get_last_error.argtypes = [C.c_void_p]
+    L.sirius_cuda_get_last_error.restype = C.c_char_p
+    L.sirius_cuda_configure.argtypes = [C.c_void_p, _P(abi.TraceConfig)]
+    L.sirius_cuda_trace_frames.argtypes = [C.c_void_p, C.c_void_p, C.c_int32, C.c_void_p, C.c_void_p, C.c_void_p]
+    L.sirius_cuda_trace_frames_device.argtypes = [C.c_void_p, C.c_void_p, C.c_int32, C.c_int64, C.c_void_p,
+                                                  C.c_void_p, C.c_void_p, C.c_void_p]
+    L.sirius_cuda_trace_rays.argtypes = [C.c_void_p, _P(abi.Metric), C.c_double, C.c_double, C.c_void_p,
+                                         C.c_int64, C.c_void_p]
+    L.sirius_cuda_metric_evaluate.argtypes = [C.c_void_p, _P(abi.Metric), C.c_void_p, C.c_int64, C.c_int32,
+                                              C.c_void_p, C.c_void_p]
+    L.sirius_cuda_dp45_step.argtypes = [C.c_void_p, _P(abi.Metric), C.c_void_p, C.c_void_p, C.c_void_p,
+                                        C.c_void_p, C.c_int64]
+    L.sirius_cuda_last_stats.argtypes = [C.c_void_p, _P(abi.LaunchStats)]
+    L.sirius_cuda_autotune.argtypes = [C.c_void_p, C.c_void_p, C.c_int32, _P(abi.TraceConfig)]
+    L.sirius_cuda_measure_fma_peak.argtypes = [C.c_void_p, C.c_int32, _P(C.c_double)]
+    return L
+
+
+def frames_array(frames):
+    """Pack frames into a ctypes array, assigning contiguous ray offsets."""
+    arr = (abi.Frame * len(frames))(*frames)
+    off = 0
+    for f in arr:
+        f.ray_offset = off
+        off += f.camera.width * f.camera.height
+    return arr, off
+
+
+class Engine:
+    """One handle on one CUDA device (mirrors the lifecycle of sirius_optix_*)."""
+
+    def __init__(self, device=0, config=None, lib=None):
+        self.lib = lib or load_library()
+        h = C.c_void_p()
+        rc = self.lib.sirius_cuda_create(device, C.byref(h))
+        if rc != abi.OK:
+            raise SiriusError(rc, "sirius_cuda_create failed (no sm_100 device or CUDA error)")
+        self.h = h
+        self.config = config or abi.default_config()
+        self.configure(self.config)
+
+    def close(self):
+        if self.h:
+            self.lib.sirius_cuda_destroy(self.h)
+            self.h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    def _check(self, rc):
+        if rc != abi.OK:
+            raise SiriusError(rc, self.lib.sirius_cuda_get_last_error(self.h).decode())
+
+    def configure(self, cfg):
+        self._check(self.lib.sirius_cuda_configure(self.h, C.byref(cfg)))
+        self.config = cfg
+
+    def trace_frames(self, frames, results=True, image=True, spectra=False):
+        arr, total = frames_array(frames)
+        nb = self.config.n_bins if self.config.enable_volumetric else 0
+        res = np.zeros(total, dtype=abi.result_dtype()) if results else None
+        img = np.zeros(total, dtype=np.float32) if image else None
+        spc = np.zeros((total, max(nb, 1)), dtype=np.float32) if (spectra and nb) else None
+        self._check(self.lib.sirius_cuda_trace_frames(
+            self.h, C.addressof(arr), len(frames), res.ctypes.data if res is not None else None,
+            img.ctypes.data if img is not None else None, spc.ctypes.data if spc is not None else None))
+        return res, img, (spc[:, :nb] if spc is not None else None)
+
+    def trace_frames_into(self, frames_arr, n_frames, results_ptr, image_ptr, spectra_ptr):
+        """Host entry point with caller-owned host buffers (raw addresses, e.g. pinned memory)."""
+        self._check(self.lib.sirius_cuda_trace_frames(self.h, frames_arr, n_frames, results_ptr, image_ptr,
+                                                      spectra_ptr))
+
+    def trace_frames_device(self, d_frames, n_frames, total, d_results, d_image, d_spectra, stream):
+        """Device entry point: all pointers are device addresses; stream is a cudaStream_t address."""
+        self._check(self.lib.sirius_cuda_trace_frames_device(self.h, d_frames, n_frames, total, d_results, d_image,
+                                                             d_spectra, stream))
+
+    def trace_rays(self, metric, rays, disk_inner=0.0, disk_outer=20.0):
+        n = len(rays)
+        arr = (abi.CameraRay * n)(*rays)
+        out = np.zeros(n, dtype=abi.result_dtype())
+        self._check(self.lib.sirius_cuda_trace_rays(self.h, C.byref(metric), disk_inner, disk_outer,
+                                                    C.addressof(arr), n, out.ctypes.data))
+        return out
+
+    def metric_evaluate(self, metric, pos, precision=abi.PRECISION_FP64):
+        pos = np.ascontiguousarray(pos, dtype=np.float64).reshape(-1, 4)
+        n = len(pos)
+        g = np.zeros((n, 4, 4))
+        dg = np.zeros((n, 4, 4, 4))
+        self._check(self.lib.sirius_cuda_metric_evaluate(self.h, C.byref(metric), pos.ctypes.data, n, precision,
+                                                         g.ctypes.data, dg.ctypes.data))
+        return g, dg
+
+    def dp45_step(self, metric, state, h):
+        s = np.array(state, dtype=np.float64).reshape(-1, 8).copy()
+        hh = np.array(h, dtype=np.float64).reshape(-1).copy()
+        acc = np.zeros(len(s), dtype=np.int32)
+        err = np.zeros(len(s))
+        self._check(self.lib.sirius_cuda_dp45_step(self.h, C.byref(metric), s.ctypes.data, hh.ctypes.data,
+                                                   acc.ctypes.data, err.ctypes.data, len(s)))
+        return s, hh, acc, err
+
+    def stats(self):
+        st = abi.LaunchStats()
+        self._check(self.lib.sirius_cuda_last_stats(self.h, C.byref(st)))
+        return st
+
+    def autotune(self, frames):
+        arr, _ = frames_array(frames)
+        out = abi.TraceConfig()
+        self._check(self.lib.sirius_cuda_autotune(self.h, C.addressof(arr), len(frames), C.byref(out)))
+        self.config = out
+        return out
+
+    def fma_peak(self, precision):
+        v = C.c_double()
+        self._check(self.lib.sirius_cuda_measure_fma_peak(self.h, precision, C.byref(v)))
+        return v.value
