@@ -1,0 +1,362 @@
+"""Benchmark: Mrays/s of the geodesic engine on the Kerr a = 0.9, 1024^2 workload.
+
+Workload (one "step" = one full frame traced):
+  Kerr a = 0.9, M = 1, 1024 x 1024 pinhole camera at r_obs = 100 M, FOV 30 deg,
+  inclination drawn from U[10, 89] deg with a recorded seed; mixed precision
+  (FP32 dual-number RHS, FP64 state, FP64 constraint re-projection every step,
+  FP64 RHS + error control inside 1.5 r_ph(retrograde) and 2 r_+); DP45 at
+  rtol = atol = 1e-8, h in [1e-9, 2], escape at R > 200 M (RenderSession's),
+  horizon at r < 1.01 r_+; Novikov-Thorne disk r_in = r_ISCO, r_out = 30 M plus
+  volumetric transfer over 16 log-spaced frequency bins.
+The reference arm (--impl reference) runs the reference's own CPU tracer
+(oracle/_ref, GeodesicTracer) on a bounded pixel sample of the same frame with
+all host threads.
+
+Usage: python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference]
+Under torchrun each rank renders its own frame (weak scaling, no data collective).
+"""
+import argparse
+import ctypes as C
+import json
+import math
+import os
+import subprocess
+import sys
+import threading
+import time
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, ROOT)
+
+WIDTH = HEIGHT = 1024
+SEED = 0
+N_BINS = 16
+MEASURED_PEAKS = os.path.join(ROOT, "MEASURED_PEAKS.json")
+
+
+def inclination_deg(seed=SEED):
+    import numpy as np
+    return float(np.random.default_rng(seed).uniform(10.0, 89.0))
+
+
+def workload_config(abi, precision):
+    return abi.default_config(abs_tolerance=1e-8, rel_tolerance=1e-8, min_step=1e-9, max_step=2.0, initial_step=0.1,
+                              escape_radius=200.0, horizon_factor=1.01, max_steps=10000, precision=precision,
+                              enable_volumetric=1, n_bins=N_BINS, nu_min=1e-2, nu_max=1e2, vol_spectral_index=0.7,
+                              vol_substeps=4, projection_period=1, island_factor=1.5)
+
+
+def workload_frame(abi, width=WIDTH, height=HEIGHT):
+    cam = abi.make_camera(r=100.0, theta_deg=inclination_deg(), fov=30.0, width=width, height=height)
+    return abi.make_frame(abi.make_metric(M=1.0, a=0.9), cam, 0.0, 30.0)
+
+
+def workload_desc():
+    return {"workload": "kerr_a0.9_1024x1024_mixed_dp45_nt_disk_vol16", "metric_family": "kerr_schild",
+            "spin": 0.9, "resolution": [WIDTH, HEIGHT], "r_obs": 100.0, "inclination_deg": round(inclination_deg(), 4),
+            "seed": SEED, "fov_deg": 30.0, "tolerance": 1e-8, "escape_radius": 200.0, "horizon_factor": 1.01,
+            "disk": [None, 30.0], "volumetric_bins": N_BINS, "precision": "fp32 rhs + fp64 state/projection/island",
+            "l2": "inputs are 168-byte frame descriptors; the 24 MiB L2 working set is flushed by a 256 MiB write "
+                  "between timed steps"}
+
+
+# --------------------------------------------------------------- clocks ----
+class ClockSampler:
+    """nvidia-smi samples during the timed region (SM clock, throttle reasons)."""
+    FIELDS = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+              "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+              "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, device):
+        self.device = device
+        self.proc = None
+        self.lines = []
+
+    def start(self):
+        try:
+            self.proc = subprocess.Popen(["nvidia-smi", "-i", str(self.device), f"--query-gpu={self.FIELDS}",
+                                          "--format=csv,noheader,nounits", "-lms", "200"],
+                                         stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
+            self.thread = threading.Thread(target=self._read, daemon=True)
+            self.thread.start()
+        except OSError:
+            self.proc = None
+
+    def _read(self):
+        for line in self.proc.stdout:
+            self.lines.append(line.strip())
+
+    def stop(self):
+        if self.proc is None:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["nvidia-smi unavailable"]}
+        self.proc.terminate()
+        try:
+            self.proc.wait(timeout=5)
+        except subprocess.TimeoutExpired:
+            self.proc.kill()
+        sm, mx, reasons = [], None, set()
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        for ln in self.lines:
+            parts = [p.strip() for p in ln.split(",")]
+            if len(parts) < 9:
+                continue
+            try:
+                sm.append(float(parts[1]))
+                mx = float(parts[2])
+            except ValueError:
+                continue
+            for n, v in zip(names, parts[5:9]):
+                if v.lower() == "active":
+                    reasons.add(n)
+        sm.sort()
+        return {"sm_mhz": sm[len(sm) // 2] if sm else None, "sm_max_mhz": mx, "reasons": sorted(reasons),
+                "samples": len(sm)}
+
+
+# -------------------------------------------------------------- reference --
+def run_reference(args):
+    """The reference's own CPU tracer on a bounded strided pixel sample of the frame."""
+    rank = int(os.environ.get("RANK", "0"))
+    if rank != 0:
+        return
+    from oracle.pyoracle import Oracle, Reference, ref_available, ref_config_from
+    from sirius_b200 import abi
+    cfg = workload_config(abi, abi.PRECISION_FP64)
+    fr = workload_frame(abi)
+    threads = os.cpu_count() or 1
+    kind = "reference" if ref_available() else "port"
+    if kind == "reference":
+        ref = Reference()
+        # the reference's TracerConfig: thin disk (it cannot run its volumetric march together with the disk)
+        rcfg = ref_config_from(cfg, float(Oracle().isco(0.9)), 30.0)
+        rcfg.enable_volumetric = 0
+
+    # calibrate a sample that takes ~4 s per step
+    npix = WIDTH * HEIGHT
+
+    def run_sample(n):
+        stride = max(npix // n, 1)
+        t0 = time.perf_counter()
+        if kind == "reference":
+            # rows sampled with a stride; each call traces a contiguous block of one row
+            rows = max(n // WIDTH, 1)
+            row_stride = max(HEIGHT // rows, 1)
+            for r in range(rows):
+                ref.trace_frame(1.0, 0.9, rcfg, fr.camera, (r * row_stride) * WIDTH, WIDTH, threads=threads,
+                                keep=False)
+            n_done = rows * WIDTH
+        else:
+            orc = Oracle()
+            rows = max(n // WIDTH, 1)
+            row_stride = max(HEIGHT // rows, 1)
+            for r in range(rows):
+                orc.trace_frame(fr, cfg, (r * row_stride) * WIDTH, WIDTH, threads=threads)
+            n_done = rows * WIDTH
+        return time.perf_counter() - t0, n_done
+
+    dt, n = run_sample(WIDTH)
+    rate = n / dt
+    n_step = int(min(max(rate * 4.0, WIDTH), npix))
+    times, counts = [], []
+    for i in range(args.warmup + args.steps):
+        dt, n = run_sample(n_step)
+        if i >= args.warmup:
+            times.append(dt)
+            counts.append(n)
+    value = sum(counts) / sum(times) / 1e6
+    sample = (f"{counts[0]} pixels per step ({counts[0] // WIDTH} full rows evenly spaced over the 1024^2 frame), "
+              f"RenderSession-style atomic pixel queue, {threads} threads, the reference's TracerConfig with the "
+              f"workload's tolerances (thin disk; its gray volumetric march replaces the disk, so it is off)")
+    line = {"metric": "Mrays/s", "value": value, "unit": "Mrays/s", "impl": "reference", "n_gpus": args.gpus,
+            "steps": args.steps, "warmup": args.warmup, "ms_per_step": 1e3 * sum(times) / len(times),
+            "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f64",
+            "data": "synthetic (seeded camera frame)", "config": workload_desc(),
+            "cpu_baseline": {"value": value, "unit": "Mrays/s", "cores": threads, "kind": kind, "sample": sample},
+            "e2e": {"value": value, "unit": "Mrays/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
+    print(json.dumps(line), flush=True)
+
+
+# -------------------------------------------------------------------- ours --
+def cpu_baseline_sample(seconds=12.0):
+    """The reference tracer (or the oracle port) on the box's host cores, rank 0 at N = 1."""
+    from oracle.pyoracle import Oracle, Reference, ref_available, ref_config_from
+    from sirius_b200 import abi
+    cfg = workload_config(abi, abi.PRECISION_FP64)
+    fr = workload_frame(abi)
+    threads = os.cpu_count() or 1
+    if ref_available():
+        ref = Reference()
+        rcfg = ref_config_from(cfg, float(Oracle().isco(0.9)), 30.0)
+        rcfg.enable_volumetric = 0
+        kind = "reference"
+
+        def row(r):
+            ref.trace_frame(1.0, 0.9, rcfg, fr.camera, r * WIDTH, WIDTH, threads=threads, keep=False)
+    else:
+        orc = Oracle()
+        kind = "port"
+
+        def row(r):
+            orc.trace_frame(fr, cfg, r * WIDTH, WIDTH, threads=threads)
+    t0 = time.perf_counter()
+    rows = 0
+    order = [(i * 97) % HEIGHT for i in range(HEIGHT)]  # rows spread over the frame
+    while time.perf_counter() - t0 < seconds and rows < HEIGHT:
+        row(order[rows])
+        rows += 1
+    dt = time.perf_counter() - t0
+    return {"value": rows * WIDTH / dt / 1e6, "unit": "Mrays/s", "cores": threads, "kind": kind,
+            "sample": f"{rows} full rows ({rows * WIDTH} rays) of the 1024^2 frame spread over its height, "
+                      f"{dt:.1f} s, RenderSession-style pixel queue over {threads} threads; thin disk only "
+                      f"(the reference's gray volumetric march replaces its disk)"}
+
+
+def main():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=10)
+    ap.add_argument("--warmup", type=int, default=3)
+    ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
+    ap.add_argument("--no-extras", action="store_true", help="skip the FP64 comparator and the CPU baseline")
+    args = ap.parse_args()
+    if args.impl == "reference":
+        run_reference(args)
+        return
+
+    import numpy as np
+    import torch
+    import torch.distributed as dist
+
+    from sirius_b200 import abi
+    from sirius_b200.engine import Engine, flop_count
+
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    torch.cuda.set_device(local)
+    if world > 1:
+        import datetime
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=120))
+    dev = torch.device("cuda", local)
+    stream = torch.cuda.current_stream(dev)
+
+    eng = Engine(local, config=workload_config(abi, abi.PRECISION_MIXED))
+    frame = workload_frame(abi)
+    frames = (abi.Frame * 1)(frame)
+    frames[0].ray_offset = 0
+    total = WIDTH * HEIGHT
+    fbytes = bytes(frames)
+    d_frames = torch.frombuffer(bytearray(fbytes), dtype=torch.uint8).to(dev)
+    d_image = torch.empty(total, dtype=torch.float32, device=dev)
+    d_spectra = torch.empty(total * N_BINS, dtype=torch.float32, device=dev)
+    flush = torch.empty(256 * 1024 * 1024 // 4, dtype=torch.float32, device=dev)
+
+    def step():
+        eng.trace_frames_device(d_frames.data_ptr(), 1, total, None, d_image.data_ptr(), d_spectra.data_ptr(),
+                                stream.cuda_stream)
+
+    for _ in range(max(args.warmup, 3)):
+        step()
+    torch.cuda.synchronize()
+    if world > 1:
+        dist.barrier()
+    torch.cuda.synchronize()
+    clocks = ClockSampler(local)
+    clocks.start()
+    ev = [(torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)) for _ in range(args.steps)]
+    kernel_ms, accepted, rejected, fp64 = [], 0, 0, 0
+    for i in range(args.steps):
+        flush.zero_()
+        ev[i][0].record(stream)
+        step()
+        ev[i][1].record(stream)
+        st = eng.stats()  # synchronises on the library's stream: per-launch kernel time (CUDA events)
+        kernel_ms.append(st.kernel_ms)
+        accepted += st.accepted_steps
+        rejected += st.rejected_steps
+        fp64 += st.fp64_steps
+    torch.cuda.synchronize()
+    if world > 1:
+        dist.barrier()
+    torch.cuda.synchronize()
+    clk = clocks.stop()
+    step_ms = [a.elapsed_time(b) for a, b in ev]
+    t_ms = torch.tensor([sum(step_ms)], dtype=torch.float64, device=dev)
+    if world > 1:
+        dist.all_reduce(t_ms, op=dist.ReduceOp.MAX)
+    t_total = float(t_ms.item())
+    value = world * total * args.steps / (t_total * 1e-3) / 1e6
+
+    # end to end through the host entry point: frame descriptor H2D, image + spectra D2H (pinned)
+    h_img = torch.empty(total, dtype=torch.float32, pin_memory=True)
+    h_spc = torch.empty(total * N_BINS, dtype=torch.float32, pin_memory=True)
+    fr_arr = (abi.Frame * 1)(frame)
+    for _ in range(2):
+        eng.trace_frames_into(C.addressof(fr_arr), 1, None, h_img.data_ptr(), h_spc.data_ptr())
+    if world > 1:
+        dist.barrier()
+    t0 = time.perf_counter()
+    for _ in range(args.steps):
+        eng.trace_frames_into(C.addressof(fr_arr), 1, None, h_img.data_ptr(), h_spc.data_ptr())
+    t_e2e = torch.tensor([time.perf_counter() - t0], dtype=torch.float64, device=dev)
+    if world > 1:
+        dist.all_reduce(t_e2e, op=dist.ReduceOp.MAX)
+    e2e = world * total * args.steps / float(t_e2e.item()) / 1e6
+
+    # roofline of the trace kernel: algorithmic operations / kernel time vs the measured FP32 SIMT peak
+    rhs_f, att_f, acc_f = flop_count(frame.metric)
+    flops = accepted * acc_f + rejected * att_f
+    kernel_s = sum(kernel_ms) * 1e-3
+    achieved = flops / kernel_s / 1e12
+    peak32 = eng.fma_peak(1) / 1e12
+    peak64 = eng.fma_peak(0) / 1e12
+
+    line = {"metric": "Mrays/s", "value": value, "unit": "Mrays/s", "n_gpus": world, "steps": args.steps,
+            "warmup": args.warmup, "ms_per_step": t_total / args.steps, "higher_is_better": True, "scaling": "weak",
+            "vs_baseline": None, "dtype": "f32+f64",
+            "data": "synthetic (seeded camera frame; no dataset)", "config": workload_desc(),
+            "e2e": {"value": e2e, "unit": "Mrays/s", "h2d_bytes_per_step": C.sizeof(abi.Frame),
+                    "d2h_bytes_per_step": total * 4 * (1 + N_BINS)},
+            "gpu_launches": args.steps,
+            "roofline": {"bound": "fp32_simt", "achieved": achieved, "peak": peak32, "unit": "TFLOP/s",
+                         "frac": achieved / peak32, "traffic": None,
+                         "peak_source": "measured FMA-chain microbenchmark (sirius_cuda_measure_fma_peak)",
+                         "fp64_peak": peak64, "flops_per_accepted_step": acc_f, "flops_per_rhs": rhs_f,
+                         "kernel": "trace_kernel<mixed>"},
+            "steps_per_ray": accepted / (total * args.steps), "rejected_per_ray": rejected / (total * args.steps),
+            "fp64_island_step_fraction": fp64 / max(accepted, 1), "clocks": clk}
+
+    if rank == 0 and world == 1 and not args.no_extras:
+        # the plain FP64 GPU integrator on the same frame (one thread per ray), and the error vs it
+        img_mixed = d_image.cpu().numpy().astype(np.float64)
+        spc_mixed = d_spectra.cpu().numpy().reshape(total, N_BINS).astype(np.float64)
+        eng.configure(workload_config(abi, abi.PRECISION_FP64))
+        cfg64 = workload_config(abi, abi.PRECISION_FP64)
+        cfg64.blocks_per_sm = -1
+        eng.configure(cfg64)
+        ms64 = []
+        for i in range(3):
+            step()
+            st = eng.stats()
+            if i > 0:
+                ms64.append(st.kernel_ms)
+        img64 = d_image.cpu().numpy().astype(np.float64)
+        spc64 = d_spectra.cpu().numpy().reshape(total, N_BINS).astype(np.float64)
+        err = np.abs(img_mixed - img64) / img64.max()
+        serr = np.abs(spc_mixed - spc64) / spc64.max(axis=0, keepdims=True)
+        line["fp64_plain"] = {"kernel_ms": float(np.mean(ms64)),
+                              "mrays_per_s": total / (np.mean(ms64) * 1e-3) / 1e6,
+                              "speedup_of_mixed": float(np.mean(ms64)) / (sum(kernel_ms) / len(kernel_ms))}
+        line["error_vs_fp64"] = {"image_linf_rel": float(err.max()), "image_p99_rel": float(np.percentile(err, 99)),
+                                 "spectra_linf_rel": float(serr.max()),
+                                 "spectra_p99_rel": float(np.percentile(serr, 99))}
+        line["cpu_baseline"] = cpu_baseline_sample()
+    if rank == 0:
+        print(json.dumps(line), flush=True)
+    eng.close()
+    if world > 1:
+        dist.destroy_process_group()
+
+
+if __name__ == "__main__":
+    main()

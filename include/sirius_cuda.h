@@ -290,6 +290,13 @@ int sirius_cuda_autotune(sirius_cuda_handle handle, const sirius_frame* frames, 
  * (one FMA = 2 FLOP); precision 0 = FP64, 1 = FP32. ------------------------- */
 int sirius_cuda_measure_fma_peak(sirius_cuda_handle handle, int32_t precision, double* flops_per_s);
 
+/* ---- algorithmic operation count (host only, no device needed): one
+ * right-hand-side evaluation of the metric family as the kernels compute it,
+ * one DP45 attempt (6 evaluations + stage algebra) and one accepted step
+ * (attempt + FP64 re-projection). The roofline numerator of the benchmark. */
+int sirius_cuda_flop_count(const sirius_metric* metric, double* rhs_flops, double* attempt_flops,
+                           double* accepted_step_flops);
+
 #ifdef __cplusplus
 }
 #endif

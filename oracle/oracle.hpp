@@ -688,11 +688,12 @@ bool kepler_ut(const sirius_metric& m, const R pos[4], R r_bl, R& ut, R& Omega) 
 // GTRC001A.cpp:82-106); the isometry (t, phi) -> (-t, -phi) maps it onto the
 // physical photon that reaches the azimuth-mirrored camera, and leaves p.u
 // unchanged, so this g is the physical redshift of that (left-right mirrored) image.
+// E = -p_t and L_z = x p_y - y p_x are the ray's conserved quantities (taken
+// from one consistent state), pos the emitter position.
 template <class R>
-R redshift_exact(const TraceContext& ctx, const R pos[4], R r_bl, const R p[4], R sqrt_m_gtt_cam) {
+R redshift_exact(const TraceContext& ctx, const R pos[4], R r_bl, R E, R Lz, R sqrt_m_gtt_cam) {
     R ut, Om;
     if (!kepler_ut(ctx.metric, pos, r_bl, ut, Om)) return R(0);
-    const R E = -p[0], Lz = pos[1] * p[2] - pos[2] * p[1];
     const R den = sqrt_m_gtt_cam * ut * (R(1) - Om * Lz / E);
     return den > R(0) ? R(1) / den : R(0);
 }
@@ -798,29 +799,48 @@ void hermite_point(const R x0[4], const R x1[4], const R k0[4], const R k1[4], R
     for (int i = 0; i < 4; ++i) out[i] = h00 * x0[i] + h10 * h * k0[i] + h01 * x1[i] + h11 * h * k1[i];
 }
 
+// Event location of the equatorial crossing inside an accepted step: DP45
+// sub-steps from the step's start state (x0, p0, f(x0, p0)), the sub-step
+// length corrected by Newton on z(l) (dz/dl = k^z), seeded by the cubic
+// Hermite root; two sub-steps and a final first-order correction put z at
+// rounding level, independent of the step sequence that bracketed it.
+template <class R>
+void locate_equator(const sirius_metric& m, const sirius_trace_config& c, const R x0[4], const R p0[4],
+                    const R kx0[4], const R kp0[4], R hs, R xc[4]) {
+    R xn[4], pn[4], k7x[4], k7p[4];
+    for (int it = 0; it < 2; ++it) {
+        dp45_attempt(m, c, x0, p0, hs, kx0, kp0, xn, pn, k7x, k7p, false);
+        if (it == 0) hs -= xn[3] / k7x[3];
+    }
+    const R dl = -xn[3] / k7x[3];
+    for (int i = 0; i < 4; ++i) xc[i] = xn[i] + dl * k7x[i];
+    xc[3] = R(0);
+}
+
 // Volumetric emission of the engine (the BASELINE profile): over one step segment
-// x0 -> x1 of affine length h, n_sub midpoint samples on the straight segment
-// (as GTRC001A.cpp:943-958 marches it), camera-first accumulation per bin:
+// x0 -> x1 of affine length h, n_sub midpoint samples on the step's cubic
+// Hermite interpolant (the reference marches the chord, GTRC001A.cpp:943-958),
+// camera-first accumulation per bin:
 //   I_b += T_b S (1 - e^{-dtau}),  T_b *= e^{-dtau},
 //   j = j0 r^-2 exp(-z^2 / (2 (h_z r)^2)) nu_em^-s,  alpha = c_a j,
 //   dtau = alpha (nu_cam / g) dl,  S = g^3 / c_a   (I_b stored as nu_b^3 I_inv).
 template <class R>
-void volumetric_segment(const TraceContext& ctx, const R x0[4], const R x1[4], const R p[4], R h, R sqrt_m_gtt_cam,
-                        const R* nu, Spectra& sp) {
+void volumetric_segment(const TraceContext& ctx, const R x0[4], const R x1[4], const R k0[4], const R k1[4],
+                        const R p[4], R h, R sqrt_m_gtt_cam, const R* nu, Spectra& sp) {
     const auto& c = ctx.cfg;
     const int ns = std::max(1, c.vol_substeps);
-    const R E = -p[0];
+    const R E = -p[0], Lz = x1[1] * p[2] - x1[2] * p[1];  // p is the state at x1
     const R nu_cam = E / sqrt_m_gtt_cam;
     for (int s = 0; s < ns; ++s) {
         const R f = (R(s) + R(0.5)) / R(ns);
         R xs[4], d[4];
-        for (int i = 0; i < 4; ++i) xs[i] = x0[i] + f * (x1[i] - x0[i]);
+        hermite_point(x0, x1, k0, k1, h, f, xs);  // the step's cubic Hermite interpolant
         const R r = radial(ctx.metric, xs, d);
         if (r < R(ctx.disk_inner) || r > R(ctx.disk_outer)) continue;
         const R zr = xs[3] / (R(c.vol_height_ratio) * r);
         if (std::abs(zr) > R(4)) continue;
         const R jsp = R(c.vol_j0) / (r * r) * std::exp(R(-0.5) * zr * zr);
-        const R g = redshift_exact(ctx, xs, r, p, sqrt_m_gtt_cam);
+        const R g = redshift_exact(ctx, xs, r, E, Lz, sqrt_m_gtt_cam);
         if (!(g > R(0))) continue;
         const R dl = h / R(ns);
         const R S = g * g * g / R(c.vol_alpha_over_j);
@@ -985,8 +1005,8 @@ void trace_ray(const TraceContext& ctx, const double origin[4], const double dir
             continue;
         }
         // accepted
-        R x0[4], k0v[4];
-        for (int i = 0; i < 4; ++i) { x0[i] = x[i]; k0v[i] = compat ? k[i] : k1x[i]; }
+        R x0[4], k0v[4], p0[4], k0p[4];
+        for (int i = 0; i < 4; ++i) { x0[i] = x[i]; k0v[i] = compat ? k[i] : k1x[i]; p0[i] = p[i]; k0p[i] = k1p[i]; }
         const R hstep = h;
         h = optimal_step(h, err, c, compat);
         ++steps;
@@ -1129,7 +1149,7 @@ void trace_ray(const TraceContext& ctx, const double origin[4], const double dir
                 }
                 continue;
             }
-            volumetric_segment(ctx, x0, x, p, hstep, sqrt_m_gtt_cam, nu, sp);
+            volumetric_segment(ctx, x0, x, k0v, k, p, hstep, sqrt_m_gtt_cam, nu, sp);
         }
 
         // thin disk crossing (GTRC001A.h:404-431, GTRC001A.cpp:468-555)
@@ -1144,8 +1164,7 @@ void trace_ray(const TraceContext& ctx, const double origin[4], const double dir
             xc[1] = R(xcx); xc[2] = R(ycx);
         } else {
             const R s = hermite_z_root(x0[3], x[3], k0v[3], k[3], hstep);
-            hermite_point(x0, x, k0v, k, hstep, s, xc);
-            xc[3] = 0;
+            locate_equator(m, c, x0, p0, k0v, k0p, s * hstep, xc);
             rc = double(radial(m, xc, d));
             phc = std::atan2(double(xc[2]), double(xc[1]));
         }
@@ -1160,11 +1179,11 @@ void trace_ray(const TraceContext& ctx, const double origin[4], const double dir
                 const double vel[4] = {double(k[0]), double(k[1]), double(k[2]), double(k[3])};
                 res.disk_g[n] = float(redshift_compat(m, float(rc), float(phc), vel));
             } else {
-                res.disk_g[n] = float(redshift_exact(ctx, xc, R(rc), p, sqrt_m_gtt_cam));
+                res.disk_g[n] = float(redshift_exact(ctx, xc, R(rc), -p[0], x[1] * p[2] - x[2] * p[1], sqrt_m_gtt_cam));
             }
             const double F = nt_flux(rc, m.M != 0 ? m.a / m.M : 0.0, ctx.disk_inner, ctx.disk_outer);
             res.disk_flux[n] = float(F);
-            const double gg = compat ? double(res.disk_g[n]) : double(redshift_exact(ctx, xc, R(rc), p, sqrt_m_gtt_cam));
+            const double gg = compat ? double(res.disk_g[n]) : double(redshift_exact(ctx, xc, R(rc), -p[0], x[1] * p[2] - x[2] * p[1], sqrt_m_gtt_cam));
             intensity += std::exp(-c.crossing_weight_decay * n) * gg * gg * gg * gg * F;
             if (n == 0) res.outcome = SIRIUS_DISK_HIT;
             res.n_crossings = n + 1;

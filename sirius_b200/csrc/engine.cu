@@ -187,12 +187,13 @@ __device__ void end_ray(const Params& P, Ray& s, int outcome, float magnificatio
 }
 
 // Volumetric transfer over the accepted segment x0 -> x1 (affine length h):
-// midpoint samples on the straight segment (GTRC001A.cpp:943-958), camera-first
+// midpoint samples on the step's cubic Hermite interpolant (the reference
+// marches the chord, GTRC001A.cpp:943-958), camera-first
 // accumulation per bin: I_b += T_b S (1 - e^-dtau), T_b = e^-tau_b,
 //   j = j0 r^-2 exp(-z^2/(2 (h_z r)^2)) nu_em^-s, alpha = c_a j,
 //   dtau = alpha (nu_cam/g) dl, S = g^3 / c_a.  (vol: [2b] = I_b, [2b+1] = tau_b, stride blockDim)
 __device__ void volumetric_segment(const Params& P, const FrameDev& F, const double x0[4], const double x1[4],
-                                   const double p[4], double h, float* vol) {
+                                   const double k0[4], const double k1[4], const double p[4], double h, float* vol) {
     const CfgDev& c = P.c;
     const int ns = c.vol_sub > 0 ? c.vol_sub : 1;
     const float E = float(-p[0]);
@@ -200,10 +201,13 @@ __device__ void volumetric_segment(const Params& P, const FrameDev& F, const dou
     const float nu_cam = E / float(F.sqrt_m_gtt_cam);
     const float dl = float(h) / float(ns);
     for (int s = 0; s < ns; ++s) {
-        const double f = (s + 0.5) / ns;
-        const float xs = float(x0[1] + f * (x1[1] - x0[1]));
-        const float ys = float(x0[2] + f * (x1[2] - x0[2]));
-        const float zs = float(x0[3] + f * (x1[3] - x0[3]));
+        // sample on the step's cubic Hermite interpolant
+        const double q = (s + 0.5) / ns, q2 = q * q, q3 = q2 * q;
+        const double h00 = 2.0 * q3 - 3.0 * q2 + 1.0, h10 = (q3 - 2.0 * q2 + q) * h, h01 = -2.0 * q3 + 3.0 * q2,
+                     h11 = (q3 - q2) * h;
+        const float xs = float(h00 * x0[1] + h10 * k0[1] + h01 * x1[1] + h11 * k1[1]);
+        const float ys = float(h00 * x0[2] + h10 * k0[2] + h01 * x1[2] + h11 * k1[2]);
+        const float zs = float(h00 * x0[3] + h10 * k0[3] + h01 * x1[3] + h11 * k1[3]);
         KSPieces<float> KP;
         ks_pieces(F.m, xs, ys, zs, KP);
         const float r = KP.r;
@@ -256,7 +260,17 @@ __device__ int advance(const Params& P, Ray& s, float& magnification, int& flags
 #pragma unroll
     for (int i = 0; i < 4; ++i) { x0[i] = s.x[i]; k0[i] = s.kx[i]; }
     const double hstep = s.h;
-    s.h = optimal_step(s.h, err, c);
+    // equatorial crossing inside the step: locate it from the step's start
+    // state before that state is replaced
+    const bool disk_on = m.family == SIRIUS_METRIC_KERR_SCHILD && c.enable_disk && F.has_horizon;
+    double xc1 = 0.0, xc2 = 0.0;
+    const bool cross = disk_on && (s.x[3] * xn[3] < 0.0);
+    if (cross) {
+        const double hs = hermite_root(s.x[3], xn[3], s.kx[3], k7x[3], hstep) * hstep;
+        if (island) locate_equator<double>(m, c, s.x, s.p, s.kx, s.kp, hs, xc1, xc2);
+        else locate_equator<float>(m, c, s.x, s.p, s.kx, s.kp, hs, xc1, xc2);
+    }
+    s.h = MIXED ? optimal_step_fast(s.h, err, c) : optimal_step(s.h, err, c);
     ++s.steps;
     if (island && MIXED) ++s.fp64_steps;
     bool bad = false;
@@ -320,25 +334,18 @@ __device__ int advance(const Params& P, Ray& s, float& magnification, int& flags
     if (m.family != SIRIUS_METRIC_KERR_SCHILD || !c.enable_disk || !F.has_horizon) {
         return s.steps >= c.max_steps ? (s.ncross > 0 ? SIRIUS_DISK_HIT : SIRIUS_MAX_STEPS) : -1;
     }
-    if (c.enable_vol && vol) volumetric_segment(P, F, x0, s.x, s.p, hstep, vol);
+    if (c.enable_vol && vol) volumetric_segment(P, F, x0, s.x, k0, s.kx, s.p, hstep, vol);
 
-    // thin-disk crossing (GTRC001A.h:404-431, GTRC001A.cpp:468-555): cubic
-    // Hermite location of z = 0 inside the step, BL radius, exact redshift
-    if (x0[3] * s.x[3] < 0.0) {
-        const double sc = hermite_root(x0[3], s.x[3], k0[3], s.kx[3], hstep);
-        const double q2 = sc * sc, q3 = q2 * sc;
-        const double h00 = 2.0 * q3 - 3.0 * q2 + 1.0, h10 = q3 - 2.0 * q2 + sc, h01 = -2.0 * q3 + 3.0 * q2,
-                     h11 = q3 - q2;
-        double xc[4];
-#pragma unroll
-        for (int i = 0; i < 4; ++i) xc[i] = h00 * x0[i] + h10 * hstep * k0[i] + h01 * s.x[i] + h11 * hstep * s.kx[i];
-        xc[3] = 0.0;
+    // thin-disk crossing (GTRC001A.h:404-431, GTRC001A.cpp:468-555): event-located
+    // z = 0 point, its BL radius, the exact redshift with the ray's conserved E, L_z
+    if (cross) {
+        const double xc[4] = {0.0, xc1, xc2, 0.0};
         InvForm CF;
         inv_form(m, xc, CF);
         const double rc = CF.r;
         if (rc >= F.disk_in && rc <= F.disk_out && s.ncross < SIRIUS_MAX_CROSSINGS) {
             const int n = s.ncross;
-            const double E = -s.p[0], Lz = xc[1] * s.p[2] - xc[2] * s.p[1];
+            const double E = -s.p[0], Lz = s.x[1] * s.p[2] - s.x[2] * s.p[1];
             const double g = kepler_g<double>(m, xc[1], xc[2], 0.0, rc, E, Lz, F.sqrt_m_gtt_cam);
             const double Fl = nt_flux(rc, F.a_star, F.isco, F.disk_in, F.disk_out);
             s.intensity += exp(-c.decay * n) * g * g * g * g * Fl;
@@ -363,8 +370,8 @@ __device__ int advance(const Params& P, Ray& s, float& magnification, int& flags
 }
 
 // Persistent tracer. Dynamic shared memory: 2 * nbins floats per thread (volumetric bins).
-template <bool MIXED>
-__global__ void __launch_bounds__(128) trace_kernel(Params P) {
+template <bool MIXED, int MINB>
+__global__ void __launch_bounds__(128, MINB) trace_kernel(Params P) {
     extern __shared__ float smem[];
     float* vol = (P.c.enable_vol && P.c.nbins > 0) ? smem + threadIdx.x : nullptr;
     const int lane = threadIdx.x & 31;
@@ -440,6 +447,26 @@ __global__ void __launch_bounds__(128) trace_kernel(Params P) {
         atomicAdd(&P.counters[0], acc);
         atomicAdd(&P.counters[1], rej0);
         atomicAdd(&P.counters[2], f64);
+    }
+}
+
+using TraceFn = void (*)(Params);
+constexpr int kDefaultMinBlocks = 2;
+
+TraceFn pick_kernel(bool mixed, int minb) {
+    if (mixed) {
+        switch (minb) {
+            case 1: return trace_kernel<true, 1>;
+            case 3: return trace_kernel<true, 3>;
+            case 4: return trace_kernel<true, 4>;
+            default: return trace_kernel<true, 2>;
+        }
+    }
+    switch (minb) {
+        case 1: return trace_kernel<false, 1>;
+        case 3: return trace_kernel<false, 3>;
+        case 4: return trace_kernel<false, 4>;
+        default: return trace_kernel<false, 2>;
     }
 }
 
@@ -552,18 +579,7 @@ double isco_host(double a_star) {
                        : 3 + Z2 + std::sqrt((3 - Z1) * (3 + Z1 + 2 * Z2));
 }
 
-MetricDev make_metric(const sirius_metric& s) {
-    MetricDev m{};
-    m.family = s.family;
-    m.shape = s.shape;
-    m.M = s.M; m.a = s.a; m.Q = s.Q; m.Lambda = s.Lambda;
-    m.a2 = s.a * s.a; m.Q2 = s.Q * s.Q; m.lam3 = s.Lambda / 3.0; m.sqrtM = std::sqrt(std::max(s.M, 0.0));
-    m.has_lambda = std::fabs(s.Lambda) > 1e-15;
-    m.b0 = s.b0; m.Phi0 = s.Phi0; m.gtt_mt = -std::exp(2.0 * s.Phi0);
-    m.vs = s.vs; m.sigma = s.sigma; m.Rb = s.R;
-    m.inv_2tanhsR = (s.sigma * s.R != 0.0) ? 1.0 / (2.0 * std::tanh(s.sigma * s.R)) : 0.0;
-    return m;
-}
+MetricDev make_metric(const sirius_metric& s) { return metric_dev(s); }
 
 int validate_metric(Handle* H, const sirius_metric& m) {
     if (m.family < 0 || m.family > 2) return fail(H, SIRIUS_ERR_INVALID_ARGUMENT, "unknown metric family");
@@ -692,15 +708,16 @@ int launch_trace(Handle* H, int n_frames, long long total, sirius_ray_result* d_
     P.refill_threshold = c.refill_threshold > 0 ? c.refill_threshold : 24;
     const int block = 128;  // matches __launch_bounds__
     const size_t shmem = size_t(2) * P.c.nbins * block * sizeof(float);
+    // register budget: blocks_per_sm in 1..4 selects the kernel compiled for that
+    // many resident 128-thread blocks per SM (fewer registers, possibly spills)
+    const int minb = c.blocks_per_sm > 0 ? std::min(c.blocks_per_sm, 4) : kDefaultMinBlocks;
+    const TraceFn fn = pick_kernel(mixed, minb);
     int grid;
     if (P.persistent) {
         int per_sm = c.blocks_per_sm;
         if (per_sm <= 0) {
             int occ = 0;
-            if (mixed)
-                CK(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, trace_kernel<true>, block, shmem));
-            else
-                CK(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, trace_kernel<false>, block, shmem));
+            CK(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, fn, block, shmem));
             per_sm = std::max(occ, 1);
         }
         grid = H->num_sms * per_sm;
@@ -714,8 +731,7 @@ int launch_trace(Handle* H, int n_frames, long long total, sirius_ray_result* d_
     // whole-launch bound on the device clock (each warp measures from its own start)
     P.watchdog_ns = c.watchdog_ms > 0 ? (unsigned long long)c.watchdog_ms * 1000000ull : ~0ull;
     if (timed) CK(cudaEventRecord(H->ev[1], st));
-    if (mixed) trace_kernel<true><<<grid, block, shmem, st>>>(P);
-    else trace_kernel<false><<<grid, block, shmem, st>>>(P);
+    fn<<<grid, block, shmem, st>>>(P);
     CK(cudaGetLastError());
     if (timed) CK(cudaEventRecord(H->ev[2], st));
     H->stats.grid_blocks = grid;

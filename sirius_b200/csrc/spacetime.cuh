@@ -30,8 +30,22 @@ struct MetricDev {
     double vs, sigma, Rb, inv_2tanhsR;  // Alcubierre
 };
 
+// Host: the per-metric constants the device code reads.
+inline MetricDev metric_dev(const sirius_metric& s) {
+    MetricDev m{};
+    m.family = s.family;
+    m.shape = s.shape;
+    m.M = s.M; m.a = s.a; m.Q = s.Q; m.Lambda = s.Lambda;
+    m.a2 = s.a * s.a; m.Q2 = s.Q * s.Q; m.lam3 = s.Lambda / 3.0; m.sqrtM = std::sqrt(s.M > 0.0 ? s.M : 0.0);
+    m.has_lambda = std::fabs(s.Lambda) > 1e-15;
+    m.b0 = s.b0; m.Phi0 = s.Phi0; m.gtt_mt = -std::exp(2.0 * s.Phi0);
+    m.vs = s.vs; m.sigma = s.sigma; m.Rb = s.R;
+    m.inv_2tanhsR = (s.sigma * s.R != 0.0) ? 1.0 / (2.0 * std::tanh(s.sigma * s.R)) : 0.0;
+    return m;
+}
+
 template <class T>
-__device__ __forceinline__ T tmax(T a, T b) { return a > b ? a : b; }
+SIRIUS_HD __forceinline__ T tmax(T a, T b) { return a > b ? a : b; }
 
 // ---------------------------------------------------------------------------
 // Kerr-Schild family (PHMT100A.h:198-396): H and l_i as dual numbers.
@@ -45,7 +59,7 @@ struct KSPieces {
 };
 
 template <class T>
-__device__ __forceinline__ void ks_pieces(const MetricDev& m, T x, T y, T z, KSPieces<T>& o) {
+SIRIUS_HD __forceinline__ void ks_pieces(const MetricDev& m, T x, T y, T z, KSPieces<T>& o) {
     const T a = T(m.a), a2 = T(m.a2);
     const T R2 = x * x + y * y + z * z;
     const T Rm2 = R2 - a2;
@@ -69,7 +83,7 @@ __device__ __forceinline__ void ks_pieces(const MetricDev& m, T x, T y, T z, KSP
 }
 
 template <class T>
-__device__ __forceinline__ void ks_rhs(const MetricDev& m, const T x[4], const T p[4], T k[4], T f[4]) {
+SIRIUS_HD __forceinline__ void ks_rhs(const MetricDev& m, const T x[4], const T p[4], T k[4], T f[4]) {
     KSPieces<T> P;
     ks_pieces(m, x[1], x[2], x[3], P);
     const T H = P.H.v, l1 = P.l1.v, l2 = P.l2.v, l3 = P.l3.v;
@@ -104,7 +118,7 @@ __device__ __forceinline__ void ks_rhs(const MetricDev& m, const T x[4], const T
 // >= 1.001 b0 as the reference does (:293); g diagonal.
 // ---------------------------------------------------------------------------
 template <class T>
-__device__ __forceinline__ D3<T> mt_grr(const MetricDev& m, T r) {
+SIRIUS_HD __forceinline__ D3<T> mt_grr(const MetricDev& m, T r) {
     const T b0 = T(m.b0);
     const D3<T> R = dvar(tmax(r, b0 * T(1.001)), 0);
     D3<T> b;
@@ -117,7 +131,7 @@ __device__ __forceinline__ D3<T> mt_grr(const MetricDev& m, T r) {
 }
 
 template <class T>
-__device__ __forceinline__ void mt_rhs(const MetricDev& m, const T x[4], const T p[4], T k[4], T f[4]) {
+SIRIUS_HD __forceinline__ void mt_rhs(const MetricDev& m, const T x[4], const T p[4], T k[4], T f[4]) {
     const T r = tmax(x[1], T(m.b0) * T(1.001));
     const T s = sin(x[2]), c = cos(x[2]);
     const T s2 = tmax(s * s, T(1e-24));
@@ -138,7 +152,7 @@ __device__ __forceinline__ void mt_rhs(const MetricDev& m, const T x[4], const T
 // g_tt = -(1 - v^2 f^2), g_tx = -v f;  g^{tt} = -1, g^{tx} = -v f, g^{xx} = 1 - v^2 f^2.
 // ---------------------------------------------------------------------------
 template <class T>
-__device__ __forceinline__ D3<T> alc_f(const MetricDev& m, T x, T y, T z) {
+SIRIUS_HD __forceinline__ D3<T> alc_f(const MetricDev& m, T x, T y, T z) {
     const T rs = tmax(sqrt_(x * x + y * y + z * z), T(1e-10));
     const T irs = rcp_(rs);
     const D3<T> R = dwith(rs, x * irs, y * irs, z * irs);
@@ -147,7 +161,7 @@ __device__ __forceinline__ D3<T> alc_f(const MetricDev& m, T x, T y, T z) {
 }
 
 template <class T>
-__device__ __forceinline__ void alc_rhs(const MetricDev& m, const T x[4], const T p[4], T k[4], T f[4]) {
+SIRIUS_HD __forceinline__ void alc_rhs(const MetricDev& m, const T x[4], const T p[4], T k[4], T f[4]) {
     const D3<T> F = alc_f(m, x[1], x[2], x[3]);
     const T v = T(m.vs), vf = v * F.v;
     k[0] = -p[0] - vf * p[1];
@@ -163,7 +177,7 @@ __device__ __forceinline__ void alc_rhs(const MetricDev& m, const T x[4], const 
 }
 
 template <class T>
-__device__ __forceinline__ void rhs(const MetricDev& m, const T x[4], const T p[4], T k[4], T f[4]) {
+SIRIUS_HD __forceinline__ void rhs(const MetricDev& m, const T x[4], const T p[4], T k[4], T f[4]) {
     if (m.family == SIRIUS_METRIC_KERR_SCHILD) ks_rhs(m, x, p, k, f);
     else if (m.family == SIRIUS_METRIC_MORRIS_THORNE) mt_rhs(m, x, p, k, f);
     else alc_rhs(m, x, p, k, f);

@@ -247,16 +247,38 @@ __device__ __forceinline__ double dp45_attempt(const MetricDev& m, const CfgDev&
     }
     T q7x[4], q7p[4];
     rhs(m, xs, ps, q7x, q7p);
-    double en = 0.0;
+    T en = T(0);
 #pragma unroll
     for (int i = 0; i < 4; ++i) {
         k7x[i] = double(q7x[i]);
         k7p[i] = double(q7p[i]);
         const T ex = e1 * k1x[i] + e3 * k3x[i] + e4 * k4x[i] + e5 * k5x[i] + e6 * k6x[i] + e7 * q7x[i];
-        const double e = h * double(ex) / (c.atol + c.rtol * fabs(xn[i]));
-        en += e * e;
+        if constexpr (sizeof(T) == sizeof(double)) {
+            const double e = h * double(ex) / (c.atol + c.rtol * fabs(xn[i]));
+            en += e * e;
+        } else {  // the estimate needs a few digits only
+            const float e = ht * ex * rcp_(float(c.atol) + float(c.rtol) * fabsf(xs[i]));
+            en += e * e;
+        }
     }
-    return sqrt(0.25 * en);
+    return double(sqrt_(T(0.25) * en));
+}
+
+// Event location of the equatorial crossing inside an accepted step: DP45
+// sub-steps from the step's start state (x0, p0, f(x0, p0)), the sub-step
+// length corrected by Newton on z(l) (dz/dl = k^z), seeded by the cubic
+// Hermite root; two sub-steps and a final first-order correction.
+template <class T>
+__device__ __noinline__ void locate_equator(const MetricDev& m, const CfgDev& c, const double x0[4],
+                                            const double p0[4], const double kx0[4], const double kp0[4], double hs,
+                                            double& xc1, double& xc2) {
+    double xn[4], pn[4], k7x[4], k7p[4];
+    dp45_attempt<T>(m, c, x0, p0, hs, kx0, kp0, xn, pn, k7x, k7p);
+    hs -= xn[3] / k7x[3];
+    dp45_attempt<T>(m, c, x0, p0, hs, kx0, kp0, xn, pn, k7x, k7p);
+    const double dl = -xn[3] / k7x[3];
+    xc1 = xn[1] + dl * k7x[1];
+    xc2 = xn[2] + dl * k7x[2];
 }
 
 // Geodesic::computeOptimalStep (PHGD001A.cpp:471-483).
@@ -265,6 +287,14 @@ __device__ __forceinline__ double optimal_step(double h, double err, const CfgDe
     double fac = c.safety * pow(1.0 / err, 0.2);
     fac = fmax(c.shrink, fmin(c.grow, fac));
     return fmax(c.hmin, fmin(c.hmax, h * fac));
+}
+
+// Step control in FP32 for the mixed path (the factor needs a few digits only).
+__device__ __forceinline__ double optimal_step_fast(double h, double err, const CfgDev& c) {
+    if (err < 1e-15) return fmin(h * c.grow, c.hmax);
+    float fac = float(c.safety) * exp2f(-0.2f * __log2f(float(err)));
+    fac = fmaxf(float(c.shrink), fminf(float(c.grow), fac));
+    return fmax(c.hmin, fmin(c.hmax, h * double(fac)));
 }
 
 // Cubic Hermite interpolation of z over the accepted step; bisection for z = 0.

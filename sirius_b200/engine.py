@@ -22,6 +22,7 @@ EXPORTS = [
     "sirius_cuda_get_last_error", "sirius_cuda_configure", "sirius_cuda_trace_frames",
     "sirius_cuda_trace_frames_device", "sirius_cuda_trace_rays", "sirius_cuda_metric_evaluate",
     "sirius_cuda_dp45_step", "sirius_cuda_last_stats", "sirius_cuda_autotune", "sirius_cuda_measure_fma_peak",
+    "sirius_cuda_flop_count",
 ]
 
 
@@ -54,7 +55,18 @@ def load_library(path=LIB_PATH):
     L.sirius_cuda_last_stats.argtypes = [C.c_void_p, _P(abi.LaunchStats)]
     L.sirius_cuda_autotune.argtypes = [C.c_void_p, C.c_void_p, C.c_int32, _P(abi.TraceConfig)]
     L.sirius_cuda_measure_fma_peak.argtypes = [C.c_void_p, C.c_int32, _P(C.c_double)]
+    L.sirius_cuda_flop_count.argtypes = [_P(abi.Metric), _P(C.c_double), _P(C.c_double), _P(C.c_double)]
     return L
+
+
+def flop_count(metric, lib=None):
+    """(rhs, attempt, accepted step) algorithmic operation counts of the kernels' formulation."""
+    lib = lib or load_library()
+    a, b, c = C.c_double(), C.c_double(), C.c_double()
+    rc = lib.sirius_cuda_flop_count(C.byref(metric), C.byref(a), C.byref(b), C.byref(c))
+    if rc != abi.OK:
+        raise SiriusError(rc, "sirius_cuda_flop_count failed")
+    return a.value, b.value, c.value
 
 
 def frames_array(frames):
