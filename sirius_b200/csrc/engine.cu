@@ -20,6 +20,7 @@
 #include <cstring>
 #include <new>
 #include <string>
+#include <type_traits>
 #include <vector>
 
 #include "trace.cuh"
@@ -67,9 +68,14 @@ __device__ __forceinline__ int find_frame(const FrameDev* frames, int n, long lo
     return lo;
 }
 
-// Per-ray state held in registers between steps.
+// Per-ray state held in registers between steps. K is the storage type of the
+// first-same-as-last derivative f(x, p): float on the mixed path (the FP64
+// island recomputes it in FP64), double on the all-FP64 path.
+template <bool MIXED>
 struct Ray {
-    double x[4], p[4], kx[4], kp[4];
+    using K = typename std::conditional<MIXED, float, double>::type;
+    double x[4], p[4];
+    K k[8];
     double h;
     double intensity;
     float min_r, null_max, tphi, prev_z;
@@ -85,8 +91,8 @@ __device__ __forceinline__ void write_default_crossings(sirius_ray_result* R) {
     }
 }
 
-__device__ __forceinline__ void invariants(const MetricDev& m, const InvForm& F, const double x[4], const double p[4],
-                                           float& E, float& Lz, float& Q) {
+__device__ void invariants(const MetricDev& m, const InvForm& F, const double x[4], const double p[4], float& E,
+                           float& Lz, float& Q) {
     E = float(-p[0]);
     if (m.family == SIRIUS_METRIC_MORRIS_THORNE) {
         const double s = sin(x[2]), c = cos(x[2]);
@@ -104,7 +110,9 @@ __device__ __forceinline__ void invariants(const MetricDev& m, const InvForm& F,
     Q = float(pth * pth + ct * ct * (-m.a2 * e * e + L * L / (st * st)));
 }
 
-__device__ void begin_ray(const Params& P, Ray& s, long long idx, float* vol) {
+template <bool MIXED>
+__device__ __noinline__ void begin_ray(const Params& P, Ray<MIXED>& s, long long idx, float* vol) {
+    using K = typename Ray<MIXED>::K;
     s.idx = idx;
     s.frame = P.n_frames > 1 ? find_frame(P.frames, P.n_frames, idx) : 0;
     const FrameDev& F = P.frames[s.frame];
@@ -117,7 +125,9 @@ __device__ void begin_ray(const Params& P, Ray& s, long long idx, float* vol) {
         camera_dir(F, int(pix % F.width), int(pix / F.width), dir);
     }
     init_state(F, dir, s.x, s.p);
-    rhs<double>(F.m, s.x, s.p, s.kx, s.kp);
+    K xk[4], pk[4];
+    for (int i = 0; i < 4; ++i) { xk[i] = K(s.x[i]); pk[i] = K(s.p[i]); }
+    rhs<K>(F.m, xk, pk, s.k, s.k + 4);
     s.h = P.c.h0;
     s.intensity = 0.0;
     s.min_r = 1e10f;
@@ -134,13 +144,12 @@ __device__ void begin_ray(const Params& P, Ray& s, long long idx, float* vol) {
         invariants(F.m, IF, s.x, s.p, E, L, Q);
         R->E0 = E; R->Lz0 = L; R->Carter0 = Q;
         // impact parameter heuristic (GTRC001A.cpp:208-233)
-        double k[4];
-        for (int i = 0; i < 4; ++i) k[i] = s.kx[i];
         float b = 0.f;
         if (F.m.family != SIRIUS_METRIC_MORRIS_THORNE) {
+            const double k1 = double(s.k[1]), k2 = double(s.k[2]), k3 = double(s.k[3]);
             const double R0 = sqrt(s.x[1] * s.x[1] + s.x[2] * s.x[2] + s.x[3] * s.x[3]);
-            const double vm = sqrt(k[1] * k[1] + k[2] * k[2] + k[3] * k[3]);
-            const double vrad = (k[1] * s.x[1] + k[2] * s.x[2] + k[3] * s.x[3]) / R0;
+            const double vm = sqrt(k1 * k1 + k2 * k2 + k3 * k3);
+            const double vrad = (k1 * s.x[1] + k2 * s.x[2] + k3 * s.x[3]) / R0;
             b = float(R0 * sqrt(fmax(vm * vm - vrad * vrad, 0.0)) / fmax(vm, 1e-10));
         }
         R->impact_parameter = b;
@@ -149,7 +158,9 @@ __device__ void begin_ray(const Params& P, Ray& s, long long idx, float* vol) {
         for (int b = 0; b < P.c.nbins; ++b) { vol[2 * b * blockDim.x] = 0.f; vol[(2 * b + 1) * blockDim.x] = 0.f; }
 }
 
-__device__ void end_ray(const Params& P, Ray& s, int outcome, float magnification, int flags, float* vol) {
+template <bool MIXED>
+__device__ __noinline__ void end_ray(const Params& P, const Ray<MIXED>& s, int outcome, float magnification, int flags,
+                                     const float* vol) {
     const FrameDev& F = P.frames[s.frame];
     if (P.image) P.image[s.idx] = float(s.intensity);
     if (P.spectra && vol)
@@ -167,7 +178,7 @@ __device__ void end_ray(const Params& P, Ray& s, int outcome, float magnificatio
     for (int i = 0; i < 4; ++i) {
         R->final_x[i] = s.x[i];
         R->final_p[i] = s.p[i];
-        R->final_k[i] = float(s.kx[i]);
+        R->final_k[i] = float(s.k[i]);
     }
     R->equatorial_crossings = s.eq;
     R->image_order = s.eq >= 1 ? (s.eq + 1) / 2 : 0;
@@ -188,12 +199,13 @@ __device__ void end_ray(const Params& P, Ray& s, int outcome, float magnificatio
 
 // Volumetric transfer over the accepted segment x0 -> x1 (affine length h):
 // midpoint samples on the step's cubic Hermite interpolant (the reference
-// marches the chord, GTRC001A.cpp:943-958), camera-first
-// accumulation per bin: I_b += T_b S (1 - e^-dtau), T_b = e^-tau_b,
+// marches the chord, GTRC001A.cpp:943-958), camera-first accumulation per bin:
+// I_b += T_b S (1 - e^-dtau), T_b = e^-tau_b,
 //   j = j0 r^-2 exp(-z^2/(2 (h_z r)^2)) nu_em^-s, alpha = c_a j,
 //   dtau = alpha (nu_cam/g) dl, S = g^3 / c_a.  (vol: [2b] = I_b, [2b+1] = tau_b, stride blockDim)
-__device__ void volumetric_segment(const Params& P, const FrameDev& F, const double x0[4], const double x1[4],
-                                   const double k0[4], const double k1[4], const double p[4], double h, float* vol) {
+__device__ __noinline__ void volumetric_segment(const Params& P, const FrameDev& F, const double x0[4],
+                                                const double x1[4], const float k0[4], const float k1[4],
+                                                const double p[4], double h, float* vol) {
     const CfgDev& c = P.c;
     const int ns = c.vol_sub > 0 ? c.vol_sub : 1;
     const float E = float(-p[0]);
@@ -217,7 +229,7 @@ __device__ void volumetric_segment(const Params& P, const FrameDev& F, const dou
         const float g = kepler_g<float>(F.m, xs, ys, zs, r, E, Lz, float(F.sqrt_m_gtt_cam));
         if (!(g > 0.f)) continue;
         const float jsp = float(c.vol_j0) / (r * r) * __expf(-0.5f * zr * zr);
-        const float gs = __powf(g, float(c.vol_s));          // nu_em^-s = (g/nu_b)^s
+        const float gs = __powf(g, float(c.vol_s));  // nu_em^-s = (g/nu_b)^s
         const float dt0 = float(c.vol_aoj) * jsp * gs * (nu_cam / g) * dl;
         const float S = g * g * g / float(c.vol_aoj);
         for (int b = 0; b < c.nbins; ++b) {
@@ -230,55 +242,99 @@ __device__ void volumetric_segment(const Params& P, const FrameDev& F, const dou
     }
 }
 
+// A disk crossing at the event-located point (xc1, xc2, 0): BL radius, exact
+// redshift with the ray's conserved E and L_z (from the state x, p), flux.
+// Returns true when the crossing lies on the disk (GTRC001A.cpp:468-555).
+__device__ __noinline__ bool record_crossing(const Params& P, const FrameDev& F, long long idx, int n, double xc1,
+                                             double xc2, const double x[4], const double p[4], double& intensity) {
+    const MetricDev& m = F.m;
+    const double xc[4] = {0.0, xc1, xc2, 0.0};
+    InvForm CF;
+    inv_form(m, xc, CF);
+    const double rc = CF.r;
+    if (!(rc >= F.disk_in && rc <= F.disk_out)) return false;
+    const double E = -p[0], Lz = x[1] * p[2] - x[2] * p[1];
+    const double g = kepler_g<double>(m, xc1, xc2, 0.0, rc, E, Lz, F.sqrt_m_gtt_cam);
+    const double Fl = nt_flux(rc, F.a_star, F.isco, F.disk_in, F.disk_out);
+    intensity += exp(-P.c.decay * n) * g * g * g * g * Fl;
+    if (P.results) {
+        sirius_ray_result* R = P.results + idx;
+        R->disk_r[n] = float(rc);
+        R->disk_phi[n] = float(atan2(xc2, xc1));
+        R->disk_g[n] = float(g);
+        R->disk_flux[n] = float(Fl);
+    }
+    return true;
+}
+
+// The FP64 island attempt of the mixed path: f(x, p) recomputed in FP64, a DP45
+// attempt in FP64; the derivative at the candidate point returned in float for
+// the FP32 steps that may follow.
+__device__ __noinline__ double island_attempt(const MetricDev& m, const CfgDev& c, const double x[4],
+                                              const double p[4], double h, double xn[4], double pn[4], float k7f[8]) {
+    double k1[8], k7[8];
+    rhs<double>(m, x, p, k1, k1 + 4);
+    const double err = dp45_attempt<double>(m, c, x, p, h, k1, xn, pn, k7);
+#pragma unroll
+    for (int i = 0; i < 8; ++i) k7f[i] = float(k7[i]);
+    return err;
+}
+
 // One iteration of the ray state machine: a DP45 attempt, and on acceptance
 // the termination checks. Returns -1 while the ray continues, else its outcome.
 template <bool MIXED>
-__device__ int advance(const Params& P, Ray& s, float& magnification, int& flags, float* vol) {
+__device__ __forceinline__ int advance(const Params& P, Ray<MIXED>& s, float& magnification, int& flags, float* vol) {
+    using K = typename Ray<MIXED>::K;
     const FrameDev& F = P.frames[s.frame];
     const MetricDev& m = F.m;
     const CfgDev& c = P.c;
-    double xn[4], pn[4], k7x[4], k7p[4];
+    double xn[4], pn[4];
+    K k7[8];
     bool island = true;
-    if (MIXED) {
+    double err;
+    if constexpr (MIXED) {
         // FP64 island: inside island_factor * r_ph (retrograde) or near the horizon
         const double R2 = s.x[1] * s.x[1] + s.x[2] * s.x[2] + s.x[3] * s.x[3];
         island = (m.family == SIRIUS_METRIC_MORRIS_THORNE) ? (s.x[1] < F.island_r) : (R2 < F.island_r * F.island_r);
+        if (island) err = island_attempt(m, c, s.x, s.p, s.h, xn, pn, k7);
+        else err = dp45_attempt<float>(m, c, s.x, s.p, s.h, s.k, xn, pn, k7);
+    } else {
+        err = dp45_attempt<double>(m, c, s.x, s.p, s.h, s.k, xn, pn, k7);
     }
-    double err;
-    if (island) err = dp45_attempt<double>(m, c, s.x, s.p, s.h, s.kx, s.kp, xn, pn, k7x, k7p);
-    else err = dp45_attempt<float>(m, c, s.x, s.p, s.h, s.kx, s.kp, xn, pn, k7x, k7p);
     ++s.attempts;
     if (!(err <= 1.0)) {
         ++s.rejected;
-        s.h = optimal_step(s.h, isfinite(err) ? err : 1e10, c);
+        s.h = MIXED ? optimal_step_fast(s.h, isfinite(err) ? err : 1e10, c)
+                    : optimal_step(s.h, isfinite(err) ? err : 1e10, c);
         if (s.h <= c.hmin) { ++s.steps; return SIRIUS_STEP_UNDERFLOW; }
         if (s.attempts > c.max_steps * 64 + 1024) return SIRIUS_STEP_UNDERFLOW;
         return -1;
     }
     // accepted
-    double x0[4], k0[4];
-#pragma unroll
-    for (int i = 0; i < 4; ++i) { x0[i] = s.x[i]; k0[i] = s.kx[i]; }
     const double hstep = s.h;
-    // equatorial crossing inside the step: locate it from the step's start
-    // state before that state is replaced
     const bool disk_on = m.family == SIRIUS_METRIC_KERR_SCHILD && c.enable_disk && F.has_horizon;
+    // equatorial crossing inside the step: locate it from the step's start state
     double xc1 = 0.0, xc2 = 0.0;
     const bool cross = disk_on && (s.x[3] * xn[3] < 0.0);
     if (cross) {
-        const double hs = hermite_root(s.x[3], xn[3], s.kx[3], k7x[3], hstep) * hstep;
-        if (island) locate_equator<double>(m, c, s.x, s.p, s.kx, s.kp, hs, xc1, xc2);
-        else locate_equator<float>(m, c, s.x, s.p, s.kx, s.kp, hs, xc1, xc2);
+        const double hs = hermite_root(s.x[3], xn[3], double(s.k[3]), double(k7[3]), hstep) * hstep;
+        if (island || !MIXED) locate_equator<double>(m, c, s.x, s.p, hs, xc1, xc2);
+        else locate_equator<float>(m, c, s.x, s.p, hs, xc1, xc2);
     }
+    double x0[4];
+    float k0f[4];
+#pragma unroll
+    for (int i = 0; i < 4; ++i) { x0[i] = s.x[i]; k0f[i] = float(s.k[i]); }
     s.h = MIXED ? optimal_step_fast(s.h, err, c) : optimal_step(s.h, err, c);
     ++s.steps;
-    if (island && MIXED) ++s.fp64_steps;
+    if (MIXED && island) ++s.fp64_steps;
     bool bad = false;
 #pragma unroll
-    for (int i = 0; i < 4; ++i) {
-        bad |= !isfinite(xn[i]) || !isfinite(pn[i]) || !isfinite(k7x[i]);
-        s.x[i] = xn[i]; s.p[i] = pn[i]; s.kx[i] = k7x[i]; s.kp[i] = k7p[i];
-    }
+    for (int i = 0; i < 4; ++i) bad |= !isfinite(xn[i]) || !isfinite(pn[i]) || !isfinite(double(k7[i]));
+#pragma unroll
+    for (int i = 0; i < 4; ++i) { s.x[i] = xn[i]; s.p[i] = pn[i]; }
+#pragma unroll
+    for (int i = 0; i < 8; ++i) s.k[i] = k7[i];
     if (bad) { flags |= SIRIUS_FLAG_NUMERICAL_FAILURE; return SIRIUS_NUMERICAL_FAILURE; }
 
     // FP64 constraint re-projection (E, L_z and Carter preserving)
@@ -306,9 +362,10 @@ __device__ int advance(const Params& P, Ray& s, float& magnification, int& flags
     if (c.spiral && !mt && (sidx % 100) == 0 && sidx > 100) {
         const float ratio = s.min_r / float(F.r_ph_pro);
         if (ratio < 1.5f && ratio > 0.9f && s.tphi > 2.f * float(kPi)) {
+            const double k1 = double(s.k[1]), k2 = double(s.k[2]), k3 = double(s.k[3]);
             const double Reu = sqrt(s.x[1] * s.x[1] + s.x[2] * s.x[2] + s.x[3] * s.x[3]);
-            const double vrad = (s.x[1] * s.kx[1] + s.x[2] * s.kx[2] + s.x[3] * s.kx[3]) / Reu;
-            const double vt = sqrt(s.kx[1] * s.kx[1] + s.kx[2] * s.kx[2] + s.kx[3] * s.kx[3]);
+            const double vrad = (s.x[1] * k1 + s.x[2] * k2 + s.x[3] * k3) / Reu;
+            const double vt = sqrt(k1 * k1 + k2 * k2 + k3 * k3);
             if (fabs(vrad) / fmax(vt, 1e-10) < 0.3) return s.ncross > 0 ? SIRIUS_DISK_HIT : SIRIUS_SPIRALING;
         }
     }
@@ -320,7 +377,8 @@ __device__ int advance(const Params& P, Ray& s, float& magnification, int& flags
     {
         const double Resc = mt ? s.x[1] : sqrt(s.x[1] * s.x[1] + s.x[2] * s.x[2] + s.x[3] * s.x[3]);
         if (Resc > c.escape_r) {
-            const double vrad = mt ? s.kx[1] : (s.x[1] * s.kx[1] + s.x[2] * s.kx[2] + s.x[3] * s.kx[3]);
+            const double vrad = mt ? double(s.k[1])
+                                   : (s.x[1] * double(s.k[1]) + s.x[2] * double(s.k[2]) + s.x[3] * double(s.k[3]));
             if (vrad > 0.0) {
                 const float ratio = s.min_r / float(F.r_ph_pro);
                 if (ratio < 1.5f) {
@@ -331,32 +389,17 @@ __device__ int advance(const Params& P, Ray& s, float& magnification, int& flags
             }
         }
     }
-    if (m.family != SIRIUS_METRIC_KERR_SCHILD || !c.enable_disk || !F.has_horizon) {
-        return s.steps >= c.max_steps ? (s.ncross > 0 ? SIRIUS_DISK_HIT : SIRIUS_MAX_STEPS) : -1;
+    if (!disk_on) return s.steps >= c.max_steps ? (s.ncross > 0 ? SIRIUS_DISK_HIT : SIRIUS_MAX_STEPS) : -1;
+    if (c.enable_vol && vol) {
+        float k1f[4];
+#pragma unroll
+        for (int i = 0; i < 4; ++i) k1f[i] = float(s.k[i]);
+        volumetric_segment(P, F, x0, s.x, k0f, k1f, s.p, hstep, vol);
     }
-    if (c.enable_vol && vol) volumetric_segment(P, F, x0, s.x, k0, s.kx, s.p, hstep, vol);
-
-    // thin-disk crossing (GTRC001A.h:404-431, GTRC001A.cpp:468-555): event-located
-    // z = 0 point, its BL radius, the exact redshift with the ray's conserved E, L_z
-    if (cross) {
-        const double xc[4] = {0.0, xc1, xc2, 0.0};
-        InvForm CF;
-        inv_form(m, xc, CF);
-        const double rc = CF.r;
-        if (rc >= F.disk_in && rc <= F.disk_out && s.ncross < SIRIUS_MAX_CROSSINGS) {
-            const int n = s.ncross;
-            const double E = -s.p[0], Lz = s.x[1] * s.p[2] - s.x[2] * s.p[1];
-            const double g = kepler_g<double>(m, xc[1], xc[2], 0.0, rc, E, Lz, F.sqrt_m_gtt_cam);
-            const double Fl = nt_flux(rc, F.a_star, F.isco, F.disk_in, F.disk_out);
-            s.intensity += exp(-c.decay * n) * g * g * g * g * Fl;
-            if (P.results) {
-                sirius_ray_result* R = P.results + s.idx;
-                R->disk_r[n] = float(rc);
-                R->disk_phi[n] = float(atan2(xc[2], xc[1]));
-                R->disk_g[n] = float(g);
-                R->disk_flux[n] = float(Fl);
-            }
-            s.ncross = n + 1;
+    // thin-disk crossing (GTRC001A.h:404-431, GTRC001A.cpp:468-555)
+    if (cross && s.ncross < SIRIUS_MAX_CROSSINGS) {
+        if (record_crossing(P, F, s.idx, s.ncross, xc1, xc2, s.x, s.p, s.intensity)) {
+            ++s.ncross;
             const float ratio = s.min_r / float(F.r_ph_pro);
             if (ratio < 1.5f) {
                 flags |= SIRIUS_FLAG_PHOTON_RING;
@@ -376,7 +419,7 @@ __global__ void __launch_bounds__(128, MINB) trace_kernel(Params P) {
     float* vol = (P.c.enable_vol && P.c.nbins > 0) ? smem + threadIdx.x : nullptr;
     const int lane = threadIdx.x & 31;
     const unsigned lt_mask = (1u << lane) - 1u;
-    Ray s;
+    Ray<MIXED> s;
     bool alive = false;
     float magnification = 1.f;
     int flags = 0;
@@ -386,7 +429,7 @@ __global__ void __launch_bounds__(128, MINB) trace_kernel(Params P) {
 
     if (!P.persistent) {
         const long long idx = (long long)blockIdx.x * blockDim.x + threadIdx.x;
-        if (idx < P.total) { begin_ray(P, s, idx, vol); alive = true; }
+        if (idx < P.total) { begin_ray<MIXED>(P, s, idx, vol); alive = true; }
         exhausted = true;
     }
     for (unsigned iter = 0;; ++iter) {
@@ -401,7 +444,7 @@ __global__ void __launch_bounds__(128, MINB) trace_kernel(Params P) {
                 if (!alive) {
                     const unsigned long long idx = base + __popc(dead & lt_mask);
                     if (idx < (unsigned long long)P.total) {
-                        begin_ray(P, s, (long long)idx, vol);
+                        begin_ray<MIXED>(P, s, (long long)idx, vol);
                         alive = true;
                         magnification = 1.f;
                         flags = 0;
@@ -418,7 +461,7 @@ __global__ void __launch_bounds__(128, MINB) trace_kernel(Params P) {
                 if (stop) {
                     // watchdog: abandon the remaining queue and close the live rays
                     exhausted = true;
-                    if (alive) { end_ray(P, s, SIRIUS_MAX_STEPS, magnification, flags, vol); alive = false; }
+                    if (alive) { end_ray<MIXED>(P, s, SIRIUS_MAX_STEPS, magnification, flags, vol); alive = false; }
                 }
             }
         }
@@ -429,7 +472,7 @@ __global__ void __launch_bounds__(128, MINB) trace_kernel(Params P) {
         if (alive) {
             const int out = advance<MIXED>(P, s, magnification, flags, vol);
             if (out >= 0) {
-                end_ray(P, s, out, magnification, flags, vol);
+                end_ray<MIXED>(P, s, out, magnification, flags, vol);
                 acc += s.steps;
                 rej0 += s.rejected;
                 f64 += s.fp64_steps;
@@ -492,10 +535,10 @@ __global__ void dp45_step_kernel(MetricDev m, CfgDev c, double* state, double* h
                                  long long n) {
     const long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x;
     if (i >= n) return;
-    double x[4], p[4], kx[4], kp[4], xn[4], pn[4], k7x[4], k7p[4];
+    double x[4], p[4], k1[8], xn[4], pn[4], k7[8];
     for (int j = 0; j < 4; ++j) { x[j] = state[8 * i + j]; p[j] = state[8 * i + 4 + j]; }
-    rhs<double>(m, x, p, kx, kp);
-    const double e = dp45_attempt<double>(m, c, x, p, h[i], kx, kp, xn, pn, k7x, k7p);
+    rhs<double>(m, x, p, k1, k1 + 4);
+    const double e = dp45_attempt<double>(m, c, x, p, h[i], k1, xn, pn, k7);
     err[i] = e;
     accepted[i] = e <= 1.0 ? 1 : 0;
     if (e <= 1.0)
@@ -544,6 +587,10 @@ struct Handle {
     int* d_status = nullptr;
     cudaEvent_t ev[4] = {};
     sirius_launch_stats stats{};
+    // a device-entry launch whose statistics are read on the next sirius_cuda_last_stats
+    bool pending = false;
+    cudaStream_t pending_stream = nullptr;
+    long long pending_total = 0;
 };
 
 int fail(Handle* h, int code, const std::string& msg) {
@@ -910,6 +957,9 @@ int sirius_cuda_trace_frames_device(sirius_cuda_handle h, const sirius_frame* d_
     rc = launch_trace(H, n_frames, total, d_results, d_image, d_spectra, nullptr, st, true);
     if (rc != SIRIUS_OK) return rc;
     CK(cudaEventRecord(H->ev[3], st));
+    H->pending = true;
+    H->pending_stream = st;
+    H->pending_total = total;
     return SIRIUS_OK;
 }
 
@@ -1003,6 +1053,13 @@ int sirius_cuda_dp45_step(sirius_cuda_handle h, const sirius_metric* metric, dou
 int sirius_cuda_last_stats(sirius_cuda_handle h, sirius_launch_stats* out) {
     Handle* H = static_cast<Handle*>(h);
     if (!H || !out) return SIRIUS_ERR_INVALID_ARGUMENT;
+    if (H->pending) {  // a stream-ordered launch: wait for it and read its counters and events
+        H->pending = false;
+        CK(cudaSetDevice(H->device));
+        const int rc = finish_stats(H, H->pending_stream, H->pending_total, true);
+        *out = H->stats;
+        return rc;
+    }
     *out = H->stats;
     return SIRIUS_OK;
 }

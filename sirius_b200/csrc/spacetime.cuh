@@ -277,6 +277,35 @@ __device__ __forceinline__ double project_null(const MetricDev& m, const InvForm
 }
 
 // ---------------------------------------------------------------------------
+// The metric alone, FP64, closed form (no derivatives): g[16].
+// ---------------------------------------------------------------------------
+__device__ __forceinline__ void metric_g(const MetricDev& m, const double x[4], double g[16]) {
+    for (int i = 0; i < 16; ++i) g[i] = 0.0;
+    if (m.family == SIRIUS_METRIC_MORRIS_THORNE) {
+        const double r = fmax(x[1], m.b0 * 1.001);
+        const double s = sin(x[2]);
+        g[0] = m.gtt_mt;
+        g[5] = mt_grr<double>(m, x[1]).v;
+        g[10] = r * r;
+        g[15] = r * r * s * s;
+        return;
+    }
+    if (m.family == SIRIUS_METRIC_ALCUBIERRE) {
+        const double vf = m.vs * alc_f<double>(m, x[1], x[2], x[3]).v;
+        g[0] = -(1.0 - vf * vf);
+        g[1] = g[4] = -vf;
+        g[5] = g[10] = g[15] = 1.0;
+        return;
+    }
+    InvForm F;
+    inv_form(m, x, F);
+    const double l[4] = {1.0, F.l[1], F.l[2], F.l[3]};  // covariant l
+    for (int a = 0; a < 4; ++a)
+        for (int b = 0; b < 4; ++b) g[4 * a + b] = ((a == b) ? (a == 0 ? -1.0 : 1.0) : 0.0) + F.H * l[a] * l[b];
+    if (m.has_lambda) g[0] -= m.lam3 * (x[1] * x[1] + x[2] * x[2] + x[3] * x[3]);
+}
+
+// ---------------------------------------------------------------------------
 // Full metric and derivatives (IMetric::evaluate): g[16], dg[64], dg[l*16+m*4+n].
 // ---------------------------------------------------------------------------
 template <class T>

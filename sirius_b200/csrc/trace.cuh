@@ -153,24 +153,26 @@ __device__ __forceinline__ double null_k0(const double g[16], const double k[4])
     return fmax(kp, km);
 }
 
-// Initial state from a camera ray (GTRC001A.cpp:15-134 without float roundings).
+// Initial state from a camera ray (GTRC001A.cpp:15-134 without float roundings):
+// spherical map of the camera position, spherical -> Cartesian velocity,
+// normalizeNull for k^0, p = g k.
 __device__ __forceinline__ void init_state(const FrameDev& F, const double dir[4], double x[4], double p[4]) {
     const double r = F.cam_r, st = F.cam_st, ct = F.cam_ct, sp = F.cam_sp, cp = F.cam_cp;
     const double vr = dir[1], vth = dir[2] / r;
     double vph = dir[3] / (r * st);
     if (fabs(st) < 1e-10) vph = 0.0;
     double k[4];
-    double g[16], dg[64];
+    double g[16];
     if (F.m.family == SIRIUS_METRIC_MORRIS_THORNE) {
         x[0] = F.cam_t; x[1] = r; x[2] = F.cam_th; x[3] = F.cam_ph;
-        metric_full<double>(F.m, x, g, dg);
+        metric_g(F.m, x, g);
         k[1] = vr / sqrt(g[5]); k[2] = vth; k[3] = vph;
     } else {
         x[0] = F.cam_t; x[1] = r * st * cp; x[2] = r * st * sp; x[3] = r * ct;
         k[1] = vr * st * cp + r * vth * ct * cp - r * vph * st * sp;
         k[2] = vr * st * sp + r * vth * ct * sp + r * vph * st * cp;
         k[3] = vr * ct - r * vth * st;
-        metric_full<double>(F.m, x, g, dg);
+        metric_g(F.m, x, g);
     }
     k[0] = 0.0;
     k[0] = null_k0(g, k);
@@ -182,82 +184,109 @@ __device__ __forceinline__ void init_state(const FrameDev& F, const double dir[4
 }
 
 // ---------------------------------------------------------------------------
-// Dormand-Prince 5(4) attempt (tableau: Dormand & Prince 1980; PHGD001A.cpp:16-79).
-// T is the stage precision: float for the FP32 bulk, double for FP64.
-// The state (x, p) stays in FP64; stage points are x + h sum a_ij k_j in T;
-// the update is accumulated in FP64 from the T-precision weighted sum.
-// On entry (kx, kp) = f(x, p). Returns the scaled RMS position error
-// (computeRK45ErrorNorm, PHGD001A.cpp:508-517).
+// Dormand-Prince 5(4) tableau (Dormand & Prince 1980; PHGD001A.cpp:16-79) in
+// sliding-window form: DP_A[j][s] = a_{j+2+s, j+1}, the weight of k_{j+1} in
+// the input of stage j+2+s (row 7 = the fifth-order weights b, first same as
+// last); DP_E[j] = b_{j+1} - b*_{j+1}. Rows are read with a warp-uniform index
+// (constant-cache broadcast).
 // ---------------------------------------------------------------------------
 template <class T>
+struct DPTable {
+    T A[6][6];
+    T E[7];
+};
+#define SIRIUS_DP45_TABLE(T)                                                                                      \
+    {{{T(1.0 / 5.0), T(3.0 / 40.0), T(44.0 / 45.0), T(19372.0 / 6561.0), T(9017.0 / 3168.0), T(35.0 / 384.0)},      \
+      {T(9.0 / 40.0), T(-56.0 / 15.0), T(-25360.0 / 2187.0), T(-355.0 / 33.0), T(0), T(0)},                        \
+      {T(32.0 / 9.0), T(64448.0 / 6561.0), T(46732.0 / 5247.0), T(500.0 / 1113.0), T(0), T(0)},                    \
+      {T(-212.0 / 729.0), T(49.0 / 176.0), T(125.0 / 192.0), T(0), T(0), T(0)},                                     \
+      {T(-5103.0 / 18656.0), T(-2187.0 / 6784.0), T(0), T(0), T(0), T(0)},                                          \
+      {T(11.0 / 84.0), T(0), T(0), T(0), T(0), T(0)}},                                                              \
+     {T(35.0 / 384.0 - 5179.0 / 57600.0), T(0), T(500.0 / 1113.0 - 7571.0 / 16695.0),                              \
+      T(125.0 / 192.0 - 393.0 / 640.0), T(-2187.0 / 6784.0 + 92097.0 / 339200.0), T(11.0 / 84.0 - 187.0 / 2100.0),  \
+      T(-1.0 / 40.0)}}
+__constant__ DPTable<float> kDPf = SIRIUS_DP45_TABLE(float);
+__constant__ DPTable<double> kDPd = SIRIUS_DP45_TABLE(double);
+
+template <class T>
+__device__ __forceinline__ const DPTable<T>& dp_table();
+template <>
+__device__ __forceinline__ const DPTable<float>& dp_table<float>() { return kDPf; }
+template <>
+__device__ __forceinline__ const DPTable<double>& dp_table<double>() { return kDPd; }
+
+// One DP45 attempt on y = (x^mu, p_mu) with the stage arithmetic in T (float:
+// the FP32 bulk; double: FP64). The state stays in FP64; stage inputs are
+// x + h acc where acc = sum_j a_sj k_j accumulates in T in a sliding window, so
+// the six right-hand sides share one call site (a compact loop body keeps the
+// instruction stream in cache). On entry k1 = f(x, p); on exit (xn, pn) is the
+// fifth-order solution and k7 = f(xn, pn) (first same as last). Returns the
+// scaled RMS error of the position components (computeRK45ErrorNorm,
+// PHGD001A.cpp:508-517).
+template <class T>
 __device__ __forceinline__ double dp45_attempt(const MetricDev& m, const CfgDev& c, const double x[4], const double p[4],
-                                               double h, const double kx[4], const double kp[4], double xn[4],
-                                               double pn[4], double k7x[4], double k7p[4]) {
-    const T a21 = T(1.0 / 5.0);
-    const T a31 = T(3.0 / 40.0), a32 = T(9.0 / 40.0);
-    const T a41 = T(44.0 / 45.0), a42 = T(-56.0 / 15.0), a43 = T(32.0 / 9.0);
-    const T a51 = T(19372.0 / 6561.0), a52 = T(-25360.0 / 2187.0), a53 = T(64448.0 / 6561.0), a54 = T(-212.0 / 729.0);
-    const T a61 = T(9017.0 / 3168.0), a62 = T(-355.0 / 33.0), a63 = T(46732.0 / 5247.0), a64 = T(49.0 / 176.0),
-            a65 = T(-5103.0 / 18656.0);
-    const T b1 = T(35.0 / 384.0), b3 = T(500.0 / 1113.0), b4 = T(125.0 / 192.0), b5 = T(-2187.0 / 6784.0),
-            b6 = T(11.0 / 84.0);
-    const T e1 = T(35.0 / 384.0 - 5179.0 / 57600.0), e3 = T(500.0 / 1113.0 - 7571.0 / 16695.0),
-            e4 = T(125.0 / 192.0 - 393.0 / 640.0), e5 = T(-2187.0 / 6784.0 + 92097.0 / 339200.0),
-            e6 = T(11.0 / 84.0 - 187.0 / 2100.0), e7 = T(-1.0 / 40.0);
+                                               double h, const T k1[8], double xn[4], double pn[4], T k7[8]) {
+    const DPTable<T>& D = dp_table<T>();
     const T ht = T(h);
-    T X[4], P[4], k1x[4], k1p[4], k2x[4], k2p[4], k3x[4], k3p[4], k4x[4], k4p[4], k5x[4], k5p[4], k6x[4], k6p[4];
-    T xs[4], ps[4];
+    T X[8];
 #pragma unroll
-    for (int i = 0; i < 4; ++i) { X[i] = T(x[i]); P[i] = T(p[i]); k1x[i] = T(kx[i]); k1p[i] = T(kp[i]); }
+    for (int i = 0; i < 4; ++i) { X[i] = T(x[i]); X[4 + i] = T(p[i]); }
+    T acc[6][8];
+    T eacc[4];
+    T kc[8];
 #pragma unroll
-    for (int i = 0; i < 4; ++i) { xs[i] = X[i] + ht * (a21 * k1x[i]); ps[i] = P[i] + ht * (a21 * k1p[i]); }
-    rhs(m, xs, ps, k2x, k2p);
+    for (int i = 0; i < 8; ++i) {
+        kc[i] = k1[i];
 #pragma unroll
-    for (int i = 0; i < 4; ++i) {
-        xs[i] = X[i] + ht * (a31 * k1x[i] + a32 * k2x[i]);
-        ps[i] = P[i] + ht * (a31 * k1p[i] + a32 * k2p[i]);
+        for (int s = 0; s < 6; ++s) acc[s][i] = T(0);
     }
-    rhs(m, xs, ps, k3x, k3p);
 #pragma unroll
-    for (int i = 0; i < 4; ++i) {
-        xs[i] = X[i] + ht * (a41 * k1x[i] + a42 * k2x[i] + a43 * k3x[i]);
-        ps[i] = P[i] + ht * (a41 * k1p[i] + a42 * k2p[i] + a43 * k3p[i]);
-    }
-    rhs(m, xs, ps, k4x, k4p);
+    for (int i = 0; i < 4; ++i) eacc[i] = T(0);
+#pragma unroll 1
+    for (int j = 0; j < 6; ++j) {
+        // fold k_{j+1} into the inputs of every later stage, and into the error
 #pragma unroll
-    for (int i = 0; i < 4; ++i) {
-        xs[i] = X[i] + ht * (a51 * k1x[i] + a52 * k2x[i] + a53 * k3x[i] + a54 * k4x[i]);
-        ps[i] = P[i] + ht * (a51 * k1p[i] + a52 * k2p[i] + a53 * k3p[i] + a54 * k4p[i]);
-    }
-    rhs(m, xs, ps, k5x, k5p);
+        for (int s = 0; s < 6; ++s) {
+            const T a = D.A[j][s];
 #pragma unroll
-    for (int i = 0; i < 4; ++i) {
-        xs[i] = X[i] + ht * (a61 * k1x[i] + a62 * k2x[i] + a63 * k3x[i] + a64 * k4x[i] + a65 * k5x[i]);
-        ps[i] = P[i] + ht * (a61 * k1p[i] + a62 * k2p[i] + a63 * k3p[i] + a64 * k4p[i] + a65 * k5p[i]);
-    }
-    rhs(m, xs, ps, k6x, k6p);
+            for (int i = 0; i < 8; ++i) acc[s][i] += a * kc[i];
+        }
+        const T e = D.E[j];
 #pragma unroll
-    for (int i = 0; i < 4; ++i) {
-        const T sx = b1 * k1x[i] + b3 * k3x[i] + b4 * k4x[i] + b5 * k5x[i] + b6 * k6x[i];
-        const T sp = b1 * k1p[i] + b3 * k3p[i] + b4 * k4p[i] + b5 * k5p[i] + b6 * k6p[i];
-        xn[i] = x[i] + h * double(sx);
-        pn[i] = p[i] + h * double(sp);
-        xs[i] = T(xn[i]);
-        ps[i] = T(pn[i]);
+        for (int i = 0; i < 4; ++i) eacc[i] += e * kc[i];
+        T xs[4], ps[4];
+        if (j == 5) {  // stage 7 is the solution point
+#pragma unroll
+            for (int i = 0; i < 4; ++i) {
+                xn[i] = x[i] + h * double(acc[0][i]);
+                pn[i] = p[i] + h * double(acc[0][4 + i]);
+                xs[i] = T(xn[i]);
+                ps[i] = T(pn[i]);
+            }
+        } else {
+#pragma unroll
+            for (int i = 0; i < 4; ++i) { xs[i] = X[i] + ht * acc[0][i]; ps[i] = X[4 + i] + ht * acc[0][4 + i]; }
+        }
+        rhs(m, xs, ps, kc, kc + 4);
+        // slide the window: the next stage's input moves to slot 0
+#pragma unroll
+        for (int s = 0; s < 5; ++s)
+#pragma unroll
+            for (int i = 0; i < 8; ++i) acc[s][i] = acc[s + 1][i];
+#pragma unroll
+        for (int i = 0; i < 8; ++i) acc[5][i] = T(0);
     }
-    T q7x[4], q7p[4];
-    rhs(m, xs, ps, q7x, q7p);
     T en = T(0);
 #pragma unroll
     for (int i = 0; i < 4; ++i) {
-        k7x[i] = double(q7x[i]);
-        k7p[i] = double(q7p[i]);
-        const T ex = e1 * k1x[i] + e3 * k3x[i] + e4 * k4x[i] + e5 * k5x[i] + e6 * k6x[i] + e7 * q7x[i];
+        k7[i] = kc[i];
+        k7[4 + i] = kc[4 + i];
+        const T ex = eacc[i] + D.E[6] * kc[i];
         if constexpr (sizeof(T) == sizeof(double)) {
             const double e = h * double(ex) / (c.atol + c.rtol * fabs(xn[i]));
             en += e * e;
         } else {  // the estimate needs a few digits only
-            const float e = ht * ex * rcp_(float(c.atol) + float(c.rtol) * fabsf(xs[i]));
+            const float e = ht * ex * rcp_(float(c.atol) + float(c.rtol) * fabsf(float(xn[i])));
             en += e * e;
         }
     }
@@ -265,20 +294,22 @@ __device__ __forceinline__ double dp45_attempt(const MetricDev& m, const CfgDev&
 }
 
 // Event location of the equatorial crossing inside an accepted step: DP45
-// sub-steps from the step's start state (x0, p0, f(x0, p0)), the sub-step
-// length corrected by Newton on z(l) (dz/dl = k^z), seeded by the cubic
-// Hermite root; two sub-steps and a final first-order correction.
+// sub-steps from the step's start state (x0, p0) with f(x0, p0) recomputed in
+// T, the sub-step length corrected by Newton on z(l) (dz/dl = k^z), seeded by
+// the cubic Hermite root; two sub-steps and a final first-order correction.
 template <class T>
 __device__ __noinline__ void locate_equator(const MetricDev& m, const CfgDev& c, const double x0[4],
-                                            const double p0[4], const double kx0[4], const double kp0[4], double hs,
-                                            double& xc1, double& xc2) {
-    double xn[4], pn[4], k7x[4], k7p[4];
-    dp45_attempt<T>(m, c, x0, p0, hs, kx0, kp0, xn, pn, k7x, k7p);
-    hs -= xn[3] / k7x[3];
-    dp45_attempt<T>(m, c, x0, p0, hs, kx0, kp0, xn, pn, k7x, k7p);
-    const double dl = -xn[3] / k7x[3];
-    xc1 = xn[1] + dl * k7x[1];
-    xc2 = xn[2] + dl * k7x[2];
+                                            const double p0[4], double hs, double& xc1, double& xc2) {
+    T xk[4], pk[4], k0[8], k7[8];
+    for (int i = 0; i < 4; ++i) { xk[i] = T(x0[i]); pk[i] = T(p0[i]); }
+    rhs<T>(m, xk, pk, k0, k0 + 4);
+    double xn[4], pn[4];
+    dp45_attempt<T>(m, c, x0, p0, hs, k0, xn, pn, k7);
+    hs -= xn[3] / double(k7[3]);
+    dp45_attempt<T>(m, c, x0, p0, hs, k0, xn, pn, k7);
+    const double dl = -xn[3] / double(k7[3]);
+    xc1 = xn[1] + dl * double(k7[1]);
+    xc2 = xn[2] + dl * double(k7[2]);
 }
 
 // Geodesic::computeOptimalStep (PHGD001A.cpp:471-483).
