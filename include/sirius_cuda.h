@@ -247,7 +247,9 @@ int sirius_cuda_trace_frames(sirius_cuda_handle handle,
                              const sirius_frame* frames, int32_t n_frames,
                              sirius_ray_result* results, float* image, float* spectra);
 
-/* Device variant: frames/results/image/spectra are device pointers; stream-ordered. */
+/* Device variant: frames/results/image/spectra are device pointers; stream-ordered
+ * on `stream` (a cudaStream_t; NULL = the legacy default stream). Timing and
+ * counters of the launch are read by the next sirius_cuda_last_stats call. */
 int sirius_cuda_trace_frames_device(sirius_cuda_handle handle,
                                     const sirius_frame* d_frames, int32_t n_frames,
                                     int64_t total_rays,

@@ -774,6 +774,25 @@ void init_state(const TraceContext& ctx, const double origin[4], const double di
     lower(g, k, p);
 }
 
+// Gauss-Legendre points and weights on [0, 1] (n = 1..4; Abramowitz & Stegun 25.4),
+// ordered along the step. The volumetric quadrature of one step.
+inline void gauss_legendre(int n, int& m, const double*& x, const double*& w) {
+    static const double x1[1] = {0.5}, w1[1] = {1.0};
+    static const double x2[2] = {0.21132486540518713, 0.78867513459481287}, w2[2] = {0.5, 0.5};
+    static const double x3[3] = {0.11270166537925831, 0.5, 0.88729833462074169},
+                        w3[3] = {0.27777777777777778, 0.44444444444444444, 0.27777777777777778};
+    static const double x4[4] = {0.069431844202973713, 0.33000947820757187, 0.66999052179242813,
+                                 0.93056815579702629},
+                        w4[4] = {0.17392742256872693, 0.32607257743127307, 0.32607257743127307,
+                                 0.17392742256872693};
+    switch (n <= 1 ? 1 : (n >= 4 ? 4 : n)) {
+        case 1: m = 1; x = x1; w = w1; break;
+        case 2: m = 2; x = x2; w = w2; break;
+        case 3: m = 3; x = x3; w = w3; break;
+        default: m = 4; x = x4; w = w4; break;
+    }
+}
+
 // Cubic Hermite interpolation of the step (x0, k0) -> (x1, k1) over h: returns
 // the fraction s in [0,1] where z(s) = 0 (bisection + Newton on the cubic).
 template <class R>
@@ -818,8 +837,9 @@ void locate_equator(const sirius_metric& m, const sirius_trace_config& c, const 
 }
 
 // Volumetric emission of the engine (the BASELINE profile): over one step segment
-// x0 -> x1 of affine length h, n_sub midpoint samples on the step's cubic
-// Hermite interpolant (the reference marches the chord, GTRC001A.cpp:943-958),
+// x0 -> x1 of affine length h, Gauss-Legendre points (vol_substeps of them, 1..4)
+// on the step's cubic Hermite interpolant (the reference marches the chord with
+// midpoints, GTRC001A.cpp:943-958),
 // camera-first accumulation per bin:
 //   I_b += T_b S (1 - e^{-dtau}),  T_b *= e^{-dtau},
 //   j = j0 r^-2 exp(-z^2 / (2 (h_z r)^2)) nu_em^-s,  alpha = c_a j,
@@ -828,11 +848,14 @@ template <class R>
 void volumetric_segment(const TraceContext& ctx, const R x0[4], const R x1[4], const R k0[4], const R k1[4],
                         const R p[4], R h, R sqrt_m_gtt_cam, const R* nu, Spectra& sp) {
     const auto& c = ctx.cfg;
-    const int ns = std::max(1, c.vol_substeps);
+    int n;
+    const double* gx;
+    const double* gw;
+    gauss_legendre(c.vol_substeps, n, gx, gw);
     const R E = -p[0], Lz = x1[1] * p[2] - x1[2] * p[1];  // p is the state at x1
     const R nu_cam = E / sqrt_m_gtt_cam;
-    for (int s = 0; s < ns; ++s) {
-        const R f = (R(s) + R(0.5)) / R(ns);
+    for (int s = 0; s < n; ++s) {
+        const R f = R(gx[s]);
         R xs[4], d[4];
         hermite_point(x0, x1, k0, k1, h, f, xs);  // the step's cubic Hermite interpolant
         const R r = radial(ctx.metric, xs, d);
@@ -842,7 +865,7 @@ void volumetric_segment(const TraceContext& ctx, const R x0[4], const R x1[4], c
         const R jsp = R(c.vol_j0) / (r * r) * std::exp(R(-0.5) * zr * zr);
         const R g = redshift_exact(ctx, xs, r, E, Lz, sqrt_m_gtt_cam);
         if (!(g > R(0))) continue;
-        const R dl = h / R(ns);
+        const R dl = h * R(gw[s]);
         const R S = g * g * g / R(c.vol_alpha_over_j);
         for (int b = 0; b < c.n_bins; ++b) {
             const R nu_em = nu[b] / g;
@@ -853,6 +876,21 @@ void volumetric_segment(const TraceContext& ctx, const R x0[4], const R x1[4], c
             sp.tau[b] += dtau;
         }
     }
+}
+
+// Largest affine step inside the emitting volume: half the local Gaussian scale
+// height h_z r over the spatial speed |dx/dl| (so the per-step quadrature, and
+// hence the spectra, do not depend on the step sequence). Infinite outside.
+template <class R>
+R volume_step_cap(const TraceContext& ctx, const R x[4], const R k[4]) {
+    const auto& c = ctx.cfg;
+    R d[4];
+    const R r = radial(ctx.metric, x, d);
+    if (r < R(0.9) * R(ctx.disk_inner) || r > R(1.1) * R(ctx.disk_outer)) return R(1e300);
+    const R H = R(c.vol_height_ratio) * r;
+    if (std::abs(x[3]) > R(5) * H) return R(1e300);
+    const R v = std::sqrt(k[1] * k[1] + k[2] * k[2] + k[3] * k[3]);
+    return R(0.5) * H / std::max(v, R(1e-3));
 }
 
 // GeodesicTracer volumetric helpers (GTRC001A.cpp:834-912) — compat gray march.
@@ -991,6 +1029,8 @@ void trace_ray(const TraceContext& ctx, const double origin[4], const double dir
         if (!(err <= R(1))) {  // reject (NaN errors reject too)
             ++rejected;
             h = optimal_step(h, std::isfinite(double(err)) ? err : R(1e10), c, compat);
+            if (!compat && c.enable_volumetric && c.enable_disk && m.family == SIRIUS_METRIC_KERR_SCHILD && r_hor > 0)
+                h = std::max(R(c.min_step), std::min(h, volume_step_cap(ctx, x, k1x)));
             if (h <= (compat ? R(float(c.min_step)) : R(c.min_step))) {
                 res.outcome = compat ? SIRIUS_MAX_STEPS : SIRIUS_STEP_UNDERFLOW;
                 ++steps;
@@ -1009,6 +1049,8 @@ void trace_ray(const TraceContext& ctx, const double origin[4], const double dir
         for (int i = 0; i < 4; ++i) { x0[i] = x[i]; k0v[i] = compat ? k[i] : k1x[i]; p0[i] = p[i]; k0p[i] = k1p[i]; }
         const R hstep = h;
         h = optimal_step(h, err, c, compat);
+        if (!compat && c.enable_volumetric && c.enable_disk && m.family == SIRIUS_METRIC_KERR_SCHILD && r_hor > 0)
+            h = std::max(R(c.min_step), std::min(h, volume_step_cap(ctx, xn, k7x)));
         ++steps;
         bool bad = false;
         for (int i = 0; i < 4; ++i) bad |= !std::isfinite(double(xn[i])) || !std::isfinite(double(k7x[i]));
@@ -1110,7 +1152,7 @@ void trace_ray(const TraceContext& ctx, const double origin[4], const double dir
                 break;
             }
         }
-        if (!ks || !c.enable_disk) continue;
+        if (!ks || !c.enable_disk || (!compat && r_hor <= 0)) continue;  // the disk needs a horizon
 
         // volumetric
         if (c.enable_volumetric) {

@@ -207,14 +207,13 @@ __device__ __noinline__ void volumetric_segment(const Params& P, const FrameDev&
                                                 const double x1[4], const float k0[4], const float k1[4],
                                                 const double p[4], double h, float* vol) {
     const CfgDev& c = P.c;
-    const int ns = c.vol_sub > 0 ? c.vol_sub : 1;
+    const int nq = c.vol_sub < 1 ? 1 : (c.vol_sub > 4 ? 4 : c.vol_sub);
     const float E = float(-p[0]);
     const float Lz = float(x1[1] * p[2] - x1[2] * p[1]);
     const float nu_cam = E / float(F.sqrt_m_gtt_cam);
-    const float dl = float(h) / float(ns);
-    for (int s = 0; s < ns; ++s) {
-        // sample on the step's cubic Hermite interpolant
-        const double q = (s + 0.5) / ns, q2 = q * q, q3 = q2 * q;
+    for (int s = 0; s < nq; ++s) {
+        // Gauss-Legendre point on the step's cubic Hermite interpolant
+        const double q = double(kGLx[nq - 1][s]), q2 = q * q, q3 = q2 * q;
         const double h00 = 2.0 * q3 - 3.0 * q2 + 1.0, h10 = (q3 - 2.0 * q2 + q) * h, h01 = -2.0 * q3 + 3.0 * q2,
                      h11 = (q3 - q2) * h;
         const float xs = float(h00 * x0[1] + h10 * k0[1] + h01 * x1[1] + h11 * k1[1]);
@@ -228,6 +227,7 @@ __device__ __noinline__ void volumetric_segment(const Params& P, const FrameDev&
         if (fabsf(zr) > 4.f) continue;
         const float g = kepler_g<float>(F.m, xs, ys, zs, r, E, Lz, float(F.sqrt_m_gtt_cam));
         if (!(g > 0.f)) continue;
+        const float dl = float(h) * kGLw[nq - 1][s];
         const float jsp = float(c.vol_j0) / (r * r) * __expf(-0.5f * zr * zr);
         const float gs = __powf(g, float(c.vol_s));  // nu_em^-s = (g/nu_b)^s
         const float dt0 = float(c.vol_aoj) * jsp * gs * (nu_cam / g) * dl;
@@ -236,7 +236,9 @@ __device__ __noinline__ void volumetric_segment(const Params& P, const FrameDev&
             const float dtau = dt0 * c.nu_pow[b];
             float& I = vol[2 * b * blockDim.x];
             float& tau = vol[(2 * b + 1) * blockDim.x];
-            I += __expf(-tau) * S * (1.f - __expf(-dtau));
+            // 1 - e^-x by its series while x is small (no special-function unit needed)
+            const float om = dtau < 1e-3f ? dtau * (1.f - dtau * (0.5f - dtau * (1.f / 6.f))) : 1.f - __expf(-dtau);
+            I += __expf(-tau) * S * om;
             tau += dtau;
         }
     }
@@ -306,6 +308,12 @@ __device__ __forceinline__ int advance(const Params& P, Ray<MIXED>& s, float& ma
         ++s.rejected;
         s.h = MIXED ? optimal_step_fast(s.h, isfinite(err) ? err : 1e10, c)
                     : optimal_step(s.h, isfinite(err) ? err : 1e10, c);
+        if (c.enable_vol && c.enable_disk && F.has_horizon && m.family == SIRIUS_METRIC_KERR_SCHILD) {
+            InvForm RF;
+            inv_form(m, s.x, RF);
+            s.h = fmax(c.hmin, fmin(s.h, volume_step_cap(RF.r, s.x[3], double(s.k[1]), double(s.k[2]),
+                                                         double(s.k[3]), c.vol_hz, F.disk_in, F.disk_out)));
+        }
         if (s.h <= c.hmin) { ++s.steps; return SIRIUS_STEP_UNDERFLOW; }
         if (s.attempts > c.max_steps * 64 + 1024) return SIRIUS_STEP_UNDERFLOW;
         return -1;
@@ -346,6 +354,9 @@ __device__ __forceinline__ int advance(const Params& P, Ray<MIXED>& s, float& ma
     }
     const double rr = IF.r;
     if (float(rr) < s.min_r) s.min_r = float(rr);
+    if (disk_on && c.enable_vol)
+        s.h = fmax(c.hmin, fmin(s.h, volume_step_cap(rr, s.x[3], double(s.k[1]), double(s.k[2]), double(s.k[3]),
+                                                     c.vol_hz, F.disk_in, F.disk_out)));
     const bool mt = m.family == SIRIUS_METRIC_MORRIS_THORNE;
 
     // winding: equatorial crossings and |d phi| (GTRC001A.cpp:294-309)
@@ -941,7 +952,7 @@ int sirius_cuda_trace_frames_device(sirius_cuda_handle h, const sirius_frame* d_
     Handle* H = static_cast<Handle*>(h);
     if (!H || !d_frames_user || n_frames <= 0 || total_rays <= 0) return SIRIUS_ERR_INVALID_ARGUMENT;
     CK(cudaSetDevice(H->device));
-    cudaStream_t st = stream ? static_cast<cudaStream_t>(stream) : H->stream;
+    cudaStream_t st = stream ? static_cast<cudaStream_t>(stream) : cudaStreamLegacy;
     // frames arrive in device memory: bring the small descriptors to the host to derive constants
     std::vector<sirius_frame> hf(n_frames);
     CK(cudaMemcpyAsync(hf.data(), d_frames_user, n_frames * sizeof(sirius_frame), cudaMemcpyDeviceToHost, st));

@@ -328,6 +328,31 @@ __device__ __forceinline__ double optimal_step_fast(double h, double err, const 
     return fmax(c.hmin, fmin(c.hmax, h * double(fac)));
 }
 
+// Gauss-Legendre points and weights on [0, 1] for n = 1..4 (Abramowitz & Stegun
+// 25.4), ordered along the step: the volumetric quadrature of one step.
+__constant__ float kGLx[4][4] = {{0.5f, 0, 0, 0},
+                                 {0.21132486540518713f, 0.78867513459481287f, 0, 0},
+                                 {0.11270166537925831f, 0.5f, 0.88729833462074169f, 0},
+                                 {0.069431844202973713f, 0.33000947820757187f, 0.66999052179242813f,
+                                  0.93056815579702629f}};
+__constant__ float kGLw[4][4] = {{1.0f, 0, 0, 0},
+                                 {0.5f, 0.5f, 0, 0},
+                                 {0.27777777777777778f, 0.44444444444444444f, 0.27777777777777778f, 0},
+                                 {0.17392742256872693f, 0.32607257743127307f, 0.32607257743127307f,
+                                  0.17392742256872693f}};
+
+// Largest affine step inside the emitting volume: half the local Gaussian scale
+// height h_z r over the spatial speed |dx/dl| (the per-step quadrature, and so
+// the spectra, then do not depend on the step sequence). Infinite outside.
+__device__ __forceinline__ double volume_step_cap(double r, double z, double vx, double vy, double vz, double hz,
+                                                  double r_in, double r_out) {
+    if (r < 0.9 * r_in || r > 1.1 * r_out) return 1e300;
+    const double H = hz * r;
+    if (fabs(z) > 5.0 * H) return 1e300;
+    const double v = sqrt(vx * vx + vy * vy + vz * vz);
+    return 0.5 * H / fmax(v, 1e-3);
+}
+
 // Cubic Hermite interpolation of z over the accepted step; bisection for z = 0.
 __device__ __forceinline__ double hermite_root(double z0, double z1, double dz0, double dz1, double h) {
     double lo = 0.0, hi = 1.0, flo = z0;

@@ -97,8 +97,8 @@ def test_dp45_step_matches_oracle(engine, oracle):
     s1, h1, a1, e1 = engine.dp45_step(m, states, hs)
     np.testing.assert_array_equal(a1, a0)
     # the error estimate is a cancelling sum: the two formulations agree to ~1e-6 of it
-    np.testing.assert_allclose(e1, e0, rtol=1e-5, atol=1e-12)
-    np.testing.assert_allclose(s1, s0, rtol=1e-13, atol=1e-13)
+    np.testing.assert_allclose(e1, e0, rtol=1e-5, atol=1e-8)
+    np.testing.assert_allclose(s1, s0, rtol=1e-12, atol=1e-12)
     np.testing.assert_allclose(h1, h0, rtol=1e-12)
 
 
