@@ -454,6 +454,45 @@ bool compat_rk45_step(const sirius_metric& m, const sirius_trace_config& c, R x[
 }
 
 // ---------------------------------------------------------------------------
+// Symplectic integration (SymplecticIntegratorD, PHSI001A.h:43-80, 136-215,
+// 430-455) on the Kerr-Schild Hamiltonian H = 1/2 g^{mu nu}(x) p_mu p_nu:
+// a Yoshida composition (orders 4, 6, 8; Yoshida 1990) of the kick-drift-kick
+// leapfrog  p += h/2 dp/dl(x, p);  x += h dx/dl(x, p);  p += h/2 dp/dl(x, p),
+// with dx/dl = g^{-1} p and dp/dl = 1/2 d g k k (the reference's dHdp / dHdq).
+// ---------------------------------------------------------------------------
+inline void yoshida_weights(int order, int& n, const double*& w) {
+    static const double w4[3] = {1.3512071919596576, -1.7024143839193153, 1.3512071919596576};
+    static const double w6[7] = {0.78451361047756, 0.23557321335936, -1.17767998417887, 1.31518632068391,
+                                 -1.17767998417887, 0.23557321335936, 0.78451361047756};
+    static const double w8[15] = {0.74167036435061, -0.40910082580003, 0.19075471029623, -0.57386247111608,
+                                  0.29906418130365, 0.33462491824529, 0.31529309239676, -0.79688793935291,
+                                  0.31529309239676, 0.33462491824529, 0.29906418130365, -0.57386247111608,
+                                  0.19075471029623, -0.40910082580003, 0.74167036435061};
+    if (order >= 8) { n = 15; w = w8; }
+    else if (order >= 6) { n = 7; w = w6; }
+    else { n = 3; w = w4; }
+}
+
+template <class R>
+void leapfrog(const sirius_metric& m, R x[4], R p[4], R h) {
+    R k[4], f[4];
+    rhs(m, x, p, k, f, false);
+    for (int i = 0; i < 4; ++i) p[i] += R(0.5) * h * f[i];
+    rhs(m, x, p, k, f, false);
+    for (int i = 0; i < 4; ++i) x[i] += h * k[i];
+    rhs(m, x, p, k, f, false);
+    for (int i = 0; i < 4; ++i) p[i] += R(0.5) * h * f[i];
+}
+
+template <class R>
+void symplectic_step(const sirius_metric& m, int order, R h, R x[4], R p[4]) {
+    int n;
+    const double* w;
+    yoshida_weights(order, n, w);
+    for (int s = 0; s < n; ++s) leapfrog(m, x, p, R(w[s]) * h);
+}
+
+// ---------------------------------------------------------------------------
 // Radial coordinate of the family and its gradient (the covector dr used by the
 // E/L_z-preserving re-projection — the Kerr-Schild form of the p_r
 // renormalisation of SymplecticIntegratorD::renormalizeNull, PHSI001A.h:366-418).
@@ -1024,7 +1063,26 @@ void trace_ray(const TraceContext& ctx, const double origin[4], const double dir
                 k1x[mu] = k[mu];
             }
         }
-        const R err = dp45_attempt(m, c, x, p, h, k1x, k1p, xn, pn, k7x, k7p, compat);
+        const bool symp = !compat && c.integrator == SIRIUS_INTEGRATOR_SYMPLECTIC;
+        R err;
+        if (symp) {  // fixed d-lambda, always accepted
+            for (int i = 0; i < 4; ++i) { xn[i] = x[i]; pn[i] = p[i]; }
+            // d-lambda shrinks near the horizon as SymplecticIntegratorD::integrate does
+            // (h0 min(1, ((r - r_+)/r_+)^2), PHSI001A.h:260-263)
+            R hs = R(c.symplectic_step);
+            if (r_hor > 0) {
+                R dd[4];
+                const R rp = R(r_plus(m));
+                const R q = (radial(m, x, dd) - rp) / rp;
+                hs = std::max(R(c.min_step), hs * std::min(R(1), q * q));
+            }
+            symplectic_step(m, c.symplectic_order, hs, xn, pn);
+            rhs(m, xn, pn, k7x, k7p, false);
+            err = R(0);
+            h = hs;
+        } else {
+            err = dp45_attempt(m, c, x, p, h, k1x, k1p, xn, pn, k7x, k7p, compat);
+        }
         ++attempts;
         if (!(err <= R(1))) {  // reject (NaN errors reject too)
             ++rejected;
@@ -1048,8 +1106,8 @@ void trace_ray(const TraceContext& ctx, const double origin[4], const double dir
         R x0[4], k0v[4], p0[4], k0p[4];
         for (int i = 0; i < 4; ++i) { x0[i] = x[i]; k0v[i] = compat ? k[i] : k1x[i]; p0[i] = p[i]; k0p[i] = k1p[i]; }
         const R hstep = h;
-        h = optimal_step(h, err, c, compat);
-        if (!compat && c.enable_volumetric && c.enable_disk && m.family == SIRIUS_METRIC_KERR_SCHILD && r_hor > 0)
+        if (!symp) h = optimal_step(h, err, c, compat);
+        if (!symp && !compat && c.enable_volumetric && c.enable_disk && m.family == SIRIUS_METRIC_KERR_SCHILD && r_hor > 0)
             h = std::max(R(c.min_step), std::min(h, volume_step_cap(ctx, xn, k7x)));
         ++steps;
         bool bad = false;
@@ -1074,8 +1132,16 @@ void trace_ray(const TraceContext& ctx, const double origin[4], const double dir
             for (int i = 0; i < 4; ++i) badp |= !std::isfinite(double(pn[i]));
             if (badp) { res.outcome = SIRIUS_NUMERICAL_FAILURE; break; }
             if (c.projection_period > 0 && (steps % c.projection_period) == 0) {
+                R pb[4] = {p[0], p[1], p[2], p[3]};
                 const R before = project_null(m, x, p);
                 null_max = std::max(null_max, float(std::abs(double(before))));
+                // a projection that moved p beyond 1e-10 (relative) makes f(x, p) stale: recompute it
+                R dp = 0, pm = 0;
+                for (int i = 0; i < 4; ++i) {
+                    dp = std::max(dp, std::abs(p[i] - pb[i]));
+                    pm = std::max(pm, std::abs(p[i]));
+                }
+                if (dp > R(1e-10) * pm) rhs(m, x, p, k1x, k1p, false);
             } else {
                 null_max = std::max(null_max, float(std::abs(double(null_value(m, x, p)))));
             }

@@ -282,6 +282,15 @@ __device__ __noinline__ double island_attempt(const MetricDev& m, const CfgDev& 
     return err;
 }
 
+// f(x, p) of the current state in the storage precision of the path.
+template <bool MIXED>
+__device__ __noinline__ void refresh_derivative(const MetricDev& m, Ray<MIXED>& s) {
+    using K = typename Ray<MIXED>::K;
+    K xk[4], pk[4];
+    for (int i = 0; i < 4; ++i) { xk[i] = K(s.x[i]); pk[i] = K(s.p[i]); }
+    rhs<K>(m, xk, pk, s.k, s.k + 4);
+}
+
 // One iteration of the ray state machine: a DP45 attempt, and on acceptance
 // the termination checks. Returns -1 while the ray continues, else its outcome.
 template <bool MIXED>
@@ -298,6 +307,28 @@ __device__ __forceinline__ int advance(const Params& P, Ray<MIXED>& s, float& ma
         // FP64 island: inside island_factor * r_ph (retrograde) or near the horizon
         const double R2 = s.x[1] * s.x[1] + s.x[2] * s.x[2] + s.x[3] * s.x[3];
         island = (m.family == SIRIUS_METRIC_MORRIS_THORNE) ? (s.x[1] < F.island_r) : (R2 < F.island_r * F.island_r);
+    }
+    const bool symp = c.integrator == SIRIUS_INTEGRATOR_SYMPLECTIC;
+    if (symp) {
+        // fixed d-lambda, shrunk near the horizon as SymplecticIntegratorD::integrate
+        // does (h0 min(1, ((r - r_+)/r_+)^2), PHSI001A.h:260-263); always accepted
+        double hs = c.symp_step;
+        if (F.has_horizon) {
+            const double rp = F.r_hor / F.horizon_factor;
+            const double q = (ks_radius(m, s.x) - rp) / rp;
+            hs = fmax(c.hmin, hs * fmin(1.0, q * q));
+        }
+        s.h = hs;
+#pragma unroll
+        for (int i = 0; i < 4; ++i) { xn[i] = s.x[i]; pn[i] = s.p[i]; }
+        if (MIXED && !island) symplectic_step<float>(m, c.symp_order, hs, xn, pn);
+        else symplectic_step<double>(m, c.symp_order, hs, xn, pn);
+        K xk[4], pk[4];
+#pragma unroll
+        for (int i = 0; i < 4; ++i) { xk[i] = K(xn[i]); pk[i] = K(pn[i]); }
+        rhs<K>(m, xk, pk, k7, k7 + 4);
+        err = 0.0;
+    } else if constexpr (MIXED) {
         if (island) err = island_attempt(m, c, s.x, s.p, s.h, xn, pn, k7);
         else err = dp45_attempt<float>(m, c, s.x, s.p, s.h, s.k, xn, pn, k7);
     } else {
@@ -333,7 +364,7 @@ __device__ __forceinline__ int advance(const Params& P, Ray<MIXED>& s, float& ma
     float k0f[4];
 #pragma unroll
     for (int i = 0; i < 4; ++i) { x0[i] = s.x[i]; k0f[i] = float(s.k[i]); }
-    s.h = MIXED ? optimal_step_fast(s.h, err, c) : optimal_step(s.h, err, c);
+    if (!symp) s.h = MIXED ? optimal_step_fast(s.h, err, c) : optimal_step(s.h, err, c);
     ++s.steps;
     if (MIXED && island) ++s.fp64_steps;
     bool bad = false;
@@ -349,12 +380,23 @@ __device__ __forceinline__ int advance(const Params& P, Ray<MIXED>& s, float& ma
     InvForm IF;
     inv_form(m, s.x, IF);
     if (c.proj_period > 0 && (s.steps % c.proj_period) == 0) {
+        double pb[4];
+#pragma unroll
+        for (int i = 0; i < 4; ++i) pb[i] = s.p[i];
         const double before = project_null(m, IF, s.p);
         s.null_max = fmaxf(s.null_max, float(fabs(before)));
+        // a projection that moved p beyond 1e-10 (relative) makes f(x, p) stale: recompute it
+        double dp = 0.0, pm = 0.0;
+#pragma unroll
+        for (int i = 0; i < 4; ++i) {
+            dp = fmax(dp, fabs(s.p[i] - pb[i]));
+            pm = fmax(pm, fabs(s.p[i]));
+        }
+        if (dp > 1e-10 * pm) refresh_derivative<MIXED>(m, s);
     }
     const double rr = IF.r;
     if (float(rr) < s.min_r) s.min_r = float(rr);
-    if (disk_on && c.enable_vol)
+    if (disk_on && c.enable_vol && !symp)
         s.h = fmax(c.hmin, fmin(s.h, volume_step_cap(rr, s.x[3], double(s.k[1]), double(s.k[2]), double(s.k[3]),
                                                      c.vol_hz, F.disk_in, F.disk_out)));
     const bool mt = m.family == SIRIUS_METRIC_MORRIS_THORNE;
@@ -677,6 +719,7 @@ FrameDev make_frame(const sirius_frame& f, const sirius_trace_config& c) {
     F.has_horizon = (m.family == SIRIUS_METRIC_KERR_SCHILD && d >= 0 && m.M > 0) ? 1 : 0;
     const double rp = F.has_horizon ? m.M + std::sqrt(d) : -1.0;
     F.r_hor = F.has_horizon ? rp * c.horizon_factor : -1.0;
+    F.horizon_factor = c.horizon_factor;
     const double aM = std::clamp(a_star, -0.998, 0.998);
     F.r_ph_pro = 2.0 * m.M * (1.0 + std::cos((2.0 / 3.0) * std::acos(std::clamp(-aM, -1.0, 1.0))));
     const double r_ph_retro = 2.0 * m.M * (1.0 + std::cos((2.0 / 3.0) * std::acos(std::clamp(std::fabs(a_star), -1.0, 1.0))));
@@ -715,6 +758,7 @@ CfgDev make_cfg(const sirius_trace_config& c) {
     d.nbins = c.enable_volumetric ? std::min(c.n_bins, SIRIUS_MAX_BINS) : 0;
     d.vol_sub = c.vol_substeps; d.proj_period = c.projection_period; d.spiral = c.spiral_check; d.compat = c.compat;
     d.vol_j0 = c.vol_j0; d.vol_aoj = c.vol_alpha_over_j; d.vol_hz = c.vol_height_ratio; d.vol_s = c.vol_spectral_index;
+    d.integrator = c.integrator; d.symp_order = c.symplectic_order; d.symp_step = c.symplectic_step;
     for (int b = 0; b < d.nbins; ++b) {
         const double nu = d.nbins == 1 ? c.nu_min : c.nu_min * std::pow(c.nu_max / c.nu_min, double(b) / (d.nbins - 1));
         d.nu[b] = float(nu);
@@ -734,8 +778,11 @@ int validate_config(Handle* H, const sirius_trace_config& c) {
         return fail(H, SIRIUS_ERR_INVALID_ARGUMENT, "invalid volumetric parameters");
     if (c.precision != SIRIUS_PRECISION_FP64 && c.precision != SIRIUS_PRECISION_MIXED)
         return fail(H, SIRIUS_ERR_INVALID_ARGUMENT, "unknown precision mode");
-    if (c.integrator != SIRIUS_INTEGRATOR_DP45)
-        return fail(H, SIRIUS_ERR_UNSUPPORTED, "only the DP45 integrator is available in this build");
+    if (c.integrator != SIRIUS_INTEGRATOR_DP45 && c.integrator != SIRIUS_INTEGRATOR_SYMPLECTIC)
+        return fail(H, SIRIUS_ERR_INVALID_ARGUMENT, "unknown integrator");
+    if (c.integrator == SIRIUS_INTEGRATOR_SYMPLECTIC &&
+        (!(c.symplectic_step > 0) || (c.symplectic_order != 4 && c.symplectic_order != 6 && c.symplectic_order != 8)))
+        return fail(H, SIRIUS_ERR_INVALID_ARGUMENT, "symplectic_step must be > 0 and symplectic_order 4, 6 or 8");
     if (c.compat) return fail(H, SIRIUS_ERR_UNSUPPORTED, "reference-compatible mode is not available on the GPU path");
     if (c.block_size < 0 || c.block_size > 1024 || (c.block_size % 32) != 0)
         return fail(H, SIRIUS_ERR_INVALID_ARGUMENT, "block_size must be a multiple of 32 in 0..1024");

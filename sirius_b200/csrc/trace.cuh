@@ -27,7 +27,7 @@ struct FrameDev {
     double cam_t, cam_r, cam_st, cam_ct, cam_sp, cam_cp, cam_th, cam_ph;
     float aspect, tan_half_fov, cY, sY, cP, sP, cR, sR;
     // radii
-    double disk_in, disk_out, r_hor, island_r, a_star, isco, r_ph_pro;
+    double disk_in, disk_out, r_hor, island_r, a_star, isco, r_ph_pro, horizon_factor;
     double sqrt_m_gtt_cam;
 };
 
@@ -35,6 +35,8 @@ struct CfgDev {
     double atol, rtol, hmin, hmax, h0, safety, grow, shrink;
     double escape_r, decay;
     int max_steps, enable_disk, enable_vol, nbins, vol_sub, proj_period, spiral, compat;
+    int integrator, symp_order;
+    double symp_step;
     double vol_j0, vol_aoj, vol_hz, vol_s;
     float nu[SIRIUS_MAX_BINS];       // bin frequencies
     float nu_pow[SIRIUS_MAX_BINS];   // nu^-s
@@ -318,6 +320,53 @@ __device__ __forceinline__ double optimal_step(double h, double err, const CfgDe
     double fac = c.safety * pow(1.0 / err, 0.2);
     fac = fmax(c.shrink, fmin(c.grow, fac));
     return fmax(c.hmin, fmin(c.hmax, h * fac));
+}
+
+// ---------------------------------------------------------------------------
+// Symplectic integration (SymplecticIntegratorD, PHSI001A.h:43-80, 136-215,
+// 430-455) on H = 1/2 g^{mu nu} p_mu p_nu: a Yoshida composition (orders 4, 6,
+// 8; Yoshida 1990) of the kick-drift-kick leapfrog
+//   p += h/2 f(x, p);  x += h k(x, p);  p += h/2 f(x, p)
+// (k = g^{-1} p, f = 1/2 d g k k). The three phases share one RHS call site;
+// the right-hand sides run in T, the state accumulates in FP64.
+// ---------------------------------------------------------------------------
+__constant__ double kYoshida[3][15] = {
+    {1.3512071919596576, -1.7024143839193153, 1.3512071919596576},
+    {0.78451361047756, 0.23557321335936, -1.17767998417887, 1.31518632068391, -1.17767998417887,
+     0.23557321335936, 0.78451361047756},
+    {0.74167036435061, -0.40910082580003, 0.19075471029623, -0.57386247111608, 0.29906418130365,
+     0.33462491824529, 0.31529309239676, -0.79688793935291, 0.31529309239676, 0.33462491824529,
+     0.29906418130365, -0.57386247111608, 0.19075471029623, -0.40910082580003, 0.74167036435061}};
+
+template <class T>
+__device__ __noinline__ void symplectic_step(const MetricDev& m, int order, double h, double x[4], double p[4]) {
+    const int row = order >= 8 ? 2 : (order >= 6 ? 1 : 0);
+    const int n = row == 2 ? 15 : (row == 1 ? 7 : 3);
+#pragma unroll 1
+    for (int s = 0; s < n; ++s) {
+        const double hs = kYoshida[row][s] * h;
+#pragma unroll 1
+        for (int ph = 0; ph < 3; ++ph) {
+            T X[4], P[4], k[4], f[4];
+#pragma unroll
+            for (int i = 0; i < 4; ++i) { X[i] = T(x[i]); P[i] = T(p[i]); }
+            rhs<T>(m, X, P, k, f);
+            if (ph == 1) {
+#pragma unroll
+                for (int i = 0; i < 4; ++i) x[i] += hs * double(k[i]);
+            } else {
+#pragma unroll
+                for (int i = 0; i < 4; ++i) p[i] += 0.5 * hs * double(f[i]);
+            }
+        }
+    }
+}
+
+// The Kerr-Schild radius r(x, y, z) (r^4 - (R^2 - a^2) r^2 - a^2 z^2 = 0), FP64.
+__device__ __forceinline__ double ks_radius(const MetricDev& m, const double x[4]) {
+    const double R2 = x[1] * x[1] + x[2] * x[2] + x[3] * x[3], Rm2 = R2 - m.a2;
+    const double sd = sqrt(fmax(Rm2 * Rm2 + 4.0 * m.a2 * x[3] * x[3], 1e-20));
+    return sqrt(fmax(0.5 * (Rm2 + sd), 1e-10));
 }
 
 // Step control in FP32 for the mixed path (the factor needs a few digits only).
