@@ -166,6 +166,10 @@ typedef struct sirius_trace_config {
     int32_t projection_period;   /* FP64 constraint re-projection every N accepted steps (0 = never) */
     int32_t spiral_check;        /* 1: the reference's spiral early-out (GTRC001A.cpp:322-352) */
     double island_factor;        /* FP64 island: r_BL < island_factor * r_ph(retrograde) or r_BL < 2 r_+ */
+    double critical_band;        /* mixed precision, Kerr-Newman frames: a ray whose radial potential
+                                    R(r) = ((r^2+a^2)E - a L)^2 - Delta (Q + (L - a E)^2) has
+                                    |min R / (E^2 r^4)| < critical_band (it skims the photon region)
+                                    runs every step in FP64 */
     double symplectic_step;      /* fixed d-lambda of the symplectic integrator */
     int32_t symplectic_order;    /* 4, 6 or 8 (Yoshida) */
     int32_t block_size;          /* threads per block (0 = autotuned / default) */

@@ -84,7 +84,7 @@ class TraceConfig(C.Structure):
                 ("vol_spectral_index", C.c_double), ("vol_substeps", C.c_int32),
                 ("integrator", C.c_int32), ("precision", C.c_int32), ("compat", C.c_int32),
                 ("projection_period", C.c_int32), ("spiral_check", C.c_int32),
-                ("island_factor", C.c_double), ("symplectic_step", C.c_double),
+                ("island_factor", C.c_double), ("critical_band", C.c_double), ("symplectic_step", C.c_double),
                 ("symplectic_order", C.c_int32), ("block_size", C.c_int32),
                 ("refill_threshold", C.c_int32), ("blocks_per_sm", C.c_int32),
                 ("watchdog_ms", C.c_int32), ("reserved", C.c_int32 * 5)]
@@ -158,6 +158,7 @@ def default_config(**overrides):
     c.projection_period = 1
     c.spiral_check = 0
     c.island_factor = 1.5
+    c.critical_band = 0.05
     c.symplectic_step = 0.01
     c.symplectic_order = 4
     c.block_size = 0

@@ -81,8 +81,27 @@ struct Ray {
     float min_r, null_max, tphi, prev_z;
     int steps, rejected, attempts, ncross, eq, fp64_steps;
     int frame;
+    int crit;  // mixed path: the ray skims the photon region, every step in FP64
     long long idx;
 };
+
+// Kerr-Newman radial potential of a null ray, R(r) = ((r^2+a^2) E - a L)^2 -
+// Delta (Q + (L - a E)^2), Delta = r^2 - 2 M r + a^2 + Q_e^2: a double root marks
+// the critical curve. Returns min R / (E^2 r^4) over the photon region
+// r in [1.0001 r_+, 4.5 M] (48 samples).
+__device__ __noinline__ double radial_potential_gap(const MetricDev& m, double rp, double E, double L, double Q) {
+    double best = 1e300;
+    const double r0 = 1.0001 * rp, r1 = 4.5 * m.M;
+    for (int i = 0; i < 48; ++i) {
+        const double r = r0 + (r1 - r0) * (i / 47.0);
+        const double A = (r * r + m.a2) * E - m.a * L;
+        const double D = r * r - 2.0 * m.M * r + m.a2 + m.Q2;
+        const double La = L - m.a * E;
+        const double R = (A * A - D * (Q + La * La)) / (E * E * r * r * r * r);
+        best = fmin(best, R);
+    }
+    return best;
+}
 
 __device__ __forceinline__ void write_default_crossings(sirius_ray_result* R) {
 #pragma unroll
@@ -135,6 +154,14 @@ __device__ __noinline__ void begin_ray(const Params& P, Ray<MIXED>& s, long long
     s.tphi = 0.f;
     s.prev_z = float(s.x[3]);
     s.steps = s.rejected = s.attempts = s.ncross = s.eq = s.fp64_steps = 0;
+    s.crit = 0;
+    if (MIXED && F.gate && P.c.crit_band > 0.0) {
+        InvForm GF;
+        inv_form(F.m, s.x, GF);
+        float E, L, Q;
+        invariants(F.m, GF, s.x, s.p, E, L, Q);
+        s.crit = fabs(radial_potential_gap(F.m, F.r_plus, double(E), double(L), double(Q))) < P.c.crit_band;
+    }
     if (P.results) {
         sirius_ray_result* R = P.results + idx;
         write_default_crossings(R);
@@ -155,7 +182,7 @@ __device__ __noinline__ void begin_ray(const Params& P, Ray<MIXED>& s, long long
         R->impact_parameter = b;
     }
     if (vol)
-        for (int b = 0; b < P.c.nbins; ++b) { vol[2 * b * blockDim.x] = 0.f; vol[(2 * b + 1) * blockDim.x] = 0.f; }
+        for (int b = 0; b < P.c.nbins; ++b) { vol[2 * b * blockDim.x] = 0.f; vol[(2 * b + 1) * blockDim.x] = 1.f; }
 }
 
 template <bool MIXED>
@@ -189,10 +216,10 @@ __device__ __noinline__ void end_ray(const Params& P, const Ray<MIXED>& s, int o
     R->null_drift_max = s.null_max;
     R->null_final = float(fabs(inv_apply(F.m, IF, s.p, s.p)));
     R->magnification = magnification;
-    float tau = 0.f;
+    float tmin = 1.f;
     if (vol)
-        for (int b = 0; b < P.c.nbins; ++b) tau = fmaxf(tau, vol[(2 * b + 1) * blockDim.x]);
-    R->optical_depth = tau;
+        for (int b = 0; b < P.c.nbins; ++b) tmin = fminf(tmin, vol[(2 * b + 1) * blockDim.x]);
+    R->optical_depth = tmin > 0.f ? -logf(tmin) : 1e30f;
     R->fp64_steps = s.fp64_steps;
     R->flags = flags;
 }
@@ -202,7 +229,7 @@ __device__ __noinline__ void end_ray(const Params& P, const Ray<MIXED>& s, int o
 // marches the chord, GTRC001A.cpp:943-958), camera-first accumulation per bin:
 // I_b += T_b S (1 - e^-dtau), T_b = e^-tau_b,
 //   j = j0 r^-2 exp(-z^2/(2 (h_z r)^2)) nu_em^-s, alpha = c_a j,
-//   dtau = alpha (nu_cam/g) dl, S = g^3 / c_a.  (vol: [2b] = I_b, [2b+1] = tau_b, stride blockDim)
+//   dtau = alpha (nu_cam/g) dl, S = g^3 / c_a.  (vol: [2b] = I_b, [2b+1] = T_b, stride blockDim)
 __device__ __noinline__ void volumetric_segment(const Params& P, const FrameDev& F, const double x0[4],
                                                 const double x1[4], const float k0[4], const float k1[4],
                                                 const double p[4], double h, float* vol) {
@@ -235,11 +262,11 @@ __device__ __noinline__ void volumetric_segment(const Params& P, const FrameDev&
         for (int b = 0; b < c.nbins; ++b) {
             const float dtau = dt0 * c.nu_pow[b];
             float& I = vol[2 * b * blockDim.x];
-            float& tau = vol[(2 * b + 1) * blockDim.x];
+            float& Tr = vol[(2 * b + 1) * blockDim.x];  // transmittance e^-tau to the camera
             // 1 - e^-x by its series while x is small (no special-function unit needed)
             const float om = dtau < 1e-3f ? dtau * (1.f - dtau * (0.5f - dtau * (1.f / 6.f))) : 1.f - __expf(-dtau);
-            I += __expf(-tau) * S * om;
-            tau += dtau;
+            I += Tr * S * om;
+            Tr *= 1.f - om;
         }
     }
 }
@@ -306,7 +333,8 @@ __device__ __forceinline__ int advance(const Params& P, Ray<MIXED>& s, float& ma
     if constexpr (MIXED) {
         // FP64 island: inside island_factor * r_ph (retrograde) or near the horizon
         const double R2 = s.x[1] * s.x[1] + s.x[2] * s.x[2] + s.x[3] * s.x[3];
-        island = (m.family == SIRIUS_METRIC_MORRIS_THORNE) ? (s.x[1] < F.island_r) : (R2 < F.island_r * F.island_r);
+        island = s.crit ||
+                 ((m.family == SIRIUS_METRIC_MORRIS_THORNE) ? (s.x[1] < F.island_r) : (R2 < F.island_r * F.island_r));
     }
     const bool symp = c.integrator == SIRIUS_INTEGRATOR_SYMPLECTIC;
     if (symp) {
@@ -314,8 +342,7 @@ __device__ __forceinline__ int advance(const Params& P, Ray<MIXED>& s, float& ma
         // does (h0 min(1, ((r - r_+)/r_+)^2), PHSI001A.h:260-263); always accepted
         double hs = c.symp_step;
         if (F.has_horizon) {
-            const double rp = F.r_hor / F.horizon_factor;
-            const double q = (ks_radius(m, s.x) - rp) / rp;
+            const double q = (ks_radius(m, s.x) - F.r_plus) / F.r_plus;
             hs = fmax(c.hmin, hs * fmin(1.0, q * q));
         }
         s.h = hs;
@@ -719,7 +746,9 @@ FrameDev make_frame(const sirius_frame& f, const sirius_trace_config& c) {
     F.has_horizon = (m.family == SIRIUS_METRIC_KERR_SCHILD && d >= 0 && m.M > 0) ? 1 : 0;
     const double rp = F.has_horizon ? m.M + std::sqrt(d) : -1.0;
     F.r_hor = F.has_horizon ? rp * c.horizon_factor : -1.0;
-    F.horizon_factor = c.horizon_factor;
+    F.r_plus = rp;
+    // the radial-potential gate applies to Kerr-Newman frames (separable: no Lambda term)
+    F.gate = (F.has_horizon && std::fabs(m.Lambda) <= 1e-15) ? 1 : 0;
     const double aM = std::clamp(a_star, -0.998, 0.998);
     F.r_ph_pro = 2.0 * m.M * (1.0 + std::cos((2.0 / 3.0) * std::acos(std::clamp(-aM, -1.0, 1.0))));
     const double r_ph_retro = 2.0 * m.M * (1.0 + std::cos((2.0 / 3.0) * std::acos(std::clamp(std::fabs(a_star), -1.0, 1.0))));
@@ -759,6 +788,7 @@ CfgDev make_cfg(const sirius_trace_config& c) {
     d.vol_sub = c.vol_substeps; d.proj_period = c.projection_period; d.spiral = c.spiral_check; d.compat = c.compat;
     d.vol_j0 = c.vol_j0; d.vol_aoj = c.vol_alpha_over_j; d.vol_hz = c.vol_height_ratio; d.vol_s = c.vol_spectral_index;
     d.integrator = c.integrator; d.symp_order = c.symplectic_order; d.symp_step = c.symplectic_step;
+    d.crit_band = c.critical_band;
     for (int b = 0; b < d.nbins; ++b) {
         const double nu = d.nbins == 1 ? c.nu_min : c.nu_min * std::pow(c.nu_max / c.nu_min, double(b) / (d.nbins - 1));
         d.nu[b] = float(nu);
@@ -887,7 +917,7 @@ int sirius_cuda_default_config(sirius_trace_config* c) {
     c->enable_volumetric = 0; c->n_bins = 0; c->nu_min = 1e-2; c->nu_max = 1e2; c->vol_j0 = 1.0;
     c->vol_alpha_over_j = 0.1; c->vol_height_ratio = 0.1; c->vol_spectral_index = 0.7; c->vol_substeps = 4;
     c->integrator = SIRIUS_INTEGRATOR_DP45; c->precision = SIRIUS_PRECISION_FP64; c->compat = 0;
-    c->projection_period = 1; c->spiral_check = 0; c->island_factor = 1.5; c->symplectic_step = 0.01;
+    c->projection_period = 1; c->spiral_check = 0; c->island_factor = 1.5; c->critical_band = 0.05; c->symplectic_step = 0.01;
     c->symplectic_order = 4; c->block_size = 0; c->refill_threshold = 0; c->blocks_per_sm = 0; c->watchdog_ms = 30000;
     return SIRIUS_OK;
 }

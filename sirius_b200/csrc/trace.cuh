@@ -22,12 +22,12 @@ constexpr double kPi = 3.14159265358979323846;
 struct FrameDev {
     MetricDev m;
     long long ray_offset, n_rays;
-    int width, height, projection, has_horizon;
+    int width, height, projection, has_horizon, gate;
     // camera
     double cam_t, cam_r, cam_st, cam_ct, cam_sp, cam_cp, cam_th, cam_ph;
     float aspect, tan_half_fov, cY, sY, cP, sP, cR, sR;
     // radii
-    double disk_in, disk_out, r_hor, island_r, a_star, isco, r_ph_pro, horizon_factor;
+    double disk_in, disk_out, r_hor, r_plus, island_r, a_star, isco, r_ph_pro;
     double sqrt_m_gtt_cam;
 };
 
@@ -36,7 +36,7 @@ struct CfgDev {
     double escape_r, decay;
     int max_steps, enable_disk, enable_vol, nbins, vol_sub, proj_period, spiral, compat;
     int integrator, symp_order;
-    double symp_step;
+    double symp_step, crit_band;
     double vol_j0, vol_aoj, vol_hz, vol_s;
     float nu[SIRIUS_MAX_BINS];       // bin frequencies
     float nu_pow[SIRIUS_MAX_BINS];   // nu^-s
