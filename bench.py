@@ -331,9 +331,6 @@ def main():
         img_mixed = d_image.cpu().numpy().astype(np.float64)
         spc_mixed = d_spectra.cpu().numpy().reshape(total, N_BINS).astype(np.float64)
         eng.configure(workload_config(abi, abi.PRECISION_FP64))
-        cfg64 = workload_config(abi, abi.PRECISION_FP64)
-        cfg64.blocks_per_sm = -1
-        eng.configure(cfg64)
         ms64 = []
         for i in range(3):
             step()

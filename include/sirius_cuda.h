@@ -173,8 +173,12 @@ typedef struct sirius_trace_config {
     double symplectic_step;      /* fixed d-lambda of the symplectic integrator */
     int32_t symplectic_order;    /* 4, 6 or 8 (Yoshida) */
     int32_t block_size;          /* threads per block (0 = autotuned / default) */
-    int32_t refill_threshold;    /* refill a warp when fewer than this many lanes are live (1..32) */
-    int32_t blocks_per_sm;       /* persistent grid = SMs * blocks_per_sm (0 = occupancy based) */
+    int32_t refill_threshold;    /* persistent mode: refill a warp when fewer than this many lanes are
+                                    live (1..32; 0 = 1, i.e. only once the whole warp is done, which keeps
+                                    the 32 rays of a warp on neighbouring pixels and so coherent) */
+    int32_t blocks_per_sm;       /* 0 = one thread per ray, a block per 128 consecutive rays (default);
+                                    1..4 = persistent grid of SMs * blocks_per_sm blocks that pull rays
+                                    from a queue; < 0 = persistent, occupancy-sized grid */
     int32_t watchdog_ms;         /* bound on any spin-wait inside the kernels */
     int32_t reserved[5];
 } sirius_trace_config;
@@ -286,8 +290,9 @@ int sirius_cuda_dp45_step(sirius_cuda_handle handle, const sirius_metric* metric
 /* ---- statistics of the last trace call ---------------------------------------- */
 int sirius_cuda_last_stats(sirius_cuda_handle handle, sirius_launch_stats* out_stats);
 
-/* ---- autotuner: times block size x refill threshold x blocks/SM on the given
- * frames and stores the best setting in the handle's configuration.
+/* ---- autotuner: times the one-thread-per-ray launch and the persistent launch
+ * (blocks/SM x refill threshold) on the given frames and stores the best
+ * setting in the handle's configuration.
  * The chosen values are written to *out_config (may be NULL). ---------------- */
 int sirius_cuda_autotune(sirius_cuda_handle handle, const sirius_frame* frames, int32_t n_frames,
                          sirius_trace_config* out_config);

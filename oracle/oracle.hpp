@@ -875,14 +875,35 @@ void locate_equator(const sirius_metric& m, const sirius_trace_config& c, const 
     xc[3] = R(0);
 }
 
-// Volumetric emission of the engine (the BASELINE profile): over one step segment
-// x0 -> x1 of affine length h, Gauss-Legendre points (vol_substeps of them, 1..4)
-// on the step's cubic Hermite interpolant (the reference marches the chord with
-// midpoints, GTRC001A.cpp:943-958),
-// camera-first accumulation per bin:
+// Volumetric emission of the engine: over one step segment x0 -> x1 of affine
+// length h, Gauss-Legendre points (vol_substeps of them, 1..4) on the step's
+// cubic Hermite interpolant (the reference marches the chord with midpoints,
+// GTRC001A.cpp:943-958), restricted to the part of the step inside the
+// emitting annulus r_in <= r <= r_out (the annulus edges are discontinuities of
+// j, so the step is split there), camera-first accumulation per bin:
 //   I_b += T_b S (1 - e^{-dtau}),  T_b *= e^{-dtau},
-//   j = j0 r^-2 exp(-z^2 / (2 (h_z r)^2)) nu_em^-s,  alpha = c_a j,
-//   dtau = alpha (nu_cam / g) dl,  S = g^3 / c_a   (I_b stored as nu_b^3 I_inv).
+//   j = j0 r^-2 exp(-z^2 / (2 (h_z r)^2)) nu_em^-s  (|z| <= kVolCutoff h_z r),
+//   alpha = c_a j,  dtau = alpha (nu_cam / g) dl,  S = g^3 / c_a
+// (I_b stored as nu_b^3 I_inv).
+constexpr double kVolCutoff = 6.0;  // emission beyond 6 scale heights (e^-18 of the peak) is dropped
+
+// The Hermite parameter in [0, 1] at which r crosses `edge` between the step's
+// ends, by bisection (r(0) and r(1) lie on opposite sides of `edge`).
+template <class R>
+R annulus_edge(const sirius_metric& m, const R x0[4], const R x1[4], const R k0[4], const R k1[4], R h, R r0,
+               R edge) {
+    R lo = R(0), hi = R(1);
+    const bool inside_lo = r0 < edge;
+    for (int it = 0; it < 30; ++it) {
+        const R f = R(0.5) * (lo + hi);
+        R xs[4], d[4];
+        hermite_point(x0, x1, k0, k1, h, f, xs);
+        if ((radial(m, xs, d) < edge) == inside_lo) lo = f;
+        else hi = f;
+    }
+    return R(0.5) * (lo + hi);
+}
+
 template <class R>
 void volumetric_segment(const TraceContext& ctx, const R x0[4], const R x1[4], const R k0[4], const R k1[4],
                         const R p[4], R h, R sqrt_m_gtt_cam, const R* nu, Spectra& sp) {
@@ -893,18 +914,26 @@ void volumetric_segment(const TraceContext& ctx, const R x0[4], const R x1[4], c
     gauss_legendre(c.vol_substeps, n, gx, gw);
     const R E = -p[0], Lz = x1[1] * p[2] - x1[2] * p[1];  // p is the state at x1
     const R nu_cam = E / sqrt_m_gtt_cam;
+    const R rin = R(ctx.disk_inner), rout = R(ctx.disk_outer);
+    R d[4];
+    const R r0 = radial(ctx.metric, x0, d), r1 = radial(ctx.metric, x1, d);
+    const bool in0 = r0 >= rin && r0 <= rout, in1 = r1 >= rin && r1 <= rout;
+    R fa = R(0), fb = R(1);
+    if (in0 && !in1) fb = annulus_edge(ctx.metric, x0, x1, k0, k1, h, r0, r1 < rin ? rin : rout);
+    if (!in0 && in1) fa = annulus_edge(ctx.metric, x0, x1, k0, k1, h, r0, r0 < rin ? rin : rout);
+    const R span = fb - fa;
     for (int s = 0; s < n; ++s) {
-        const R f = R(gx[s]);
-        R xs[4], d[4];
+        const R f = fa + span * R(gx[s]);
+        R xs[4];
         hermite_point(x0, x1, k0, k1, h, f, xs);  // the step's cubic Hermite interpolant
         const R r = radial(ctx.metric, xs, d);
-        if (r < R(ctx.disk_inner) || r > R(ctx.disk_outer)) continue;
+        if (r < rin || r > rout) continue;
         const R zr = xs[3] / (R(c.vol_height_ratio) * r);
-        if (std::abs(zr) > R(4)) continue;
+        if (std::abs(zr) > R(kVolCutoff)) continue;
         const R jsp = R(c.vol_j0) / (r * r) * std::exp(R(-0.5) * zr * zr);
         const R g = redshift_exact(ctx, xs, r, E, Lz, sqrt_m_gtt_cam);
         if (!(g > R(0))) continue;
-        const R dl = h * R(gw[s]);
+        const R dl = h * span * R(gw[s]);
         const R S = g * g * g / R(c.vol_alpha_over_j);
         for (int b = 0; b < c.n_bins; ++b) {
             const R nu_em = nu[b] / g;
@@ -917,19 +946,21 @@ void volumetric_segment(const TraceContext& ctx, const R x0[4], const R x1[4], c
     }
 }
 
-// Largest affine step inside the emitting volume: half the local Gaussian scale
-// height h_z r over the spatial speed |dx/dl| (so the per-step quadrature, and
-// hence the spectra, do not depend on the step sequence). Infinite outside.
+// Largest affine step near the emitting volume, so that the per-step
+// quadrature, and hence the spectra, do not depend on the step sequence: half
+// the local scale height h_z r over the spatial speed |dx/dl| inside the
+// emitting region (r_in <= r <= r_out, |z| <= kVolCutoff h_z r), and outside it
+// the distance to that region, so that no step jumps into its interior.
 template <class R>
 R volume_step_cap(const TraceContext& ctx, const R x[4], const R k[4]) {
     const auto& c = ctx.cfg;
     R d[4];
     const R r = radial(ctx.metric, x, d);
-    if (r < R(0.9) * R(ctx.disk_inner) || r > R(1.1) * R(ctx.disk_outer)) return R(1e300);
-    const R H = R(c.vol_height_ratio) * r;
-    if (std::abs(x[3]) > R(5) * H) return R(1e300);
+    const R rin = R(ctx.disk_inner), rout = R(ctx.disk_outer);
+    const R H = R(c.vol_height_ratio) * std::min(std::max(r, rin), rout);
+    const R dist = std::max(std::max(rin - r, r - rout), std::abs(x[3]) - R(kVolCutoff) * H);
     const R v = std::sqrt(k[1] * k[1] + k[2] * k[2] + k[3] * k[3]);
-    return R(0.5) * H / std::max(v, R(1e-3));
+    return std::max(R(0.5) * H, dist) / std::max(v, R(1e-3));
 }
 
 // GeodesicTracer volumetric helpers (GTRC001A.cpp:834-912) — compat gray march.

@@ -49,6 +49,8 @@ struct Params {
     int* status;                          // [0] watchdog flag
     int persistent;
     int refill_threshold;
+    int family;                           // >= 0: trace only the rays of frames of this family
+    unsigned long long* clock0;           // launch start on the device clock (first warp stamps it)
     unsigned long long watchdog_ns;       // globaltimer bound for the whole launch, per warp
     CfgDev c;
 };
@@ -129,11 +131,11 @@ __device__ void invariants(const MetricDev& m, const InvForm& F, const double x[
     Q = float(pth * pth + ct * ct * (-m.a2 * e * e + L * L / (st * st)));
 }
 
-template <bool MIXED>
-__device__ __noinline__ void begin_ray(const Params& P, Ray<MIXED>& s, long long idx, float* vol) {
+template <bool MIXED, int FAM>
+__device__ __noinline__ void begin_ray(const Params& P, Ray<MIXED>& s, long long idx, int frame, float* vol) {
     using K = typename Ray<MIXED>::K;
     s.idx = idx;
-    s.frame = P.n_frames > 1 ? find_frame(P.frames, P.n_frames, idx) : 0;
+    s.frame = frame;
     const FrameDev& F = P.frames[s.frame];
     double dir[4];
     if (P.host_rays) {
@@ -146,7 +148,7 @@ __device__ __noinline__ void begin_ray(const Params& P, Ray<MIXED>& s, long long
     init_state(F, dir, s.x, s.p);
     K xk[4], pk[4];
     for (int i = 0; i < 4; ++i) { xk[i] = K(s.x[i]); pk[i] = K(s.p[i]); }
-    rhs<K>(F.m, xk, pk, s.k, s.k + 4);
+    rhs<K, FAM>(F.m, xk, pk, s.k, s.k + 4);
     s.h = P.c.h0;
     s.intensity = 0.0;
     s.min_r = 1e10f;
@@ -172,7 +174,7 @@ __device__ __noinline__ void begin_ray(const Params& P, Ray<MIXED>& s, long long
         R->E0 = E; R->Lz0 = L; R->Carter0 = Q;
         // impact parameter heuristic (GTRC001A.cpp:208-233)
         float b = 0.f;
-        if (F.m.family != SIRIUS_METRIC_MORRIS_THORNE) {
+        if (!is_family<FAM>(F.m, SIRIUS_METRIC_MORRIS_THORNE)) {
             const double k1 = double(s.k[1]), k2 = double(s.k[2]), k3 = double(s.k[3]);
             const double R0 = sqrt(s.x[1] * s.x[1] + s.x[2] * s.x[2] + s.x[3] * s.x[3]);
             const double vm = sqrt(k1 * k1 + k2 * k2 + k3 * k3);
@@ -224,9 +226,28 @@ __device__ __noinline__ void end_ray(const Params& P, const Ray<MIXED>& s, int o
     R->flags = flags;
 }
 
+// A point of the step's cubic Hermite interpolant at parameter q in [0, 1].
+__device__ __forceinline__ void hermite_xyz(const double x0[4], const double x1[4], const float k0[4],
+                                            const float k1[4], double h, double q, float& xs, float& ys, float& zs) {
+    const double q2 = q * q, q3 = q2 * q;
+    const double h00 = 2.0 * q3 - 3.0 * q2 + 1.0, h10 = (q3 - 2.0 * q2 + q) * h, h01 = -2.0 * q3 + 3.0 * q2,
+                 h11 = (q3 - q2) * h;
+    xs = float(h00 * x0[1] + h10 * k0[1] + h01 * x1[1] + h11 * k1[1]);
+    ys = float(h00 * x0[2] + h10 * k0[2] + h01 * x1[2] + h11 * k1[2]);
+    zs = float(h00 * x0[3] + h10 * k0[3] + h01 * x1[3] + h11 * k1[3]);
+}
+
+__device__ __forceinline__ float ks_r(const MetricDev& m, float x, float y, float z) {
+    const float a2 = float(m.a2), R2 = x * x + y * y + z * z, Rm2 = R2 - a2;
+    const float sd = sqrtf(fmaxf(Rm2 * Rm2 + 4.f * a2 * z * z, 1e-20f));
+    return sqrtf(fmaxf(0.5f * (Rm2 + sd), 1e-10f));
+}
+
 // Volumetric transfer over the accepted segment x0 -> x1 (affine length h):
-// midpoint samples on the step's cubic Hermite interpolant (the reference
-// marches the chord, GTRC001A.cpp:943-958), camera-first accumulation per bin:
+// Gauss-Legendre points on the step's cubic Hermite interpolant (the reference
+// marches the chord with midpoints, GTRC001A.cpp:943-958) over the part of the
+// step inside the emitting annulus r_in <= r <= r_out (its edges, where j jumps,
+// are located by bisection), camera-first accumulation per bin:
 // I_b += T_b S (1 - e^-dtau), T_b = e^-tau_b,
 //   j = j0 r^-2 exp(-z^2/(2 (h_z r)^2)) nu_em^-s, alpha = c_a j,
 //   dtau = alpha (nu_cam/g) dl, S = g^3 / c_a.  (vol: [2b] = I_b, [2b+1] = T_b, stride blockDim)
@@ -238,36 +259,70 @@ __device__ __noinline__ void volumetric_segment(const Params& P, const FrameDev&
     const float E = float(-p[0]);
     const float Lz = float(x1[1] * p[2] - x1[2] * p[1]);
     const float nu_cam = E / float(F.sqrt_m_gtt_cam);
-    for (int s = 0; s < nq; ++s) {
-        // Gauss-Legendre point on the step's cubic Hermite interpolant
-        const double q = double(kGLx[nq - 1][s]), q2 = q * q, q3 = q2 * q;
-        const double h00 = 2.0 * q3 - 3.0 * q2 + 1.0, h10 = (q3 - 2.0 * q2 + q) * h, h01 = -2.0 * q3 + 3.0 * q2,
-                     h11 = (q3 - q2) * h;
-        const float xs = float(h00 * x0[1] + h10 * k0[1] + h01 * x1[1] + h11 * k1[1]);
-        const float ys = float(h00 * x0[2] + h10 * k0[2] + h01 * x1[2] + h11 * k1[2]);
-        const float zs = float(h00 * x0[3] + h10 * k0[3] + h01 * x1[3] + h11 * k1[3]);
-        KSPieces<float> KP;
-        ks_pieces(F.m, xs, ys, zs, KP);
-        const float r = KP.r;
-        if (r < float(F.disk_in) || r > float(F.disk_out)) continue;
+    const float rin = float(F.disk_in), rout = float(F.disk_out);
+    const float r0 = ks_r(F.m, float(x0[1]), float(x0[2]), float(x0[3]));
+    const float r1 = ks_r(F.m, float(x1[1]), float(x1[2]), float(x1[3]));
+    // steps that cannot reach the emitting region (the step cap keeps a step
+    // that starts outside it from jumping in)
+    const float hz = float(c.vol_hz), z0 = float(x0[3]), z1 = float(x1[3]);
+    if (r0 > rout && r1 > rout) return;
+    if (z0 * z1 > 0.f && fabsf(z0) > float(kVolCutoff) * hz * fminf(fmaxf(r0, rin), rout) &&
+        fabsf(z1) > float(kVolCutoff) * hz * fminf(fmaxf(r1, rin), rout))
+        return;
+    const bool in0 = r0 >= rin && r0 <= rout, in1 = r1 >= rin && r1 <= rout;
+    double fa = 0.0, fb = 1.0;
+    if (in0 != in1) {
+        const float edge = in0 ? (r1 < rin ? rin : rout) : (r0 < rin ? rin : rout);
+        const bool below_lo = r0 < edge;
+        double lo = 0.0, hi = 1.0;
+        for (int it = 0; it < 24; ++it) {
+            const double q = 0.5 * (lo + hi);
+            float xs, ys, zs;
+            hermite_xyz(x0, x1, k0, k1, h, q, xs, ys, zs);
+            if ((ks_r(F.m, xs, ys, zs) < edge) == below_lo) lo = q;
+            else hi = q;
+        }
+        if (in0) fb = 0.5 * (lo + hi);
+        else fa = 0.5 * (lo + hi);
+    }
+    const double span = fb - fa;
+    // per Gauss-Legendre point: optical depth per unit nu^-s and source function
+    float dt0[4], S[4];
+#pragma unroll
+    for (int s = 0; s < 4; ++s) {
+        dt0[s] = 0.f;
+        S[s] = 0.f;
+        if (s >= nq) continue;
+        float xs, ys, zs;
+        hermite_xyz(x0, x1, k0, k1, h, fa + span * double(kGLx[nq - 1][s]), xs, ys, zs);
+        const float r = ks_r(F.m, xs, ys, zs);
+        if (r < rin || r > rout) continue;
         const float zr = zs / (float(c.vol_hz) * r);
-        if (fabsf(zr) > 4.f) continue;
+        if (fabsf(zr) > float(kVolCutoff)) continue;
         const float g = kepler_g<float>(F.m, xs, ys, zs, r, E, Lz, float(F.sqrt_m_gtt_cam));
         if (!(g > 0.f)) continue;
-        const float dl = float(h) * kGLw[nq - 1][s];
+        const float dl = float(h * span) * kGLw[nq - 1][s];
         const float jsp = float(c.vol_j0) / (r * r) * __expf(-0.5f * zr * zr);
         const float gs = __powf(g, float(c.vol_s));  // nu_em^-s = (g/nu_b)^s
-        const float dt0 = float(c.vol_aoj) * jsp * gs * (nu_cam / g) * dl;
-        const float S = g * g * g / float(c.vol_aoj);
-        for (int b = 0; b < c.nbins; ++b) {
-            const float dtau = dt0 * c.nu_pow[b];
-            float& I = vol[2 * b * blockDim.x];
-            float& Tr = vol[(2 * b + 1) * blockDim.x];  // transmittance e^-tau to the camera
+        dt0[s] = float(c.vol_aoj) * jsp * gs * (nu_cam / g) * dl;
+        S[s] = g * g * g / float(c.vol_aoj);
+    }
+    if (dt0[0] == 0.f && dt0[1] == 0.f && dt0[2] == 0.f && dt0[3] == 0.f) return;
+    for (int b = 0; b < c.nbins; ++b) {
+        float& I = vol[2 * b * blockDim.x];
+        float& Tr = vol[(2 * b + 1) * blockDim.x];  // transmittance e^-tau to the camera
+        float Ib = I, Tb = Tr;
+        const float cb = c.nu_pow[b];
+#pragma unroll
+        for (int s = 0; s < 4; ++s) {
+            const float dtau = dt0[s] * cb;
             // 1 - e^-x by its series while x is small (no special-function unit needed)
             const float om = dtau < 1e-3f ? dtau * (1.f - dtau * (0.5f - dtau * (1.f / 6.f))) : 1.f - __expf(-dtau);
-            I += Tr * S * om;
-            Tr *= 1.f - om;
+            Ib += Tb * S[s] * om;
+            Tb *= 1.f - om;
         }
+        I = Ib;
+        Tr = Tb;
     }
 }
 
@@ -299,28 +354,29 @@ __device__ __noinline__ bool record_crossing(const Params& P, const FrameDev& F,
 // The FP64 island attempt of the mixed path: f(x, p) recomputed in FP64, a DP45
 // attempt in FP64; the derivative at the candidate point returned in float for
 // the FP32 steps that may follow.
+template <int FAM>
 __device__ __noinline__ double island_attempt(const MetricDev& m, const CfgDev& c, const double x[4],
                                               const double p[4], double h, double xn[4], double pn[4], float k7f[8]) {
     double k1[8], k7[8];
-    rhs<double>(m, x, p, k1, k1 + 4);
-    const double err = dp45_attempt<double>(m, c, x, p, h, k1, xn, pn, k7);
+    rhs<double, FAM>(m, x, p, k1, k1 + 4);
+    const double err = dp45_attempt_lowreg<FAM>(m, c, x, p, h, k1, xn, pn, k7);
 #pragma unroll
     for (int i = 0; i < 8; ++i) k7f[i] = float(k7[i]);
     return err;
 }
 
 // f(x, p) of the current state in the storage precision of the path.
-template <bool MIXED>
+template <bool MIXED, int FAM>
 __device__ __noinline__ void refresh_derivative(const MetricDev& m, Ray<MIXED>& s) {
     using K = typename Ray<MIXED>::K;
     K xk[4], pk[4];
     for (int i = 0; i < 4; ++i) { xk[i] = K(s.x[i]); pk[i] = K(s.p[i]); }
-    rhs<K>(m, xk, pk, s.k, s.k + 4);
+    rhs<K, FAM>(m, xk, pk, s.k, s.k + 4);
 }
 
 // One iteration of the ray state machine: a DP45 attempt, and on acceptance
 // the termination checks. Returns -1 while the ray continues, else its outcome.
-template <bool MIXED>
+template <bool MIXED, int FAM>
 __device__ __forceinline__ int advance(const Params& P, Ray<MIXED>& s, float& magnification, int& flags, float* vol) {
     using K = typename Ray<MIXED>::K;
     const FrameDev& F = P.frames[s.frame];
@@ -334,7 +390,8 @@ __device__ __forceinline__ int advance(const Params& P, Ray<MIXED>& s, float& ma
         // FP64 island: inside island_factor * r_ph (retrograde) or near the horizon
         const double R2 = s.x[1] * s.x[1] + s.x[2] * s.x[2] + s.x[3] * s.x[3];
         island = s.crit ||
-                 ((m.family == SIRIUS_METRIC_MORRIS_THORNE) ? (s.x[1] < F.island_r) : (R2 < F.island_r * F.island_r));
+                 (is_family<FAM>(m, SIRIUS_METRIC_MORRIS_THORNE) ? (s.x[1] < F.island_r)
+                                                                 : (R2 < F.island_r * F.island_r));
     }
     const bool symp = c.integrator == SIRIUS_INTEGRATOR_SYMPLECTIC;
     if (symp) {
@@ -348,25 +405,25 @@ __device__ __forceinline__ int advance(const Params& P, Ray<MIXED>& s, float& ma
         s.h = hs;
 #pragma unroll
         for (int i = 0; i < 4; ++i) { xn[i] = s.x[i]; pn[i] = s.p[i]; }
-        if (MIXED && !island) symplectic_step<float>(m, c.symp_order, hs, xn, pn);
-        else symplectic_step<double>(m, c.symp_order, hs, xn, pn);
+        if (MIXED && !island) symplectic_step<float, FAM>(m, c.symp_order, hs, xn, pn);
+        else symplectic_step<double, FAM>(m, c.symp_order, hs, xn, pn);
         K xk[4], pk[4];
 #pragma unroll
         for (int i = 0; i < 4; ++i) { xk[i] = K(xn[i]); pk[i] = K(pn[i]); }
         rhs<K>(m, xk, pk, k7, k7 + 4);
         err = 0.0;
     } else if constexpr (MIXED) {
-        if (island) err = island_attempt(m, c, s.x, s.p, s.h, xn, pn, k7);
-        else err = dp45_attempt<float>(m, c, s.x, s.p, s.h, s.k, xn, pn, k7);
+        if (island) err = island_attempt<FAM>(m, c, s.x, s.p, s.h, xn, pn, k7);
+        else err = dp45_attempt<float, FAM>(m, c, s.x, s.p, s.h, s.k, xn, pn, k7);
     } else {
-        err = dp45_attempt<double>(m, c, s.x, s.p, s.h, s.k, xn, pn, k7);
+        err = dp45_attempt<double, FAM>(m, c, s.x, s.p, s.h, s.k, xn, pn, k7);
     }
     ++s.attempts;
     if (!(err <= 1.0)) {
         ++s.rejected;
         s.h = MIXED ? optimal_step_fast(s.h, isfinite(err) ? err : 1e10, c)
                     : optimal_step(s.h, isfinite(err) ? err : 1e10, c);
-        if (c.enable_vol && c.enable_disk && F.has_horizon && m.family == SIRIUS_METRIC_KERR_SCHILD) {
+        if (c.enable_vol && c.enable_disk && F.has_horizon && is_family<FAM>(m, SIRIUS_METRIC_KERR_SCHILD)) {
             InvForm RF;
             inv_form(m, s.x, RF);
             s.h = fmax(c.hmin, fmin(s.h, volume_step_cap(RF.r, s.x[3], double(s.k[1]), double(s.k[2]),
@@ -378,14 +435,14 @@ __device__ __forceinline__ int advance(const Params& P, Ray<MIXED>& s, float& ma
     }
     // accepted
     const double hstep = s.h;
-    const bool disk_on = m.family == SIRIUS_METRIC_KERR_SCHILD && c.enable_disk && F.has_horizon;
+    const bool disk_on = is_family<FAM>(m, SIRIUS_METRIC_KERR_SCHILD) && c.enable_disk && F.has_horizon;
     // equatorial crossing inside the step: locate it from the step's start state
     double xc1 = 0.0, xc2 = 0.0;
     const bool cross = disk_on && (s.x[3] * xn[3] < 0.0);
     if (cross) {
         const double hs = hermite_root(s.x[3], xn[3], double(s.k[3]), double(k7[3]), hstep) * hstep;
-        if (island || !MIXED) locate_equator<double>(m, c, s.x, s.p, hs, xc1, xc2);
-        else locate_equator<float>(m, c, s.x, s.p, hs, xc1, xc2);
+        if (island || !MIXED) locate_equator<double, FAM>(m, c, s.x, s.p, hs, xc1, xc2);
+        else locate_equator<float, FAM>(m, c, s.x, s.p, hs, xc1, xc2);
     }
     double x0[4];
     float k0f[4];
@@ -419,14 +476,14 @@ __device__ __forceinline__ int advance(const Params& P, Ray<MIXED>& s, float& ma
             dp = fmax(dp, fabs(s.p[i] - pb[i]));
             pm = fmax(pm, fabs(s.p[i]));
         }
-        if (dp > 1e-10 * pm) refresh_derivative<MIXED>(m, s);
+        if (dp > 1e-10 * pm) refresh_derivative<MIXED, FAM>(m, s);
     }
     const double rr = IF.r;
     if (float(rr) < s.min_r) s.min_r = float(rr);
     if (disk_on && c.enable_vol && !symp)
         s.h = fmax(c.hmin, fmin(s.h, volume_step_cap(rr, s.x[3], double(s.k[1]), double(s.k[2]), double(s.k[3]),
                                                      c.vol_hz, F.disk_in, F.disk_out)));
-    const bool mt = m.family == SIRIUS_METRIC_MORRIS_THORNE;
+    const bool mt = is_family<FAM>(m, SIRIUS_METRIC_MORRIS_THORNE);
 
     // winding: equatorial crossings and |d phi| (GTRC001A.cpp:294-309)
     if (!mt) {
@@ -493,7 +550,7 @@ __device__ __forceinline__ int advance(const Params& P, Ray<MIXED>& s, float& ma
 }
 
 // Persistent tracer. Dynamic shared memory: 2 * nbins floats per thread (volumetric bins).
-template <bool MIXED, int MINB>
+template <bool MIXED, int MINB, int FAM>
 __global__ void __launch_bounds__(128, MINB) trace_kernel(Params P) {
     extern __shared__ float smem[];
     float* vol = (P.c.enable_vol && P.c.nbins > 0) ? smem + threadIdx.x : nullptr;
@@ -505,11 +562,24 @@ __global__ void __launch_bounds__(128, MINB) trace_kernel(Params P) {
     int flags = 0;
     unsigned long long acc = 0, rej0 = 0, f64 = 0;
     bool exhausted = false;
-    const unsigned long long t_start = globaltimer();
+    // the watchdog bounds the whole launch: every warp measures from the first warp's start
+    unsigned long long t_start = 0;
+    if (lane == 0) {
+        const unsigned long long now = globaltimer();
+        const unsigned long long first = atomicCAS(P.clock0, 0ull, now);
+        t_start = first ? first : now;
+    }
+    t_start = __shfl_sync(kFull, t_start, 0);
 
     if (!P.persistent) {
         const long long idx = (long long)blockIdx.x * blockDim.x + threadIdx.x;
-        if (idx < P.total) { begin_ray<MIXED>(P, s, idx, vol); alive = true; }
+        if (idx < P.total) {
+            const int frame = P.n_frames > 1 ? find_frame(P.frames, P.n_frames, idx) : 0;
+            if (P.family < 0 || P.frames[frame].m.family == P.family) {
+                begin_ray<MIXED, FAM>(P, s, idx, frame, vol);
+                alive = true;
+            }
+        }
         exhausted = true;
     }
     for (unsigned iter = 0;; ++iter) {
@@ -524,25 +594,26 @@ __global__ void __launch_bounds__(128, MINB) trace_kernel(Params P) {
                 if (!alive) {
                     const unsigned long long idx = base + __popc(dead & lt_mask);
                     if (idx < (unsigned long long)P.total) {
-                        begin_ray<MIXED>(P, s, (long long)idx, vol);
+                        const int frame = P.n_frames > 1 ? find_frame(P.frames, P.n_frames, (long long)idx) : 0;
+                        begin_ray<MIXED, FAM>(P, s, (long long)idx, frame, vol);
                         alive = true;
                         magnification = 1.f;
                         flags = 0;
                     }
                 }
             }
-            if ((iter & 255u) == 0) {
-                int stop = 0;
-                if (lane == 0) {
-                    if (globaltimer() - t_start > P.watchdog_ns) atomicOr(P.status, 1);
-                    stop = *((volatile int*)P.status) & 1;
-                }
-                stop = __shfl_sync(kFull, stop, 0);
-                if (stop) {
-                    // watchdog: abandon the remaining queue and close the live rays
-                    exhausted = true;
-                    if (alive) { end_ray<MIXED>(P, s, SIRIUS_MAX_STEPS, magnification, flags, vol); alive = false; }
-                }
+        }
+        if ((iter & 255u) == 0) {
+            int stop = 0;
+            if (lane == 0) {
+                if (globaltimer() - t_start > P.watchdog_ns) atomicOr(P.status, 1);
+                stop = *((volatile int*)P.status) & 1;
+            }
+            stop = __shfl_sync(kFull, stop, 0);
+            if (stop) {
+                // watchdog: abandon the remaining queue and close the live rays
+                exhausted = true;
+                if (alive) { end_ray<MIXED>(P, s, SIRIUS_MAX_STEPS, magnification, flags, vol); alive = false; }
             }
         }
         if (__ballot_sync(kFull, alive) == 0) {
@@ -550,7 +621,7 @@ __global__ void __launch_bounds__(128, MINB) trace_kernel(Params P) {
             continue;
         }
         if (alive) {
-            const int out = advance<MIXED>(P, s, magnification, flags, vol);
+            const int out = advance<MIXED, FAM>(P, s, magnification, flags, vol);
             if (out >= 0) {
                 end_ray<MIXED>(P, s, out, magnification, flags, vol);
                 acc += s.steps;
@@ -576,20 +647,32 @@ __global__ void __launch_bounds__(128, MINB) trace_kernel(Params P) {
 using TraceFn = void (*)(Params);
 constexpr int kDefaultMinBlocks = 2;
 
-TraceFn pick_kernel(bool mixed, int minb) {
-    if (mixed) {
-        switch (minb) {
-            case 1: return trace_kernel<true, 1>;
-            case 3: return trace_kernel<true, 3>;
-            case 4: return trace_kernel<true, 4>;
-            default: return trace_kernel<true, 2>;
-        }
-    }
+template <bool MIXED, int FAM>
+TraceFn pick_minb(int minb) {
     switch (minb) {
-        case 1: return trace_kernel<false, 1>;
-        case 3: return trace_kernel<false, 3>;
-        case 4: return trace_kernel<false, 4>;
-        default: return trace_kernel<false, 2>;
+        case 1: return trace_kernel<MIXED, 1, FAM>;
+        case 3: return trace_kernel<MIXED, 3, FAM>;
+        case 4: return trace_kernel<MIXED, 4, FAM>;
+        default: return trace_kernel<MIXED, 2, FAM>;
+    }
+}
+
+// A kernel specialised for one metric family carries only that family's
+// right-hand side (a smaller loop body and register set); kAnyFamily
+// dispatches per ray. The Kerr-Schild kernels come in every register budget.
+TraceFn pick_kernel(bool mixed, int minb, int fam) {
+    switch (fam) {
+        case SIRIUS_METRIC_KERR_SCHILD:
+            return mixed ? pick_minb<true, SIRIUS_METRIC_KERR_SCHILD>(minb)
+                         : pick_minb<false, SIRIUS_METRIC_KERR_SCHILD>(minb);
+        case SIRIUS_METRIC_MORRIS_THORNE:
+            return mixed ? trace_kernel<true, 2, SIRIUS_METRIC_MORRIS_THORNE>
+                         : trace_kernel<false, 2, SIRIUS_METRIC_MORRIS_THORNE>;
+        case SIRIUS_METRIC_ALCUBIERRE:
+            return mixed ? trace_kernel<true, 2, SIRIUS_METRIC_ALCUBIERRE>
+                         : trace_kernel<false, 2, SIRIUS_METRIC_ALCUBIERRE>;
+        default:
+            return mixed ? trace_kernel<true, 2, kAnyFamily> : trace_kernel<false, 2, kAnyFamily>;
     }
 }
 
@@ -671,6 +754,7 @@ struct Handle {
     bool pending = false;
     cudaStream_t pending_stream = nullptr;
     long long pending_total = 0;
+    int family_mask = 0;  // bit f: a frame of the last upload is of metric family f
 };
 
 int fail(Handle* h, int code, const std::string& msg) {
@@ -835,24 +919,40 @@ int launch_trace(Handle* H, int n_frames, long long total, sirius_ray_result* d_
     P.host_rays = d_rays;
     P.queue = H->d_queue;
     P.counters = H->d_queue + 1;
+    P.clock0 = H->d_queue + 4;
     P.status = H->d_status;
     P.c = make_cfg(c);
     const bool mixed = c.precision == SIRIUS_PRECISION_MIXED;
-    // persistent unless blocks_per_sm < 0 (plain one-thread-per-ray launch)
-    P.persistent = c.blocks_per_sm >= 0 ? 1 : 0;
-    P.refill_threshold = c.refill_threshold > 0 ? c.refill_threshold : 24;
+    // one thread per ray unless blocks_per_sm != 0 (persistent warps pulling rays
+    // from a queue). Consecutive rays are neighbouring pixels, whose geodesics
+    // take the same branches: a warp refilled lane by lane mixes rays at
+    // different stages of their paths and diverges, so refills default to whole warps.
+    P.persistent = c.blocks_per_sm != 0 ? 1 : 0;
+    P.refill_threshold = c.refill_threshold > 0 ? c.refill_threshold : 1;
     const int block = 128;  // matches __launch_bounds__
     const size_t shmem = size_t(2) * P.c.nbins * block * sizeof(float);
     // register budget: blocks_per_sm in 1..4 selects the kernel compiled for that
     // many resident 128-thread blocks per SM (fewer registers, possibly spills)
     const int minb = c.blocks_per_sm > 0 ? std::min(c.blocks_per_sm, 4) : kDefaultMinBlocks;
-    const TraceFn fn = pick_kernel(mixed, minb);
+    // the families present: one family -> its specialised kernel; several ->
+    // one launch per family (each thread skips the rays of other families), so
+    // a ray's result never depends on what else shares the batch; the
+    // persistent queue serves every family from one generic kernel
+    std::vector<int> fams;
+    for (int f = 0; f < 3; ++f)
+        if (H->family_mask & (1 << f)) fams.push_back(f);
+    P.family = -1;
+    std::vector<std::pair<TraceFn, int>> launches;
+    if (fams.size() == 1) launches.push_back({pick_kernel(mixed, minb, fams[0]), -1});
+    else if (!P.persistent)
+        for (int f : fams) launches.push_back({pick_kernel(mixed, minb, f), f});
+    else launches.push_back({pick_kernel(mixed, minb, kAnyFamily), -1});
     int grid;
     if (P.persistent) {
         int per_sm = c.blocks_per_sm;
-        if (per_sm <= 0) {
+        if (per_sm < 0) {
             int occ = 0;
-            CK(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, fn, block, shmem));
+            CK(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, launches[0].first, block, shmem));
             per_sm = std::max(occ, 1);
         }
         grid = H->num_sms * per_sm;
@@ -861,17 +961,21 @@ int launch_trace(Handle* H, int n_frames, long long total, sirius_ray_result* d_
     } else {
         grid = int((total + block - 1) / block);
     }
-    CK(cudaMemsetAsync(H->d_queue, 0, 4 * sizeof(unsigned long long), st));
+    // [0] queue cursor, [1..3] counters, [4] launch start: all start at zero
+    CK(cudaMemsetAsync(H->d_queue, 0, 5 * sizeof(unsigned long long), st));
     CK(cudaMemsetAsync(H->d_status, 0, sizeof(int), st));
-    // whole-launch bound on the device clock (each warp measures from its own start)
+    // whole-launch bound on the device clock, measured from the first warp's start
     P.watchdog_ns = c.watchdog_ms > 0 ? (unsigned long long)c.watchdog_ms * 1000000ull : ~0ull;
     if (timed) CK(cudaEventRecord(H->ev[1], st));
-    fn<<<grid, block, shmem, st>>>(P);
-    CK(cudaGetLastError());
+    for (const auto& L : launches) {
+        P.family = L.second;
+        L.first<<<grid, block, shmem, st>>>(P);
+        CK(cudaGetLastError());
+    }
     if (timed) CK(cudaEventRecord(H->ev[2], st));
     H->stats.grid_blocks = grid;
     H->stats.block_size = block;
-    H->stats.kernel_launches = 1;
+    H->stats.kernel_launches = int(launches.size());
     return SIRIUS_OK;
 }
 
@@ -992,6 +1096,8 @@ static int upload_frames(Handle* H, const sirius_frame* frames, int n, long long
         fd[i] = make_frame(f, H->cfg);
         total += fd[i].n_rays;
     }
+    H->family_mask = 0;
+    for (int i = 0; i < n; ++i) H->family_mask |= 1 << frames[i].metric.family;
     int rc = ensure(H, H->d_frames, H->frames_cap, size_t(n));
     if (rc != SIRIUS_OK) return rc;
     CK(cudaMemcpyAsync(H->d_frames, fd.data(), n * sizeof(FrameDev), cudaMemcpyHostToDevice, H->stream));
@@ -1161,23 +1267,22 @@ int sirius_cuda_autotune(sirius_cuda_handle h, const sirius_frame* frames, int32
     if (rc != SIRIUS_OK) return rc;
     if ((rc = ensure(H, H->d_image, H->image_cap, size_t(total))) != SIRIUS_OK) return rc;
     const sirius_trace_config base = H->cfg;
-    const int thresholds[] = {8, 16, 24, 28, 32};
-    const int per_sm[] = {1, 2, 3, 4};
+    // (blocks/SM, threshold): (0, -) is the one-thread-per-ray launch
+    const int candidates[][2] = {{0, 1}, {1, 1}, {2, 1}, {3, 1}, {4, 1}, {2, 4}, {2, 8}, {3, 4}};
     double best = 1e300;
     sirius_trace_config best_cfg = base;
-    for (int t : thresholds)
-        for (int b : per_sm) {
-            H->cfg = base;
-            H->cfg.refill_threshold = t;
-            H->cfg.blocks_per_sm = b;
-            CK(cudaEventRecord(H->ev[0], H->stream));
-            rc = launch_trace(H, n_frames, total, nullptr, H->d_image, nullptr, nullptr, H->stream, true);
-            if (rc != SIRIUS_OK) { H->cfg = base; return rc; }
-            CK(cudaEventRecord(H->ev[3], H->stream));
-            rc = finish_stats(H, H->stream, total, true);
-            if (rc != SIRIUS_OK) { H->cfg = base; return rc; }
-            if (H->stats.kernel_ms < best) { best = H->stats.kernel_ms; best_cfg = H->cfg; }
-        }
+    for (const auto& cand : candidates) {
+        H->cfg = base;
+        H->cfg.blocks_per_sm = cand[0];
+        H->cfg.refill_threshold = cand[1];
+        CK(cudaEventRecord(H->ev[0], H->stream));
+        rc = launch_trace(H, n_frames, total, nullptr, H->d_image, nullptr, nullptr, H->stream, true);
+        if (rc != SIRIUS_OK) { H->cfg = base; return rc; }
+        CK(cudaEventRecord(H->ev[3], H->stream));
+        rc = finish_stats(H, H->stream, total, true);
+        if (rc != SIRIUS_OK) { H->cfg = base; return rc; }
+        if (H->stats.kernel_ms < best) { best = H->stats.kernel_ms; best_cfg = H->cfg; }
+    }
     H->cfg = best_cfg;
     if (out) *out = best_cfg;
     return SIRIUS_OK;

@@ -176,11 +176,25 @@ SIRIUS_HD __forceinline__ void alc_rhs(const MetricDev& m, const T x[4], const T
     f[3] = q * F.d[2];
 }
 
-template <class T>
+// FAM selects the metric family at compile time (a kernel specialised for one
+// family carries one right-hand side); kAnyFamily dispatches on m.family.
+constexpr int kAnyFamily = -1;
+
+template <class T, int FAM = kAnyFamily>
 SIRIUS_HD __forceinline__ void rhs(const MetricDev& m, const T x[4], const T p[4], T k[4], T f[4]) {
-    if (m.family == SIRIUS_METRIC_KERR_SCHILD) ks_rhs(m, x, p, k, f);
+    if constexpr (FAM == SIRIUS_METRIC_KERR_SCHILD) ks_rhs(m, x, p, k, f);
+    else if constexpr (FAM == SIRIUS_METRIC_MORRIS_THORNE) mt_rhs(m, x, p, k, f);
+    else if constexpr (FAM == SIRIUS_METRIC_ALCUBIERRE) alc_rhs(m, x, p, k, f);
+    else if (m.family == SIRIUS_METRIC_KERR_SCHILD) ks_rhs(m, x, p, k, f);
     else if (m.family == SIRIUS_METRIC_MORRIS_THORNE) mt_rhs(m, x, p, k, f);
     else alc_rhs(m, x, p, k, f);
+}
+
+// Whether a ray of family FAM (or, for kAnyFamily, of m.family) is of family F.
+template <int FAM>
+SIRIUS_HD __forceinline__ bool is_family(const MetricDev& m, int F) {
+    if constexpr (FAM == kAnyFamily) return m.family == F;
+    else return FAM == F;
 }
 
 // ---------------------------------------------------------------------------

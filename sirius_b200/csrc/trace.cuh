@@ -225,7 +225,7 @@ __device__ __forceinline__ const DPTable<double>& dp_table<double>() { return kD
 // fifth-order solution and k7 = f(xn, pn) (first same as last). Returns the
 // scaled RMS error of the position components (computeRK45ErrorNorm,
 // PHGD001A.cpp:508-517).
-template <class T>
+template <class T, int FAM = kAnyFamily>
 __device__ __forceinline__ double dp45_attempt(const MetricDev& m, const CfgDev& c, const double x[4], const double p[4],
                                                double h, const T k1[8], double xn[4], double pn[4], T k7[8]) {
     const DPTable<T>& D = dp_table<T>();
@@ -269,7 +269,7 @@ __device__ __forceinline__ double dp45_attempt(const MetricDev& m, const CfgDev&
 #pragma unroll
             for (int i = 0; i < 4; ++i) { xs[i] = X[i] + ht * acc[0][i]; ps[i] = X[4 + i] + ht * acc[0][4 + i]; }
         }
-        rhs(m, xs, ps, kc, kc + 4);
+        rhs<T, FAM>(m, xs, ps, kc, kc + 4);
         // slide the window: the next stage's input moves to slot 0
 #pragma unroll
         for (int s = 0; s < 5; ++s)
@@ -295,20 +295,70 @@ __device__ __forceinline__ double dp45_attempt(const MetricDev& m, const CfgDev&
     return double(sqrt_(T(0.25) * en));
 }
 
+// The same DP45 attempt in FP64 with the stage derivatives in a thread-local
+// array indexed at run time (L1-resident local memory instead of registers): the
+// rare FP64 island steps of the mixed path then do not set its register budget.
+// Butcher form: stage s input = x + h sum_{j<s} a_sj k_j, with the tableau rows
+// of DP_A read back as a_{s, j+1} = A[j][s-1-j].
+template <int FAM = kAnyFamily>
+__device__ __forceinline__ double dp45_attempt_lowreg(const MetricDev& m, const CfgDev& c, const double x[4],
+                                                      const double p[4], double h, const double k1[8], double xn[4],
+                                                      double pn[4], double k7[8]) {
+    const DPTable<double>& D = kDPd;
+    double K[7][8];
+#pragma unroll
+    for (int i = 0; i < 8; ++i) K[0][i] = k1[i];
+#pragma unroll 1
+    for (int s = 1; s < 7; ++s) {
+        double sx[8];
+#pragma unroll
+        for (int i = 0; i < 8; ++i) sx[i] = 0.0;
+#pragma unroll 1
+        for (int j = 0; j < s; ++j) {
+            const double a = D.A[j][s - 1 - j];
+#pragma unroll
+            for (int i = 0; i < 8; ++i) sx[i] += a * K[j][i];
+        }
+        double xs[4], ps[4];
+#pragma unroll
+        for (int i = 0; i < 4; ++i) {
+            xs[i] = x[i] + h * sx[i];
+            ps[i] = p[i] + h * sx[4 + i];
+        }
+        if (s == 6) {
+#pragma unroll
+            for (int i = 0; i < 4; ++i) { xn[i] = xs[i]; pn[i] = ps[i]; }
+        }
+        rhs<double, FAM>(m, xs, ps, K[s], K[s] + 4);
+    }
+    double en = 0.0;
+#pragma unroll 1
+    for (int i = 0; i < 4; ++i) {
+        double ex = 0.0;
+#pragma unroll 1
+        for (int j = 0; j < 7; ++j) ex += D.E[j] * K[j][i];
+        const double e = h * ex / (c.atol + c.rtol * fabs(xn[i]));
+        en += e * e;
+    }
+#pragma unroll
+    for (int i = 0; i < 8; ++i) k7[i] = K[6][i];
+    return sqrt(0.25 * en);
+}
+
 // Event location of the equatorial crossing inside an accepted step: DP45
 // sub-steps from the step's start state (x0, p0) with f(x0, p0) recomputed in
 // T, the sub-step length corrected by Newton on z(l) (dz/dl = k^z), seeded by
 // the cubic Hermite root; two sub-steps and a final first-order correction.
-template <class T>
+template <class T, int FAM = kAnyFamily>
 __device__ __noinline__ void locate_equator(const MetricDev& m, const CfgDev& c, const double x0[4],
                                             const double p0[4], double hs, double& xc1, double& xc2) {
     T xk[4], pk[4], k0[8], k7[8];
     for (int i = 0; i < 4; ++i) { xk[i] = T(x0[i]); pk[i] = T(p0[i]); }
-    rhs<T>(m, xk, pk, k0, k0 + 4);
+    rhs<T, FAM>(m, xk, pk, k0, k0 + 4);
     double xn[4], pn[4];
-    dp45_attempt<T>(m, c, x0, p0, hs, k0, xn, pn, k7);
+    dp45_attempt<T, FAM>(m, c, x0, p0, hs, k0, xn, pn, k7);
     hs -= xn[3] / double(k7[3]);
-    dp45_attempt<T>(m, c, x0, p0, hs, k0, xn, pn, k7);
+    dp45_attempt<T, FAM>(m, c, x0, p0, hs, k0, xn, pn, k7);
     const double dl = -xn[3] / double(k7[3]);
     xc1 = xn[1] + dl * double(k7[1]);
     xc2 = xn[2] + dl * double(k7[2]);
@@ -338,7 +388,7 @@ __constant__ double kYoshida[3][15] = {
      0.33462491824529, 0.31529309239676, -0.79688793935291, 0.31529309239676, 0.33462491824529,
      0.29906418130365, -0.57386247111608, 0.19075471029623, -0.40910082580003, 0.74167036435061}};
 
-template <class T>
+template <class T, int FAM = kAnyFamily>
 __device__ __noinline__ void symplectic_step(const MetricDev& m, int order, double h, double x[4], double p[4]) {
     const int row = order >= 8 ? 2 : (order >= 6 ? 1 : 0);
     const int n = row == 2 ? 15 : (row == 1 ? 7 : 3);
@@ -350,7 +400,7 @@ __device__ __noinline__ void symplectic_step(const MetricDev& m, int order, doub
             T X[4], P[4], k[4], f[4];
 #pragma unroll
             for (int i = 0; i < 4; ++i) { X[i] = T(x[i]); P[i] = T(p[i]); }
-            rhs<T>(m, X, P, k, f);
+            rhs<T, FAM>(m, X, P, k, f);
             if (ph == 1) {
 #pragma unroll
                 for (int i = 0; i < 4; ++i) x[i] += hs * double(k[i]);
@@ -390,16 +440,20 @@ __constant__ float kGLw[4][4] = {{1.0f, 0, 0, 0},
                                  {0.17392742256872693f, 0.32607257743127307f, 0.32607257743127307f,
                                   0.17392742256872693f}};
 
-// Largest affine step inside the emitting volume: half the local Gaussian scale
-// height h_z r over the spatial speed |dx/dl| (the per-step quadrature, and so
-// the spectra, then do not depend on the step sequence). Infinite outside.
+// Emission beyond this many scale heights (e^-18 of the peak) is dropped.
+constexpr double kVolCutoff = 6.0;
+
+// Largest affine step near the emitting volume, so that the per-step
+// quadrature, and hence the spectra, do not depend on the step sequence: half
+// the local scale height hz r over the spatial speed |dx/dl| inside the emitting
+// region (r_in <= r <= r_out, |z| <= kVolCutoff hz r), and outside it the
+// distance to that region, so that no step jumps into its interior.
 __device__ __forceinline__ double volume_step_cap(double r, double z, double vx, double vy, double vz, double hz,
                                                   double r_in, double r_out) {
-    if (r < 0.9 * r_in || r > 1.1 * r_out) return 1e300;
-    const double H = hz * r;
-    if (fabs(z) > 5.0 * H) return 1e300;
+    const double H = hz * fmin(fmax(r, r_in), r_out);
+    const double dist = fmax(fmax(r_in - r, r - r_out), fabs(z) - kVolCutoff * H);
     const double v = sqrt(vx * vx + vy * vy + vz * vz);
-    return 0.5 * H / fmax(v, 1e-3);
+    return fmax(0.5 * H, dist) / fmax(v, 1e-3);
 }
 
 // Cubic Hermite interpolation of z over the accepted step; bisection for z = 0.
@@ -417,11 +471,13 @@ __device__ __forceinline__ double hermite_root(double z0, double z1, double dz0,
 // Keplerian emitter at BL radius rbl seen from the camera: g = (p.u_obs)/(p.u_em),
 // u_em = u^t (d_t + Omega d_phi) with u^t from the Killing norms at the point
 // (g_tt = -1 + H, g_t,phi = H (l.xi), g_phi,phi = x^2 + y^2 + H (l.xi)^2 in KS).
+// rbl is the Kerr-Schild r of (x, y, z): H and l follow from it without derivatives.
 template <class T>
 __device__ __forceinline__ T kepler_g(const MetricDev& m, T x, T y, T z, T rbl, T E, T Lz, T sqrt_m_gtt_cam) {
-    KSPieces<T> P;
-    ks_pieces(m, x, y, z, P);
-    const T H = P.H.v, lxi = -y * P.l1.v + x * P.l2.v;
+    const T r2 = rbl * rbl, iden = rcp_(r2 + T(m.a2));
+    const T l1 = (rbl * x + T(m.a) * y) * iden, l2 = (rbl * y - T(m.a) * x) * iden;
+    const T H = (T(2.0 * m.M) * rbl - T(m.Q2)) * r2 * rcp_(r2 * r2 + T(m.a2) * z * z);
+    const T lxi = -y * l1 + x * l2;
     T gtt = -T(1) + H;
     if (m.has_lambda) gtt -= T(m.lam3) * (x * x + y * y + z * z);
     const T gtp = H * lxi, gpp = x * x + y * y + H * lxi * lxi;
