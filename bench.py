@@ -32,6 +32,10 @@ WIDTH = HEIGHT = 1024
 SEED = 0
 N_BINS = 16
 MEASURED_PEAKS = os.path.join(ROOT, "MEASURED_PEAKS.json")
+# DRAM bytes (read + write) per ray of the trace kernel, from one ncu capture of
+# the 256^2 case of this workload (profiles/trace_kernel_mixed_kerr256_full.md):
+# (1.83 + 9.13) MB / 65,536 rays; traffic grows with the ray count.
+TRAFFIC_BYTES_PER_RAY = 167.2
 
 
 def inclination_deg(seed=SEED):
@@ -51,13 +55,13 @@ def workload_frame(abi, width=WIDTH, height=HEIGHT):
     return abi.make_frame(abi.make_metric(M=1.0, a=0.9), cam, 0.0, 30.0)
 
 
-def workload_desc():
-    return {"workload": "kerr_a0.9_1024x1024_mixed_dp45_nt_disk_vol16", "metric_family": "kerr_schild",
-            "spin": 0.9, "resolution": [WIDTH, HEIGHT], "r_obs": 100.0, "inclination_deg": round(inclination_deg(), 4),
+def workload_desc(size=WIDTH):
+    return {"workload": f"kerr_a0.9_{size}x{size}_mixed_dp45_nt_disk_vol16", "metric_family": "kerr_schild",
+            "spin": 0.9, "resolution": [size, size], "r_obs": 100.0, "inclination_deg": round(inclination_deg(), 4),
             "seed": SEED, "fov_deg": 30.0, "tolerance": 1e-8, "escape_radius": 200.0, "horizon_factor": 1.01,
             "disk": [None, 30.0], "volumetric_bins": N_BINS, "precision": "fp32 rhs + fp64 state/projection/island",
-            "l2": "inputs are 168-byte frame descriptors; the 24 MiB L2 working set is flushed by a 256 MiB write "
-                  "between timed steps"}
+            "l2": "inputs are 168-byte frame descriptors; the outputs (4 B image + 64 B spectra per ray) are "
+                  "written once per ray; a 256 MiB write flushes the 126 MB L2 between timed steps"}
 
 
 # --------------------------------------------------------------- clocks ----
@@ -218,6 +222,8 @@ def main():
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
     ap.add_argument("--no-extras", action="store_true", help="skip the FP64 comparator and the CPU baseline")
+    ap.add_argument("--size", type=int, default=WIDTH,
+                    help="frame side (default 1024, the workload; smaller sides are profiling cases)")
     args = ap.parse_args()
     if args.impl == "reference":
         run_reference(args)
@@ -241,10 +247,10 @@ def main():
     stream = torch.cuda.current_stream(dev)
 
     eng = Engine(local, config=workload_config(abi, abi.PRECISION_MIXED))
-    frame = workload_frame(abi)
+    frame = workload_frame(abi, args.size, args.size)
     frames = (abi.Frame * 1)(frame)
     frames[0].ray_offset = 0
-    total = WIDTH * HEIGHT
+    total = args.size * args.size
     fbytes = bytes(frames)
     d_frames = torch.frombuffer(bytearray(fbytes), dtype=torch.uint8).to(dev)
     d_image = torch.empty(total, dtype=torch.float32, device=dev)
@@ -314,12 +320,13 @@ def main():
     line = {"metric": "Mrays/s", "value": value, "unit": "Mrays/s", "n_gpus": world, "steps": args.steps,
             "warmup": args.warmup, "ms_per_step": t_total / args.steps, "higher_is_better": True, "scaling": "weak",
             "vs_baseline": None, "dtype": "f32+f64",
-            "data": "synthetic (seeded camera frame; no dataset)", "config": workload_desc(),
+            "data": "synthetic (seeded camera frame; no dataset)", "config": workload_desc(args.size),
             "e2e": {"value": e2e, "unit": "Mrays/s", "h2d_bytes_per_step": C.sizeof(abi.Frame),
                     "d2h_bytes_per_step": total * 4 * (1 + N_BINS)},
             "gpu_launches": args.steps,
             "roofline": {"bound": "fp32_simt", "achieved": achieved, "peak": peak32, "unit": "TFLOP/s",
-                         "frac": achieved / peak32, "traffic": None,
+                         "frac": achieved / peak32, "traffic": TRAFFIC_BYTES_PER_RAY * total,
+                         "traffic_unit": "bytes per launch (ncu, 256^2 capture scaled by rays)",
                          "peak_source": "measured FMA-chain microbenchmark (sirius_cuda_measure_fma_peak)",
                          "fp64_peak": peak64, "flops_per_accepted_step": acc_f, "flops_per_rhs": rhs_f,
                          "kernel": "trace_kernel<mixed>"},

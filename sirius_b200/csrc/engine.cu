@@ -906,21 +906,32 @@ int validate_config(Handle* H, const sirius_trace_config& c) {
 }
 
 // Launch the tracer over [0, total) of already-uploaded frames.
+// Device scratch of one launch: the frame descriptors, the queue cursor and
+// counters ([0] cursor, [1..3] counters, [4] launch start) and the status word.
+struct LaunchScratch {
+    const FrameDev* frames;
+    unsigned long long* queue;
+    int* status;
+};
+
 int launch_trace(Handle* H, int n_frames, long long total, sirius_ray_result* d_results, float* d_image,
-                 float* d_spectra, const sirius_camera_ray* d_rays, cudaStream_t st, bool timed) {
+                 float* d_spectra, const sirius_camera_ray* d_rays, cudaStream_t st, bool timed,
+                 const LaunchScratch* scratch = nullptr) {
     const sirius_trace_config& c = H->cfg;
+    const LaunchScratch own{H->d_frames, H->d_queue, H->d_status};
+    const LaunchScratch& S = scratch ? *scratch : own;
     Params P{};
-    P.frames = H->d_frames;
+    P.frames = S.frames;
     P.n_frames = n_frames;
     P.total = total;
     P.results = d_results;
     P.image = d_image;
     P.spectra = d_spectra;
     P.host_rays = d_rays;
-    P.queue = H->d_queue;
-    P.counters = H->d_queue + 1;
-    P.clock0 = H->d_queue + 4;
-    P.status = H->d_status;
+    P.queue = S.queue;
+    P.counters = S.queue + 1;
+    P.clock0 = S.queue + 4;
+    P.status = S.status;
     P.c = make_cfg(c);
     const bool mixed = c.precision == SIRIUS_PRECISION_MIXED;
     // one thread per ray unless blocks_per_sm != 0 (persistent warps pulling rays
@@ -938,21 +949,33 @@ int launch_trace(Handle* H, int n_frames, long long total, sirius_ray_result* d_
     // one launch per family (each thread skips the rays of other families), so
     // a ray's result never depends on what else shares the batch; the
     // persistent queue serves every family from one generic kernel
-    std::vector<int> fams;
+    int fams[3], n_fams = 0;
     for (int f = 0; f < 3; ++f)
-        if (H->family_mask & (1 << f)) fams.push_back(f);
+        if (H->family_mask & (1 << f)) fams[n_fams++] = f;
     P.family = -1;
-    std::vector<std::pair<TraceFn, int>> launches;
-    if (fams.size() == 1) launches.push_back({pick_kernel(mixed, minb, fams[0]), -1});
-    else if (!P.persistent)
-        for (int f : fams) launches.push_back({pick_kernel(mixed, minb, f), f});
-    else launches.push_back({pick_kernel(mixed, minb, kAnyFamily), -1});
+    TraceFn launch_fn[3];
+    int launch_family[3], n_launches = 0;
+    if (n_fams == 1) {
+        launch_fn[0] = pick_kernel(mixed, minb, fams[0]);
+        launch_family[0] = -1;
+        n_launches = 1;
+    } else if (!P.persistent) {
+        for (int i = 0; i < n_fams; ++i) {
+            launch_fn[i] = pick_kernel(mixed, minb, fams[i]);
+            launch_family[i] = fams[i];
+        }
+        n_launches = n_fams;
+    } else {
+        launch_fn[0] = pick_kernel(mixed, minb, kAnyFamily);
+        launch_family[0] = -1;
+        n_launches = 1;
+    }
     int grid;
     if (P.persistent) {
         int per_sm = c.blocks_per_sm;
         if (per_sm < 0) {
             int occ = 0;
-            CK(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, launches[0].first, block, shmem));
+            CK(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, launch_fn[0], block, shmem));
             per_sm = std::max(occ, 1);
         }
         grid = H->num_sms * per_sm;
@@ -962,20 +985,20 @@ int launch_trace(Handle* H, int n_frames, long long total, sirius_ray_result* d_
         grid = int((total + block - 1) / block);
     }
     // [0] queue cursor, [1..3] counters, [4] launch start: all start at zero
-    CK(cudaMemsetAsync(H->d_queue, 0, 5 * sizeof(unsigned long long), st));
-    CK(cudaMemsetAsync(H->d_status, 0, sizeof(int), st));
+    CK(cudaMemsetAsync(S.queue, 0, 5 * sizeof(unsigned long long), st));
+    CK(cudaMemsetAsync(S.status, 0, sizeof(int), st));
     // whole-launch bound on the device clock, measured from the first warp's start
     P.watchdog_ns = c.watchdog_ms > 0 ? (unsigned long long)c.watchdog_ms * 1000000ull : ~0ull;
     if (timed) CK(cudaEventRecord(H->ev[1], st));
-    for (const auto& L : launches) {
-        P.family = L.second;
-        L.first<<<grid, block, shmem, st>>>(P);
+    for (int i = 0; i < n_launches; ++i) {
+        P.family = launch_family[i];
+        launch_fn[i]<<<grid, block, shmem, st>>>(P);
         CK(cudaGetLastError());
     }
     if (timed) CK(cudaEventRecord(H->ev[2], st));
     H->stats.grid_blocks = grid;
     H->stats.block_size = block;
-    H->stats.kernel_launches = int(launches.size());
+    H->stats.kernel_launches = n_launches;
     return SIRIUS_OK;
 }
 
