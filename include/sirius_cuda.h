@@ -264,6 +264,27 @@ int sirius_cuda_trace_frames_device(sirius_cuda_handle handle,
                                     sirius_ray_result* d_results, float* d_image, float* d_spectra,
                                     void* stream);
 
+/* Allocation-free form of sirius_cuda_trace_frames_device (no counterpart in the
+ * reference): same arguments, same results, but the launch scratch (frame
+ * descriptors, ray-queue and step counters, status word) lives in a static
+ * device array of the library, so the call makes no device allocation. For
+ * callers that cannot let a library allocate: a host whose own allocator
+ * already holds the device memory it is given, or a frame loop that cannot
+ * afford the implicit device-wide synchronisation of cudaMalloc/cudaFree.
+ * Limits: at most SIRIUS_STATIC_MAX_FRAMES frames per call (more is rejected
+ * with SIRIUS_ERR_INVALID_ARGUMENT). The counters and status word must start a
+ * launch at zero; the call zeroes them on `stream` itself. The scratch is one
+ * per device: overlapping calls on one device (other streams, handles or host
+ * threads) race on it and must be serialised by the caller. The scratch address
+ * is resolved on the first call per device; make that first call before any
+ * stream capture. sirius_cuda_last_stats does not describe these launches. */
+#define SIRIUS_STATIC_MAX_FRAMES 64
+int sirius_cuda_trace_frames_static(sirius_cuda_handle handle,
+                                    const sirius_frame* d_frames, int32_t n_frames,
+                                    int64_t total_rays,
+                                    sirius_ray_result* d_results, float* d_image, float* d_spectra,
+                                    void* stream);
+
 /* ---- batch form of GeodesicTracer::trace(const CameraRay&) (GTRC001A.h:220) ----
  * Host-generated rays through one metric; disk_inner <= 0 selects the ISCO. */
 int sirius_cuda_trace_rays(sirius_cuda_handle handle, const sirius_metric* metric,

@@ -8,6 +8,7 @@ import ctypes as C
 ABI_VERSION = 1
 MAX_BINS = 32
 MAX_CROSSINGS = 4
+STATIC_MAX_FRAMES = 64  # SIRIUS_STATIC_MAX_FRAMES
 
 # status
 OK = 0

@@ -18,6 +18,7 @@
 #include <cmath>
 #include <cstdio>
 #include <cstring>
+#include <mutex>
 #include <new>
 #include <string>
 #include <type_traits>
@@ -1029,6 +1030,41 @@ int finish_stats(Handle* H, cudaStream_t st, long long total, bool timed) {
 // ---------------------------------------------------------------------------
 // C ABI
 // ---------------------------------------------------------------------------
+// ---------------------------------------------------------------------------
+// Library-owned scratch of sirius_cuda_trace_frames_static: a file-scope
+// device array, so that entry point allocates nothing. Its queue/counter words
+// and status word must be zero when a launch starts (the entry point zeroes
+// them on its stream before each launch); the frame descriptors are rewritten
+// by every call. One array per device: calls in flight at the same time on one
+// device (other streams, other handles, other host threads) share it and race.
+// ---------------------------------------------------------------------------
+namespace {
+struct StaticScratch {
+    FrameDev frames[SIRIUS_STATIC_MAX_FRAMES];
+    unsigned long long queue[8];  // [0] cursor, [1..3] counters, [4] launch start
+    int status;
+};
+constexpr int kStaticMaxDevices = 64;
+}  // namespace
+
+static __device__ __align__(256) unsigned char g_static_scratch[sizeof(StaticScratch)];
+static_assert(sizeof(StaticScratch) <= 64 * 1024, "static scratch stays modest");
+
+namespace {
+// The device address of g_static_scratch on `device`, resolved once per device
+// (the first call per device should come before any stream capture).
+StaticScratch* static_scratch(int device) {
+    static void* addr[kStaticMaxDevices] = {};
+    static std::once_flag once[kStaticMaxDevices];
+    std::call_once(once[device], [device] {
+        void* p = nullptr;
+        if (cudaGetSymbolAddress(&p, g_static_scratch) == cudaSuccess) addr[device] = p;
+        else cudaGetLastError();
+    });
+    return static_cast<StaticScratch*>(addr[device]);
+}
+}  // namespace
+
 extern "C" {
 
 int sirius_cuda_abi_version(void) { return SIRIUS_CUDA_ABI_VERSION; }
@@ -1178,6 +1214,49 @@ int sirius_cuda_trace_frames_device(sirius_cuda_handle h, const sirius_frame* d_
     H->pending_stream = st;
     H->pending_total = total;
     return SIRIUS_OK;
+}
+
+int sirius_cuda_trace_frames_static(sirius_cuda_handle h, const sirius_frame* d_frames_user, int32_t n_frames,
+                                    int64_t total_rays, sirius_ray_result* d_results, float* d_image, float* d_spectra,
+                                    void* stream) {
+    Handle* H = static_cast<Handle*>(h);
+    if (!H || !d_frames_user || n_frames <= 0 || total_rays <= 0) return SIRIUS_ERR_INVALID_ARGUMENT;
+    if (n_frames > SIRIUS_STATIC_MAX_FRAMES)
+        return fail(H, SIRIUS_ERR_INVALID_ARGUMENT, "sirius_cuda_trace_frames_static takes at most "
+                                                    "SIRIUS_STATIC_MAX_FRAMES (64) frames per call");
+    if (H->device < 0 || H->device >= kStaticMaxDevices)
+        return fail(H, SIRIUS_ERR_INVALID_ARGUMENT, "device ordinal beyond the static scratch table");
+    CK(cudaSetDevice(H->device));
+    StaticScratch* scratch = static_scratch(H->device);
+    if (!scratch) return fail(H, SIRIUS_ERR_CUDA, "cudaGetSymbolAddress failed for the static scratch");
+    cudaStream_t st = stream ? static_cast<cudaStream_t>(stream) : cudaStreamLegacy;
+    // frame descriptors: device -> host (stack) -> per-frame constants -> static scratch
+    sirius_frame hf[SIRIUS_STATIC_MAX_FRAMES];
+    FrameDev fd[SIRIUS_STATIC_MAX_FRAMES];
+    CK(cudaMemcpyAsync(hf, d_frames_user, n_frames * sizeof(sirius_frame), cudaMemcpyDeviceToHost, st));
+    CK(cudaStreamSynchronize(st));
+    long long total = 0;
+    int mask = 0;
+    for (int i = 0; i < n_frames; ++i) {
+        const sirius_frame& f = hf[i];
+        int rc = validate_metric(H, f.metric);
+        if (rc != SIRIUS_OK) return rc;
+        if (f.camera.width <= 0 || f.camera.height <= 0 || !(f.camera.r > 0))
+            return fail(H, SIRIUS_ERR_INVALID_ARGUMENT, "camera needs width, height > 0 and r > 0");
+        if (f.camera.projection != SIRIUS_CAMERA_PINHOLE && f.camera.projection != SIRIUS_CAMERA_EQUIRECTANGULAR)
+            return fail(H, SIRIUS_ERR_INVALID_ARGUMENT, "unknown camera projection");
+        if (f.ray_offset != total)
+            return fail(H, SIRIUS_ERR_INVALID_ARGUMENT, "frames must be contiguous: ray_offset[i] = sum of previous pixel counts");
+        fd[i] = make_frame(f, H->cfg);
+        total += fd[i].n_rays;
+        mask |= 1 << f.metric.family;
+    }
+    if (total != total_rays) return fail(H, SIRIUS_ERR_INVALID_ARGUMENT, "total_rays does not match the frames");
+    // a pageable source: the copy has been staged when cudaMemcpyAsync returns
+    CK(cudaMemcpyAsync(scratch->frames, fd, n_frames * sizeof(FrameDev), cudaMemcpyHostToDevice, st));
+    H->family_mask = mask;
+    const LaunchScratch ls{scratch->frames, scratch->queue, &scratch->status};
+    return launch_trace(H, n_frames, total, d_results, d_image, d_spectra, nullptr, st, false, &ls);
 }
 
 int sirius_cuda_trace_rays(sirius_cuda_handle h, const sirius_metric* metric, double disk_inner, double disk_outer,

@@ -22,7 +22,7 @@ EXPORTS = [
     "sirius_cuda_get_last_error", "sirius_cuda_configure", "sirius_cuda_trace_frames",
     "sirius_cuda_trace_frames_device", "sirius_cuda_trace_rays", "sirius_cuda_metric_evaluate",
     "sirius_cuda_dp45_step", "sirius_cuda_last_stats", "sirius_cuda_autotune", "sirius_cuda_measure_fma_peak",
-    "sirius_cuda_flop_count",
+    "sirius_cuda_flop_count", "sirius_cuda_trace_frames_static",
 ]
 
 
@@ -45,6 +45,8 @@ def load_library(path=LIB_PATH):
     L.sirius_cuda_configure.argtypes = [C.c_void_p, _P(abi.TraceConfig)]
     L.sirius_cuda_trace_frames.argtypes = [C.c_void_p, C.c_void_p, C.c_int32, C.c_void_p, C.c_void_p, C.c_void_p]
     L.sirius_cuda_trace_frames_device.argtypes = [C.c_void_p, C.c_void_p, C.c_int32, C.c_int64, C.c_void_p,
+                                                  C.c_void_p, C.c_void_p, C.c_void_p]
+    L.sirius_cuda_trace_frames_static.argtypes = [C.c_void_p, C.c_void_p, C.c_int32, C.c_int64, C.c_void_p,
                                                   C.c_void_p, C.c_void_p, C.c_void_p]
     L.sirius_cuda_trace_rays.argtypes = [C.c_void_p, _P(abi.Metric), C.c_double, C.c_double, C.c_void_p,
                                          C.c_int64, C.c_void_p]
@@ -130,6 +132,12 @@ class Engine:
     def trace_frames_device(self, d_frames, n_frames, total, d_results, d_image, d_spectra, stream):
         """Device entry point: all pointers are device addresses; stream is a cudaStream_t address."""
         self._check(self.lib.sirius_cuda_trace_frames_device(self.h, d_frames, n_frames, total, d_results, d_image,
+                                                             d_spectra, stream))
+
+    def trace_frames_static(self, d_frames, n_frames, total, d_results, d_image, d_spectra, stream):
+        """As trace_frames_device, with the launch scratch in the library's static
+        device array: no device allocation (at most SIRIUS_STATIC_MAX_FRAMES frames)."""
+        self._check(self.lib.sirius_cuda_trace_frames_static(self.h, d_frames, n_frames, total, d_results, d_image,
                                                              d_spectra, stream))
 
     def trace_rays(self, metric, rays, disk_inner=0.0, disk_outer=20.0):
