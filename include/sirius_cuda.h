@@ -285,6 +285,18 @@ int sirius_cuda_trace_frames_static(sirius_cuda_handle handle,
                                     sirius_ray_result* d_results, float* d_image, float* d_spectra,
                                     void* stream);
 
+/* ---- surrogate MLP (no counterpart in the reference) ---------------------------
+ * 5 -> 256 -> 256 -> 256 -> 256 -> 4, SiLU after the hidden layers, BF16
+ * weights and activations with FP32 accumulation on the tensor cores.
+ * params: host array of SIRIUS_SURROGATE_PARAMS floats in torch nn.Linear
+ *   order (out x in): W1[256][5] b1[256] W2[256][256] b2 W3 b3 W4 b4 W5[4][256] b5[4].
+ * infer: d_features = n x 5 floats, d_out = n x 4 floats (device), stream-ordered
+ *   on `stream` and synchronous on return. */
+#define SIRIUS_SURROGATE_PARAMS 199940
+int sirius_cuda_surrogate_load(sirius_cuda_handle handle, const float* params, int64_t n_params);
+int sirius_cuda_surrogate_infer(sirius_cuda_handle handle, const float* d_features, int64_t n, float* d_out,
+                                void* stream);
+
 /* ---- batch form of GeodesicTracer::trace(const CameraRay&) (GTRC001A.h:220) ----
  * Host-generated rays through one metric; disk_inner <= 0 selects the ISCO. */
 int sirius_cuda_trace_rays(sirius_cuda_handle handle, const sirius_metric* metric,

@@ -9,6 +9,7 @@ ABI_VERSION = 1
 MAX_BINS = 32
 MAX_CROSSINGS = 4
 STATIC_MAX_FRAMES = 64  # SIRIUS_STATIC_MAX_FRAMES
+SURROGATE_PARAMS = 199940  # SIRIUS_SURROGATE_PARAMS
 
 # status
 OK = 0

@@ -25,6 +25,7 @@
 #include <vector>
 
 #include "trace.cuh"
+#include "surrogate.cuh"
 
 using namespace sirius;
 
@@ -756,6 +757,8 @@ struct Handle {
     cudaStream_t pending_stream = nullptr;
     long long pending_total = 0;
     int family_mask = 0;  // bit f: a frame of the last upload is of metric family f
+    unsigned char* d_surrogate = nullptr;  // packed surrogate weight image (surrogate::kImageBytes)
+    int* d_sur_err = nullptr;
 };
 
 int fail(Handle* h, int code, const std::string& msg) {
@@ -1118,6 +1121,7 @@ int sirius_cuda_destroy(sirius_cuda_handle h) {
     if (H->stream) cudaStreamSynchronize(H->stream);
     cudaFree(H->d_frames); cudaFree(H->d_results); cudaFree(H->d_image); cudaFree(H->d_spectra);
     cudaFree(H->d_rays); cudaFree(H->d_queue); cudaFree(H->d_status);
+    cudaFree(H->d_surrogate); cudaFree(H->d_sur_err);
     for (auto& e : H->ev) if (e) cudaEventDestroy(e);
     if (H->stream) cudaStreamDestroy(H->stream);
     delete H;
@@ -1413,6 +1417,57 @@ int sirius_cuda_measure_fma_peak(sirius_cuda_handle h, int32_t precision, double
     cudaFree(dout);
     const double flops = 2.0 * 8.0 * 16.0 * double(iters) * double(grid) * double(block);
     *flops_per_s = flops / (double(best) * 1e-3);
+    return SIRIUS_OK;
+}
+
+int sirius_cuda_surrogate_load(sirius_cuda_handle h, const float* params, int64_t n_params) {
+    Handle* H = static_cast<Handle*>(h);
+    if (!H || !params) return SIRIUS_ERR_INVALID_ARGUMENT;
+    if (n_params != surrogate::kParams)
+        return fail(H, SIRIUS_ERR_INVALID_ARGUMENT, "surrogate parameter count must be SIRIUS_SURROGATE_PARAMS");
+    CK(cudaSetDevice(H->device));
+    std::vector<unsigned char> img(surrogate::kImageBytes);
+    surrogate::pack_weights(params, img.data());
+    if (!H->d_surrogate) {
+        if (cudaMalloc((void**)&H->d_surrogate, surrogate::kImageBytes) != cudaSuccess)
+            return fail(H, SIRIUS_ERR_OUT_OF_MEMORY, "cudaMalloc surrogate weights");
+        if (cudaMalloc((void**)&H->d_sur_err, sizeof(int)) != cudaSuccess)
+            return fail(H, SIRIUS_ERR_OUT_OF_MEMORY, "cudaMalloc surrogate status");
+        CK(cudaFuncSetAttribute(surrogate::mlp_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                surrogate::kSmBytes));
+    }
+    CK(cudaMemcpyAsync(H->d_surrogate, img.data(), surrogate::kImageBytes, cudaMemcpyHostToDevice, H->stream));
+    CK(cudaStreamSynchronize(H->stream));
+    return SIRIUS_OK;
+}
+
+// launches the MLP on n feature rows (device buffers) on stream st
+static int surrogate_launch(Handle* H, const float* d_features, long long n, float* d_out, cudaStream_t st) {
+    if (!H->d_surrogate) return fail(H, SIRIUS_ERR_NOT_CONFIGURED, "no surrogate weights loaded");
+    if (n <= 0) return SIRIUS_OK;
+    const long long tiles = (n + surrogate::kTileM - 1) / surrogate::kTileM;
+    const int grid = int(std::min<long long>(tiles, H->num_sms));
+    // bound on any wait inside the kernel: the configured watchdog (default 30 s)
+    const unsigned long long limit = (unsigned long long)(H->cfg.watchdog_ms > 0 ? H->cfg.watchdog_ms : 30000) * 1000000ull;
+    surrogate::mlp_kernel<<<grid, surrogate::kThreads, surrogate::kSmBytes, st>>>(H->d_surrogate, d_features, n, d_out,
+                                                                               H->d_sur_err, limit);
+    CK(cudaGetLastError());
+    return SIRIUS_OK;
+}
+
+int sirius_cuda_surrogate_infer(sirius_cuda_handle h, const float* d_features, int64_t n, float* d_out,
+                                void* stream) {
+    Handle* H = static_cast<Handle*>(h);
+    if (!H || !d_features || !d_out || n < 0) return SIRIUS_ERR_INVALID_ARGUMENT;
+    CK(cudaSetDevice(H->device));
+    cudaStream_t st = stream ? static_cast<cudaStream_t>(stream) : cudaStreamLegacy;
+    if (H->d_sur_err) CK(cudaMemsetAsync(H->d_sur_err, 0, sizeof(int), st));
+    int rc = surrogate_launch(H, d_features, n, d_out, st);
+    if (rc != SIRIUS_OK) return rc;
+    int err = 0;
+    CK(cudaMemcpyAsync(&err, H->d_sur_err, sizeof(int), cudaMemcpyDeviceToHost, st));
+    CK(cudaStreamSynchronize(st));
+    if (err) return fail(H, SIRIUS_ERR_TIMEOUT, "surrogate MLP kernel stopped by its wait bound");
     return SIRIUS_OK;
 }
 

@@ -1,0 +1,398 @@
+// surrogate.cuh — the BF16 surrogate MLP on the 5th-generation tensor cores.
+//
+// Network (the surrogate configuration): 5 -> 256 -> 256 -> 256 -> 256 -> 4,
+// SiLU after each hidden layer, BF16 weights and activations, FP32
+// accumulation, FP32 biases. One CTA of 256 threads owns one SM and walks
+// 128-row tiles of the input:
+//
+//   * A operand (activations, 128 x K) and B operand (weights, N x K) sit in
+//     shared memory, both K-major, in the no-swizzle core-matrix layout of the
+//     UMMA shared-memory descriptor: element (row, k) at byte
+//       (row % 8) * 16 + (row / 8) * SBO + (k / 8) * 128 + (k % 8) * 2,
+//     SBO = (K / 8) * 128 (8-row groups back to back, each group K/8 core
+//     matrices of 8 rows x 16 bytes).
+//   * One thread issues tcgen05.mma (M = 128, N = 256 or 16, K = 16 per
+//     instruction) into a 128-lane x 256-column FP32 accumulator in TMEM and
+//     commits to an mbarrier.
+//   * The 128 KB weight images of layers 2-4 stream from global memory by a
+//     bulk TMA copy (cp.async.bulk, no tensor map, no multicast) into one
+//     buffer, each issued as soon as the previous layer's MMAs have drained it,
+//     so the copy overlaps the epilogue. Layer 1 (K padded 5 -> 16) and layer 5
+//     (N padded 4 -> 16) weights and all biases stay resident.
+//   * Epilogue: 8 warps read the accumulator with tcgen05.ld (warp w: TMEM lanes
+//     32 (w % 4).., columns 128 (w / 4)..), add the bias, apply SiLU
+//     x (1 + tanh(x / 2)) / 2 (one MUFU op), round to BF16 and write the next
+//     layer's A operand.
+//
+// Every mbarrier wait is bounded by the device clock; on a timeout the block
+// agrees (a block-wide vote) to stop, records an error flag, waits (bounded)
+// for its copy in flight and frees its TMEM.
+#pragma once
+
+#include <cuda_bf16.h>
+#include <cstdint>
+
+namespace sirius {
+namespace surrogate {
+
+constexpr int kIn = 5, kInPad = 16, kHid = 256, kOut = 4, kOutPad = 16, kTileM = 128, kThreads = 256;
+// packed weight image (bytes): W2 | W3 | W4 | W1 | W5 | b1 b2 b3 b4 (256 f32 each) | b5 (16 f32)
+constexpr int kBigBytes = kHid * kHid * 2;            // 131072
+constexpr int kW1Bytes = kHid * kInPad * 2;           // 8192
+constexpr int kW5Bytes = kOutPad * kHid * 2;          // 8192
+constexpr int kBiasBytes = (4 * kHid + kOutPad) * 4;  // 4160
+constexpr int kOffW1 = 3 * kBigBytes, kOffW5 = kOffW1 + kW1Bytes, kOffBias = kOffW5 + kW5Bytes;
+constexpr int kImageBytes = kOffBias + kBiasBytes;
+// host parameter vector (PyTorch nn.Linear order, out x in): W1 b1 W2 b2 W3 b3 W4 b4 W5 b5
+constexpr long long kParams = (long long)kHid * kIn + kHid + 3LL * (kHid * kHid + kHid) + kOut * kHid + kOut;
+
+// shared memory map of the kernel
+constexpr int kSmWbuf = 0, kSmW1 = kBigBytes, kSmW5 = kSmW1 + kW1Bytes, kSmA = kSmW5 + kW5Bytes,
+              kSmBias = kSmA + kTileM * kHid * 2, kSmBar = kSmBias + kBiasBytes, kSmTmemSlot = kSmBar + 16,
+              kSmBytes = kSmTmemSlot + 16;
+static_assert(kSmBytes <= 227 * 1024, "the MLP kernel's shared memory fits one SM");
+static_assert(kSmBar % 8 == 0, "mbarriers are 8-byte aligned");
+
+// byte offset of element (row, k) in a K-major core-matrix image with K columns
+__host__ __device__ inline int packed_offset(int row, int k, int K) {
+    return (row % 8) * 16 + (row / 8) * (K / 8) * 128 + (k / 8) * 128 + (k % 8) * 2;
+}
+
+#ifdef __CUDACC__
+__device__ __forceinline__ uint32_t smem_u32(const void* p) {
+    return static_cast<uint32_t>(__cvta_generic_to_shared(p));
+}
+
+// UMMA shared-memory descriptor: no swizzle, K-major; LBO = 128 B (next core
+// matrix along K), SBO = stride between 8-row groups; version 1 (sm_100).
+__device__ __forceinline__ uint64_t smem_desc(uint32_t addr, uint32_t sbo_bytes) {
+    return uint64_t((addr & 0x3FFFF) >> 4) | (uint64_t(128 >> 4) << 16) | (uint64_t(sbo_bytes >> 4) << 32) |
+           (uint64_t(1) << 46);
+}
+
+// Instruction descriptor of kind::f16: D F32, A and B BF16, both K-major, M = 128.
+__device__ __forceinline__ uint32_t instr_desc(int n) {
+    return (1u << 4) | (1u << 7) | (1u << 10) | (uint32_t(n >> 3) << 17) | (uint32_t(128 >> 4) << 24);
+}
+
+__device__ __forceinline__ void mma_bf16(uint32_t tmem_d, uint64_t adesc, uint64_t bdesc, uint32_t idesc,
+                                         uint32_t accumulate) {
+    asm volatile(
+        "{\n\t.reg .pred p;\n\tsetp.ne.b32 p, %4, 0;\n\t"
+        "tcgen05.mma.cta_group::1.kind::f16 [%0], %1, %2, %3, {%5, %6, %7, %8}, p;\n\t}\n" ::"r"(tmem_d),
+        "l"(adesc), "l"(bdesc), "r"(idesc), "r"(accumulate), "r"(0), "r"(0), "r"(0), "r"(0));
+}
+
+__device__ __forceinline__ void mma_commit(uint32_t bar) {
+    asm volatile("tcgen05.commit.cta_group::1.mbarrier::arrive::one.shared::cluster.b64 [%0];" ::"r"(bar)
+                 : "memory");
+}
+
+__device__ __forceinline__ void mbar_init(uint32_t bar, uint32_t count) {
+    asm volatile("mbarrier.init.shared::cta.b64 [%0], %1;" ::"r"(bar), "r"(count) : "memory");
+}
+
+__device__ __forceinline__ bool mbar_test(uint32_t bar, uint32_t phase) {
+    uint32_t done;
+    asm volatile(
+        "{\n\t.reg .pred p;\n\tmbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2;\n\t"
+        "selp.u32 %0, 1, 0, p;\n\t}\n"
+        : "=r"(done)
+        : "r"(bar), "r"(phase)
+        : "memory");
+    return done != 0;
+}
+
+__device__ __forceinline__ unsigned long long dev_clock_ns() {
+    unsigned long long t;
+    asm volatile("mov.u64 %0, %globaltimer;" : "=l"(t));
+    return t;
+}
+
+// Wait for the mbarrier phase, at most limit_ns on the device clock.
+__device__ __forceinline__ bool mbar_wait(uint32_t bar, uint32_t phase, unsigned long long limit_ns) {
+    if (mbar_test(bar, phase)) return true;
+    const unsigned long long t0 = dev_clock_ns();
+    while (!mbar_test(bar, phase))
+        if (dev_clock_ns() - t0 > limit_ns) return false;
+    return true;
+}
+
+__device__ __forceinline__ void bulk_load(uint32_t dst, const void* src, uint32_t bytes, uint32_t bar) {
+    asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;" ::"r"(bar), "r"(bytes) : "memory");
+    asm volatile("cp.async.bulk.shared::cluster.global.mbarrier::complete_tx::bytes [%0], [%1], %2, [%3];" ::"r"(
+                     dst),
+                 "l"(src), "r"(bytes), "r"(bar)
+                 : "memory");
+}
+
+__device__ __forceinline__ void fence_async_smem() { asm volatile("fence.proxy.async.shared::cta;" ::: "memory"); }
+__device__ __forceinline__ void tc_fence_before() { asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory"); }
+__device__ __forceinline__ void tc_fence_after() { asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory"); }
+
+// 32 consecutive FP32 accumulator columns of this thread's TMEM lane.
+__device__ __forceinline__ void tmem_ld32(uint32_t taddr, float v[32]) {
+    uint32_t r[32];
+    asm volatile(
+        "tcgen05.ld.sync.aligned.32x32b.x32.b32 {%0, %1, %2, %3, %4, %5, %6, %7, %8, %9, %10, %11, %12, %13, %14, "
+        "%15, %16, %17, %18, %19, %20, %21, %22, %23, %24, %25, %26, %27, %28, %29, %30, %31}, [%32];"
+        : "=r"(r[0]), "=r"(r[1]), "=r"(r[2]), "=r"(r[3]), "=r"(r[4]), "=r"(r[5]), "=r"(r[6]), "=r"(r[7]),
+          "=r"(r[8]), "=r"(r[9]), "=r"(r[10]), "=r"(r[11]), "=r"(r[12]), "=r"(r[13]), "=r"(r[14]), "=r"(r[15]),
+          "=r"(r[16]), "=r"(r[17]), "=r"(r[18]), "=r"(r[19]), "=r"(r[20]), "=r"(r[21]), "=r"(r[22]), "=r"(r[23]),
+          "=r"(r[24]), "=r"(r[25]), "=r"(r[26]), "=r"(r[27]), "=r"(r[28]), "=r"(r[29]), "=r"(r[30]), "=r"(r[31])
+        : "r"(taddr));
+    asm volatile("tcgen05.wait::ld.sync.aligned;" ::: "memory");
+#pragma unroll
+    for (int i = 0; i < 32; ++i) v[i] = __uint_as_float(r[i]);
+}
+
+// 16 consecutive FP32 accumulator columns of this thread's TMEM lane.
+__device__ __forceinline__ void tmem_ld16(uint32_t taddr, float v[16]) {
+    uint32_t r[16];
+    asm volatile(
+        "tcgen05.ld.sync.aligned.32x32b.x16.b32 {%0, %1, %2, %3, %4, %5, %6, %7, %8, %9, %10, %11, %12, %13, %14, "
+        "%15}, [%16];"
+        : "=r"(r[0]), "=r"(r[1]), "=r"(r[2]), "=r"(r[3]), "=r"(r[4]), "=r"(r[5]), "=r"(r[6]), "=r"(r[7]),
+          "=r"(r[8]), "=r"(r[9]), "=r"(r[10]), "=r"(r[11]), "=r"(r[12]), "=r"(r[13]), "=r"(r[14]), "=r"(r[15])
+        : "r"(taddr));
+    asm volatile("tcgen05.wait::ld.sync.aligned;" ::: "memory");
+#pragma unroll
+    for (int i = 0; i < 16; ++i) v[i] = __uint_as_float(r[i]);
+}
+
+__device__ __forceinline__ float silu(float x) {
+    float t;
+    asm("tanh.approx.f32 %0, %1;" : "=f"(t) : "f"(0.5f * x));
+    return 0.5f * x * (1.f + t);
+}
+
+__device__ __forceinline__ uint32_t pack_bf16x2(float lo, float hi) {
+    const __nv_bfloat162 p = __floats2bfloat162_rn(lo, hi);
+    return *reinterpret_cast<const uint32_t*>(&p);
+}
+
+// Hidden-layer epilogue: accumulator + bias -> SiLU -> BF16 A operand (K = 256).
+__device__ __forceinline__ void epilogue_hidden(uint32_t tmem, const float* bias, unsigned char* A) {
+    const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+    const int q = warp & 3, half = warp >> 2;
+    const int row = q * 32 + lane;
+    unsigned char* arow = A + (row % 8) * 16 + (row / 8) * (kHid / 8) * 128;
+#pragma unroll 1
+    for (int c = 0; c < 4; ++c) {
+        const int col0 = half * 128 + c * 32;
+        float v[32];
+        tmem_ld32(tmem + (uint32_t(q * 32) << 16) + uint32_t(col0), v);
+#pragma unroll
+        for (int g = 0; g < 4; ++g) {
+            uint4 w;
+            const int k = col0 + g * 8;
+            w.x = pack_bf16x2(silu(v[g * 8 + 0] + bias[k + 0]), silu(v[g * 8 + 1] + bias[k + 1]));
+            w.y = pack_bf16x2(silu(v[g * 8 + 2] + bias[k + 2]), silu(v[g * 8 + 3] + bias[k + 3]));
+            w.z = pack_bf16x2(silu(v[g * 8 + 4] + bias[k + 4]), silu(v[g * 8 + 5] + bias[k + 5]));
+            w.w = pack_bf16x2(silu(v[g * 8 + 6] + bias[k + 6]), silu(v[g * 8 + 7] + bias[k + 7]));
+            *reinterpret_cast<uint4*>(arow + (k / 8) * 128) = w;
+        }
+    }
+}
+
+// out[n x 4] = MLP(feat[n x 5]). err[0] |= 1 when a wait timed out.
+__global__ void __launch_bounds__(kThreads, 1)
+    mlp_kernel(const unsigned char* __restrict__ wimg, const float* __restrict__ feat, long long n,
+               float* __restrict__ out, int* err, unsigned long long wait_limit_ns) {
+    extern __shared__ __align__(1024) unsigned char sm[];
+    unsigned char* Wbuf = sm + kSmWbuf;
+    unsigned char* W1s = sm + kSmW1;
+    unsigned char* W5s = sm + kSmW5;
+    unsigned char* A = sm + kSmA;
+    float* bias = reinterpret_cast<float*>(sm + kSmBias);
+    uint32_t* tslot = reinterpret_cast<uint32_t*>(sm + kSmTmemSlot);
+    const uint32_t bar_mma = smem_u32(sm + kSmBar), bar_tma = smem_u32(sm + kSmBar + 8);
+    const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
+    const long long ntiles = (n + kTileM - 1) / kTileM;
+
+    if (tid == 0) {
+        mbar_init(bar_mma, 1);
+        mbar_init(bar_tma, 1);
+        asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
+    }
+    if (warp == 0) {
+        asm volatile("tcgen05.alloc.cta_group::1.sync.aligned.shared::cta.b32 [%0], %1;" ::"r"(smem_u32(tslot)),
+                     "r"(256));
+        asm volatile("tcgen05.relinquish_alloc_permit.cta_group::1.sync.aligned;");
+    }
+    // resident operands: W1, W5 and the biases
+    {
+        const uint4* src1 = reinterpret_cast<const uint4*>(wimg + kOffW1);
+        uint4* dst1 = reinterpret_cast<uint4*>(W1s);
+        for (int i = tid; i < (kW1Bytes + kW5Bytes) / 16; i += kThreads) dst1[i] = src1[i];  // W1 | W5 contiguous
+        const float4* srcb = reinterpret_cast<const float4*>(wimg + kOffBias);
+        float4* dstb = reinterpret_cast<float4*>(bias);
+        for (int i = tid; i < kBiasBytes / 16; i += kThreads) dstb[i] = srcb[i];
+    }
+    fence_async_smem();
+    tc_fence_before();
+    __syncthreads();
+    tc_fence_after();
+    const uint32_t tmem = *tslot;
+
+    uint32_t ph_mma = 0, ph_tma = 0;
+    bool tma_pending = false;
+    bool ok = true;
+    if (tid == 0 && blockIdx.x < ntiles) bulk_load(smem_u32(Wbuf), wimg, kBigBytes, bar_tma);
+    tma_pending = blockIdx.x < ntiles;
+
+    for (long long tile = blockIdx.x; tile < ntiles; tile += gridDim.x) {
+        const long long row0 = tile * kTileM;
+        // X tile: 128 rows x 16 BF16 (features 0..4, zero padding)
+        {
+            const int r = tid >> 1, chunk = tid & 1;
+            uint4 w = make_uint4(0, 0, 0, 0);
+            const long long gr = row0 + r;
+            if (chunk == 0 && gr < n) {
+                const float* f = feat + gr * kIn;
+                w.x = pack_bf16x2(f[0], f[1]);
+                w.y = pack_bf16x2(f[2], f[3]);
+                w.z = pack_bf16x2(f[4], 0.f);
+            }
+            *reinterpret_cast<uint4*>(A + packed_offset(r, chunk * 8, kInPad)) = w;
+        }
+        fence_async_smem();
+        __syncthreads();
+        // layer 1: K = 16, one instruction
+        if (tid == 0) {
+            tc_fence_after();
+            mma_bf16(tmem, smem_desc(smem_u32(A), (kInPad / 8) * 128), smem_desc(smem_u32(W1s), (kInPad / 8) * 128),
+                     instr_desc(kHid), 0u);
+            mma_commit(bar_mma);
+        }
+        ok = mbar_wait(bar_mma, ph_mma, wait_limit_ns);
+        ph_mma ^= 1;
+        ok = __syncthreads_and(ok);
+            if (!ok) break;
+        tc_fence_after();
+        epilogue_hidden(tmem, bias, A);
+        tc_fence_before();
+        fence_async_smem();
+        __syncthreads();
+        // layers 2..4: K = 256 (16 instructions), weights streamed into Wbuf
+        for (int L = 0; L < 3 && ok; ++L) {
+            ok = mbar_wait(bar_tma, ph_tma, wait_limit_ns);
+            ok = __syncthreads_and(ok);
+            if (!ok) break;
+            ph_tma ^= 1;
+            tma_pending = false;
+            if (tid == 0) {
+                tc_fence_after();
+#pragma unroll 1
+                for (int s = 0; s < kHid / 16; ++s)
+                    mma_bf16(tmem, smem_desc(smem_u32(A) + s * 256, (kHid / 8) * 128),
+                             smem_desc(smem_u32(Wbuf) + s * 256, (kHid / 8) * 128), instr_desc(kHid), s > 0);
+                mma_commit(bar_mma);
+            }
+            ok = mbar_wait(bar_mma, ph_mma, wait_limit_ns);
+            ph_mma ^= 1;
+            ok = __syncthreads_and(ok);
+            if (!ok) break;
+            // Wbuf is drained: bring the next layer's weights (or layer 2's for the next tile)
+            const bool more = L < 2 || tile + gridDim.x < ntiles;
+            if (more) {
+                if (tid == 0) bulk_load(smem_u32(Wbuf), wimg + size_t(L < 2 ? L + 1 : 0) * kBigBytes, kBigBytes, bar_tma);
+                tma_pending = true;
+            }
+            tc_fence_after();
+            epilogue_hidden(tmem, bias + (L + 1) * kHid, A);
+            tc_fence_before();
+            fence_async_smem();
+            __syncthreads();
+        }
+        if (!ok) break;
+        // layer 5: N = 16 (4 outputs used), K = 256
+        if (tid == 0) {
+            tc_fence_after();
+#pragma unroll 1
+            for (int s = 0; s < kHid / 16; ++s)
+                mma_bf16(tmem, smem_desc(smem_u32(A) + s * 256, (kHid / 8) * 128),
+                         smem_desc(smem_u32(W5s) + s * 256, (kHid / 8) * 128), instr_desc(kOutPad), s > 0);
+            mma_commit(bar_mma);
+        }
+        ok = mbar_wait(bar_mma, ph_mma, wait_limit_ns);
+        ph_mma ^= 1;
+        ok = __syncthreads_and(ok);
+            if (!ok) break;
+        tc_fence_after();
+        if (warp < 4) {
+            float v[16];
+            tmem_ld16(tmem + (uint32_t(warp * 32) << 16), v);
+            const long long gr = row0 + warp * 32 + lane;
+            if (gr < n) {
+                const float* b5 = bias + 4 * kHid;
+                float4 o = make_float4(v[0] + b5[0], v[1] + b5[1], v[2] + b5[2], v[3] + b5[3]);
+                *reinterpret_cast<float4*>(out + gr * kOut) = o;
+            }
+        }
+        tc_fence_before();
+        __syncthreads();
+    }
+    if (!ok) {
+        if (tid == 0) atomicOr(err, 1);
+        // MMAs possibly still in flight complete before their TMEM is freed
+        mbar_wait(bar_mma, ph_mma, wait_limit_ns);
+    }
+    // a weight copy still in flight must land before the block exits
+    if (tma_pending) {
+        const bool landed = mbar_wait(bar_tma, ph_tma, wait_limit_ns);
+        if (!landed && tid == 0) atomicOr(err, 2);
+    }
+    tc_fence_before();
+    __syncthreads();
+    tc_fence_after();
+    if (warp == 0)
+        asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, %1;" ::"r"(tmem), "r"(256));
+}
+#endif  // __CUDACC__
+
+// Host: pack the parameter vector (W1 b1 ... W5 b5, nn.Linear order) into the
+// kernel's weight image (BF16 core-matrix layouts, FP32 biases).
+inline void pack_weights(const float* p, unsigned char* img) {
+    auto bf16 = [](float x) -> uint16_t {
+        uint32_t u;
+        __builtin_memcpy(&u, &x, 4);
+        if ((u & 0x7f800000u) == 0x7f800000u) return uint16_t(u >> 16);  // inf / nan
+        const uint32_t r = 0x7fffu + ((u >> 16) & 1u);                  // round to nearest even
+        return uint16_t((u + r) >> 16);
+    };
+    for (int i = 0; i < kImageBytes; ++i) img[i] = 0;
+    auto put = [&](int off, int rows, int K, int kin, const float* W) {
+        for (int r = 0; r < rows; ++r)
+            for (int k = 0; k < kin; ++k) {
+                const uint16_t h = bf16(W[r * kin + k]);
+                __builtin_memcpy(img + off + packed_offset(r, k, K), &h, 2);
+            }
+    };
+    const float* W1 = p;
+    const float* b1 = W1 + kHid * kIn;
+    const float* W2 = b1 + kHid;
+    const float* b2 = W2 + kHid * kHid;
+    const float* W3 = b2 + kHid;
+    const float* b3 = W3 + kHid * kHid;
+    const float* W4 = b3 + kHid;
+    const float* b4 = W4 + kHid * kHid;
+    const float* W5 = b4 + kHid;
+    const float* b5 = W5 + kOut * kHid;
+    put(0, kHid, kHid, kHid, W2);
+    put(kBigBytes, kHid, kHid, kHid, W3);
+    put(2 * kBigBytes, kHid, kHid, kHid, W4);
+    put(kOffW1, kHid, kInPad, kIn, W1);
+    put(kOffW5, kOut, kHid, kHid, W5);
+    float* bias = reinterpret_cast<float*>(img + kOffBias);
+    for (int i = 0; i < kHid; ++i) {
+        bias[i] = b1[i];
+        bias[kHid + i] = b2[i];
+        bias[2 * kHid + i] = b3[i];
+        bias[3 * kHid + i] = b4[i];
+    }
+    for (int i = 0; i < kOut; ++i) bias[4 * kHid + i] = b5[i];
+}
+
+}  // namespace surrogate
+}  // namespace sirius

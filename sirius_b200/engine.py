@@ -22,7 +22,8 @@ EXPORTS = [
     "sirius_cuda_get_last_error", "sirius_cuda_configure", "sirius_cuda_trace_frames",
     "sirius_cuda_trace_frames_device", "sirius_cuda_trace_rays", "sirius_cuda_metric_evaluate",
     "sirius_cuda_dp45_step", "sirius_cuda_last_stats", "sirius_cuda_autotune", "sirius_cuda_measure_fma_peak",
-    "sirius_cuda_flop_count", "sirius_cuda_trace_frames_static",
+    "sirius_cuda_flop_count", "sirius_cuda_trace_frames_static", "sirius_cuda_surrogate_load",
+    "sirius_cuda_surrogate_infer",
 ]
 
 
@@ -48,6 +49,8 @@ def load_library(path=LIB_PATH):
                                                   C.c_void_p, C.c_void_p, C.c_void_p]
     L.sirius_cuda_trace_frames_static.argtypes = [C.c_void_p, C.c_void_p, C.c_int32, C.c_int64, C.c_void_p,
                                                   C.c_void_p, C.c_void_p, C.c_void_p]
+    L.sirius_cuda_surrogate_load.argtypes = [C.c_void_p, C.c_void_p, C.c_int64]
+    L.sirius_cuda_surrogate_infer.argtypes = [C.c_void_p, C.c_void_p, C.c_int64, C.c_void_p, C.c_void_p]
     L.sirius_cuda_trace_rays.argtypes = [C.c_void_p, _P(abi.Metric), C.c_double, C.c_double, C.c_void_p,
                                          C.c_int64, C.c_void_p]
     L.sirius_cuda_metric_evaluate.argtypes = [C.c_void_p, _P(abi.Metric), C.c_void_p, C.c_int64, C.c_int32,
@@ -139,6 +142,15 @@ class Engine:
         device array: no device allocation (at most SIRIUS_STATIC_MAX_FRAMES frames)."""
         self._check(self.lib.sirius_cuda_trace_frames_static(self.h, d_frames, n_frames, total, d_results, d_image,
                                                              d_spectra, stream))
+
+    def surrogate_load(self, params):
+        """Surrogate MLP weights: SURROGATE_PARAMS floats, nn.Linear order (W1 b1 ... W5 b5)."""
+        p = np.ascontiguousarray(params, dtype=np.float32).ravel()
+        self._check(self.lib.sirius_cuda_surrogate_load(self.h, p.ctypes.data, p.size))
+
+    def surrogate_infer(self, d_features, n, d_out, stream=None):
+        """MLP on n x 5 device features into n x 4 device outputs."""
+        self._check(self.lib.sirius_cuda_surrogate_infer(self.h, d_features, n, d_out, stream))
 
     def trace_rays(self, metric, rays, disk_inner=0.0, disk_outer=20.0):
         n = len(rays)
