@@ -215,6 +215,71 @@ def cpu_baseline_sample(seconds=12.0):
                       f"(the reference's gray volumetric march replaces its disk)"}
 
 
+SURROGATE_SIDE = 2048
+SURROGATE_WEIGHTS = os.path.join(ROOT, "sirius_b200", "data", "surrogate_kerr.npy")
+
+
+def surrogate_config(abi, precision):
+    """Surrogate workload: thin NT disk only, no volumetric transfer; the gated
+    rays integrate in mixed precision without the FP64 near-critical rule (the
+    surrogate's error budget is 1e-3 of the image scale)."""
+    return abi.default_config(abs_tolerance=1e-8, rel_tolerance=1e-8, min_step=1e-9, max_step=2.0,
+                              initial_step=0.1, escape_radius=200.0, horizon_factor=1.01, max_steps=10000,
+                              precision=precision, enable_disk=1, enable_volumetric=0, critical_band=0.0)
+
+
+def surrogate_leg(eng, abi, np, torch, dev, stream, side=SURROGATE_SIDE, reps=3):
+    """Surrogate-gated rendering of the Kerr a = 0.9 frame at side^2 (gate +-0.3 M
+    around the critical curve, 1 % audit rays) against the plain FP64 integrator
+    on the same frame; CUDA events on the launch stream around whole calls."""
+    params = np.load(SURROGATE_WEIGHTS)
+    eng.surrogate_load(params)
+    frame = workload_frame(abi, side, side)
+    n = side * side
+    d_img = torch.empty(n, dtype=torch.float32, device=dev)
+    d_gate = torch.empty(n, dtype=torch.uint8, device=dev)
+    eng.configure(surrogate_config(abi, abi.PRECISION_FP64))
+    fp64_ms = []
+    for i in range(2):
+        _, img64, _ = eng.trace_frames([frame], results=False)
+        fp64_ms.append(eng.stats().kernel_ms)
+    eng.configure(surrogate_config(abi, abi.PRECISION_MIXED))
+    ev0, ev1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    for _ in range(2):
+        eng.render_surrogate_device([frame], d_img.data_ptr(), None, d_gate.data_ptr(), stream=stream.cuda_stream)
+    times, stats = [], None
+    for _ in range(reps):
+        ev0.record(stream)
+        stats = eng.render_surrogate_device([frame], d_img.data_ptr(), None, d_gate.data_ptr(),
+                                            stream=stream.cuda_stream)
+        ev1.record(stream)
+        torch.cuda.synchronize()
+        times.append(ev0.elapsed_time(ev1))
+    ms = float(np.mean(times))
+    img = d_img.cpu().numpy().astype(np.float64)
+    gate = d_gate.cpu().numpy()
+    err = np.abs(img - img64) / img64.max()
+    t64 = float(np.min(fp64_ms))
+    flops = 2.0 * 198912 * n
+    peaks = {}
+    if os.path.exists(MEASURED_PEAKS):
+        with open(MEASURED_PEAKS) as f:
+            peaks = json.load(f)
+    bf16_peak = float(peaks.get("bf16_tflops", 1590.0))
+    return {"workload": f"kerr_a0.9_{side}x{side}_nt_disk_surrogate_gated", "mrays_per_s": n / (ms * 1e-3) / 1e6,
+            "ms_per_frame": ms, "fp64_plain_ms": t64, "speedup_vs_fp64_plain": t64 / ms,
+            "gate_band_m": 0.3, "audit_fraction": 0.01, "gated_fraction": float(np.mean(gate == 1)),
+            "audit_fraction_measured": float(np.mean(gate == 2)), "integrated_rays": int(stats.integrated),
+            "stage_ms": {"features_gate": stats.ms_features, "mlp": stats.ms_mlp, "shade": stats.ms_shade,
+                         "integrate_gated_and_audit": stats.ms_trace},
+            "error_vs_fp64": {"image_linf_rel": float(err.max()), "image_p99_rel": float(np.percentile(err, 99)),
+                              "image_mean_rel": float(err.mean())},
+            "mlp_roofline": {"bound": "tensor", "achieved": flops / (stats.ms_mlp * 1e-3) / 1e12,
+                             "peak": bf16_peak, "unit": "TFLOP/s", "frac": flops / (stats.ms_mlp * 1e-3) / 1e12 / bf16_peak,
+                             "peak_source": "MEASURED_PEAKS.json bf16_tflops (burst)" if peaks else "fallback"},
+            "weights": "sirius_b200/data/surrogate_kerr.npy (python -m sirius_b200.surrogate_train)"}
+
+
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
@@ -354,6 +419,7 @@ def main():
         line["error_vs_fp64"] = {"image_linf_rel": float(err.max()), "image_p99_rel": float(np.percentile(err, 99)),
                                  "spectra_linf_rel": float(serr.max()),
                                  "spectra_p99_rel": float(np.percentile(serr, 99))}
+        line["surrogate"] = surrogate_leg(eng, abi, np, torch, dev, stream)
         line["cpu_baseline"] = cpu_baseline_sample()
     if rank == 0:
         print(json.dumps(line), flush=True)

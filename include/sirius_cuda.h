@@ -172,7 +172,7 @@ typedef struct sirius_trace_config {
                                     runs every step in FP64 */
     double symplectic_step;      /* fixed d-lambda of the symplectic integrator */
     int32_t symplectic_order;    /* 4, 6 or 8 (Yoshida) */
-    int32_t block_size;          /* threads per block (0 = autotuned / default) */
+    int32_t block_size;          /* threads per block of the trace kernel: 32, 64 or 128 (0 = 128) */
     int32_t refill_threshold;    /* persistent mode: refill a warp when fewer than this many lanes are
                                     live (1..32; 0 = 1, i.e. only once the whole warp is done, which keeps
                                     the 32 rays of a warp on neighbouring pixels and so coherent) */
@@ -296,6 +296,44 @@ int sirius_cuda_trace_frames_static(sirius_cuda_handle handle,
 int sirius_cuda_surrogate_load(sirius_cuda_handle handle, const float* params, int64_t n_params);
 int sirius_cuda_surrogate_infer(sirius_cuda_handle handle, const float* d_features, int64_t n, float* d_out,
                                 void* stream);
+
+/* Surrogate-gated rendering of Kerr frames (thin Novikov-Thorne disk).
+ * Per pixel: features f = (2 a* - 1, (theta_o[deg] - 47)/42, alpha/20, beta/20,
+ * (r_obs - 110)/90) with the celestial coordinates of the camera ray's own
+ * constants of motion, alpha = -L_z / (E sin theta_o), beta = p_theta / E; the MLP
+ * predicts (disk-hit logit, r_1 = 15 (1 + o_1), g_1, higher-order intensity / 1e-3)
+ * and the pixel takes g_1^4 F(r_1) + higher orders. Rays within gate_band (M) of
+ * the critical curve (Bardeen's spherical photon orbits at the camera's
+ * inclination), an audit_fraction of the others (runs of 32 consecutive pixels
+ * chosen by a hash seeded with audit_seed), and
+ * every ray of a frame that is not charge- and Lambda-free Kerr are integrated
+ * instead (the configured integrator, compacted into one launch) and overwrite
+ * their pixels. gate (optional): per pixel 0 = MLP, 1 = gated, 2 = audit. */
+typedef struct {
+    double gate_band;          /* half width of the gate around the critical curve, M (0.3) */
+    double audit_fraction;     /* fraction of ungated rays also integrated (0.01) */
+    uint32_t audit_seed;
+    int32_t reserved[5];
+} sirius_surrogate_config;
+
+typedef struct {
+    int64_t rays, integrated;
+    float ms_features, ms_mlp, ms_shade, ms_trace, ms_total;  /* CUDA-event times of the stages */
+    int32_t reserved[3];
+} sirius_surrogate_stats;
+
+/* features (n x 5 floats, device) and gate (n bytes, device, may be NULL) of the frames' pixels */
+int sirius_cuda_surrogate_features(sirius_cuda_handle handle, const sirius_frame* frames, int32_t n_frames,
+                                   const sirius_surrogate_config* config, float* d_features, uint8_t* d_gate,
+                                   void* stream);
+/* host frame descriptors, device outputs; synchronous on return */
+int sirius_cuda_render_surrogate_device(sirius_cuda_handle handle, const sirius_frame* frames, int32_t n_frames,
+                                        const sirius_surrogate_config* config, float* d_image, float* d_image_mlp,
+                                        uint8_t* d_gate, void* stream, sirius_surrogate_stats* stats);
+/* host buffers (image_mlp: the MLP's own image before the integrated rays overwrite it; may be NULL) */
+int sirius_cuda_render_surrogate(sirius_cuda_handle handle, const sirius_frame* frames, int32_t n_frames,
+                                 const sirius_surrogate_config* config, float* image, float* image_mlp,
+                                 uint8_t* gate, sirius_surrogate_stats* stats);
 
 /* ---- batch form of GeodesicTracer::trace(const CameraRay&) (GTRC001A.h:220) ----
  * Host-generated rays through one metric; disk_inner <= 0 selects the ISCO. */

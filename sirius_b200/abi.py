@@ -114,6 +114,21 @@ class LaunchStats(C.Structure):
                 ("status_flags", C.c_int32)]
 
 
+class SurrogateConfig(C.Structure):
+    _fields_ = [("gate_band", C.c_double), ("audit_fraction", C.c_double), ("audit_seed", C.c_uint32),
+                ("reserved", C.c_int32 * 5)]
+
+
+class SurrogateStats(C.Structure):
+    _fields_ = [("rays", C.c_int64), ("integrated", C.c_int64), ("ms_features", C.c_float), ("ms_mlp", C.c_float),
+                ("ms_shade", C.c_float), ("ms_trace", C.c_float), ("ms_total", C.c_float),
+                ("reserved", C.c_int32 * 3)]
+
+
+def surrogate_config(gate_band=0.3, audit_fraction=0.01, audit_seed=0):
+    return SurrogateConfig(gate_band, audit_fraction, audit_seed)
+
+
 # numpy structured dtype of RayResult (for zero-copy views of result arrays)
 def result_dtype():
     import numpy as np

@@ -33,6 +33,8 @@ static_assert(sizeof(sirius_metric) == 80, "sirius_metric layout");
 static_assert(sizeof(sirius_camera) == 64, "sirius_camera layout");
 static_assert(sizeof(sirius_frame) == 168, "sirius_frame layout");
 static_assert(sizeof(sirius_camera_ray) == 64, "sirius_camera_ray layout");
+static_assert(sizeof(sirius_surrogate_config) == 40, "sirius_surrogate_config layout");
+static_assert(sizeof(sirius_surrogate_stats) == 48, "sirius_surrogate_stats layout");
 
 namespace {
 
@@ -46,6 +48,7 @@ struct Params {
     float* image;
     float* spectra;
     const sirius_camera_ray* host_rays;  // optional: explicit camera rays (device copy)
+    const unsigned* list;                 // optional: trace only these ray indices (total = list length)
     unsigned long long* queue;            // [0] ray cursor
     unsigned long long* counters;         // [0] accepted, [1] rejected, [2] fp64 steps
     int* status;                          // [0] watchdog flag
@@ -574,8 +577,9 @@ __global__ void __launch_bounds__(128, MINB) trace_kernel(Params P) {
     t_start = __shfl_sync(kFull, t_start, 0);
 
     if (!P.persistent) {
-        const long long idx = (long long)blockIdx.x * blockDim.x + threadIdx.x;
-        if (idx < P.total) {
+        const long long gid = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+        if (gid < P.total) {
+            const long long idx = P.list ? (long long)P.list[gid] : gid;
             const int frame = P.n_frames > 1 ? find_frame(P.frames, P.n_frames, idx) : 0;
             if (P.family < 0 || P.frames[frame].m.family == P.family) {
                 begin_ray<MIXED, FAM>(P, s, idx, frame, vol);
@@ -594,8 +598,9 @@ __global__ void __launch_bounds__(128, MINB) trace_kernel(Params P) {
                 base = __shfl_sync(kFull, base, 0);
                 if (base >= (unsigned long long)P.total) exhausted = true;
                 if (!alive) {
-                    const unsigned long long idx = base + __popc(dead & lt_mask);
-                    if (idx < (unsigned long long)P.total) {
+                    const unsigned long long q = base + __popc(dead & lt_mask);
+                    if (q < (unsigned long long)P.total) {
+                        const unsigned long long idx = P.list ? (unsigned long long)P.list[q] : q;
                         const int frame = P.n_frames > 1 ? find_frame(P.frames, P.n_frames, (long long)idx) : 0;
                         begin_ray<MIXED, FAM>(P, s, (long long)idx, frame, vol);
                         alive = true;
@@ -676,6 +681,166 @@ TraceFn pick_kernel(bool mixed, int minb, int fam) {
         default:
             return mixed ? trace_kernel<true, 2, kAnyFamily> : trace_kernel<false, 2, kAnyFamily>;
     }
+}
+
+// ---------------------------------------------------------------------------
+// Surrogate-gated rendering: features and gate per pixel, the MLP on every
+// pixel, shading from its outputs, then the integrator on the compacted list
+// of gated (near-critical) and audit rays, which overwrite their pixels.
+// ---------------------------------------------------------------------------
+constexpr int kCurveN = 256;      // critical-curve points per frame, ordered by angle about its centre
+constexpr float kSurRScale = 15.f;   // MLP output 1: r_1 = 15 (1 + o_1)
+constexpr float kSurHigher = 1e-3f;  // MLP output 3: higher-order intensity / 1e-3
+
+struct SurFrameDev {
+    double sin_o, theta_deg;      // camera Boyer-Lindquist polar angle
+    float ac;                     // centre (alpha_c, 0) of the critical curve
+    int kerr;                     // 1: Kerr frame (no charge, no Lambda) the MLP covers; 0: integrate every ray
+    float ca[kCurveN], cb[kCurveN];
+};
+
+__device__ __forceinline__ unsigned audit_hash(unsigned long long idx, unsigned seed) {
+    unsigned long long z = idx * 0x9E3779B97F4A7C15ull + seed;
+    z = (z ^ (z >> 30)) * 0xBF58476D1CE4E5B9ull;
+    z = (z ^ (z >> 27)) * 0x94D049BB133111EBull;
+    return unsigned((z ^ (z >> 31)) >> 32);
+}
+
+__device__ __forceinline__ float seg_dist2(float px, float py, float ax, float ay, float bx, float by) {
+    const float ux = bx - ax, uy = by - ay, vx = px - ax, vy = py - ay;
+    const float t = fminf(fmaxf((vx * ux + vy * uy) / fmaxf(ux * ux + uy * uy, 1e-20f), 0.f), 1.f);
+    const float dx = vx - t * ux, dy = vy - t * uy;
+    return dx * dx + dy * dy;
+}
+
+// features (a, inclination, alpha, beta, r_obs), normalised; gate: 1 = within
+// `band` of the critical curve (or a frame the MLP does not cover), 2 = audit.
+__global__ void sur_features_kernel(const FrameDev* frames, const SurFrameDev* sf, int n_frames, long long total,
+                                    float band, unsigned audit_threshold, unsigned seed, float* feat,
+                                    unsigned char* gate, unsigned* block_counts) {
+    const long long idx = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+    bool take = false;
+    if (idx < total) {
+        const int f = n_frames > 1 ? find_frame(frames, n_frames, idx) : 0;
+        const FrameDev& F = frames[f];
+        const SurFrameDev& S = sf[f];
+        const long long pix = idx - F.ray_offset;
+        double dir[4], x[4], p[4];
+        camera_dir(F, int(pix % F.width), int(pix / F.width), dir);
+        init_state(F, dir, x, p);
+        // celestial coordinates from the ray's own constants of motion:
+        // alpha = -L_z / (E sin theta_o), beta = p_theta / E
+        InvForm IF;
+        inv_form(F.m, x, IF);
+        const double r = IF.r, E = -p[0], L = x[1] * p[2] - x[2] * p[1];
+        const double ct = fmin(fmax(x[3] / r, -1.0), 1.0), st = sqrt(fmax(1.0 - ct * ct, 1e-30));
+        const double pth = (ct / st) * (x[1] * p[1] + x[2] * p[2]) - r * st * p[3];
+        const float alpha = float(-L / (E * S.sin_o)), beta = float(pth / E);
+        float* o = feat + idx * 5;
+        o[0] = float(2.0 * F.a_star - 1.0);
+        o[1] = float((S.theta_deg - 47.0) / 42.0);
+        o[2] = alpha / 20.f;
+        o[3] = beta / 20.f;
+        o[4] = float((F.cam_r - 110.0) / 90.0);
+        unsigned char g = 0;
+        if (!S.kerr) {
+            g = 1;
+        } else {
+            const float dx = alpha - S.ac, dy = beta;
+            const float phi = atan2f(dy, dx);
+            const int j0 = int(floorf((phi + float(kPi)) * (kCurveN / (2.f * float(kPi)))));
+            float d2 = 1e30f;
+            for (int k = j0 - 6; k <= j0 + 6; ++k) {
+                const int a = ((k % kCurveN) + kCurveN) % kCurveN, b = (a + 1) % kCurveN;
+                d2 = fminf(d2, seg_dist2(alpha, beta, S.ca[a], S.cb[a], S.ca[b], S.cb[b]));
+            }
+            if (d2 < band * band) g = 1;
+        }
+        // audit rays come in runs of 32 consecutive pixels, so that they integrate as coherent warps
+        if (!g && audit_hash((unsigned long long)idx >> 5, seed) < audit_threshold) g = 2;
+        gate[idx] = g;
+        take = g != 0;
+    }
+    // rays to integrate, counted per block (the list is built in pixel order by
+    // sur_scan_kernel and sur_scatter_kernel)
+    __shared__ unsigned warp_counts[32];
+    const unsigned m = __ballot_sync(kFull, take);
+    if ((threadIdx.x & 31) == 0) warp_counts[threadIdx.x >> 5] = __popc(m);
+    __syncthreads();
+    if (threadIdx.x == 0) {
+        unsigned c = 0;
+        for (int w = 0; w < int(blockDim.x >> 5); ++w) c += warp_counts[w];
+        block_counts[blockIdx.x] = c;
+    }
+}
+
+// Exclusive prefix sum of the per-block counts (one block of 1024 threads);
+// block_counts[n_blocks] receives the total.
+__global__ void sur_scan_kernel(unsigned* block_counts, int n_blocks) {
+    __shared__ unsigned part[1024];
+    const int t = threadIdx.x;
+    const int per = (n_blocks + 1023) / 1024;
+    const int b0 = t * per, b1 = min(b0 + per, n_blocks);
+    unsigned sum = 0;
+    for (int b = b0; b < b1; ++b) sum += block_counts[b];
+    part[t] = sum;
+    __syncthreads();
+    for (int off = 1; off < 1024; off <<= 1) {  // Hillis-Steele inclusive scan
+        const unsigned v = t >= off ? part[t - off] : 0u;
+        __syncthreads();
+        part[t] += v;
+        __syncthreads();
+    }
+    unsigned run = t > 0 ? part[t - 1] : 0u;
+    for (int b = b0; b < b1; ++b) {
+        const unsigned c = block_counts[b];
+        block_counts[b] = run;
+        run += c;
+    }
+    if (t == 1023) block_counts[n_blocks] = part[1023];
+}
+
+// The list of rays to integrate in pixel order (same blocking as the features kernel).
+__global__ void sur_scatter_kernel(const unsigned char* gate, long long total, const unsigned* block_offsets,
+                                   unsigned* list) {
+    __shared__ unsigned warp_base[32];
+    const long long idx = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+    const bool take = idx < total && gate[idx] != 0;
+    const unsigned m = __ballot_sync(kFull, take);
+    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+    if (lane == 0) warp_base[warp] = __popc(m);
+    __syncthreads();
+    if (threadIdx.x == 0) {
+        unsigned run = block_offsets[blockIdx.x];
+        for (int w = 0; w < int(blockDim.x >> 5); ++w) {
+            const unsigned c = warp_base[w];
+            warp_base[w] = run;
+            run += c;
+        }
+    }
+    __syncthreads();
+    if (take) list[warp_base[warp] + __popc(m & ((1u << lane) - 1u))] = unsigned(idx);
+}
+
+// pixel intensity from the MLP outputs: hit logit, r_1, g_1, higher orders
+// Pixels the integrator takes (gate != 0) get only the MLP copy: the
+// integrator writes their image value.
+__global__ void sur_shade_kernel(const FrameDev* frames, int n_frames, long long total, const float* out,
+                                 const unsigned char* gate, float* image, float* image_mlp) {
+    const long long idx = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+    if (idx >= total) return;
+    const int f = n_frames > 1 ? find_frame(frames, n_frames, idx) : 0;
+    const FrameDev& F = frames[f];
+    const float4 o = reinterpret_cast<const float4*>(out)[idx];
+    double I = 0.0;
+    if (o.x > 0.f) {
+        const double r1 = fmin(fmax(double(kSurRScale) * (1.0 + double(o.y)), F.disk_in), F.disk_out);
+        const double g1 = fmax(double(o.z), 0.0);
+        I = g1 * g1 * g1 * g1 * nt_flux(r1, F.a_star, F.isco, F.disk_in, F.disk_out);
+    }
+    I += fmax(double(o.w), 0.0) * double(kSurHigher);
+    if (gate[idx] == 0) image[idx] = float(I);
+    if (image_mlp) image_mlp[idx] = float(I);
 }
 
 __global__ void metric_kernel(MetricDev m, const double* pos, long long n, int fp32, double* g, double* dg) {
@@ -759,6 +924,20 @@ struct Handle {
     int family_mask = 0;  // bit f: a frame of the last upload is of metric family f
     unsigned char* d_surrogate = nullptr;  // packed surrogate weight image (surrogate::kImageBytes)
     int* d_sur_err = nullptr;
+    // surrogate-gated rendering scratch
+    SurFrameDev* d_sur_frames = nullptr;
+    size_t sur_frames_cap = 0;
+    float* d_feat = nullptr;
+    size_t feat_cap = 0;
+    float* d_mlp_out = nullptr;
+    size_t mlp_out_cap = 0;
+    unsigned* d_list = nullptr;
+    size_t list_cap = 0;
+    unsigned char* d_gate = nullptr;
+    size_t gate_cap = 0;
+    unsigned* d_block_counts = nullptr;  // per-block counts, then offsets; [n_blocks] = list length
+    size_t block_counts_cap = 0;
+    cudaEvent_t sev[5] = {};
 };
 
 int fail(Handle* h, int code, const std::string& msg) {
@@ -902,8 +1081,8 @@ int validate_config(Handle* H, const sirius_trace_config& c) {
         (!(c.symplectic_step > 0) || (c.symplectic_order != 4 && c.symplectic_order != 6 && c.symplectic_order != 8)))
         return fail(H, SIRIUS_ERR_INVALID_ARGUMENT, "symplectic_step must be > 0 and symplectic_order 4, 6 or 8");
     if (c.compat) return fail(H, SIRIUS_ERR_UNSUPPORTED, "reference-compatible mode is not available on the GPU path");
-    if (c.block_size < 0 || c.block_size > 1024 || (c.block_size % 32) != 0)
-        return fail(H, SIRIUS_ERR_INVALID_ARGUMENT, "block_size must be a multiple of 32 in 0..1024");
+    if (c.block_size != 0 && c.block_size != 32 && c.block_size != 64 && c.block_size != 128)
+        return fail(H, SIRIUS_ERR_INVALID_ARGUMENT, "block_size must be 0, 32, 64 or 128");
     if (c.refill_threshold < 0 || c.refill_threshold > 32)
         return fail(H, SIRIUS_ERR_INVALID_ARGUMENT, "refill_threshold must be in 0..32");
     return SIRIUS_OK;
@@ -920,7 +1099,7 @@ struct LaunchScratch {
 
 int launch_trace(Handle* H, int n_frames, long long total, sirius_ray_result* d_results, float* d_image,
                  float* d_spectra, const sirius_camera_ray* d_rays, cudaStream_t st, bool timed,
-                 const LaunchScratch* scratch = nullptr) {
+                 const LaunchScratch* scratch = nullptr, const unsigned* d_list = nullptr) {
     const sirius_trace_config& c = H->cfg;
     const LaunchScratch own{H->d_frames, H->d_queue, H->d_status};
     const LaunchScratch& S = scratch ? *scratch : own;
@@ -932,6 +1111,7 @@ int launch_trace(Handle* H, int n_frames, long long total, sirius_ray_result* d_
     P.image = d_image;
     P.spectra = d_spectra;
     P.host_rays = d_rays;
+    P.list = d_list;
     P.queue = S.queue;
     P.counters = S.queue + 1;
     P.clock0 = S.queue + 4;
@@ -944,7 +1124,9 @@ int launch_trace(Handle* H, int n_frames, long long total, sirius_ray_result* d_
     // different stages of their paths and diverges, so refills default to whole warps.
     P.persistent = c.blocks_per_sm != 0 ? 1 : 0;
     P.refill_threshold = c.refill_threshold > 0 ? c.refill_threshold : 1;
-    const int block = 128;  // matches __launch_bounds__
+    // 32, 64 or 128 threads per block (__launch_bounds__ allows 128): small
+    // launches (a list of gated rays) spread over more SMs with smaller blocks
+    const int block = (c.block_size == 32 || c.block_size == 64) ? c.block_size : 128;
     const size_t shmem = size_t(2) * P.c.nbins * block * sizeof(float);
     // register budget: blocks_per_sm in 1..4 selects the kernel compiled for that
     // many resident 128-thread blocks per SM (fewer registers, possibly spills)
@@ -1122,6 +1304,9 @@ int sirius_cuda_destroy(sirius_cuda_handle h) {
     cudaFree(H->d_frames); cudaFree(H->d_results); cudaFree(H->d_image); cudaFree(H->d_spectra);
     cudaFree(H->d_rays); cudaFree(H->d_queue); cudaFree(H->d_status);
     cudaFree(H->d_surrogate); cudaFree(H->d_sur_err);
+    cudaFree(H->d_sur_frames); cudaFree(H->d_feat); cudaFree(H->d_mlp_out); cudaFree(H->d_list); cudaFree(H->d_gate);
+    cudaFree(H->d_block_counts);
+    for (auto& e : H->sev) if (e) cudaEventDestroy(e);
     for (auto& e : H->ev) if (e) cudaEventDestroy(e);
     if (H->stream) cudaStreamDestroy(H->stream);
     delete H;
@@ -1468,6 +1653,217 @@ int sirius_cuda_surrogate_infer(sirius_cuda_handle h, const float* d_features, i
     CK(cudaMemcpyAsync(&err, H->d_sur_err, sizeof(int), cudaMemcpyDeviceToHost, st));
     CK(cudaStreamSynchronize(st));
     if (err) return fail(H, SIRIUS_ERR_TIMEOUT, "surrogate MLP kernel stopped by its wait bound");
+    return SIRIUS_OK;
+}
+
+// Per-frame constants of the surrogate gate: the camera's Boyer-Lindquist
+// polar angle and the critical curve (Bardeen 1973: spherical photon orbits
+// r in [r_ph,pro, r_ph,retro] give xi = L/E, eta = Q/E^2; alpha = -xi/sin(theta_o),
+// beta = +-sqrt(eta + a^2 cos^2 theta_o - xi^2 cot^2 theta_o)), resampled at
+// kCurveN angles about its centre.
+static SurFrameDev make_sur_frame(const sirius_frame& f, const FrameDev& F) {
+    SurFrameDev S{};
+    const sirius_metric& m = f.metric;
+    const double x = F.cam_r * F.cam_st * F.cam_cp, y = F.cam_r * F.cam_st * F.cam_sp, z = F.cam_r * F.cam_ct;
+    const double a = m.a, M = m.M;
+    const double R2 = x * x + y * y + z * z, Rm2 = R2 - a * a;
+    const double rk = std::sqrt(std::max(0.5 * (Rm2 + std::sqrt(Rm2 * Rm2 + 4.0 * a * a * z * z)), 1e-20));
+    const double th = std::acos(std::clamp(z / rk, -1.0, 1.0));
+    S.sin_o = std::max(std::sin(th), 1e-6);
+    S.theta_deg = th * 180.0 / kPi;
+    S.kerr = (m.family == SIRIUS_METRIC_KERR_SCHILD && F.has_horizon && m.Q == 0.0 && m.Lambda == 0.0) ? 1 : 0;
+    if (!S.kerr) return S;
+    std::vector<std::pair<double, double>> pts;
+    const double co = std::cos(th), cot = co / S.sin_o;
+    if (std::fabs(a) < 1e-6 * M) {
+        const double R = std::sqrt(27.0) * M;
+        for (int i = 0; i < 4096; ++i) {
+            const double t = 2.0 * kPi * i / 4096.0;
+            pts.push_back({R * std::cos(t), R * std::sin(t)});
+        }
+    } else {
+        const double as = std::clamp(std::fabs(a) / M, 0.0, 1.0);
+        const double r0 = 2.0 * M * (1.0 + std::cos((2.0 / 3.0) * std::acos(-as)));
+        const double r1 = 2.0 * M * (1.0 + std::cos((2.0 / 3.0) * std::acos(as)));
+        for (int i = 0; i <= 8192; ++i) {
+            const double r = r0 + (r1 - r0) * i / 8192.0;
+            const double xi = (r * r * (3.0 * M - r) - a * a * (r + M)) / (a * (r - M));
+            const double eta = r * r * r * (4.0 * a * a * M - r * (r - 3.0 * M) * (r - 3.0 * M)) / (a * a * (r - M) * (r - M));
+            const double b2 = eta + a * a * co * co - xi * xi * cot * cot;
+            if (b2 < 0.0) continue;
+            const double al = -xi / S.sin_o, be = std::sqrt(b2);
+            pts.push_back({al, be});
+            pts.push_back({al, -be});
+        }
+    }
+    if (pts.size() < 64) { S.kerr = 0; return S; }
+    double amin = 1e300, amax = -1e300;
+    for (auto& q : pts) { amin = std::min(amin, q.first); amax = std::max(amax, q.first); }
+    const double ac = 0.5 * (amin + amax);
+    S.ac = float(ac);
+    std::vector<std::pair<double, std::pair<double, double>>> polar;
+    for (auto& q : pts) polar.push_back({std::atan2(q.second, q.first - ac), q});
+    std::sort(polar.begin(), polar.end(), [](const auto& u, const auto& v) { return u.first < v.first; });
+    const size_t np = polar.size();
+    size_t k = 0;
+    for (int j = 0; j < kCurveN; ++j) {
+        const double phi = -kPi + 2.0 * kPi * (j + 0.5) / kCurveN;
+        while (k < np && polar[k].first < phi) ++k;
+        const auto& hi = polar[k % np];
+        const auto& lo = polar[(k + np - 1) % np];
+        double p0 = lo.first, p1 = hi.first;
+        if (k == 0) p0 -= 2.0 * kPi;
+        if (k == np) p1 += 2.0 * kPi;
+        const double w = p1 > p0 ? (phi - p0) / (p1 - p0) : 0.0;
+        S.ca[j] = float(lo.second.first + w * (hi.second.first - lo.second.first));
+        S.cb[j] = float(lo.second.second + w * (hi.second.second - lo.second.second));
+    }
+    return S;
+}
+
+// Features, gate and the list of rays to integrate for the uploaded frames.
+static int surrogate_prepare(Handle* H, const sirius_frame* frames, int n_frames, long long total,
+                             const sirius_surrogate_config* sc, unsigned char* d_gate, cudaStream_t st) {
+    std::vector<SurFrameDev> sf(n_frames);
+    for (int i = 0; i < n_frames; ++i) sf[i] = make_sur_frame(frames[i], make_frame(frames[i], H->cfg));
+    int rc;
+    if ((rc = ensure(H, H->d_sur_frames, H->sur_frames_cap, size_t(n_frames))) != SIRIUS_OK) return rc;
+    if ((rc = ensure(H, H->d_feat, H->feat_cap, size_t(total) * 5)) != SIRIUS_OK) return rc;
+    if ((rc = ensure(H, H->d_list, H->list_cap, size_t(total))) != SIRIUS_OK) return rc;
+    const int block = 256;
+    const int n_blocks = int((total + block - 1) / block);
+    if ((rc = ensure(H, H->d_block_counts, H->block_counts_cap, size_t(n_blocks) + 1)) != SIRIUS_OK) return rc;
+    if (!d_gate) {
+        if ((rc = ensure(H, H->d_gate, H->gate_cap, size_t(total))) != SIRIUS_OK) return rc;
+        d_gate = H->d_gate;
+    }
+    CK(cudaMemcpyAsync(H->d_sur_frames, sf.data(), n_frames * sizeof(SurFrameDev), cudaMemcpyHostToDevice, st));
+    const double band = sc ? sc->gate_band : 0.3;
+    const double audit = sc ? std::clamp(sc->audit_fraction, 0.0, 1.0) : 0.01;
+    const unsigned thr = unsigned(std::min(audit * 4294967296.0, 4294967295.0));
+    const unsigned seed = sc ? sc->audit_seed : 0u;
+    sur_features_kernel<<<n_blocks, block, 0, st>>>(H->d_frames, H->d_sur_frames, n_frames, total, float(band), thr,
+                                                    seed, H->d_feat, d_gate, H->d_block_counts);
+    CK(cudaGetLastError());
+    sur_scan_kernel<<<1, 1024, 0, st>>>(H->d_block_counts, n_blocks);
+    CK(cudaGetLastError());
+    sur_scatter_kernel<<<n_blocks, block, 0, st>>>(d_gate, total, H->d_block_counts, H->d_list);
+    CK(cudaGetLastError());
+    return SIRIUS_OK;
+}
+
+static int render_surrogate(Handle* H, const sirius_frame* frames, int n_frames, const sirius_surrogate_config* sc,
+                            float* d_image, float* d_image_mlp, unsigned char* d_gate, cudaStream_t st,
+                            sirius_surrogate_stats* stats) {
+    if (!H->d_surrogate) return fail(H, SIRIUS_ERR_NOT_CONFIGURED, "no surrogate weights loaded");
+    for (auto& e : H->sev)
+        if (!e) CK(cudaEventCreate(&e));
+    long long total = 0;
+    cudaStream_t keep = H->stream;
+    H->stream = st;
+    int rc = upload_frames(H, frames, n_frames, &total);
+    H->stream = keep;
+    if (rc != SIRIUS_OK) return rc;
+    if (total > 0xFFFFFFFFll) return fail(H, SIRIUS_ERR_INVALID_ARGUMENT, "surrogate rendering takes < 2^32 rays");
+    if ((rc = ensure(H, H->d_mlp_out, H->mlp_out_cap, size_t(total) * 4)) != SIRIUS_OK) return rc;
+    if (!d_gate) {
+        if ((rc = ensure(H, H->d_gate, H->gate_cap, size_t(total))) != SIRIUS_OK) return rc;
+        d_gate = H->d_gate;
+    }
+    // 1. features, gate and the compacted list of rays to integrate
+    CK(cudaEventRecord(H->sev[0], st));
+    if ((rc = surrogate_prepare(H, frames, n_frames, total, sc, d_gate, st)) != SIRIUS_OK) return rc;
+    CK(cudaEventRecord(H->sev[1], st));
+    unsigned n_int = 0;
+    const long long n_blocks = (total + 255) / 256;
+    CK(cudaMemcpyAsync(&n_int, H->d_block_counts + n_blocks, sizeof(unsigned), cudaMemcpyDeviceToHost, st));
+    CK(cudaStreamSynchronize(st));
+    // 2. the MLP on every pixel and the shading of the ungated ones, then 3.
+    // the integrator on the compacted list of gated and audit rays. (Run beside
+    // the MLP, the latency-bound gated rays lose more than the overlap gains.)
+    CK(cudaMemsetAsync(H->d_sur_err, 0, sizeof(int), st));
+    if ((rc = surrogate_launch(H, H->d_feat, total, H->d_mlp_out, st)) != SIRIUS_OK) return rc;
+    CK(cudaEventRecord(H->sev[2], st));
+    sur_shade_kernel<<<int((total + 255) / 256), 256, 0, st>>>(H->d_frames, n_frames, total, H->d_mlp_out, d_gate,
+                                                               d_image, d_image_mlp);
+    CK(cudaGetLastError());
+    CK(cudaEventRecord(H->sev[3], st));
+    if (n_int > 0) {
+        rc = launch_trace(H, n_frames, (long long)n_int, nullptr, d_image, nullptr, nullptr, st, false, nullptr,
+                          H->d_list);
+        if (rc != SIRIUS_OK) return rc;
+    }
+    CK(cudaEventRecord(H->sev[4], st));
+    int err = 0, status = 0;
+    CK(cudaMemcpyAsync(&err, H->d_sur_err, sizeof(int), cudaMemcpyDeviceToHost, st));
+    CK(cudaMemcpyAsync(&status, H->d_status, sizeof(int), cudaMemcpyDeviceToHost, st));
+    CK(cudaStreamSynchronize(st));
+    if (err) return fail(H, SIRIUS_ERR_TIMEOUT, "surrogate MLP kernel stopped by its wait bound");
+    if (n_int > 0 && (status & 1)) return fail(H, SIRIUS_ERR_TIMEOUT, "trace kernel stopped by its watchdog");
+    if (stats) {
+        *stats = sirius_surrogate_stats{};
+        stats->rays = total;
+        stats->integrated = n_int;
+        float t[4] = {}, tt = 0.f;
+        for (int i = 0; i < 4; ++i) CK(cudaEventElapsedTime(&t[i], H->sev[i], H->sev[i + 1]));
+        CK(cudaEventElapsedTime(&tt, H->sev[0], H->sev[4]));
+        stats->ms_features = t[0];
+        stats->ms_mlp = t[1];
+        stats->ms_shade = t[2];
+        stats->ms_trace = t[3];
+        stats->ms_total = tt;
+    }
+    return SIRIUS_OK;
+}
+
+int sirius_cuda_surrogate_features(sirius_cuda_handle h, const sirius_frame* frames, int32_t n_frames,
+                                   const sirius_surrogate_config* sc, float* d_features, uint8_t* d_gate,
+                                   void* stream) {
+    Handle* H = static_cast<Handle*>(h);
+    if (!H || !frames || n_frames <= 0 || !d_features) return SIRIUS_ERR_INVALID_ARGUMENT;
+    CK(cudaSetDevice(H->device));
+    cudaStream_t st = stream ? static_cast<cudaStream_t>(stream) : cudaStreamLegacy;
+    long long total = 0;
+    cudaStream_t keep = H->stream;
+    H->stream = st;
+    int rc = upload_frames(H, frames, n_frames, &total);
+    H->stream = keep;
+    if (rc != SIRIUS_OK) return rc;
+    if ((rc = surrogate_prepare(H, frames, n_frames, total, sc, d_gate, st)) != SIRIUS_OK) return rc;
+    CK(cudaMemcpyAsync(d_features, H->d_feat, size_t(total) * 5 * sizeof(float), cudaMemcpyDeviceToDevice, st));
+    CK(cudaStreamSynchronize(st));
+    return SIRIUS_OK;
+}
+
+int sirius_cuda_render_surrogate_device(sirius_cuda_handle h, const sirius_frame* frames, int32_t n_frames,
+                                        const sirius_surrogate_config* sc, float* d_image, float* d_image_mlp,
+                                        uint8_t* d_gate, void* stream, sirius_surrogate_stats* stats) {
+    Handle* H = static_cast<Handle*>(h);
+    if (!H || !frames || n_frames <= 0 || !d_image) return SIRIUS_ERR_INVALID_ARGUMENT;
+    CK(cudaSetDevice(H->device));
+    cudaStream_t st = stream ? static_cast<cudaStream_t>(stream) : cudaStreamLegacy;
+    return render_surrogate(H, frames, n_frames, sc, d_image, d_image_mlp, d_gate, st, stats);
+}
+
+int sirius_cuda_render_surrogate(sirius_cuda_handle h, const sirius_frame* frames, int32_t n_frames,
+                                 const sirius_surrogate_config* sc, float* image, float* image_mlp, uint8_t* gate,
+                                 sirius_surrogate_stats* stats) {
+    Handle* H = static_cast<Handle*>(h);
+    if (!H || !frames || n_frames <= 0 || !image) return SIRIUS_ERR_INVALID_ARGUMENT;
+    CK(cudaSetDevice(H->device));
+    long long total = 0;
+    for (int i = 0; i < n_frames; ++i) total += (long long)frames[i].camera.width * frames[i].camera.height;
+    int rc;
+    if ((rc = ensure(H, H->d_image, H->image_cap, size_t(total) * (image_mlp ? 2 : 1))) != SIRIUS_OK) return rc;
+    if ((rc = ensure(H, H->d_gate, H->gate_cap, size_t(total))) != SIRIUS_OK) return rc;
+    float* d_img = H->d_image;
+    float* d_mlp = image_mlp ? H->d_image + total : nullptr;
+    rc = render_surrogate(H, frames, n_frames, sc, d_img, d_mlp, H->d_gate, H->stream, stats);
+    if (rc != SIRIUS_OK) return rc;
+    CK(cudaMemcpyAsync(image, d_img, size_t(total) * sizeof(float), cudaMemcpyDeviceToHost, H->stream));
+    if (image_mlp) CK(cudaMemcpyAsync(image_mlp, d_mlp, size_t(total) * sizeof(float), cudaMemcpyDeviceToHost, H->stream));
+    if (gate) CK(cudaMemcpyAsync(gate, H->d_gate, size_t(total), cudaMemcpyDeviceToHost, H->stream));
+    CK(cudaStreamSynchronize(H->stream));
     return SIRIUS_OK;
 }
 

@@ -23,7 +23,8 @@ EXPORTS = [
     "sirius_cuda_trace_frames_device", "sirius_cuda_trace_rays", "sirius_cuda_metric_evaluate",
     "sirius_cuda_dp45_step", "sirius_cuda_last_stats", "sirius_cuda_autotune", "sirius_cuda_measure_fma_peak",
     "sirius_cuda_flop_count", "sirius_cuda_trace_frames_static", "sirius_cuda_surrogate_load",
-    "sirius_cuda_surrogate_infer",
+    "sirius_cuda_surrogate_infer", "sirius_cuda_surrogate_features", "sirius_cuda_render_surrogate",
+    "sirius_cuda_render_surrogate_device",
 ]
 
 
@@ -51,6 +52,13 @@ def load_library(path=LIB_PATH):
                                                   C.c_void_p, C.c_void_p, C.c_void_p]
     L.sirius_cuda_surrogate_load.argtypes = [C.c_void_p, C.c_void_p, C.c_int64]
     L.sirius_cuda_surrogate_infer.argtypes = [C.c_void_p, C.c_void_p, C.c_int64, C.c_void_p, C.c_void_p]
+    L.sirius_cuda_surrogate_features.argtypes = [C.c_void_p, C.c_void_p, C.c_int32, _P(abi.SurrogateConfig),
+                                                 C.c_void_p, C.c_void_p, C.c_void_p]
+    L.sirius_cuda_render_surrogate.argtypes = [C.c_void_p, C.c_void_p, C.c_int32, _P(abi.SurrogateConfig),
+                                               C.c_void_p, C.c_void_p, C.c_void_p, _P(abi.SurrogateStats)]
+    L.sirius_cuda_render_surrogate_device.argtypes = [C.c_void_p, C.c_void_p, C.c_int32, _P(abi.SurrogateConfig),
+                                                      C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p,
+                                                      _P(abi.SurrogateStats)]
     L.sirius_cuda_trace_rays.argtypes = [C.c_void_p, _P(abi.Metric), C.c_double, C.c_double, C.c_void_p,
                                          C.c_int64, C.c_void_p]
     L.sirius_cuda_metric_evaluate.argtypes = [C.c_void_p, _P(abi.Metric), C.c_void_p, C.c_int64, C.c_int32,
@@ -151,6 +159,35 @@ class Engine:
     def surrogate_infer(self, d_features, n, d_out, stream=None):
         """MLP on n x 5 device features into n x 4 device outputs."""
         self._check(self.lib.sirius_cuda_surrogate_infer(self.h, d_features, n, d_out, stream))
+
+    def surrogate_features(self, frames, d_features, d_gate=None, config=None, stream=None):
+        """Features (n x 5) and gate (n bytes) of every pixel of the frames, into device buffers."""
+        arr, _ = frames_array(frames)
+        cfg = config or abi.surrogate_config()
+        self._check(self.lib.sirius_cuda_surrogate_features(self.h, C.addressof(arr), len(frames), C.byref(cfg),
+                                                            d_features, d_gate, stream))
+
+    def render_surrogate(self, frames, config=None, mlp_image=False):
+        """Surrogate-gated image (host): returns (image, mlp_image or None, gate, stats)."""
+        arr, total = frames_array(frames)
+        cfg = config or abi.surrogate_config()
+        img = np.zeros(total, dtype=np.float32)
+        mimg = np.zeros(total, dtype=np.float32) if mlp_image else None
+        gate = np.zeros(total, dtype=np.uint8)
+        st = abi.SurrogateStats()
+        self._check(self.lib.sirius_cuda_render_surrogate(
+            self.h, C.addressof(arr), len(frames), C.byref(cfg), img.ctypes.data,
+            mimg.ctypes.data if mimg is not None else None, gate.ctypes.data, C.byref(st)))
+        return img, mimg, gate, st
+
+    def render_surrogate_device(self, frames, d_image, d_image_mlp=None, d_gate=None, config=None, stream=None):
+        """Surrogate-gated image into device buffers; returns the stage statistics."""
+        arr, _ = frames_array(frames)
+        cfg = config or abi.surrogate_config()
+        st = abi.SurrogateStats()
+        self._check(self.lib.sirius_cuda_render_surrogate_device(self.h, C.addressof(arr), len(frames), C.byref(cfg),
+                                                                 d_image, d_image_mlp, d_gate, stream, C.byref(st)))
+        return st
 
     def trace_rays(self, metric, rays, disk_inner=0.0, disk_outer=20.0):
         n = len(rays)

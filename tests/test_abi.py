@@ -45,6 +45,8 @@ def test_struct_layouts_match_c(oracle):
     assert C.sizeof(abi.Camera) == 64
     assert C.sizeof(abi.Frame) == 168
     assert C.sizeof(abi.CameraRay) == 64
+    assert C.sizeof(abi.SurrogateConfig) == 40
+    assert C.sizeof(abi.SurrogateStats) == 48
     dt = abi.result_dtype()
     for name, _ in abi.RayResult._fields_:
         assert dt.fields[name][1] == getattr(abi.RayResult, name).offset, name

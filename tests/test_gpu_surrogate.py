@@ -7,6 +7,8 @@ after an FP32 sum whose order differs from the reference's, and evaluates the
 SiLU's sigmoid with the hardware tanh (relative error ~2^-11): an activation
 can land one BF16 step away. Outputs agree to 2 % of the output scale at worst
 and 0.2 % on average."""
+import os
+
 import numpy as np
 import pytest
 
@@ -66,3 +68,50 @@ def test_mlp_rejects_wrong_parameter_count(engine):
     from sirius_b200.engine import SiriusError
     with pytest.raises(SiriusError):
         engine.surrogate_load(np.zeros(100, dtype=np.float32))
+
+
+WEIGHTS = os.path.join(os.path.dirname(os.path.dirname(os.path.abspath(__file__))), "sirius_b200", "data",
+                       "surrogate_kerr.npy")
+
+
+def kerr_frame(side):
+    cam = abi.make_camera(r=100.0, theta_deg=60.0, width=side, height=side, fov=30.0)
+    return abi.make_frame(abi.make_metric(a=0.9), cam, 0.0, 30.0)
+
+
+def render_config(prec):
+    return abi.default_config(abs_tolerance=1e-8, rel_tolerance=1e-8, min_step=1e-9, max_step=2.0,
+                              initial_step=0.1, escape_radius=200.0, horizon_factor=1.01, max_steps=10000,
+                              precision=prec, enable_disk=1, enable_volumetric=0, critical_band=0.0)
+
+
+def test_surrogate_render_against_the_integrator(engine):
+    """Surrogate-gated frame vs the same frame fully integrated: the gated and
+    audit pixels are the integrator's own values (bit for bit); the rest come
+    from the MLP within the surrogate's error budget."""
+    engine.surrogate_load(np.load(WEIGHTS))
+    fr = kerr_frame(512)
+    engine.configure(render_config(abi.PRECISION_MIXED))
+    _, full, _ = engine.trace_frames([fr], results=False)
+    img, mimg, gate, st = engine.render_surrogate([fr], mlp_image=True)
+    taken = gate != 0
+    assert st.rays == full.size and st.integrated == int(taken.sum())
+    np.testing.assert_array_equal(img[taken], full[taken])
+    np.testing.assert_array_equal(img[~taken], mimg[~taken])
+    assert 0.004 < np.mean(gate == 2) < 0.02      # 1 % audit, in runs of 32 pixels
+    assert 0.001 < np.mean(gate == 1) < 0.05      # the +-0.3 M band around the critical curve
+    err = np.abs(img.astype(np.float64) - full) / full.max()
+    assert err.mean() < 1e-3, err.mean()
+    assert np.percentile(err, 99) < 1e-2, np.percentile(err, 99)
+
+
+def test_surrogate_integrates_frames_it_does_not_cover(engine):
+    """A Morris-Thorne frame (outside the MLP's training set) is integrated in full."""
+    engine.surrogate_load(np.load(WEIGHTS))
+    fr = abi.make_frame(abi.make_metric(family=abi.MORRIS_THORNE, b0=1.0),
+                        abi.make_camera(r=20.0, theta_deg=80.0, width=64, height=64, fov=40.0), 0.0, 20.0)
+    engine.configure(render_config(abi.PRECISION_MIXED))
+    _, full, _ = engine.trace_frames([fr], results=False)
+    img, _, gate, st = engine.render_surrogate([fr])
+    assert np.all(gate == 1) and st.integrated == full.size
+    np.testing.assert_array_equal(img, full)
