@@ -215,6 +215,75 @@ def cpu_baseline_sample(seconds=12.0):
                       f"(the reference's gray volumetric march replaces its disk)"}
 
 
+def batch_frames(abi, seed=3, n=96):
+    """The heterogeneous batch: 96 seeded frames, metric family uniform over
+    Kerr-Newman (a ~ U[0, 0.998], Q ~ U[0, sqrt(1 - a^2)]), Kerr-de Sitter
+    (Lambda ~ LogU[1e-6, 1e-3]), Morris-Thorne (b0 ~ U[0.5, 2]) and Alcubierre
+    (v_s ~ U[0.1, 2], sigma = 8, R = 1); square side ~ U{128..1024},
+    r_obs ~ U[20, 200], inclination ~ U[10, 89] deg."""
+    import numpy as np
+    rng = np.random.default_rng(seed)
+    frames = []
+    for _ in range(n):
+        kind = rng.integers(4)
+        side = int(rng.integers(128, 1025))
+        r = float(rng.uniform(20.0, 200.0))
+        th = float(rng.uniform(10.0, 89.0))
+        if kind == 0:
+            a = float(rng.uniform(0.0, 0.998))
+            m = abi.make_metric(a=a, Q=float(rng.uniform(0.0, math.sqrt(1.0 - a * a))))
+        elif kind == 1:
+            m = abi.make_metric(a=float(rng.uniform(0.0, 0.998)), Lambda=float(10 ** rng.uniform(-6.0, -3.0)))
+        elif kind == 2:
+            m = abi.make_metric(family=abi.MORRIS_THORNE, b0=float(rng.uniform(0.5, 2.0)))
+        else:
+            m = abi.make_metric(family=abi.ALCUBIERRE, vs=float(rng.uniform(0.1, 2.0)), sigma=8.0, R=1.0)
+        cam = abi.make_camera(r=r, theta_deg=th, width=side, height=side, fov=30.0)
+        frames.append(abi.make_frame(m, cam, 0.0, 30.0))
+    return frames
+
+
+def batch_leg(eng, abi):
+    """All 96 frames in one launch (persistent queue, generic kernel) and as
+    per-family launches (one thread per ray), mixed precision, thin disk."""
+    frames = batch_frames(abi)
+    total = sum(f.camera.width * f.camera.height for f in frames)
+    out = {"workload": "96 seeded frames: Kerr-Newman / Kerr-de Sitter / Morris-Thorne / Alcubierre, "
+                       "sides U{128..1024}", "rays": total}
+    for name, bps in (("persistent_one_launch", -1), ("per_family_launches", 0)):
+        cfg = workload_config(abi, abi.PRECISION_MIXED)
+        cfg.enable_volumetric = 0
+        cfg.blocks_per_sm = bps
+        eng.configure(cfg)
+        eng.trace_frames(frames, results=False, image=True)
+        eng.trace_frames(frames, results=False, image=True)
+        st = eng.stats()
+        out[name] = {"kernel_ms": st.kernel_ms, "mrays_per_s": total / (st.kernel_ms * 1e-3) / 1e6,
+                     "kernel_launches": st.kernel_launches, "steps_per_ray": st.accepted_steps / total}
+    return out
+
+
+def stress_leg(eng, abi, stride=8):
+    """The stress configuration: Kerr-Newman a = 0.998, Q = 0.05, equirectangular
+    4096 x 2048 sky map at r_obs = 15, Yoshida-4 symplectic d-lambda = 0.01 with
+    FP64 re-projection every 8 steps (<= 50k steps), thin disk + 32-bin volumetric
+    transfer. Timed on a bounded sample: every stride-th pixel in both
+    directions (the sky map at (4096/stride) x (2048/stride))."""
+    w, h = 4096 // stride, 2048 // stride
+    cam = abi.make_camera(r=15.0, theta_deg=80.0, width=w, height=h, projection=abi.CAMERA_EQUIRECTANGULAR)
+    frame = abi.make_frame(abi.make_metric(a=0.998, Q=0.05), cam, 0.0, 30.0)
+    cfg = abi.default_config(integrator=abi.INTEGRATOR_SYMPLECTIC, symplectic_order=4, symplectic_step=0.01,
+                             projection_period=8, max_steps=50000, escape_radius=60.0, horizon_factor=1.01,
+                             min_step=1e-9, enable_volumetric=1, n_bins=32, precision=abi.PRECISION_MIXED)
+    eng.configure(cfg)
+    eng.trace_frames([frame], results=False, image=True, spectra=True)
+    st = eng.stats()
+    return {"workload": f"kerr_newman_a0.998_q0.05_equirect_{w}x{h}_symplectic4_vol32 (sample of 4096x2048)",
+            "rays": w * h, "kernel_ms": st.kernel_ms, "mrays_per_s": w * h / (st.kernel_ms * 1e-3) / 1e6,
+            "steps_per_ray": st.accepted_steps / (w * h),
+            "full_map_ms_estimate": st.kernel_ms * stride * stride}
+
+
 SURROGATE_SIDE = 2048
 SURROGATE_WEIGHTS = os.path.join(ROOT, "sirius_b200", "data", "surrogate_kerr.npy")
 
@@ -287,6 +356,9 @@ def main():
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
     ap.add_argument("--no-extras", action="store_true", help="skip the FP64 comparator and the CPU baseline")
+    ap.add_argument("--surrogate-only", action="store_true",
+                    help="run only the surrogate-gated leg (at --surrogate-size) and print its JSON")
+    ap.add_argument("--surrogate-size", type=int, default=SURROGATE_SIDE)
     ap.add_argument("--size", type=int, default=WIDTH,
                     help="frame side (default 1024, the workload; smaller sides are profiling cases)")
     args = ap.parse_args()
@@ -300,6 +372,7 @@ def main():
 
     from sirius_b200 import abi
     from sirius_b200.engine import Engine, flop_count
+    from sirius_b200.shard import max_over_ranks
 
     world = int(os.environ.get("WORLD_SIZE", "1"))
     rank = int(os.environ.get("RANK", "0"))
@@ -310,6 +383,11 @@ def main():
         dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=120))
     dev = torch.device("cuda", local)
     stream = torch.cuda.current_stream(dev)
+    if args.surrogate_only:
+        eng = Engine(local)
+        print(json.dumps(surrogate_leg(eng, abi, np, torch, dev, stream, side=args.surrogate_size)), flush=True)
+        eng.close()
+        return
 
     eng = Engine(local, config=workload_config(abi, abi.PRECISION_MIXED))
     frame = workload_frame(abi, args.size, args.size)
@@ -352,10 +430,8 @@ def main():
     torch.cuda.synchronize()
     clk = clocks.stop()
     step_ms = [a.elapsed_time(b) for a, b in ev]
-    t_ms = torch.tensor([sum(step_ms)], dtype=torch.float64, device=dev)
-    if world > 1:
-        dist.all_reduce(t_ms, op=dist.ReduceOp.MAX)
-    t_total = float(t_ms.item())
+    # device time of the K steps, the maximum over ranks (each rank renders its own frame)
+    t_total = max_over_ranks(sum(step_ms), dist if world > 1 else None, dev)
     value = world * total * args.steps / (t_total * 1e-3) / 1e6
 
     # end to end through the host entry point: frame descriptor H2D, image + spectra D2H (pinned)
@@ -369,10 +445,8 @@ def main():
     t0 = time.perf_counter()
     for _ in range(args.steps):
         eng.trace_frames_into(C.addressof(fr_arr), 1, None, h_img.data_ptr(), h_spc.data_ptr())
-    t_e2e = torch.tensor([time.perf_counter() - t0], dtype=torch.float64, device=dev)
-    if world > 1:
-        dist.all_reduce(t_e2e, op=dist.ReduceOp.MAX)
-    e2e = world * total * args.steps / float(t_e2e.item()) / 1e6
+    t_e2e = max_over_ranks(time.perf_counter() - t0, dist if world > 1 else None, dev)
+    e2e = world * total * args.steps / t_e2e / 1e6
 
     # roofline of the trace kernel: algorithmic operations / kernel time vs the measured FP32 SIMT peak
     rhs_f, att_f, acc_f = flop_count(frame.metric)
@@ -420,6 +494,8 @@ def main():
                                  "spectra_linf_rel": float(serr.max()),
                                  "spectra_p99_rel": float(np.percentile(serr, 99))}
         line["surrogate"] = surrogate_leg(eng, abi, np, torch, dev, stream)
+        line["heterogeneous_batch"] = batch_leg(eng, abi)
+        line["stress_symplectic"] = stress_leg(eng, abi)
         line["cpu_baseline"] = cpu_baseline_sample()
     if rank == 0:
         print(json.dumps(line), flush=True)
