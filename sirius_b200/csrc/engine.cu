@@ -58,7 +58,17 @@ struct Params {
     unsigned long long* clock0;           // launch start on the device clock (first warp stamps it)
     unsigned long long watchdog_ns;       // globaltimer bound for the whole launch, per warp
     CfgDev c;
+    FrameDev f0;                          // the frame of a one-frame launch (read from the parameter bank)
 };
+
+// The frame of ray state s: a one-frame launch (UNI) reads it, metric included,
+// from the kernel's parameter bank, whose constants the arithmetic takes as
+// operands instead of loading them from global memory.
+template <bool UNI>
+__device__ __forceinline__ const FrameDev& frame_of(const Params& P, int frame) {
+    if constexpr (UNI) return P.f0;
+    else return P.frames[frame];
+}
 
 __device__ __forceinline__ unsigned long long globaltimer() {
     unsigned long long t;
@@ -136,12 +146,12 @@ __device__ void invariants(const MetricDev& m, const InvForm& F, const double x[
     Q = float(pth * pth + ct * ct * (-m.a2 * e * e + L * L / (st * st)));
 }
 
-template <bool MIXED, int FAM>
+template <bool MIXED, int FAM, bool UNI>
 __device__ __noinline__ void begin_ray(const Params& P, Ray<MIXED>& s, long long idx, int frame, float* vol) {
     using K = typename Ray<MIXED>::K;
     s.idx = idx;
     s.frame = frame;
-    const FrameDev& F = P.frames[s.frame];
+    const FrameDev& F = frame_of<UNI>(P, s.frame);
     double dir[4];
     if (P.host_rays) {
         const sirius_camera_ray& cr = P.host_rays[idx];
@@ -192,10 +202,10 @@ __device__ __noinline__ void begin_ray(const Params& P, Ray<MIXED>& s, long long
         for (int b = 0; b < P.c.nbins; ++b) { vol[2 * b * blockDim.x] = 0.f; vol[(2 * b + 1) * blockDim.x] = 1.f; }
 }
 
-template <bool MIXED>
+template <bool MIXED, bool UNI>
 __device__ __noinline__ void end_ray(const Params& P, const Ray<MIXED>& s, int outcome, float magnification, int flags,
                                      const float* vol) {
-    const FrameDev& F = P.frames[s.frame];
+    const FrameDev& F = frame_of<UNI>(P, s.frame);
     if (P.image) P.image[s.idx] = float(s.intensity);
     if (P.spectra && vol)
         for (int b = 0; b < P.c.nbins; ++b) P.spectra[s.idx * P.c.nbins + b] = vol[2 * b * blockDim.x];
@@ -381,10 +391,10 @@ __device__ __noinline__ void refresh_derivative(const MetricDev& m, Ray<MIXED>& 
 
 // One iteration of the ray state machine: a DP45 attempt, and on acceptance
 // the termination checks. Returns -1 while the ray continues, else its outcome.
-template <bool MIXED, int FAM>
+template <bool MIXED, int FAM, bool UNI>
 __device__ __forceinline__ int advance(const Params& P, Ray<MIXED>& s, float& magnification, int& flags, float* vol) {
     using K = typename Ray<MIXED>::K;
-    const FrameDev& F = P.frames[s.frame];
+    const FrameDev& F = frame_of<UNI>(P, s.frame);
     const MetricDev& m = F.m;
     const CfgDev& c = P.c;
     double xn[4], pn[4];
@@ -555,8 +565,8 @@ __device__ __forceinline__ int advance(const Params& P, Ray<MIXED>& s, float& ma
 }
 
 // Persistent tracer. Dynamic shared memory: 2 * nbins floats per thread (volumetric bins).
-template <bool MIXED, int MINB, int FAM>
-__global__ void __launch_bounds__(128, MINB) trace_kernel(Params P) {
+template <bool MIXED, int MINB, int FAM, bool UNI>
+__global__ void __launch_bounds__(128, MINB) trace_kernel(const __grid_constant__ Params P) {
     extern __shared__ float smem[];
     float* vol = (P.c.enable_vol && P.c.nbins > 0) ? smem + threadIdx.x : nullptr;
     const int lane = threadIdx.x & 31;
@@ -582,7 +592,7 @@ __global__ void __launch_bounds__(128, MINB) trace_kernel(Params P) {
             const long long idx = P.list ? (long long)P.list[gid] : gid;
             const int frame = P.n_frames > 1 ? find_frame(P.frames, P.n_frames, idx) : 0;
             if (P.family < 0 || P.frames[frame].m.family == P.family) {
-                begin_ray<MIXED, FAM>(P, s, idx, frame, vol);
+                begin_ray<MIXED, FAM, UNI>(P, s, idx, frame, vol);
                 alive = true;
             }
         }
@@ -602,7 +612,7 @@ __global__ void __launch_bounds__(128, MINB) trace_kernel(Params P) {
                     if (q < (unsigned long long)P.total) {
                         const unsigned long long idx = P.list ? (unsigned long long)P.list[q] : q;
                         const int frame = P.n_frames > 1 ? find_frame(P.frames, P.n_frames, (long long)idx) : 0;
-                        begin_ray<MIXED, FAM>(P, s, (long long)idx, frame, vol);
+                        begin_ray<MIXED, FAM, UNI>(P, s, (long long)idx, frame, vol);
                         alive = true;
                         magnification = 1.f;
                         flags = 0;
@@ -620,7 +630,7 @@ __global__ void __launch_bounds__(128, MINB) trace_kernel(Params P) {
             if (stop) {
                 // watchdog: abandon the remaining queue and close the live rays
                 exhausted = true;
-                if (alive) { end_ray<MIXED>(P, s, SIRIUS_MAX_STEPS, magnification, flags, vol); alive = false; }
+                if (alive) { end_ray<MIXED, UNI>(P, s, SIRIUS_MAX_STEPS, magnification, flags, vol); alive = false; }
             }
         }
         if (__ballot_sync(kFull, alive) == 0) {
@@ -628,9 +638,9 @@ __global__ void __launch_bounds__(128, MINB) trace_kernel(Params P) {
             continue;
         }
         if (alive) {
-            const int out = advance<MIXED, FAM>(P, s, magnification, flags, vol);
+            const int out = advance<MIXED, FAM, UNI>(P, s, magnification, flags, vol);
             if (out >= 0) {
-                end_ray<MIXED>(P, s, out, magnification, flags, vol);
+                end_ray<MIXED, UNI>(P, s, out, magnification, flags, vol);
                 acc += s.steps;
                 rej0 += s.rejected;
                 f64 += s.fp64_steps;
@@ -654,32 +664,36 @@ __global__ void __launch_bounds__(128, MINB) trace_kernel(Params P) {
 using TraceFn = void (*)(Params);
 constexpr int kDefaultMinBlocks = 2;
 
-template <bool MIXED, int FAM>
+template <bool MIXED, int FAM, bool UNI>
 TraceFn pick_minb(int minb) {
     switch (minb) {
-        case 1: return trace_kernel<MIXED, 1, FAM>;
-        case 3: return trace_kernel<MIXED, 3, FAM>;
-        case 4: return trace_kernel<MIXED, 4, FAM>;
-        default: return trace_kernel<MIXED, 2, FAM>;
+        case 1: return trace_kernel<MIXED, 1, FAM, UNI>;
+        case 3: return trace_kernel<MIXED, 3, FAM, UNI>;
+        case 4: return trace_kernel<MIXED, 4, FAM, UNI>;
+        default: return trace_kernel<MIXED, 2, FAM, UNI>;
     }
 }
 
 // A kernel specialised for one metric family carries only that family's
 // right-hand side (a smaller loop body and register set); kAnyFamily
-// dispatches per ray. The Kerr-Schild kernels come in every register budget.
-TraceFn pick_kernel(bool mixed, int minb, int fam) {
+// dispatches per ray. The Kerr-Schild kernels come in every register budget,
+// and for one-frame launches (uni) with the frame in the parameter bank.
+TraceFn pick_kernel(bool mixed, int minb, int fam, bool uni = false) {
     switch (fam) {
         case SIRIUS_METRIC_KERR_SCHILD:
-            return mixed ? pick_minb<true, SIRIUS_METRIC_KERR_SCHILD>(minb)
-                         : pick_minb<false, SIRIUS_METRIC_KERR_SCHILD>(minb);
+            if (uni)
+                return mixed ? pick_minb<true, SIRIUS_METRIC_KERR_SCHILD, true>(minb)
+                             : pick_minb<false, SIRIUS_METRIC_KERR_SCHILD, true>(minb);
+            return mixed ? pick_minb<true, SIRIUS_METRIC_KERR_SCHILD, false>(minb)
+                         : pick_minb<false, SIRIUS_METRIC_KERR_SCHILD, false>(minb);
         case SIRIUS_METRIC_MORRIS_THORNE:
-            return mixed ? trace_kernel<true, 2, SIRIUS_METRIC_MORRIS_THORNE>
-                         : trace_kernel<false, 2, SIRIUS_METRIC_MORRIS_THORNE>;
+            return mixed ? trace_kernel<true, 2, SIRIUS_METRIC_MORRIS_THORNE, false>
+                         : trace_kernel<false, 2, SIRIUS_METRIC_MORRIS_THORNE, false>;
         case SIRIUS_METRIC_ALCUBIERRE:
-            return mixed ? trace_kernel<true, 2, SIRIUS_METRIC_ALCUBIERRE>
-                         : trace_kernel<false, 2, SIRIUS_METRIC_ALCUBIERRE>;
+            return mixed ? trace_kernel<true, 2, SIRIUS_METRIC_ALCUBIERRE, false>
+                         : trace_kernel<false, 2, SIRIUS_METRIC_ALCUBIERRE, false>;
         default:
-            return mixed ? trace_kernel<true, 2, kAnyFamily> : trace_kernel<false, 2, kAnyFamily>;
+            return mixed ? trace_kernel<true, 2, kAnyFamily, false> : trace_kernel<false, 2, kAnyFamily, false>;
     }
 }
 
@@ -922,6 +936,7 @@ struct Handle {
     cudaStream_t pending_stream = nullptr;
     long long pending_total = 0;
     int family_mask = 0;  // bit f: a frame of the last upload is of metric family f
+    FrameDev frame0{};    // the first frame of the last upload (a one-frame launch's parameter copy)
     unsigned char* d_surrogate = nullptr;  // packed surrogate weight image (surrogate::kImageBytes)
     int* d_sur_err = nullptr;
     // surrogate-gated rendering scratch
@@ -1112,6 +1127,7 @@ int launch_trace(Handle* H, int n_frames, long long total, sirius_ray_result* d_
     P.spectra = d_spectra;
     P.host_rays = d_rays;
     P.list = d_list;
+    if (n_frames == 1) P.f0 = H->frame0;
     P.queue = S.queue;
     P.counters = S.queue + 1;
     P.clock0 = S.queue + 4;
@@ -1142,7 +1158,7 @@ int launch_trace(Handle* H, int n_frames, long long total, sirius_ray_result* d_
     TraceFn launch_fn[3];
     int launch_family[3], n_launches = 0;
     if (n_fams == 1) {
-        launch_fn[0] = pick_kernel(mixed, minb, fams[0]);
+        launch_fn[0] = pick_kernel(mixed, minb, fams[0], n_frames == 1);
         launch_family[0] = -1;
         n_launches = 1;
     } else if (!P.persistent) {
@@ -1346,6 +1362,7 @@ static int upload_frames(Handle* H, const sirius_frame* frames, int n, long long
     }
     H->family_mask = 0;
     for (int i = 0; i < n; ++i) H->family_mask |= 1 << frames[i].metric.family;
+    H->frame0 = fd[0];
     int rc = ensure(H, H->d_frames, H->frames_cap, size_t(n));
     if (rc != SIRIUS_OK) return rc;
     CK(cudaMemcpyAsync(H->d_frames, fd.data(), n * sizeof(FrameDev), cudaMemcpyHostToDevice, H->stream));
@@ -1444,6 +1461,7 @@ int sirius_cuda_trace_frames_static(sirius_cuda_handle h, const sirius_frame* d_
     // a pageable source: the copy has been staged when cudaMemcpyAsync returns
     CK(cudaMemcpyAsync(scratch->frames, fd, n_frames * sizeof(FrameDev), cudaMemcpyHostToDevice, st));
     H->family_mask = mask;
+    H->frame0 = fd[0];
     const LaunchScratch ls{scratch->frames, scratch->queue, &scratch->status};
     return launch_trace(H, n_frames, total, d_results, d_image, d_spectra, nullptr, st, false, &ls);
 }
