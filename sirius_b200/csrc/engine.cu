@@ -475,25 +475,41 @@ __device__ __forceinline__ int advance(const Params& P, Ray<MIXED>& s, float& ma
     for (int i = 0; i < 8; ++i) s.k[i] = k7[i];
     if (bad) { flags |= SIRIUS_FLAG_NUMERICAL_FAILURE; return SIRIUS_NUMERICAL_FAILURE; }
 
-    // FP64 constraint re-projection (E, L_z and Carter preserving)
-    InvForm IF;
-    inv_form(m, s.x, IF);
-    if (c.proj_period > 0 && (s.steps % c.proj_period) == 0) {
+    // constraint re-projection (E, L_z and Carter preserving); the mixed path
+    // forms only the null value in FP64 (Kerr-Schild without Lambda)
+    double rr;
+    const bool project = c.proj_period > 0 && (s.steps % c.proj_period) == 0;
+    const bool ks_fast = MIXED && is_family<FAM>(m, SIRIUS_METRIC_KERR_SCHILD) && !m.has_lambda;
+    if (project) {
         double pb[4];
 #pragma unroll
         for (int i = 0; i < 4; ++i) pb[i] = s.p[i];
-        const double before = project_null(m, IF, s.p);
+        double before;
+        if (ks_fast) {
+            before = project_null_ks_mixed(m, s.x, s.p, rr);
+        } else {
+            InvForm IF;
+            inv_form(m, s.x, IF);
+            rr = IF.r;
+            before = project_null(m, IF, s.p);
+        }
         s.null_max = fmaxf(s.null_max, float(fabs(before)));
-        // a projection that moved p beyond 1e-10 (relative) makes f(x, p) stale: recompute it
+        // a projection that moved p beyond what the stored f(x, p) resolves
+        // (1e-10 relative in FP64, 1e-6 with FP32 storage) makes it stale: recompute it
         double dp = 0.0, pm = 0.0;
 #pragma unroll
         for (int i = 0; i < 4; ++i) {
             dp = fmax(dp, fabs(s.p[i] - pb[i]));
             pm = fmax(pm, fabs(s.p[i]));
         }
-        if (dp > 1e-10 * pm) refresh_derivative<MIXED, FAM>(m, s);
+        if (dp > (MIXED ? 1e-6 : 1e-10) * pm) refresh_derivative<MIXED, FAM>(m, s);
+    } else if (ks_fast) {
+        rr = ks_radius(m, s.x);
+    } else {
+        InvForm IF;
+        inv_form(m, s.x, IF);
+        rr = IF.r;
     }
-    const double rr = IF.r;
     if (float(rr) < s.min_r) s.min_r = float(rr);
     if (disk_on && c.enable_vol && !symp)
         s.h = fmax(c.hmin, fmin(s.h, volume_step_cap(rr, s.x[3], double(s.k[1]), double(s.k[2]), double(s.k[3]),

@@ -290,6 +290,48 @@ __device__ __forceinline__ double project_null(const MetricDev& m, const InvForm
     return C;
 }
 
+// The same re-projection for the mixed-precision path, Kerr-Schild family
+// without Lambda. Only the null value C = g^{-1}(p, p) needs FP64: it is a
+// difference of O(p^2) terms that must survive to ~1e-16 of them, so r, H and
+// l are FP64 (their three reciprocals from one division). The direction dr and
+// the coefficients A = g^{-1}(dr, dr), B = 2 g^{-1}(p, dr) only set alpha =
+// C / q, which needs single-precision relative accuracy; they are FP32, and
+// the constraint left after the update is ~1e-7 C. Returns C; r_out = r.
+__device__ __forceinline__ double project_null_ks_mixed(const MetricDev& m, const double x[4], double p[4],
+                                                        double& r_out) {
+    const double X = x[1], Y = x[2], Z = x[3];
+    const double a = m.a, a2 = m.a2;
+    const double R2 = X * X + Y * Y + Z * Z, Rm2 = R2 - a2;
+    const double sd = sqrt(fmax(Rm2 * Rm2 + 4.0 * a2 * Z * Z, 1e-20));
+    const double r2 = fmax(0.5 * (Rm2 + sd), 1e-10);
+    const double r = sqrt(r2);
+    r_out = r;
+    const double den = r2 + a2, hden = r2 * r2 + a2 * Z * Z;
+    const double t = 1.0 / (den * r * hden);
+    const double iden = t * r * hden, ir = t * den * hden, ihden = t * den * r;
+    const double l1 = (r * X + a * Y) * iden, l2 = (r * Y - a * X) * iden, l3 = Z * ir;
+    const double H = (2.0 * m.M * r - m.Q2) * r2 * ihden;
+    const double lp = -p[0] + l1 * p[1] + l2 * p[2] + l3 * p[3];
+    const double C = -p[0] * p[0] + p[1] * p[1] + p[2] * p[2] + p[3] * p[3] - H * lp * lp;
+    const float rf = float(r), isd = 1.f / float(sd);
+    const float d1 = rf * float(X) * isd, d2 = rf * float(Y) * isd, d3 = float(Z) * float(den) * isd / rf;
+    const float Hf = float(H);
+    const float ld = float(l1) * d1 + float(l2) * d2 + float(l3) * d3;
+    const float A = d1 * d1 + d2 * d2 + d3 * d3 - Hf * ld * ld;
+    const float pd = float(p[1]) * d1 + float(p[2]) * d2 + float(p[3]) * d3;
+    const float B = 2.f * (pd - Hf * float(lp) * ld);
+    const float Cf = float(C);
+    const float disc = B * B - 4.f * A * Cf;
+    if (!(disc >= 0.f) || fabsf(A) < 1e-15f) return C;
+    const float q = -0.5f * (B + copysignf(sqrtf(disc), B));
+    if (q == 0.f) return C;
+    const double alpha = double(Cf / q);
+    p[1] += alpha * double(d1);
+    p[2] += alpha * double(d2);
+    p[3] += alpha * double(d3);
+    return C;
+}
+
 // ---------------------------------------------------------------------------
 // The metric alone, FP64, closed form (no derivatives): g[16].
 // ---------------------------------------------------------------------------
