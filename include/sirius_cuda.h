@@ -266,8 +266,9 @@ int sirius_cuda_trace_frames_device(sirius_cuda_handle handle,
 
 /* Allocation-free form of sirius_cuda_trace_frames_device (no counterpart in the
  * reference): same arguments, same results, but the launch scratch (frame
- * descriptors, ray-queue and step counters, status word) lives in a static
- * device array of the library, so the call makes no device allocation. For
+ * descriptors, ray-queue and step counters, status word, per-frame disk flux
+ * tables; 150 KB in all) lives in a static device array of the library, held
+ * by every GPU that loads it, so the call makes no device allocation. For
  * callers that cannot let a library allocate: a host whose own allocator
  * already holds the device memory it is given, or a frame loop that cannot
  * afford the implicit device-wide synchronisation of cudaMalloc/cudaFree.

@@ -49,6 +49,7 @@ struct Params {
     float* spectra;
     const sirius_camera_ray* host_rays;  // optional: explicit camera rays (device copy)
     const unsigned* list;                 // optional: trace only these ray indices (total = list length)
+    const float* flux;                    // optional: per-frame disk flux tables (mixed path), kFluxN each
     unsigned long long* queue;            // [0] ray cursor
     unsigned long long* counters;         // [0] accepted, [1] rejected, [2] fp64 steps
     int* status;                          // [0] watchdog flag
@@ -344,6 +345,59 @@ __device__ __noinline__ void volumetric_segment(const Params& P, const FrameDev&
 // A disk crossing at the event-located point (xc1, xc2, 0): BL radius, exact
 // redshift with the ray's conserved E and L_z (from the state x, p), flux.
 // Returns true when the crossing lies on the disk (GTRC001A.cpp:468-555).
+// Per-frame table of the Page-Thorne flux for the mixed path: kFluxN samples
+// at u = sqrt((r - r_in) / (r_out - r_in)) in [0, 1] (F ~ (r - r_ISCO) near the
+// inner edge is smooth in u), read by cubic Lagrange interpolation, followed by
+// kFluxN cell flags. The flux as the reference defines it switches to an
+// approximate form where the full expression is not positive (PHAD001A.h:321-361),
+// which leaves a kink; a cell whose interpolant misses the exact flux at its
+// midpoint by more than 1e-6 (relative) is flagged, and a crossing there
+// evaluates the 16-point quadrature itself, as the FP64 path does everywhere.
+constexpr int kFluxN = 256;
+constexpr int kFluxTable = 2 * kFluxN;  // floats per frame: samples, then cell flags
+
+__device__ __forceinline__ double flux_cubic(const float* t, double x) {
+    int j = int(x) - 1;
+    j = j < 0 ? 0 : (j > kFluxN - 4 ? kFluxN - 4 : j);
+    const double f = x - j;  // position within the samples j..j+3, in [0, 3]
+    const double w0 = -(f - 1.0) * (f - 2.0) * (f - 3.0) / 6.0, w1 = f * (f - 2.0) * (f - 3.0) / 2.0,
+                 w2 = -f * (f - 1.0) * (f - 3.0) / 2.0, w3 = f * (f - 1.0) * (f - 2.0) / 6.0;
+    return w0 * t[j] + w1 * t[j + 1] + w2 * t[j + 2] + w3 * t[j + 3];
+}
+
+// One block of kFluxN threads per frame.
+__global__ void __launch_bounds__(kFluxN) flux_table_kernel(const FrameDev* frames, float* table) {
+    __shared__ float node[kFluxN];
+    const FrameDev& F = frames[blockIdx.x];
+    const int j = threadIdx.x;
+    const bool disk = F.m.family == SIRIUS_METRIC_KERR_SCHILD && F.has_horizon;
+    const double span = F.disk_out - F.disk_in;
+    float v = 0.f;
+    if (disk) {
+        const double u = double(j) / (kFluxN - 1);
+        v = float(nt_flux(F.disk_in + span * u * u, F.a_star, F.isco, F.disk_in, F.disk_out));
+    }
+    node[j] = v;
+    __syncthreads();
+    float flag = 0.f;
+    if (disk && j < kFluxN - 1) {
+        const double x = j + 0.5, u = x / (kFluxN - 1);
+        const double exact = nt_flux(F.disk_in + span * u * u, F.a_star, F.isco, F.disk_in, F.disk_out);
+        if (fabs(flux_cubic(node, x) - exact) > 1e-6 * fabs(exact)) flag = 1.f;
+    }
+    float* t = table + size_t(blockIdx.x) * kFluxTable;
+    t[j] = v;
+    t[kFluxN + j] = flag;
+}
+
+__device__ __forceinline__ double flux_lookup(const float* t, const FrameDev& F, double r) {
+    const double u = sqrt(fmin(fmax((r - F.disk_in) / (F.disk_out - F.disk_in), 0.0), 1.0));
+    const double x = u * (kFluxN - 1);
+    const int cell = min(int(x), kFluxN - 2);
+    if (t[kFluxN + cell] != 0.f) return nt_flux(r, F.a_star, F.isco, F.disk_in, F.disk_out);
+    return flux_cubic(t, x);
+}
+
 __device__ __noinline__ bool record_crossing(const Params& P, const FrameDev& F, long long idx, int n, double xc1,
                                              double xc2, const double x[4], const double p[4], double& intensity) {
     const MetricDev& m = F.m;
@@ -354,7 +408,8 @@ __device__ __noinline__ bool record_crossing(const Params& P, const FrameDev& F,
     if (!(rc >= F.disk_in && rc <= F.disk_out)) return false;
     const double E = -p[0], Lz = x[1] * p[2] - x[2] * p[1];
     const double g = kepler_g<double>(m, xc1, xc2, 0.0, rc, E, Lz, F.sqrt_m_gtt_cam);
-    const double Fl = nt_flux(rc, F.a_star, F.isco, F.disk_in, F.disk_out);
+    const double Fl = P.flux ? flux_lookup(P.flux + size_t(F.flux_slot) * kFluxTable, F, rc)
+                             : nt_flux(rc, F.a_star, F.isco, F.disk_in, F.disk_out);
     intensity += exp(-P.c.decay * n) * g * g * g * g * Fl;
     if (P.results) {
         sirius_ray_result* R = P.results + idx;
@@ -456,8 +511,12 @@ __device__ __forceinline__ int advance(const Params& P, Ray<MIXED>& s, float& ma
     const bool cross = disk_on && (s.x[3] * xn[3] < 0.0);
     if (cross) {
         const double hs = hermite_root(s.x[3], xn[3], double(s.k[3]), double(k7[3]), hstep) * hstep;
-        if (island || !MIXED) locate_equator<double, FAM>(m, c, s.x, s.p, hs, xc1, xc2);
-        else locate_equator<float, FAM>(m, c, s.x, s.p, hs, xc1, xc2);
+        if constexpr (MIXED) {
+            if (island) locate_equator<double, FAM>(m, c, s.x, s.p, hs, xc1, xc2);
+            else locate_equator_f32<FAM>(m, c, s.x, s.p, s.k, hs, xc1, xc2);
+        } else {
+            locate_equator<double, FAM>(m, c, s.x, s.p, hs, xc1, xc2);
+        }
     }
     double x0[4];
     float k0f[4];
@@ -941,6 +1000,8 @@ struct Handle {
     size_t image_cap = 0;
     float* d_spectra = nullptr;
     size_t spectra_cap = 0;
+    float* d_flux = nullptr;  // per-frame disk flux tables of the mixed path
+    size_t flux_cap = 0;
     sirius_camera_ray* d_rays = nullptr;
     size_t rays_cap = 0;
     unsigned long long* d_queue = nullptr;  // [0] cursor, [1..3] counters
@@ -1121,18 +1182,24 @@ int validate_config(Handle* H, const sirius_trace_config& c) {
 
 // Launch the tracer over [0, total) of already-uploaded frames.
 // Device scratch of one launch: the frame descriptors, the queue cursor and
-// counters ([0] cursor, [1..3] counters, [4] launch start) and the status word.
+// counters ([0] cursor, [1..3] counters, [4] launch start), the status word and
+// room for the per-frame disk flux tables (kFluxTable floats per frame).
 struct LaunchScratch {
     const FrameDev* frames;
     unsigned long long* queue;
     int* status;
+    float* flux;
 };
 
 int launch_trace(Handle* H, int n_frames, long long total, sirius_ray_result* d_results, float* d_image,
                  float* d_spectra, const sirius_camera_ray* d_rays, cudaStream_t st, bool timed,
                  const LaunchScratch* scratch = nullptr, const unsigned* d_list = nullptr) {
     const sirius_trace_config& c = H->cfg;
-    const LaunchScratch own{H->d_frames, H->d_queue, H->d_status};
+    if (!scratch && (c.precision == SIRIUS_PRECISION_MIXED)) {
+        const int rc = ensure(H, H->d_flux, H->flux_cap, size_t(n_frames) * kFluxTable);
+        if (rc != SIRIUS_OK) return rc;
+    }
+    const LaunchScratch own{H->d_frames, H->d_queue, H->d_status, H->d_flux};
     const LaunchScratch& S = scratch ? *scratch : own;
     Params P{};
     P.frames = S.frames;
@@ -1208,6 +1275,15 @@ int launch_trace(Handle* H, int n_frames, long long total, sirius_ray_result* d_
     // whole-launch bound on the device clock, measured from the first warp's start
     P.watchdog_ns = c.watchdog_ms > 0 ? (unsigned long long)c.watchdog_ms * 1000000ull : ~0ull;
     if (timed) CK(cudaEventRecord(H->ev[1], st));
+    // the mixed path reads the disk flux from per-frame tables
+    P.flux = nullptr;
+    int extra_launches = 0;
+    if (mixed && c.enable_disk && (H->family_mask & (1 << SIRIUS_METRIC_KERR_SCHILD)) && S.flux) {
+        flux_table_kernel<<<n_frames, kFluxN, 0, st>>>(S.frames, S.flux);
+        CK(cudaGetLastError());
+        P.flux = S.flux;
+        extra_launches = 1;
+    }
     for (int i = 0; i < n_launches; ++i) {
         P.family = launch_family[i];
         launch_fn[i]<<<grid, block, shmem, st>>>(P);
@@ -1216,7 +1292,7 @@ int launch_trace(Handle* H, int n_frames, long long total, sirius_ray_result* d_
     if (timed) CK(cudaEventRecord(H->ev[2], st));
     H->stats.grid_blocks = grid;
     H->stats.block_size = block;
-    H->stats.kernel_launches = n_launches;
+    H->stats.kernel_launches = n_launches + extra_launches;
     return SIRIUS_OK;
 }
 
@@ -1260,12 +1336,13 @@ struct StaticScratch {
     FrameDev frames[SIRIUS_STATIC_MAX_FRAMES];
     unsigned long long queue[8];  // [0] cursor, [1..3] counters, [4] launch start
     int status;
+    float flux[SIRIUS_STATIC_MAX_FRAMES * kFluxTable];  // the mixed path's disk flux tables
 };
 constexpr int kStaticMaxDevices = 64;
 }  // namespace
 
 static __device__ __align__(256) unsigned char g_static_scratch[sizeof(StaticScratch)];
-static_assert(sizeof(StaticScratch) <= 64 * 1024, "static scratch stays modest");
+static_assert(sizeof(StaticScratch) <= 160 * 1024, "static scratch stays modest");
 
 namespace {
 // The device address of g_static_scratch on `device`, resolved once per device
@@ -1334,6 +1411,7 @@ int sirius_cuda_destroy(sirius_cuda_handle h) {
     cudaSetDevice(H->device);
     if (H->stream) cudaStreamSynchronize(H->stream);
     cudaFree(H->d_frames); cudaFree(H->d_results); cudaFree(H->d_image); cudaFree(H->d_spectra);
+    cudaFree(H->d_flux);
     cudaFree(H->d_rays); cudaFree(H->d_queue); cudaFree(H->d_status);
     cudaFree(H->d_surrogate); cudaFree(H->d_sur_err);
     cudaFree(H->d_sur_frames); cudaFree(H->d_feat); cudaFree(H->d_mlp_out); cudaFree(H->d_list); cudaFree(H->d_gate);
@@ -1374,6 +1452,7 @@ static int upload_frames(Handle* H, const sirius_frame* frames, int n, long long
         if (f.ray_offset != total)
             return fail(H, SIRIUS_ERR_INVALID_ARGUMENT, "frames must be contiguous: ray_offset[i] = sum of previous pixel counts");
         fd[i] = make_frame(f, H->cfg);
+        fd[i].flux_slot = i;
         total += fd[i].n_rays;
     }
     H->family_mask = 0;
@@ -1470,6 +1549,7 @@ int sirius_cuda_trace_frames_static(sirius_cuda_handle h, const sirius_frame* d_
         if (f.ray_offset != total)
             return fail(H, SIRIUS_ERR_INVALID_ARGUMENT, "frames must be contiguous: ray_offset[i] = sum of previous pixel counts");
         fd[i] = make_frame(f, H->cfg);
+        fd[i].flux_slot = i;
         total += fd[i].n_rays;
         mask |= 1 << f.metric.family;
     }
@@ -1478,7 +1558,7 @@ int sirius_cuda_trace_frames_static(sirius_cuda_handle h, const sirius_frame* d_
     CK(cudaMemcpyAsync(scratch->frames, fd, n_frames * sizeof(FrameDev), cudaMemcpyHostToDevice, st));
     H->family_mask = mask;
     H->frame0 = fd[0];
-    const LaunchScratch ls{scratch->frames, scratch->queue, &scratch->status};
+    const LaunchScratch ls{scratch->frames, scratch->queue, &scratch->status, scratch->flux};
     return launch_trace(H, n_frames, total, d_results, d_image, d_spectra, nullptr, st, false, &ls);
 }
 

@@ -23,6 +23,7 @@ struct FrameDev {
     MetricDev m;
     long long ray_offset, n_rays;
     int width, height, projection, has_horizon, gate;
+    int flux_slot;  // index of this frame's disk flux table (its position in the launch)
     // camera
     double cam_t, cam_r, cam_st, cam_ct, cam_sp, cam_cp, cam_th, cam_ph;
     float aspect, tan_half_fov, cY, sY, cP, sP, cR, sR;
@@ -359,6 +360,22 @@ __device__ __noinline__ void locate_equator(const MetricDev& m, const CfgDev& c,
     dp45_attempt<T, FAM>(m, c, x0, p0, hs, k0, xn, pn, k7);
     hs -= xn[3] / double(k7[3]);
     dp45_attempt<T, FAM>(m, c, x0, p0, hs, k0, xn, pn, k7);
+    const double dl = -xn[3] / double(k7[3]);
+    xc1 = xn[1] + dl * double(k7[1]);
+    xc2 = xn[2] + dl * double(k7[2]);
+}
+
+// The mixed path's event location: one FP32 DP45 sub-step of length hs from
+// the step's start state with its stored f(x0, p0), then the first-order
+// correction along k. FP32 stages bound the location at ~1e-7 relative, which a
+// second sub-step would not improve.
+template <int FAM = kAnyFamily>
+__device__ __noinline__ void locate_equator_f32(const MetricDev& m, const CfgDev& c, const double x0[4],
+                                                const double p0[4], const float k0[8], double hs, double& xc1,
+                                                double& xc2) {
+    double xn[4], pn[4];
+    float k7[8];
+    dp45_attempt<float, FAM>(m, c, x0, p0, hs, k0, xn, pn, k7);
     const double dl = -xn[3] / double(k7[3]);
     xc1 = xn[1] + dl * double(k7[1]);
     xc2 = xn[2] + dl * double(k7[2]);
