@@ -97,6 +97,7 @@ struct Ray {
     double h;
     double intensity;
     float min_r, null_max, tphi, prev_z;
+    float prev_r;  // r at the start of the step (volumetric early-out)
     int steps, rejected, attempts, ncross, eq, fp64_steps;
     int frame;
     int crit;  // mixed path: the ray skims the photon region, every step in FP64
@@ -171,6 +172,7 @@ __device__ __noinline__ void begin_ray(const Params& P, Ray<MIXED>& s, long long
     s.null_max = 0.f;
     s.tphi = 0.f;
     s.prev_z = float(s.x[3]);
+    s.prev_r = float(ks_radius(F.m, s.x));
     s.steps = s.rejected = s.attempts = s.ncross = s.eq = s.fp64_steps = 0;
     s.crit = 0;
     if (MIXED && F.gate && P.c.crit_band > 0.0) {
@@ -269,37 +271,39 @@ __device__ __forceinline__ float ks_r(const MetricDev& m, float x, float y, floa
 //   dtau = alpha (nu_cam/g) dl, S = g^3 / c_a.  (vol: [2b] = I_b, [2b+1] = T_b, stride blockDim)
 __device__ __noinline__ void volumetric_segment(const Params& P, const FrameDev& F, const double x0[4],
                                                 const double x1[4], const float k0[4], const float k1[4],
-                                                const double p[4], double h, float* vol) {
+                                                const double p[4], double h, float r0, float r1, float* vol) {
     const CfgDev& c = P.c;
     const int nq = c.vol_sub < 1 ? 1 : (c.vol_sub > 4 ? 4 : c.vol_sub);
     const float E = float(-p[0]);
     const float Lz = float(x1[1] * p[2] - x1[2] * p[1]);
     const float nu_cam = E / float(F.sqrt_m_gtt_cam);
     const float rin = float(F.disk_in), rout = float(F.disk_out);
-    const float r0 = ks_r(F.m, float(x0[1]), float(x0[2]), float(x0[3]));
-    const float r1 = ks_r(F.m, float(x1[1]), float(x1[2]), float(x1[3]));
-    // steps that cannot reach the emitting region (the step cap keeps a step
-    // that starts outside it from jumping in)
-    const float hz = float(c.vol_hz), z0 = float(x0[3]), z1 = float(x1[3]);
-    if (r0 > rout && r1 > rout) return;
-    if (z0 * z1 > 0.f && fabsf(z0) > float(kVolCutoff) * hz * fminf(fmaxf(r0, rin), rout) &&
-        fabsf(z1) > float(kVolCutoff) * hz * fminf(fmaxf(r1, rin), rout))
-        return;
     const bool in0 = r0 >= rin && r0 <= rout, in1 = r1 >= rin && r1 <= rout;
     double fa = 0.0, fb = 1.0;
     if (in0 != in1) {
+        // the annulus edge on the step's Hermite interpolant: regula falsi
+        // (Illinois) on r(q) - edge over [0, 1], three evaluations
         const float edge = in0 ? (r1 < rin ? rin : rout) : (r0 < rin ? rin : rout);
-        const bool below_lo = r0 < edge;
-        double lo = 0.0, hi = 1.0;
-        for (int it = 0; it < 24; ++it) {
-            const double q = 0.5 * (lo + hi);
+        double qa = 0.0, qb = 1.0, ga = double(r0) - edge, gb = double(r1) - edge;
+        int side = 0;
+        for (int it = 0; it < 3; ++it) {
+            const double q = (qa * gb - qb * ga) / (gb - ga);
             float xs, ys, zs;
             hermite_xyz(x0, x1, k0, k1, h, q, xs, ys, zs);
-            if ((ks_r(F.m, xs, ys, zs) < edge) == below_lo) lo = q;
-            else hi = q;
+            const double g = double(ks_r(F.m, xs, ys, zs)) - edge;
+            if ((g < 0.0) == (ga < 0.0)) {
+                qa = q; ga = g;
+                if (side == -1) gb *= 0.5;
+                side = -1;
+            } else {
+                qb = q; gb = g;
+                if (side == 1) ga *= 0.5;
+                side = 1;
+            }
         }
-        if (in0) fb = 0.5 * (lo + hi);
-        else fa = 0.5 * (lo + hi);
+        const double qe = (qa * gb - qb * ga) / (gb - ga);
+        if (in0) fb = qe;
+        else fa = qe;
     }
     const double span = fb - fa;
     // per Gauss-Legendre point: optical depth per unit nu^-s and source function
@@ -618,11 +622,21 @@ __device__ __forceinline__ int advance(const Params& P, Ray<MIXED>& s, float& ma
     }
     if (!disk_on) return s.steps >= c.max_steps ? (s.ncross > 0 ? SIRIUS_DISK_HIT : SIRIUS_MAX_STEPS) : -1;
     if (c.enable_vol && vol) {
-        float k1f[4];
+        // steps that cannot reach the emitting region skip the segment (the
+        // step cap keeps a step that starts outside it from jumping in)
+        const float r0 = s.prev_r, r1 = float(rr), rin = float(F.disk_in), rout = float(F.disk_out);
+        const float zc = float(kVolCutoff * c.vol_hz), z0 = float(x0[3]), z1 = float(s.x[3]);
+        const bool beyond = (r0 > rout && r1 > rout) ||
+                            (z0 * z1 > 0.f && fabsf(z0) > zc * fminf(fmaxf(r0, rin), rout) &&
+                             fabsf(z1) > zc * fminf(fmaxf(r1, rin), rout));
+        if (!beyond) {
+            float k1f[4];
 #pragma unroll
-        for (int i = 0; i < 4; ++i) k1f[i] = float(s.k[i]);
-        volumetric_segment(P, F, x0, s.x, k0f, k1f, s.p, hstep, vol);
+            for (int i = 0; i < 4; ++i) k1f[i] = float(s.k[i]);
+            volumetric_segment(P, F, x0, s.x, k0f, k1f, s.p, hstep, r0, r1, vol);
+        }
     }
+    s.prev_r = float(rr);
     // thin-disk crossing (GTRC001A.h:404-431, GTRC001A.cpp:468-555)
     if (cross && s.ncross < SIRIUS_MAX_CROSSINGS) {
         if (record_crossing(P, F, s.idx, s.ncross, xc1, xc2, s.x, s.p, s.intensity)) {
