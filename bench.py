@@ -413,7 +413,7 @@ def main():
     clocks = ClockSampler(local)
     clocks.start()
     ev = [(torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)) for _ in range(args.steps)]
-    kernel_ms, accepted, rejected, fp64 = [], 0, 0, 0
+    kernel_ms, accepted, rejected, fp64, launches = [], 0, 0, 0, 0
     for i in range(args.steps):
         flush.zero_()
         ev[i][0].record(stream)
@@ -421,6 +421,7 @@ def main():
         ev[i][1].record(stream)
         st = eng.stats()  # synchronises on the library's stream: per-launch kernel time (CUDA events)
         kernel_ms.append(st.kernel_ms)
+        launches += st.kernel_launches
         accepted += st.accepted_steps
         rejected += st.rejected_steps
         fp64 += st.fp64_steps
@@ -462,7 +463,7 @@ def main():
             "data": "synthetic (seeded camera frame; no dataset)", "config": workload_desc(args.size),
             "e2e": {"value": e2e, "unit": "Mrays/s", "h2d_bytes_per_step": C.sizeof(abi.Frame),
                     "d2h_bytes_per_step": total * 4 * (1 + N_BINS)},
-            "gpu_launches": args.steps,
+            "gpu_launches": launches,
             "roofline": {"bound": "fp32_simt", "achieved": achieved, "peak": peak32, "unit": "TFLOP/s",
                          "frac": achieved / peak32, "traffic": TRAFFIC_BYTES_PER_RAY * total,
                          "traffic_unit": "bytes per launch (ncu, 256^2 capture scaled by rays)",
