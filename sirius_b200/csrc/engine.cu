@@ -929,7 +929,7 @@ __global__ void sur_scatter_kernel(const unsigned char* gate, long long total, c
 // Pixels the integrator takes (gate != 0) get only the MLP copy: the
 // integrator writes their image value.
 __global__ void sur_shade_kernel(const FrameDev* frames, int n_frames, long long total, const float* out,
-                                 const unsigned char* gate, float* image, float* image_mlp) {
+                                 const unsigned char* gate, const float* flux, float* image, float* image_mlp) {
     const long long idx = (long long)blockIdx.x * blockDim.x + threadIdx.x;
     if (idx >= total) return;
     const int f = n_frames > 1 ? find_frame(frames, n_frames, idx) : 0;
@@ -939,7 +939,7 @@ __global__ void sur_shade_kernel(const FrameDev* frames, int n_frames, long long
     if (o.x > 0.f) {
         const double r1 = fmin(fmax(double(kSurRScale) * (1.0 + double(o.y)), F.disk_in), F.disk_out);
         const double g1 = fmax(double(o.z), 0.0);
-        I = g1 * g1 * g1 * g1 * nt_flux(r1, F.a_star, F.isco, F.disk_in, F.disk_out);
+        I = g1 * g1 * g1 * g1 * flux_lookup(flux + size_t(F.flux_slot) * kFluxTable, F, r1);
     }
     I += fmax(double(o.w), 0.0) * double(kSurHigher);
     if (gate[idx] == 0) image[idx] = float(I);
@@ -1805,16 +1805,16 @@ static SurFrameDev make_sur_frame(const sirius_frame& f, const FrameDev& F) {
     const double co = std::cos(th), cot = co / S.sin_o;
     if (std::fabs(a) < 1e-6 * M) {
         const double R = std::sqrt(27.0) * M;
-        for (int i = 0; i < 4096; ++i) {
-            const double t = 2.0 * kPi * i / 4096.0;
+        for (int i = 0; i < 1024; ++i) {
+            const double t = 2.0 * kPi * i / 1024.0;
             pts.push_back({R * std::cos(t), R * std::sin(t)});
         }
     } else {
         const double as = std::clamp(std::fabs(a) / M, 0.0, 1.0);
         const double r0 = 2.0 * M * (1.0 + std::cos((2.0 / 3.0) * std::acos(-as)));
         const double r1 = 2.0 * M * (1.0 + std::cos((2.0 / 3.0) * std::acos(as)));
-        for (int i = 0; i <= 8192; ++i) {
-            const double r = r0 + (r1 - r0) * i / 8192.0;
+        for (int i = 0; i <= 1024; ++i) {
+            const double r = r0 + (r1 - r0) * i / 1024.0;
             const double xi = (r * r * (3.0 * M - r) - a * a * (r + M)) / (a * (r - M));
             const double eta = r * r * r * (4.0 * a * a * M - r * (r - 3.0 * M) * (r - 3.0 * M)) / (a * a * (r - M) * (r - M));
             const double b2 = eta + a * a * co * co - xi * xi * cot * cot;
@@ -1912,8 +1912,11 @@ static int render_surrogate(Handle* H, const sirius_frame* frames, int n_frames,
     CK(cudaMemsetAsync(H->d_sur_err, 0, sizeof(int), st));
     if ((rc = surrogate_launch(H, H->d_feat, total, H->d_mlp_out, st)) != SIRIUS_OK) return rc;
     CK(cudaEventRecord(H->sev[2], st));
+    if ((rc = ensure(H, H->d_flux, H->flux_cap, size_t(n_frames) * kFluxTable)) != SIRIUS_OK) return rc;
+    flux_table_kernel<<<n_frames, kFluxN, 0, st>>>(H->d_frames, H->d_flux);
+    CK(cudaGetLastError());
     sur_shade_kernel<<<int((total + 255) / 256), 256, 0, st>>>(H->d_frames, n_frames, total, H->d_mlp_out, d_gate,
-                                                               d_image, d_image_mlp);
+                                                               H->d_flux, d_image, d_image_mlp);
     CK(cudaGetLastError());
     CK(cudaEventRecord(H->sev[3], st));
     if (n_int > 0) {
