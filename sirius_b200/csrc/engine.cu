@@ -1746,8 +1746,8 @@ int sirius_cuda_surrogate_load(sirius_cuda_handle h, const float* params, int64_
             return fail(H, SIRIUS_ERR_OUT_OF_MEMORY, "cudaMalloc surrogate weights");
         if (cudaMalloc((void**)&H->d_sur_err, sizeof(int)) != cudaSuccess)
             return fail(H, SIRIUS_ERR_OUT_OF_MEMORY, "cudaMalloc surrogate status");
-        CK(cudaFuncSetAttribute(surrogate::mlp_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                surrogate::kSmBytes));
+        CK(cudaFuncSetAttribute(surrogate::mlp_kernel_ts, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                surrogate::kTsSmBytes));
     }
     CK(cudaMemcpyAsync(H->d_surrogate, img.data(), surrogate::kImageBytes, cudaMemcpyHostToDevice, H->stream));
     CK(cudaStreamSynchronize(H->stream));
@@ -1762,7 +1762,7 @@ static int surrogate_launch(Handle* H, const float* d_features, long long n, flo
     const int grid = int(std::min<long long>(tiles, H->num_sms));
     // bound on any wait inside the kernel: the configured watchdog (default 30 s)
     const unsigned long long limit = (unsigned long long)(H->cfg.watchdog_ms > 0 ? H->cfg.watchdog_ms : 30000) * 1000000ull;
-    surrogate::mlp_kernel<<<grid, surrogate::kThreads, surrogate::kSmBytes, st>>>(H->d_surrogate, d_features, n, d_out,
+    surrogate::mlp_kernel_ts<<<grid, surrogate::kThreads, surrogate::kTsSmBytes, st>>>(H->d_surrogate, d_features, n, d_out,
                                                                                H->d_sur_err, limit);
     CK(cudaGetLastError());
     return SIRIUS_OK;

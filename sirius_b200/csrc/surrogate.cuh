@@ -5,24 +5,23 @@
 // accumulation, FP32 biases. One CTA of 256 threads owns one SM and walks
 // 128-row tiles of the input:
 //
-//   * A operand (activations, 128 x K) and B operand (weights, N x K) sit in
-//     shared memory, both K-major, in the no-swizzle core-matrix layout of the
-//     UMMA shared-memory descriptor: element (row, k) at byte
-//       (row % 8) * 16 + (row / 8) * SBO + (k / 8) * 128 + (k % 8) * 2,
-//     SBO = (K / 8) * 128 (8-row groups back to back, each group K/8 core
-//     matrices of 8 rows x 16 bytes).
-//   * One thread issues tcgen05.mma (M = 128, N = 256 or 16, K = 16 per
-//     instruction) into a 128-lane x 256-column FP32 accumulator in TMEM and
-//     commits to an mbarrier.
+//   * B operands (weights, N x K) sit in shared memory, K-major, in the
+//     no-swizzle core-matrix layout of the UMMA shared-memory descriptor:
+//     element (row, k) at byte (row % 8) * 16 + (row / 8) * SBO + (k / 8) * 128
+//     + (k % 8) * 2, SBO = (K / 8) * 128.
+//   * The FP32 accumulator and the BF16 activations (the A operand of layers
+//     2-5) live in tensor memory; layer 1 reads its 16-wide padded input from
+//     shared memory. One thread issues tcgen05.mma (M = 128, N = 128 or 16,
+//     K = 16 per instruction) and commits each N-half to its own mbarrier.
 //   * The 128 KB weight images of layers 2-4 stream from global memory by a
 //     bulk TMA copy (cp.async.bulk, no tensor map, no multicast) into one
 //     buffer, each issued as soon as the previous layer's MMAs have drained it,
 //     so the copy overlaps the epilogue. Layer 1 (K padded 5 -> 16) and layer 5
 //     (N padded 4 -> 16) weights and all biases stay resident.
-//   * Epilogue: 8 warps read the accumulator with tcgen05.ld (warp w: TMEM lanes
-//     32 (w % 4).., columns 128 (w / 4)..), add the bias, apply SiLU
-//     x (1 + tanh(x / 2)) / 2 (one MUFU op), round to BF16 and write the next
-//     layer's A operand.
+//   * Epilogue: 8 warps read the accumulator with tcgen05.ld, add the bias,
+//     apply SiLU x (1 + tanh(x / 2)) / 2 (one MUFU op), round to BF16 and write
+//     the next layer's A operand with tcgen05.st; half 0 of a layer converts
+//     while the tensor core still works on half 1.
 //
 // Every mbarrier wait is bounded by the device clock; on a timeout the block
 // agrees (a block-wide vote) to stop, records an error flag, waits (bounded)
@@ -46,12 +45,6 @@ constexpr int kImageBytes = kOffBias + kBiasBytes;
 // host parameter vector (PyTorch nn.Linear order, out x in): W1 b1 W2 b2 W3 b3 W4 b4 W5 b5
 constexpr long long kParams = (long long)kHid * kIn + kHid + 3LL * (kHid * kHid + kHid) + kOut * kHid + kOut;
 
-// shared memory map of the kernel
-constexpr int kSmWbuf = 0, kSmW1 = kBigBytes, kSmW5 = kSmW1 + kW1Bytes, kSmA = kSmW5 + kW5Bytes,
-              kSmBias = kSmA + kTileM * kHid * 2, kSmBar = kSmBias + kBiasBytes, kSmTmemSlot = kSmBar + 16,
-              kSmBytes = kSmTmemSlot + 16;
-static_assert(kSmBytes <= 227 * 1024, "the MLP kernel's shared memory fits one SM");
-static_assert(kSmBar % 8 == 0, "mbarriers are 8-byte aligned");
 
 // byte offset of element (row, k) in a K-major core-matrix image with K columns
 __host__ __device__ inline int packed_offset(int row, int k, int K) {
@@ -171,60 +164,92 @@ __device__ __forceinline__ uint32_t pack_bf16x2(float lo, float hi) {
     return *reinterpret_cast<const uint32_t*>(&p);
 }
 
-// Hidden-layer epilogue: accumulator + bias -> SiLU -> BF16 A operand (K = 256).
-__device__ __forceinline__ void epilogue_hidden(uint32_t tmem, const float* bias, unsigned char* A) {
-    const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
-    const int q = warp & 3, half = warp >> 2;
-    const int row = q * 32 + lane;
-    unsigned char* arow = A + (row % 8) * 16 + (row / 8) * (kHid / 8) * 128;
+// ---------------------------------------------------------------------------
+// The MLP kernel, with its activations in tensor memory.
+//
+// TMEM (512 columns, one CTA per SM): columns [0, 256) the FP32 accumulator,
+// [256, 384) and [384, 512) two BF16 activation buffers (row m in lane m,
+// element k in column k / 2, even k in the low half), used in turn as the A
+// operand of tcgen05.mma (the form that reads A from tensor memory) and as the
+// epilogue's destination. Each layer's MMAs run as two N-halves committed to
+// separate mbarriers, so the epilogue of half 0 (TMEM -> bias -> SiLU -> BF16
+// -> tcgen05.st) overlaps the tensor core's work on half 1. Layer 1 reads its
+// 16-wide (padded) input from shared memory.
+// ---------------------------------------------------------------------------
+constexpr int kTsSmWbuf = 0, kTsSmW1 = kBigBytes, kTsSmW5 = kTsSmW1 + kW1Bytes, kTsSmX = kTsSmW5 + kW5Bytes,
+              kTsSmBias = kTsSmX + kTileM * kInPad * 2, kTsSmBar = kTsSmBias + kBiasBytes,
+              kTsSmTmemSlot = kTsSmBar + 32, kTsSmBytes = kTsSmTmemSlot + 16;
+static_assert(kTsSmBytes <= 227 * 1024, "the MLP kernel's shared memory fits one SM");
+static_assert(kTsSmBar % 8 == 0, "mbarriers are 8-byte aligned");
+constexpr uint32_t kTmemAcc = 0, kTmemA0 = 256, kTmemA1 = 384, kTmemCols = 512;
+
+__device__ __forceinline__ void mma_bf16_ts(uint32_t tmem_d, uint32_t tmem_a, uint64_t bdesc, uint32_t idesc,
+                                            uint32_t accumulate) {
+    asm volatile(
+        "{\n\t.reg .pred p;\n\tsetp.ne.b32 p, %4, 0;\n\t"
+        "tcgen05.mma.cta_group::1.kind::f16 [%0], [%1], %2, %3, {%5, %6, %7, %8}, p;\n\t}\n" ::"r"(tmem_d),
+        "r"(tmem_a), "l"(bdesc), "r"(idesc), "r"(accumulate), "r"(0), "r"(0), "r"(0), "r"(0));
+}
+
+// 16 consecutive 32-bit columns of this thread's TMEM lane.
+__device__ __forceinline__ void tmem_st16(uint32_t taddr, const uint32_t r[16]) {
+    asm volatile(
+        "tcgen05.st.sync.aligned.32x32b.x16.b32 [%0], {%1, %2, %3, %4, %5, %6, %7, %8, %9, %10, %11, %12, %13, %14, "
+        "%15, %16};" ::"r"(taddr),
+        "r"(r[0]), "r"(r[1]), "r"(r[2]), "r"(r[3]), "r"(r[4]), "r"(r[5]), "r"(r[6]), "r"(r[7]), "r"(r[8]), "r"(r[9]),
+        "r"(r[10]), "r"(r[11]), "r"(r[12]), "r"(r[13]), "r"(r[14]), "r"(r[15])
+        : "memory");
+}
+
+// Epilogue of accumulator half H (columns 128 H ..): bias + SiLU -> BF16 pairs
+// into the activation buffer at TMEM column a_next. Warp w: lanes 32 (w % 4)..,
+// columns 128 H + 64 (w / 4)...
+__device__ __forceinline__ void epilogue_half_ts(uint32_t tmem, int H, const float* bias, uint32_t a_next) {
+    const int warp = threadIdx.x >> 5;
+    const uint32_t lanes = uint32_t((warp & 3) * 32) << 16;
 #pragma unroll 1
-    for (int c = 0; c < 4; ++c) {
-        const int col0 = half * 128 + c * 32;
+    for (int c = 0; c < 2; ++c) {
+        const int col0 = 128 * H + 64 * (warp >> 2) + 32 * c;
         float v[32];
-        tmem_ld32(tmem + (uint32_t(q * 32) << 16) + uint32_t(col0), v);
+        tmem_ld32(tmem + kTmemAcc + lanes + uint32_t(col0), v);
+        uint32_t r[16];
 #pragma unroll
-        for (int g = 0; g < 4; ++g) {
-            uint4 w;
-            const int k = col0 + g * 8;
-            w.x = pack_bf16x2(silu(v[g * 8 + 0] + bias[k + 0]), silu(v[g * 8 + 1] + bias[k + 1]));
-            w.y = pack_bf16x2(silu(v[g * 8 + 2] + bias[k + 2]), silu(v[g * 8 + 3] + bias[k + 3]));
-            w.z = pack_bf16x2(silu(v[g * 8 + 4] + bias[k + 4]), silu(v[g * 8 + 5] + bias[k + 5]));
-            w.w = pack_bf16x2(silu(v[g * 8 + 6] + bias[k + 6]), silu(v[g * 8 + 7] + bias[k + 7]));
-            *reinterpret_cast<uint4*>(arow + (k / 8) * 128) = w;
-        }
+        for (int i = 0; i < 16; ++i)
+            r[i] = pack_bf16x2(silu(v[2 * i] + bias[col0 + 2 * i]), silu(v[2 * i + 1] + bias[col0 + 2 * i + 1]));
+        tmem_st16(tmem + a_next + lanes + uint32_t(col0 / 2), r);
     }
 }
 
-// out[n x 4] = MLP(feat[n x 5]). err[0] |= 1 when a wait timed out.
 __global__ void __launch_bounds__(kThreads, 1)
-    mlp_kernel(const unsigned char* __restrict__ wimg, const float* __restrict__ feat, long long n,
-               float* __restrict__ out, int* err, unsigned long long wait_limit_ns) {
+    mlp_kernel_ts(const unsigned char* __restrict__ wimg, const float* __restrict__ feat, long long n,
+                  float* __restrict__ out, int* err, unsigned long long wait_limit_ns) {
     extern __shared__ __align__(1024) unsigned char sm[];
-    unsigned char* Wbuf = sm + kSmWbuf;
-    unsigned char* W1s = sm + kSmW1;
-    unsigned char* W5s = sm + kSmW5;
-    unsigned char* A = sm + kSmA;
-    float* bias = reinterpret_cast<float*>(sm + kSmBias);
-    uint32_t* tslot = reinterpret_cast<uint32_t*>(sm + kSmTmemSlot);
-    const uint32_t bar_mma = smem_u32(sm + kSmBar), bar_tma = smem_u32(sm + kSmBar + 8);
+    unsigned char* Wbuf = sm + kTsSmWbuf;
+    unsigned char* W1s = sm + kTsSmW1;
+    unsigned char* W5s = sm + kTsSmW5;
+    unsigned char* Xs = sm + kTsSmX;
+    float* bias = reinterpret_cast<float*>(sm + kTsSmBias);
+    uint32_t* tslot = reinterpret_cast<uint32_t*>(sm + kTsSmTmemSlot);
+    const uint32_t bar_a = smem_u32(sm + kTsSmBar), bar_b = smem_u32(sm + kTsSmBar + 8),
+                   bar_tma = smem_u32(sm + kTsSmBar + 16);
     const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
     const long long ntiles = (n + kTileM - 1) / kTileM;
 
     if (tid == 0) {
-        mbar_init(bar_mma, 1);
+        mbar_init(bar_a, 1);
+        mbar_init(bar_b, 1);
         mbar_init(bar_tma, 1);
         asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
     }
     if (warp == 0) {
         asm volatile("tcgen05.alloc.cta_group::1.sync.aligned.shared::cta.b32 [%0], %1;" ::"r"(smem_u32(tslot)),
-                     "r"(256));
+                     "r"(kTmemCols));
         asm volatile("tcgen05.relinquish_alloc_permit.cta_group::1.sync.aligned;");
     }
-    // resident operands: W1, W5 and the biases
-    {
+    {  // resident operands: W1 | W5 (contiguous in the image and in shared memory) and the biases
         const uint4* src1 = reinterpret_cast<const uint4*>(wimg + kOffW1);
         uint4* dst1 = reinterpret_cast<uint4*>(W1s);
-        for (int i = tid; i < (kW1Bytes + kW5Bytes) / 16; i += kThreads) dst1[i] = src1[i];  // W1 | W5 contiguous
+        for (int i = tid; i < (kW1Bytes + kW5Bytes) / 16; i += kThreads) dst1[i] = src1[i];
         const float4* srcb = reinterpret_cast<const float4*>(wimg + kOffBias);
         float4* dstb = reinterpret_cast<float4*>(bias);
         for (int i = tid; i < kBiasBytes / 16; i += kThreads) dstb[i] = srcb[i];
@@ -235,16 +260,15 @@ __global__ void __launch_bounds__(kThreads, 1)
     tc_fence_after();
     const uint32_t tmem = *tslot;
 
-    uint32_t ph_mma = 0, ph_tma = 0;
-    bool tma_pending = false;
-    bool ok = true;
+    uint32_t ph_a = 0, ph_b = 0, ph_tma = 0;
+    bool tma_pending = false, ok = true;
     if (tid == 0 && blockIdx.x < ntiles) bulk_load(smem_u32(Wbuf), wimg, kBigBytes, bar_tma);
     tma_pending = blockIdx.x < ntiles;
+    const uint32_t idesc128 = instr_desc(128), idesc16 = instr_desc(kOutPad);
 
     for (long long tile = blockIdx.x; tile < ntiles; tile += gridDim.x) {
         const long long row0 = tile * kTileM;
-        // X tile: 128 rows x 16 BF16 (features 0..4, zero padding)
-        {
+        {  // input tile: 128 rows x 16 BF16 (features 0..4, zero padding)
             const int r = tid >> 1, chunk = tid & 1;
             uint4 w = make_uint4(0, 0, 0, 0);
             const long long gr = row0 + r;
@@ -254,27 +278,38 @@ __global__ void __launch_bounds__(kThreads, 1)
                 w.y = pack_bf16x2(f[2], f[3]);
                 w.z = pack_bf16x2(f[4], 0.f);
             }
-            *reinterpret_cast<uint4*>(A + packed_offset(r, chunk * 8, kInPad)) = w;
+            *reinterpret_cast<uint4*>(Xs + packed_offset(r, chunk * 8, kInPad)) = w;
         }
         fence_async_smem();
         __syncthreads();
-        // layer 1: K = 16, one instruction
+        // layer 1 (A from shared memory, K = 16): two N-halves
         if (tid == 0) {
             tc_fence_after();
-            mma_bf16(tmem, smem_desc(smem_u32(A), (kInPad / 8) * 128), smem_desc(smem_u32(W1s), (kInPad / 8) * 128),
-                     instr_desc(kHid), 0u);
-            mma_commit(bar_mma);
+            const uint32_t sbo = (kInPad / 8) * 128;
+            mma_bf16(tmem + kTmemAcc, smem_desc(smem_u32(Xs), sbo), smem_desc(smem_u32(W1s), sbo), idesc128, 0u);
+            mma_commit(bar_a);
+            mma_bf16(tmem + kTmemAcc + 128, smem_desc(smem_u32(Xs), sbo), smem_desc(smem_u32(W1s) + 16 * sbo, sbo),
+                     idesc128, 0u);
+            mma_commit(bar_b);
         }
-        ok = mbar_wait(bar_mma, ph_mma, wait_limit_ns);
-        ph_mma ^= 1;
+        uint32_t a_cur = kTmemA0, a_nxt = kTmemA1;
+        // epilogue of layer 1 into a_cur
+        ok = mbar_wait(bar_a, ph_a, wait_limit_ns);
+        ph_a ^= 1;
         ok = __syncthreads_and(ok);
-            if (!ok) break;
+        if (!ok) break;
         tc_fence_after();
-        epilogue_hidden(tmem, bias, A);
+        epilogue_half_ts(tmem, 0, bias, a_cur);
+        ok = mbar_wait(bar_b, ph_b, wait_limit_ns);
+        ph_b ^= 1;
+        ok = __syncthreads_and(ok);
+        if (!ok) break;
+        tc_fence_after();
+        epilogue_half_ts(tmem, 1, bias, a_cur);
+        asm volatile("tcgen05.wait::st.sync.aligned;" ::: "memory");
         tc_fence_before();
-        fence_async_smem();
         __syncthreads();
-        // layers 2..4: K = 256 (16 instructions), weights streamed into Wbuf
+        // layers 2..4 (A from tensor memory, K = 256): weights streamed into Wbuf
         for (int L = 0; L < 3 && ok; ++L) {
             ok = mbar_wait(bar_tma, ph_tma, wait_limit_ns);
             ok = __syncthreads_and(ok);
@@ -283,51 +318,66 @@ __global__ void __launch_bounds__(kThreads, 1)
             tma_pending = false;
             if (tid == 0) {
                 tc_fence_after();
+                const uint32_t sbo = (kHid / 8) * 128;
 #pragma unroll 1
-                for (int s = 0; s < kHid / 16; ++s)
-                    mma_bf16(tmem, smem_desc(smem_u32(A) + s * 256, (kHid / 8) * 128),
-                             smem_desc(smem_u32(Wbuf) + s * 256, (kHid / 8) * 128), instr_desc(kHid), s > 0);
-                mma_commit(bar_mma);
+                for (int hh = 0; hh < 2; ++hh) {
+#pragma unroll 1
+                    for (int s = 0; s < kHid / 16; ++s)
+                        mma_bf16_ts(tmem + kTmemAcc + 128 * hh, tmem + a_cur + 8 * s,
+                                    smem_desc(smem_u32(Wbuf) + hh * (kBigBytes / 2) + s * 256, sbo), idesc128,
+                                    s > 0);
+                    mma_commit(hh == 0 ? bar_a : bar_b);
+                }
             }
-            ok = mbar_wait(bar_mma, ph_mma, wait_limit_ns);
-            ph_mma ^= 1;
+            const float* b = bias + (L + 1) * kHid;
+            ok = mbar_wait(bar_a, ph_a, wait_limit_ns);
+            ph_a ^= 1;
+            ok = __syncthreads_and(ok);
+            if (!ok) break;
+            tc_fence_after();
+            epilogue_half_ts(tmem, 0, b, a_nxt);
+            ok = mbar_wait(bar_b, ph_b, wait_limit_ns);
+            ph_b ^= 1;
             ok = __syncthreads_and(ok);
             if (!ok) break;
             // Wbuf is drained: bring the next layer's weights (or layer 2's for the next tile)
-            const bool more = L < 2 || tile + gridDim.x < ntiles;
-            if (more) {
+            if (L < 2 || tile + gridDim.x < ntiles) {
                 if (tid == 0) bulk_load(smem_u32(Wbuf), wimg + size_t(L < 2 ? L + 1 : 0) * kBigBytes, kBigBytes, bar_tma);
                 tma_pending = true;
             }
             tc_fence_after();
-            epilogue_hidden(tmem, bias + (L + 1) * kHid, A);
+            epilogue_half_ts(tmem, 1, b, a_nxt);
+            asm volatile("tcgen05.wait::st.sync.aligned;" ::: "memory");
             tc_fence_before();
-            fence_async_smem();
             __syncthreads();
+            const uint32_t t = a_cur;
+            a_cur = a_nxt;
+            a_nxt = t;
         }
         if (!ok) break;
-        // layer 5: N = 16 (4 outputs used), K = 256
+        // layer 5: N = 16 (4 outputs used), A from tensor memory
         if (tid == 0) {
             tc_fence_after();
+            const uint32_t sbo = (kHid / 8) * 128;
 #pragma unroll 1
             for (int s = 0; s < kHid / 16; ++s)
-                mma_bf16(tmem, smem_desc(smem_u32(A) + s * 256, (kHid / 8) * 128),
-                         smem_desc(smem_u32(W5s) + s * 256, (kHid / 8) * 128), instr_desc(kOutPad), s > 0);
-            mma_commit(bar_mma);
+                mma_bf16_ts(tmem + kTmemAcc, tmem + a_cur + 8 * s, smem_desc(smem_u32(W5s) + s * 256, sbo), idesc16,
+                            s > 0);
+            mma_commit(bar_a);
         }
-        ok = mbar_wait(bar_mma, ph_mma, wait_limit_ns);
-        ph_mma ^= 1;
+        ok = mbar_wait(bar_a, ph_a, wait_limit_ns);
+        ph_a ^= 1;
         ok = __syncthreads_and(ok);
-            if (!ok) break;
+        if (!ok) break;
         tc_fence_after();
         if (warp < 4) {
             float v[16];
-            tmem_ld16(tmem + (uint32_t(warp * 32) << 16), v);
+            tmem_ld16(tmem + kTmemAcc + (uint32_t(warp * 32) << 16), v);
             const long long gr = row0 + warp * 32 + lane;
             if (gr < n) {
                 const float* b5 = bias + 4 * kHid;
-                float4 o = make_float4(v[0] + b5[0], v[1] + b5[1], v[2] + b5[2], v[3] + b5[3]);
-                *reinterpret_cast<float4*>(out + gr * kOut) = o;
+                *reinterpret_cast<float4*>(out + gr * kOut) =
+                    make_float4(v[0] + b5[0], v[1] + b5[1], v[2] + b5[2], v[3] + b5[3]);
             }
         }
         tc_fence_before();
@@ -335,10 +385,9 @@ __global__ void __launch_bounds__(kThreads, 1)
     }
     if (!ok) {
         if (tid == 0) atomicOr(err, 1);
-        // MMAs possibly still in flight complete before their TMEM is freed
-        mbar_wait(bar_mma, ph_mma, wait_limit_ns);
+        mbar_wait(bar_a, ph_a, wait_limit_ns);
+        mbar_wait(bar_b, ph_b, wait_limit_ns);
     }
-    // a weight copy still in flight must land before the block exits
     if (tma_pending) {
         const bool landed = mbar_wait(bar_tma, ph_tma, wait_limit_ns);
         if (!landed && tid == 0) atomicOr(err, 2);
@@ -347,7 +396,7 @@ __global__ void __launch_bounds__(kThreads, 1)
     __syncthreads();
     tc_fence_after();
     if (warp == 0)
-        asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, %1;" ::"r"(tmem), "r"(256));
+        asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, %1;" ::"r"(tmem), "r"(kTmemCols));
 }
 #endif  // __CUDACC__
 
