@@ -336,6 +336,47 @@ int sirius_cuda_render_surrogate(sirius_cuda_handle handle, const sirius_frame* 
                                  const sirius_surrogate_config* config, float* image, float* image_mlp,
                                  uint8_t* gate, sirius_surrogate_stats* stats);
 
+/* ---- surrogate training on the tensor cores (no counterpart in the reference) ----
+ * The network above, trained by the library's own tcgen05 forward and backward
+ * GEMMs and an Adam kernel; one optimiser step is captured as a CUDA graph and
+ * replayed. Training rows live on the device: d_features n x 5 floats (as
+ * sirius_cuda_surrogate_features writes them), d_targets n x 4 floats
+ * (disk hit 0/1, r_1 / 15 - 1, g_1, higher-order intensity * 1e3), d_weights n
+ * floats (the squared errors' brightness weights).
+ * Loss per batch of B rows: BCE(o_0, hit) + 100 (l_r + l_g) + 10 l_h with
+ * l_r = sum hit w (o_1 - t_1)^2 / sum hit w, l_g likewise on o_2, and
+ * l_h = sum w (o_3 - t_3)^2 / sum w. loss_parts = (BCE, l_r, l_g, l_h). */
+typedef struct {
+    int32_t batch;             /* rows per optimiser step, a multiple of 128 (16384) */
+    int32_t reserved0;
+    int64_t total_steps;       /* length of the learning-rate schedule */
+    float max_lr;              /* peak learning rate (2e-3): linear warm-up from max/25, cosine to max * 4e-6 */
+    float warmup_fraction;     /* 0.05 */
+    float beta1, beta2, eps;   /* Adam: 0.9, 0.999, 1e-8 */
+    float weight_decay;        /* decoupled (AdamW), 0 */
+    uint32_t seed;             /* key of the per-epoch row permutation */
+    int32_t reserved[5];
+} sirius_train_config;
+
+void sirius_cuda_default_train_config(sirius_train_config* config);
+/* FP32 master weights from params (host, SIRIUS_SURROGATE_PARAMS floats, nn.Linear
+ * order); Adam moments and the step counter reset to zero. */
+int sirius_cuda_train_init(sirius_cuda_handle handle, const float* params, const sirius_train_config* config);
+/* n_steps optimiser steps over rows [0, n_rows): each epoch visits the rows of
+ * n_rows / batch full batches in a fresh keyed permutation; synchronous on return. */
+int sirius_cuda_train_steps(sirius_cuda_handle handle, const float* d_features, const float* d_targets,
+                            const float* d_weights, int64_t n_rows, int64_t n_steps);
+/* loss parts of the current weights over rows [0, n_rows), in batches of the configured size
+ * (averaged, each batch weighted by its rows) */
+int sirius_cuda_train_evaluate(sirius_cuda_handle handle, const float* d_features, const float* d_targets,
+                               const float* d_weights, int64_t n_rows, float* loss_parts);
+/* loss parts and gradient (host, SIRIUS_SURROGATE_PARAMS floats, parameter order) of
+ * one batch of rows [0, n_rows), n_rows a multiple of 128 and at most the batch; no update */
+int sirius_cuda_train_gradient(sirius_cuda_handle handle, const float* d_features, const float* d_targets,
+                               const float* d_weights, int64_t n_rows, float* loss_parts, float* grad);
+/* the FP32 master weights (host) and the optimiser steps taken */
+int sirius_cuda_train_params(sirius_cuda_handle handle, float* params, int64_t* steps);
+
 /* ---- batch form of GeodesicTracer::trace(const CameraRay&) (GTRC001A.h:220) ----
  * Host-generated rays through one metric; disk_inner <= 0 selects the ISCO. */
 int sirius_cuda_trace_rays(sirius_cuda_handle handle, const sirius_metric* metric,

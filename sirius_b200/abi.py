@@ -129,6 +129,18 @@ def surrogate_config(gate_band=0.3, audit_fraction=0.01, audit_seed=0):
     return SurrogateConfig(gate_band, audit_fraction, audit_seed)
 
 
+class TrainConfig(C.Structure):
+    _fields_ = [("batch", C.c_int32), ("reserved0", C.c_int32), ("total_steps", C.c_int64), ("max_lr", C.c_float),
+                ("warmup_fraction", C.c_float), ("beta1", C.c_float), ("beta2", C.c_float), ("eps", C.c_float),
+                ("weight_decay", C.c_float), ("seed", C.c_uint32), ("reserved", C.c_int32 * 5)]
+
+
+def train_config(batch=16384, total_steps=1, max_lr=2e-3, warmup_fraction=0.05, beta1=0.9, beta2=0.999, eps=1e-8,
+                 weight_decay=0.0, seed=0):
+    """sirius_train_config (the library's defaults unless given)."""
+    return TrainConfig(batch, 0, total_steps, max_lr, warmup_fraction, beta1, beta2, eps, weight_decay, seed)
+
+
 # numpy structured dtype of RayResult (for zero-copy views of result arrays)
 def result_dtype():
     import numpy as np

@@ -26,6 +26,7 @@
 
 #include "trace.cuh"
 #include "surrogate.cuh"
+#include "train.cuh"
 
 using namespace sirius;
 
@@ -35,6 +36,7 @@ static_assert(sizeof(sirius_frame) == 168, "sirius_frame layout");
 static_assert(sizeof(sirius_camera_ray) == 64, "sirius_camera_ray layout");
 static_assert(sizeof(sirius_surrogate_config) == 40, "sirius_surrogate_config layout");
 static_assert(sizeof(sirius_surrogate_stats) == 48, "sirius_surrogate_stats layout");
+static_assert(sizeof(sirius_train_config) == 64, "sirius_train_config layout");
 
 namespace {
 
@@ -999,6 +1001,8 @@ __global__ void fma_peak_kernel(T* out, int iters, T seed) {
 // ---------------------------------------------------------------------------
 // Host side
 // ---------------------------------------------------------------------------
+struct TrainState;
+
 struct Handle {
     int device = 0;
     int num_sms = 0;
@@ -1044,6 +1048,7 @@ struct Handle {
     unsigned* d_block_counts = nullptr;  // per-block counts, then offsets; [n_blocks] = list length
     size_t block_counts_cap = 0;
     cudaEvent_t sev[5] = {};
+    TrainState* train = nullptr;  // surrogate training state (sirius_cuda_train_init)
 };
 
 int fail(Handle* h, int code, const std::string& msg) {
@@ -1373,6 +1378,214 @@ StaticScratch* static_scratch(int device) {
 }
 }  // namespace
 
+// ---------------------------------------------------------------------------
+// Surrogate training (train.cuh): device state, the launch sequence of one
+// optimiser step, and its captured graph.
+// ---------------------------------------------------------------------------
+namespace {
+struct TrainState {
+    sirius_train_config cfg{};
+    float* params = nullptr;  // FP32 master weights
+    float* grad = nullptr;
+    float* m1 = nullptr;
+    float* m2 = nullptr;
+    __nv_bfloat16* wbf = nullptr;  // BF16 copies the GEMMs read (train::kBfTotal elements)
+    train::StepState* st = nullptr;
+    int* err = nullptr;
+    long long cap = 0;  // rows the activation buffers hold
+    __nv_bfloat16* x0 = nullptr;
+    __nv_bfloat16* h[4] = {};
+    __nv_bfloat16* dy = nullptr;
+    __nv_bfloat16* dz[2] = {};
+    float* t = nullptr;
+    float* w = nullptr;
+    float* z[4] = {};
+    float* y = nullptr;
+    cudaGraphExec_t graph = nullptr;  // one optimiser step
+    const void* key[3] = {};          // the training set the graph was captured for
+    long long key_rows = 0;
+};
+
+void train_free_rows(TrainState* T) {
+    cudaFree(T->x0); cudaFree(T->dy); cudaFree(T->t); cudaFree(T->w); cudaFree(T->y);
+    for (auto* p : T->h) cudaFree(p);
+    for (auto* p : T->dz) cudaFree(p);
+    for (auto* p : T->z) cudaFree(p);
+    T->x0 = T->dy = nullptr;
+    T->t = T->w = T->y = nullptr;
+    for (auto& p : T->h) p = nullptr;
+    for (auto& p : T->dz) p = nullptr;
+    for (auto& p : T->z) p = nullptr;
+    T->cap = 0;
+}
+
+void train_drop_graph(TrainState* T) {
+    if (T->graph) cudaGraphExecDestroy(T->graph);
+    T->graph = nullptr;
+    T->key[0] = T->key[1] = T->key[2] = nullptr;
+    T->key_rows = 0;
+}
+
+void train_free(TrainState* T) {
+    if (!T) return;
+    train_drop_graph(T);
+    train_free_rows(T);
+    cudaFree(T->params); cudaFree(T->grad); cudaFree(T->m1); cudaFree(T->m2); cudaFree(T->wbf);
+    cudaFree(T->st); cudaFree(T->err);
+    delete T;
+}
+
+int train_rows(Handle* H, TrainState* T, long long rows) {
+    if (rows <= T->cap) return SIRIUS_OK;
+    train_drop_graph(T);
+    train_free_rows(T);
+    using namespace train;
+    CK(cudaMalloc((void**)&T->x0, rows * kInPad * sizeof(__nv_bfloat16)));
+    CK(cudaMalloc((void**)&T->dy, rows * kOutPad * sizeof(__nv_bfloat16)));
+    for (auto& p : T->h) CK(cudaMalloc((void**)&p, rows * kHid * sizeof(__nv_bfloat16)));
+    for (auto& p : T->dz) CK(cudaMalloc((void**)&p, rows * kHid * sizeof(__nv_bfloat16)));
+    for (auto& p : T->z) CK(cudaMalloc((void**)&p, rows * kHid * sizeof(float)));
+    CK(cudaMalloc((void**)&T->t, rows * 4 * sizeof(float)));
+    CK(cudaMalloc((void**)&T->w, rows * sizeof(float)));
+    CK(cudaMalloc((void**)&T->y, rows * kOut * sizeof(float)));
+    T->cap = rows;
+    return SIRIUS_OK;
+}
+
+unsigned long long train_wait_limit(const Handle* H) {
+    return (unsigned long long)(H->configured && H->cfg.watchdog_ms > 0 ? H->cfg.watchdog_ms : 30000) * 1000000ull;
+}
+
+template <int BN, int E>
+void gemm_launch(const train::GemmArgs& g, cudaStream_t s) {
+    const dim3 grid((g.M + train::kBM - 1) / train::kBM, (g.N + BN - 1) / BN, (g.K + g.k_per_cta - 1) / g.k_per_cta);
+    train::gemm_kernel<BN, E><<<grid, train::kGemmThreads, train::GemmSmem<BN>::Bytes, s>>>(g);
+}
+
+int train_set_attributes(Handle* H) {
+    using namespace train;
+    CK(cudaFuncSetAttribute(gemm_kernel<256, kEpiHidden>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                            GemmSmem<256>::Bytes));
+    CK(cudaFuncSetAttribute(gemm_kernel<256, kEpiDHidden>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                            GemmSmem<256>::Bytes));
+    CK(cudaFuncSetAttribute(gemm_kernel<256, kEpiDWeight>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                            GemmSmem<256>::Bytes));
+    return SIRIUS_OK;
+}
+
+constexpr long long kTrainBf[4] = {train::kBfW1, train::kBfW2, train::kBfW3, train::kBfW4};
+
+// forward over the first `rows` gathered rows: Z_l, H_l (l = 1..4) and Y
+void train_forward(const Handle* H, TrainState* T, int rows, cudaStream_t s) {
+    using namespace train;
+    GemmArgs g{};
+    g.err = T->err;
+    g.wait_limit_ns = train_wait_limit(H);
+    g.M = rows;
+    g.N = kHid;
+    for (int l = 0; l < 4; ++l) {
+        const int K = l == 0 ? kInPad : kHid;
+        g.a = Operand{l == 0 ? T->x0 : T->h[l - 1], K, 1, rows};
+        g.b = Operand{T->wbf + kTrainBf[l], K, 1, kHid};
+        g.K = g.k_per_cta = K;
+        g.e = EpiArgs{};
+        g.e.bias = T->params + kOffB[l];
+        g.e.z = T->z[l];
+        g.e.ldz = kHid;
+        g.e.h = T->h[l];
+        g.e.ldh = kHid;
+        gemm_launch<256, kEpiHidden>(g, s);
+    }
+    g.a = Operand{T->h[3], kHid, 1, rows};
+    g.b = Operand{T->wbf + kBfW5, kHid, 1, kOutPad};
+    g.N = kOutPad;
+    g.K = g.k_per_cta = kHid;
+    g.e = EpiArgs{};
+    g.e.bias = T->params + kOffB[4];
+    g.e.y = T->y;
+    g.e.ldy = kOut;
+    g.e.ny = kOut;
+    gemm_launch<16, kEpiOutput>(g, s);
+}
+
+void train_loss(TrainState* T, int rows, bool with_grad, cudaStream_t s) {
+    const int blocks = (rows + 255) / 256;
+    train::loss_sums_kernel<<<blocks, 256, 0, s>>>(T->t, T->w, rows, T->st);
+    train::loss_grad_kernel<<<blocks, 256, 0, s>>>(T->y, T->t, T->w, rows, T->st, T->dy,
+                                                   with_grad ? T->grad + train::kOffB[4] : nullptr);
+}
+
+// gradient of the batch loss into T->grad (which must hold zeros); rows a multiple of 128
+void train_backward(const Handle* H, TrainState* T, int rows, cudaStream_t s) {
+    using namespace train;
+    GemmArgs g{};
+    g.err = T->err;
+    g.wait_limit_ns = train_wait_limit(H);
+    const int kpc = std::max(64, ((rows / 64 + 63) / 64) * 64);  // batch rows per CTA in the weight gradients
+    // dW5^T = H4^T dY
+    g.a = Operand{T->h[3], kHid, 0, kHid};
+    g.b = Operand{T->dy, kOutPad, 0, kOutPad};
+    g.M = kHid; g.N = kOutPad; g.K = rows; g.k_per_cta = kpc;
+    g.e = EpiArgs{};
+    g.e.grad = T->grad + kOffW[4]; g.e.ldg = kHid; g.e.ng = kOut;
+    gemm_launch<16, kEpiDWeightT>(g, s);
+    // dH4 = dY W5 -> dZ4 (and the b4 gradient)
+    g.a = Operand{T->dy, kOutPad, 1, rows};
+    g.b = Operand{T->wbf + kBfW5, kHid, 0, kHid};
+    g.M = rows; g.N = kHid; g.K = g.k_per_cta = kOutPad;
+    g.e = EpiArgs{};
+    g.e.z = T->z[3]; g.e.ldz = kHid; g.e.h = T->dz[0]; g.e.ldh = kHid; g.e.grad = T->grad + kOffB[3];
+    gemm_launch<256, kEpiDHidden>(g, s);
+    for (int l = 3; l >= 1; --l) {  // layers 4, 3, 2
+        __nv_bfloat16* cur = T->dz[(3 - l) % 2];
+        __nv_bfloat16* nxt = T->dz[(4 - l) % 2];
+        // dW_l = dZ_l^T H_{l-1}
+        g.a = Operand{cur, kHid, 0, kHid};
+        g.b = Operand{T->h[l - 1], kHid, 0, kHid};
+        g.M = kHid; g.N = kHid; g.K = rows; g.k_per_cta = kpc;
+        g.e = EpiArgs{};
+        g.e.grad = T->grad + kOffW[l]; g.e.ldg = kHid; g.e.ng = kHid;
+        gemm_launch<256, kEpiDWeight>(g, s);
+        // dH_{l-1} = dZ_l W_l -> dZ_{l-1} (and the b_{l-1} gradient)
+        g.a = Operand{cur, kHid, 1, rows};
+        g.b = Operand{T->wbf + kTrainBf[l], kHid, 0, kHid};
+        g.M = rows; g.N = kHid; g.K = g.k_per_cta = kHid;
+        g.e = EpiArgs{};
+        g.e.z = T->z[l - 1]; g.e.ldz = kHid; g.e.h = nxt; g.e.ldh = kHid; g.e.grad = T->grad + kOffB[l - 1];
+        gemm_launch<256, kEpiDHidden>(g, s);
+    }
+    // dW1 = dZ1^T X0 (the 5 real input columns)
+    g.a = Operand{T->dz[1], kHid, 0, kHid};
+    g.b = Operand{T->x0, kInPad, 0, kInPad};
+    g.M = kHid; g.N = kInPad; g.K = rows; g.k_per_cta = kpc;
+    g.e = EpiArgs{};
+    g.e.grad = T->grad + kOffW[0]; g.e.ldg = kIn; g.e.ng = kIn;
+    gemm_launch<16, kEpiDWeight>(g, s);
+}
+
+void train_step(const Handle* H, TrainState* T, const float* feat, const float* targets, const float* weights,
+                long long n_rows, cudaStream_t s) {
+    const int B = T->cfg.batch;
+    const int spe = int(n_rows / B);
+    train::gather_kernel<<<(B + 255) / 256, 256, 0, s>>>(feat, targets, weights, n_rows, B, spe, T->cfg.seed, 0, 0,
+                                                         T->st, T->x0, T->t, T->w);
+    train_forward(H, T, B, s);
+    train_loss(T, B, true, s);
+    train_backward(H, T, B, s);
+    const train::AdamConfig c{T->cfg.max_lr, T->cfg.warmup_fraction, T->cfg.beta1, T->cfg.beta2,
+                              T->cfg.eps,    T->cfg.weight_decay,    T->cfg.total_steps};
+    train::adam_kernel<<<H->num_sms * 2, 256, 0, s>>>(T->params, T->grad, T->m1, T->m2, T->wbf, T->st, c);
+}
+
+int train_check_err(Handle* H, TrainState* T) {
+    int err = 0;
+    CK(cudaMemcpyAsync(&err, T->err, sizeof(int), cudaMemcpyDeviceToHost, H->stream));
+    CK(cudaStreamSynchronize(H->stream));
+    if (err) return fail(H, SIRIUS_ERR_TIMEOUT, "training GEMM stopped by its wait bound");
+    return SIRIUS_OK;
+}
+}  // namespace
+
 extern "C" {
 
 int sirius_cuda_abi_version(void) { return SIRIUS_CUDA_ABI_VERSION; }
@@ -1430,6 +1643,7 @@ int sirius_cuda_destroy(sirius_cuda_handle h) {
     cudaFree(H->d_surrogate); cudaFree(H->d_sur_err);
     cudaFree(H->d_sur_frames); cudaFree(H->d_feat); cudaFree(H->d_mlp_out); cudaFree(H->d_list); cudaFree(H->d_gate);
     cudaFree(H->d_block_counts);
+    train_free(H->train);
     for (auto& e : H->sev) if (e) cudaEventDestroy(e);
     for (auto& e : H->ev) if (e) cudaEventDestroy(e);
     if (H->stream) cudaStreamDestroy(H->stream);
@@ -1781,6 +1995,173 @@ int sirius_cuda_surrogate_infer(sirius_cuda_handle h, const float* d_features, i
     CK(cudaMemcpyAsync(&err, H->d_sur_err, sizeof(int), cudaMemcpyDeviceToHost, st));
     CK(cudaStreamSynchronize(st));
     if (err) return fail(H, SIRIUS_ERR_TIMEOUT, "surrogate MLP kernel stopped by its wait bound");
+    return SIRIUS_OK;
+}
+
+// ---- surrogate training ----
+void sirius_cuda_default_train_config(sirius_train_config* c) {
+    if (!c) return;
+    std::memset(c, 0, sizeof(*c));
+    c->batch = 16384;
+    c->total_steps = 1;
+    c->max_lr = 2e-3f;
+    c->warmup_fraction = 0.05f;
+    c->beta1 = 0.9f;
+    c->beta2 = 0.999f;
+    c->eps = 1e-8f;
+    c->weight_decay = 0.f;
+    c->seed = 0;
+}
+
+int sirius_cuda_train_init(sirius_cuda_handle h, const float* params, const sirius_train_config* cfg) {
+    Handle* H = static_cast<Handle*>(h);
+    if (!H || !params || !cfg) return SIRIUS_ERR_INVALID_ARGUMENT;
+    const sirius_train_config& c = *cfg;
+    if (c.batch <= 0 || c.batch % 128 != 0 || c.batch > (1 << 20))
+        return fail(H, SIRIUS_ERR_INVALID_ARGUMENT, "batch must be a positive multiple of 128, at most 2^20");
+    if (c.total_steps < 1) return fail(H, SIRIUS_ERR_INVALID_ARGUMENT, "total_steps must be >= 1");
+    if (!(c.max_lr > 0.f) || !std::isfinite(c.max_lr) || !(c.warmup_fraction >= 0.f && c.warmup_fraction <= 1.f) ||
+        !(c.beta1 >= 0.f && c.beta1 < 1.f) || !(c.beta2 >= 0.f && c.beta2 < 1.f) || !(c.eps > 0.f) ||
+        !(c.weight_decay >= 0.f))
+        return fail(H, SIRIUS_ERR_INVALID_ARGUMENT, "invalid optimiser settings");
+    for (long long i = 0; i < surrogate::kParams; ++i)
+        if (!std::isfinite(params[i])) return fail(H, SIRIUS_ERR_INVALID_ARGUMENT, "non-finite initial parameter");
+    CK(cudaSetDevice(H->device));
+    if (!H->train) {
+        TrainState* T = new (std::nothrow) TrainState;
+        if (!T) return fail(H, SIRIUS_ERR_OUT_OF_MEMORY, "training state");
+        H->train = T;
+        const size_t pb = surrogate::kParams * sizeof(float);
+        CK(cudaMalloc((void**)&T->params, pb));
+        CK(cudaMalloc((void**)&T->grad, pb));
+        CK(cudaMalloc((void**)&T->m1, pb));
+        CK(cudaMalloc((void**)&T->m2, pb));
+        CK(cudaMalloc((void**)&T->wbf, train::kBfTotal * sizeof(__nv_bfloat16)));
+        CK(cudaMalloc((void**)&T->st, sizeof(train::StepState)));
+        CK(cudaMalloc((void**)&T->err, sizeof(int)));
+        const int rc = train_set_attributes(H);
+        if (rc != SIRIUS_OK) return rc;
+    }
+    TrainState* T = H->train;
+    train_drop_graph(T);  // the captured step embeds the configuration
+    T->cfg = c;
+    const int rc = train_rows(H, T, c.batch);
+    if (rc != SIRIUS_OK) return rc;
+    const size_t pb = surrogate::kParams * sizeof(float);
+    CK(cudaMemcpyAsync(T->params, params, pb, cudaMemcpyHostToDevice, H->stream));
+    CK(cudaMemsetAsync(T->grad, 0, pb, H->stream));
+    CK(cudaMemsetAsync(T->m1, 0, pb, H->stream));
+    CK(cudaMemsetAsync(T->m2, 0, pb, H->stream));
+    CK(cudaMemsetAsync(T->wbf, 0, train::kBfTotal * sizeof(__nv_bfloat16), H->stream));
+    CK(cudaMemsetAsync(T->st, 0, sizeof(train::StepState), H->stream));
+    CK(cudaMemsetAsync(T->err, 0, sizeof(int), H->stream));
+    train::weights_to_bf16_kernel<<<H->num_sms, 256, 0, H->stream>>>(T->params, T->wbf);
+    CK(cudaGetLastError());
+    CK(cudaStreamSynchronize(H->stream));
+    return SIRIUS_OK;
+}
+
+int sirius_cuda_train_steps(sirius_cuda_handle h, const float* d_features, const float* d_targets,
+                            const float* d_weights, int64_t n_rows, int64_t n_steps) {
+    Handle* H = static_cast<Handle*>(h);
+    if (!H || !d_features || !d_targets || !d_weights || n_steps < 0) return SIRIUS_ERR_INVALID_ARGUMENT;
+    TrainState* T = H->train;
+    if (!T) return fail(H, SIRIUS_ERR_NOT_CONFIGURED, "sirius_cuda_train_init has not been called");
+    if (n_rows < T->cfg.batch || n_rows > (1LL << 40))
+        return fail(H, SIRIUS_ERR_INVALID_ARGUMENT, "n_rows must hold at least one batch");
+    CK(cudaSetDevice(H->device));
+    if (T->graph && (T->key[0] != d_features || T->key[1] != d_targets || T->key[2] != d_weights ||
+                     T->key_rows != n_rows))
+        train_drop_graph(T);
+    if (!T->graph) {
+        cudaGraph_t g = nullptr;
+        CK(cudaStreamBeginCapture(H->stream, cudaStreamCaptureModeThreadLocal));
+        train_step(H, T, d_features, d_targets, d_weights, n_rows, H->stream);
+        const cudaError_t e1 = cudaStreamEndCapture(H->stream, &g);
+        const cudaError_t e0 = cudaGetLastError();
+        if (e1 != cudaSuccess || e0 != cudaSuccess) {
+            if (g) cudaGraphDestroy(g);
+            return fail(H, SIRIUS_ERR_CUDA, std::string("capturing the training step: ") +
+                                                cudaGetErrorString(e1 != cudaSuccess ? e1 : e0));
+        }
+        const cudaError_t e2 = cudaGraphInstantiate(&T->graph, g, 0);
+        cudaGraphDestroy(g);
+        if (e2 != cudaSuccess) {
+            T->graph = nullptr;
+            return fail(H, SIRIUS_ERR_CUDA, std::string("instantiating the training step: ") + cudaGetErrorString(e2));
+        }
+        T->key[0] = d_features;
+        T->key[1] = d_targets;
+        T->key[2] = d_weights;
+        T->key_rows = n_rows;
+    }
+    for (int64_t i = 0; i < n_steps; ++i) CK(cudaGraphLaunch(T->graph, H->stream));
+    return train_check_err(H, T);
+}
+
+int sirius_cuda_train_evaluate(sirius_cuda_handle h, const float* d_features, const float* d_targets,
+                               const float* d_weights, int64_t n_rows, float* loss_parts) {
+    Handle* H = static_cast<Handle*>(h);
+    if (!H || !d_features || !d_targets || !d_weights || !loss_parts || n_rows <= 0)
+        return SIRIUS_ERR_INVALID_ARGUMENT;
+    TrainState* T = H->train;
+    if (!T) return fail(H, SIRIUS_ERR_NOT_CONFIGURED, "sirius_cuda_train_init has not been called");
+    CK(cudaSetDevice(H->device));
+    double acc[4] = {0, 0, 0, 0};
+    for (long long r0 = 0; r0 < n_rows; r0 += T->cfg.batch) {
+        const int rows = int(std::min<long long>(T->cfg.batch, n_rows - r0));
+        train::gather_kernel<<<(rows + 255) / 256, 256, 0, H->stream>>>(d_features, d_targets, d_weights, n_rows,
+                                                                        rows, 1, 0, 1, r0, T->st, T->x0, T->t, T->w);
+        train_forward(H, T, rows, H->stream);
+        train_loss(T, rows, false, H->stream);
+        CK(cudaGetLastError());
+        float sums[8];
+        CK(cudaMemcpyAsync(sums, T->st->sums, sizeof(sums), cudaMemcpyDeviceToHost, H->stream));
+        CK(cudaStreamSynchronize(H->stream));
+        for (int j = 0; j < 4; ++j) acc[j] += double(sums[2 + j]) * rows;
+    }
+    for (int j = 0; j < 4; ++j) loss_parts[j] = float(acc[j] / double(n_rows));
+    return train_check_err(H, T);
+}
+
+int sirius_cuda_train_gradient(sirius_cuda_handle h, const float* d_features, const float* d_targets,
+                               const float* d_weights, int64_t n_rows, float* loss_parts, float* grad) {
+    Handle* H = static_cast<Handle*>(h);
+    if (!H || !d_features || !d_targets || !d_weights || !grad) return SIRIUS_ERR_INVALID_ARGUMENT;
+    TrainState* T = H->train;
+    if (!T) return fail(H, SIRIUS_ERR_NOT_CONFIGURED, "sirius_cuda_train_init has not been called");
+    if (n_rows <= 0 || n_rows % 128 != 0 || n_rows > T->cfg.batch)
+        return fail(H, SIRIUS_ERR_INVALID_ARGUMENT, "n_rows must be a positive multiple of 128, at most the batch");
+    CK(cudaSetDevice(H->device));
+    const int rows = int(n_rows);
+    train::gather_kernel<<<(rows + 255) / 256, 256, 0, H->stream>>>(d_features, d_targets, d_weights, n_rows, rows,
+                                                                    1, 0, 1, 0, T->st, T->x0, T->t, T->w);
+    train_forward(H, T, rows, H->stream);
+    train_loss(T, rows, true, H->stream);
+    train_backward(H, T, rows, H->stream);
+    CK(cudaGetLastError());
+    float sums[8];
+    CK(cudaMemcpyAsync(sums, T->st->sums, sizeof(sums), cudaMemcpyDeviceToHost, H->stream));
+    CK(cudaMemcpyAsync(grad, T->grad, surrogate::kParams * sizeof(float), cudaMemcpyDeviceToHost, H->stream));
+    CK(cudaMemsetAsync(T->grad, 0, surrogate::kParams * sizeof(float), H->stream));
+    const int rc = train_check_err(H, T);
+    if (rc != SIRIUS_OK) return rc;
+    if (loss_parts)
+        for (int j = 0; j < 4; ++j) loss_parts[j] = sums[2 + j];
+    return SIRIUS_OK;
+}
+
+int sirius_cuda_train_params(sirius_cuda_handle h, float* params, int64_t* steps) {
+    Handle* H = static_cast<Handle*>(h);
+    if (!H || !params) return SIRIUS_ERR_INVALID_ARGUMENT;
+    TrainState* T = H->train;
+    if (!T) return fail(H, SIRIUS_ERR_NOT_CONFIGURED, "sirius_cuda_train_init has not been called");
+    CK(cudaSetDevice(H->device));
+    long long st = 0;
+    CK(cudaMemcpyAsync(params, T->params, surrogate::kParams * sizeof(float), cudaMemcpyDeviceToHost, H->stream));
+    CK(cudaMemcpyAsync(&st, &T->st->step, sizeof(st), cudaMemcpyDeviceToHost, H->stream));
+    CK(cudaStreamSynchronize(H->stream));
+    if (steps) *steps = st;
     return SIRIUS_OK;
 }
 

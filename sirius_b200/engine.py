@@ -24,7 +24,8 @@ EXPORTS = [
     "sirius_cuda_dp45_step", "sirius_cuda_last_stats", "sirius_cuda_autotune", "sirius_cuda_measure_fma_peak",
     "sirius_cuda_flop_count", "sirius_cuda_trace_frames_static", "sirius_cuda_surrogate_load",
     "sirius_cuda_surrogate_infer", "sirius_cuda_surrogate_features", "sirius_cuda_render_surrogate",
-    "sirius_cuda_render_surrogate_device",
+    "sirius_cuda_render_surrogate_device", "sirius_cuda_default_train_config", "sirius_cuda_train_init",
+    "sirius_cuda_train_steps", "sirius_cuda_train_evaluate", "sirius_cuda_train_gradient", "sirius_cuda_train_params",
 ]
 
 
@@ -69,6 +70,14 @@ def load_library(path=LIB_PATH):
     L.sirius_cuda_autotune.argtypes = [C.c_void_p, C.c_void_p, C.c_int32, _P(abi.TraceConfig)]
     L.sirius_cuda_measure_fma_peak.argtypes = [C.c_void_p, C.c_int32, _P(C.c_double)]
     L.sirius_cuda_flop_count.argtypes = [_P(abi.Metric), _P(C.c_double), _P(C.c_double), _P(C.c_double)]
+    L.sirius_cuda_default_train_config.argtypes = [_P(abi.TrainConfig)]
+    L.sirius_cuda_default_train_config.restype = None
+    L.sirius_cuda_train_init.argtypes = [C.c_void_p, C.c_void_p, _P(abi.TrainConfig)]
+    L.sirius_cuda_train_steps.argtypes = [C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p, C.c_int64, C.c_int64]
+    L.sirius_cuda_train_evaluate.argtypes = [C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p, C.c_int64, C.c_void_p]
+    L.sirius_cuda_train_gradient.argtypes = [C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p, C.c_int64, C.c_void_p,
+                                             C.c_void_p]
+    L.sirius_cuda_train_params.argtypes = [C.c_void_p, C.c_void_p, _P(C.c_int64)]
     return L
 
 
@@ -159,6 +168,39 @@ class Engine:
     def surrogate_infer(self, d_features, n, d_out, stream=None):
         """MLP on n x 5 device features into n x 4 device outputs."""
         self._check(self.lib.sirius_cuda_surrogate_infer(self.h, d_features, n, d_out, stream))
+
+    def train_init(self, params, config):
+        """Start training from params (SURROGATE_PARAMS floats): FP32 master weights, zero Adam moments."""
+        p = np.ascontiguousarray(params, dtype=np.float32).ravel()
+        if p.size != abi.SURROGATE_PARAMS:
+            raise ValueError(f"expected {abi.SURROGATE_PARAMS} parameters, got {p.size}")
+        self._check(self.lib.sirius_cuda_train_init(self.h, p.ctypes.data, C.byref(config)))
+
+    def train_steps(self, d_features, d_targets, d_weights, n_rows, n_steps):
+        """n_steps optimiser steps over the device-resident rows [0, n_rows)."""
+        self._check(self.lib.sirius_cuda_train_steps(self.h, d_features, d_targets, d_weights, n_rows, n_steps))
+
+    def train_evaluate(self, d_features, d_targets, d_weights, n_rows):
+        """Loss parts (BCE, l_r, l_g, l_h) of the current weights over rows [0, n_rows)."""
+        out = np.zeros(4, dtype=np.float32)
+        self._check(self.lib.sirius_cuda_train_evaluate(self.h, d_features, d_targets, d_weights, n_rows,
+                                                        out.ctypes.data))
+        return out
+
+    def train_gradient(self, d_features, d_targets, d_weights, n_rows):
+        """(loss parts, gradient) of one batch of rows [0, n_rows); no update."""
+        parts = np.zeros(4, dtype=np.float32)
+        grad = np.zeros(abi.SURROGATE_PARAMS, dtype=np.float32)
+        self._check(self.lib.sirius_cuda_train_gradient(self.h, d_features, d_targets, d_weights, n_rows,
+                                                        parts.ctypes.data, grad.ctypes.data))
+        return parts, grad
+
+    def train_params(self):
+        """(FP32 master weights, optimiser steps taken)."""
+        p = np.zeros(abi.SURROGATE_PARAMS, dtype=np.float32)
+        steps = C.c_int64()
+        self._check(self.lib.sirius_cuda_train_params(self.h, p.ctypes.data, C.byref(steps)))
+        return p, steps.value
 
     def surrogate_features(self, frames, d_features, d_gate=None, config=None, stream=None):
         """Features (n x 5) and gate (n bytes) of every pixel of the frames, into device buffers."""

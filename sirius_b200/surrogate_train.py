@@ -1,12 +1,13 @@
 """Fit the surrogate MLP (5 -> 256 -> 256 -> 256 -> 256 -> 4, SiLU) to rays
-traced by the engine, and write its parameters (nn.Linear order, float32) for
-sirius_cuda_surrogate_load.
+traced by the engine, with the library's own training kernels, and write its
+parameters (nn.Linear order, float32) for sirius_cuda_surrogate_load.
 
 Training set: 2^24 rays of 4096 Kerr frames with a* ~ U[0, 0.99], inclination
 ~ U[5, 89] deg, r_obs ~ U[20, 200] M, each a 64^2 30 deg pinhole camera (pixel
 centres with a random sub-pixel offset per frame, so alpha and beta cover the
 field of view), thin Novikov-Thorne disk r_ISCO..30 M, traced by the
-mixed-precision integrator at tol 1e-8.
+mixed-precision integrator at tol 1e-8. The last 2 % of the frames are held
+out for validation.
 
 Features are those of sirius_cuda_surrogate_features (computed by the library,
 so training and inference see the same inputs). Targets per ray:
@@ -17,11 +18,11 @@ The squared errors are weighted by the ray's brightness relative to its
 frame's brightest primary, as the image error is measured against the image
 scale.
 
-The fitting itself runs in PyTorch (an offline step, not the rendering path);
-inference runs on the library's tensor-core kernel, which rounds the inputs,
-weights and hidden activations to BF16: the last 40 % of the epochs train
-through the same roundings (straight-through gradients), so the fitted network
-is the one the kernel evaluates.
+The fit runs on the tensor cores (sirius_cuda_train_*): BF16 tcgen05 forward
+and backward GEMMs with the inference kernel's roundings, Adam on FP32 master
+weights, one optimiser step per replay of a captured CUDA graph, the rows of
+each epoch in a fresh keyed permutation. PyTorch only holds the device
+buffers of the training set.
 
 Usage: python -m sirius_b200.surrogate_train [--rays N] [--epochs E] [--out PATH]
 """
@@ -87,102 +88,58 @@ def make_dataset(eng, abi, torch, n_rays, seed, chunk_frames=256):
     return torch.cat(X), torch.cat(Y), torch.cat(W)
 
 
-def build_mlp(torch):
-    nn = torch.nn
-    layers = []
-    dims = [5, 256, 256, 256, 256]
-    for i in range(4):
-        layers += [nn.Linear(dims[i], dims[i + 1]), nn.SiLU()]
-    layers.append(nn.Linear(256, 4))
-    return nn.Sequential(*layers)
-
-
-def forward_bf16(torch, model, x):
-    """The kernel's arithmetic: BF16 inputs, weights and hidden activations, FP32
-    sums and biases; rounding with straight-through gradients."""
-    def rnd(t):
-        return t + (t.to(torch.bfloat16).to(torch.float32) - t).detach()
-    h = rnd(x)
-    lin = [m for m in model if hasattr(m, "weight")]
-    for i, m in enumerate(lin):
-        h = h @ rnd(m.weight).T + m.bias
-        if i < len(lin) - 1:
-            h = rnd(torch.nn.functional.silu(h))
-    return h
-
-
-def loss_fn(torch, out, y, w):
-    F = torch.nn.functional
-    hit = y[:, 0]
-    l_hit = F.binary_cross_entropy_with_logits(out[:, 0], hit)
-    wh = hit * w
-    wh = wh / wh.mean().clamp_min(1e-12)
-    l_r = (wh * (out[:, 1] - y[:, 1]) ** 2).mean()
-    l_g = (wh * (out[:, 2] - y[:, 2]) ** 2).mean()
-    l_h = (w * (out[:, 3] - y[:, 3]) ** 2).mean() / w.mean()
-    return l_hit + 100.0 * (l_r + l_g) + 10.0 * l_h, (l_hit, l_r, l_g, l_h)
-
-
-def flatten_params(model):
+def init_params(rng):
+    """nn.Linear's default initialisation: U(-1/sqrt(in), 1/sqrt(in)) for weights and biases."""
     parts = []
-    for m in model:
-        if hasattr(m, "weight"):
-            parts.append(m.weight.detach().float().cpu().numpy().ravel())
-            parts.append(m.bias.detach().float().cpu().numpy().ravel())
+    for o, i in [(256, 5), (256, 256), (256, 256), (256, 256), (4, 256)]:
+        bound = 1.0 / np.sqrt(i)
+        parts.append(rng.uniform(-bound, bound, size=o * i))
+        parts.append(rng.uniform(-bound, bound, size=o))
     return np.concatenate(parts).astype(np.float32)
 
 
-def train(n_rays=1 << 24, epochs=8, batch=16384, lr=2e-3, seed=0, out=DEFAULT_OUT, log=print):
-    import torch
+def total_loss(parts):
+    return parts[0] + 100.0 * (parts[1] + parts[2]) + 10.0 * parts[3]
 
+
+def train(n_rays=1 << 24, epochs=120, batch=16384, lr=2e-3, seed=0, out=DEFAULT_OUT, log=print):
     from sirius_b200 import abi
     from sirius_b200.engine import Engine
 
-    torch.manual_seed(seed)
+    import torch
+
     eng = Engine(0)
     t0 = time.time()
     X, Y, Wt = make_dataset(eng, abi, torch, n_rays, seed)
     log(f"dataset: {X.shape[0]} rays in {time.time() - t0:.1f} s, disk-hit fraction {Y[:, 0].mean().item():.3f}")
     n = X.shape[0]
-    perm = torch.randperm(n, device=X.device)
-    n_val = max(n // 50, 1)
-    val, tr = perm[:n_val], perm[n_val:]
-    model = build_mlp(torch).to(X.device)
-    opt = torch.optim.AdamW(model.parameters(), lr=lr, weight_decay=0.0)
-    steps = epochs * (tr.numel() // batch)
-    sched = torch.optim.lr_scheduler.OneCycleLR(opt, max_lr=lr, total_steps=steps, pct_start=0.05)
-    step = 0
+    n_val = max((n // 50) // (SIDE * SIDE), 1) * SIDE * SIDE  # whole frames
+    n_train = n - n_val
+    if n_train < batch:
+        raise ValueError(f"{n_train} training rows hold no batch of {batch}")
+    steps_per_epoch = n_train // batch
+    cfg = abi.train_config(batch=batch, total_steps=epochs * steps_per_epoch, max_lr=lr, seed=seed)
+    eng.train_init(init_params(np.random.default_rng(seed)), cfg)
+    xv, yv, wv = X[n_train:], Y[n_train:], Wt[n_train:]
     t0 = time.time()
-    q_from = int(0.6 * epochs)
     for ep in range(epochs):
-        fwd = (lambda x: forward_bf16(torch, model, x)) if ep >= q_from else model
-        order = tr[torch.randperm(tr.numel(), device=X.device)]
-        for i in range(0, order.numel() - batch + 1, batch):
-            idx = order[i:i + batch]
-            loss, _ = loss_fn(torch, fwd(X[idx]), Y[idx], Wt[idx])
-            opt.zero_grad(set_to_none=True)
-            loss.backward()
-            opt.step()
-            sched.step()
-            step += 1
-        with torch.no_grad():
-            outv = torch.cat([fwd(X[val[j:j + 65536]]) for j in range(0, val.numel(), 65536)])
-            _, parts = loss_fn(torch, outv, Y[val], Wt[val])
-        log(f"epoch {ep}: loss parts (hit bce, r, g, higher) = {[round(p.item(), 8) for p in parts]}, "
-            f"{time.time() - t0:.1f} s")
-    train.model = model  # the fitted torch module, for inspection
-    params = flatten_params(model)
-    assert params.size == abi.SURROGATE_PARAMS
-    os.makedirs(os.path.dirname(out), exist_ok=True)
+        eng.train_steps(X.data_ptr(), Y.data_ptr(), Wt.data_ptr(), n_train, steps_per_epoch)
+        parts = eng.train_evaluate(xv.data_ptr(), yv.data_ptr(), wv.data_ptr(), n_val)
+        log(f"epoch {ep}: validation loss parts (hit bce, r, g, higher) = {[round(float(p), 8) for p in parts]}, "
+            f"total {total_loss(parts):.6f}, {time.time() - t0:.1f} s")
+    params, steps = eng.train_params()
+    assert params.size == abi.SURROGATE_PARAMS and steps == epochs * steps_per_epoch
+    os.makedirs(os.path.dirname(os.path.abspath(out)), exist_ok=True)
     np.save(out, params)
-    log(f"wrote {out} ({params.size} parameters)")
+    log(f"wrote {out} ({params.size} parameters, {steps} optimiser steps)")
+    eng.close()
     return params
 
 
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--rays", type=int, default=1 << 24)
-    ap.add_argument("--epochs", type=int, default=8)
+    ap.add_argument("--epochs", type=int, default=120)
     ap.add_argument("--batch", type=int, default=16384)
     ap.add_argument("--lr", type=float, default=2e-3)
     ap.add_argument("--seed", type=int, default=0)

@@ -47,6 +47,7 @@ def test_struct_layouts_match_c(oracle):
     assert C.sizeof(abi.CameraRay) == 64
     assert C.sizeof(abi.SurrogateConfig) == 40
     assert C.sizeof(abi.SurrogateStats) == 48
+    assert C.sizeof(abi.TrainConfig) == 64
     dt = abi.result_dtype()
     for name, _ in abi.RayResult._fields_:
         assert dt.fields[name][1] == getattr(abi.RayResult, name).offset, name
@@ -68,6 +69,16 @@ def test_default_config_matches_render_session():
     assert (c.initial_step, c.max_step, c.min_step, c.abs_tolerance) == (0.1, 2.0, 1e-5, 5e-6)
 
 
+def test_default_train_config_matches_python_mirror():
+    lib = load_library()
+    c = abi.TrainConfig()
+    lib.sirius_cuda_default_train_config(C.byref(c))
+    py = abi.train_config()
+    for name, _ in abi.TrainConfig._fields_:
+        a, b = getattr(c, name), getattr(py, name)
+        assert (list(a) == list(b)) if name == "reserved" else (a == b), name
+
+
 def test_null_handle_and_bad_arguments_are_errors_not_crashes():
     lib = load_library()
     assert lib.sirius_cuda_get_last_error(None) == b"invalid handle"
@@ -75,6 +86,9 @@ def test_null_handle_and_bad_arguments_are_errors_not_crashes():
     assert lib.sirius_cuda_configure(None, None) == abi.ERR_INVALID_ARGUMENT
     assert lib.sirius_cuda_trace_frames(None, None, 0, None, None, None) == abi.ERR_INVALID_ARGUMENT
     assert lib.sirius_cuda_default_config(None) == abi.ERR_INVALID_ARGUMENT
+    assert lib.sirius_cuda_train_init(None, None, None) == abi.ERR_INVALID_ARGUMENT
+    assert lib.sirius_cuda_train_steps(None, None, None, None, 0, 0) == abi.ERR_INVALID_ARGUMENT
+    assert lib.sirius_cuda_train_gradient(None, None, None, None, 128, None, None) == abi.ERR_INVALID_ARGUMENT
     h = C.c_void_p()
     rc = lib.sirius_cuda_create(999, C.byref(h))
     assert rc in (abi.ERR_NO_DEVICE, abi.ERR_INVALID_ARGUMENT)
