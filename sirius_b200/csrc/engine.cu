@@ -825,6 +825,7 @@ __global__ void sur_features_kernel(const FrameDev* frames, const SurFrameDev* s
                                     unsigned char* gate, unsigned* block_counts) {
     const long long idx = (long long)blockIdx.x * blockDim.x + threadIdx.x;
     bool take = false;
+    unsigned char gate_of_thread = 0;
     if (idx < total) {
         const int f = n_frames > 1 ? find_frame(frames, n_frames, idx) : 0;
         const FrameDev& F = frames[f];
@@ -864,18 +865,24 @@ __global__ void sur_features_kernel(const FrameDev* frames, const SurFrameDev* s
         // audit rays come in runs of 32 consecutive pixels, so that they integrate as coherent warps
         if (!g && audit_hash((unsigned long long)idx >> 5, seed) < audit_threshold) g = 2;
         gate[idx] = g;
+        gate_of_thread = g;
         take = g != 0;
     }
-    // rays to integrate, counted per block (the list is built in pixel order by
-    // sur_scan_kernel and sur_scatter_kernel)
-    __shared__ unsigned warp_counts[32];
-    const unsigned m = __ballot_sync(kFull, take);
-    if ((threadIdx.x & 31) == 0) warp_counts[threadIdx.x >> 5] = __popc(m);
+    // rays to integrate, counted per block and class (gated, then audit: the
+    // list is built by sur_scan_kernel and sur_scatter_kernel with every gated
+    // ray before every audit ray, each class in pixel order)
+    __shared__ unsigned warp_counts[2][32];
+    const unsigned m1 = __ballot_sync(kFull, take && gate_of_thread == 1);
+    const unsigned m2 = __ballot_sync(kFull, take && gate_of_thread == 2);
+    if ((threadIdx.x & 31) == 0) {
+        warp_counts[0][threadIdx.x >> 5] = __popc(m1);
+        warp_counts[1][threadIdx.x >> 5] = __popc(m2);
+    }
     __syncthreads();
-    if (threadIdx.x == 0) {
+    if (threadIdx.x < 2) {
         unsigned c = 0;
-        for (int w = 0; w < int(blockDim.x >> 5); ++w) c += warp_counts[w];
-        block_counts[blockIdx.x] = c;
+        for (int w = 0; w < int(blockDim.x >> 5); ++w) c += warp_counts[threadIdx.x][w];
+        block_counts[threadIdx.x * gridDim.x + blockIdx.x] = c;
     }
 }
 
@@ -905,26 +912,33 @@ __global__ void sur_scan_kernel(unsigned* block_counts, int n_blocks) {
     if (t == 1023) block_counts[n_blocks] = part[1023];
 }
 
-// The list of rays to integrate in pixel order (same blocking as the features kernel).
+// The list of rays to integrate (same blocking as the features kernel): the
+// gated rays in pixel order, then the audit rays in pixel order.
+// block_offsets: class-1 offsets of the blocks, then their class-2 offsets.
 __global__ void sur_scatter_kernel(const unsigned char* gate, long long total, const unsigned* block_offsets,
                                    unsigned* list) {
-    __shared__ unsigned warp_base[32];
+    __shared__ unsigned warp_base[2][32];
     const long long idx = (long long)blockIdx.x * blockDim.x + threadIdx.x;
-    const bool take = idx < total && gate[idx] != 0;
-    const unsigned m = __ballot_sync(kFull, take);
+    const unsigned char g = idx < total ? gate[idx] : 0;
+    const unsigned m1 = __ballot_sync(kFull, g == 1), m2 = __ballot_sync(kFull, g == 2);
     const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
-    if (lane == 0) warp_base[warp] = __popc(m);
+    if (lane == 0) {
+        warp_base[0][warp] = __popc(m1);
+        warp_base[1][warp] = __popc(m2);
+    }
     __syncthreads();
-    if (threadIdx.x == 0) {
-        unsigned run = block_offsets[blockIdx.x];
+    if (threadIdx.x < 2) {
+        unsigned run = block_offsets[threadIdx.x * gridDim.x + blockIdx.x];
         for (int w = 0; w < int(blockDim.x >> 5); ++w) {
-            const unsigned c = warp_base[w];
-            warp_base[w] = run;
+            const unsigned c = warp_base[threadIdx.x][w];
+            warp_base[threadIdx.x][w] = run;
             run += c;
         }
     }
     __syncthreads();
-    if (take) list[warp_base[warp] + __popc(m & ((1u << lane) - 1u))] = unsigned(idx);
+    const unsigned below = (1u << lane) - 1u;
+    if (g == 1) list[warp_base[0][warp] + __popc(m1 & below)] = unsigned(idx);
+    if (g == 2) list[warp_base[1][warp] + __popc(m2 & below)] = unsigned(idx);
 }
 
 // pixel intensity from the MLP outputs: hit logit, r_1, g_1, higher orders
@@ -1045,7 +1059,7 @@ struct Handle {
     size_t list_cap = 0;
     unsigned char* d_gate = nullptr;
     size_t gate_cap = 0;
-    unsigned* d_block_counts = nullptr;  // per-block counts, then offsets; [n_blocks] = list length
+    unsigned* d_block_counts = nullptr;  // per-block gated and audit counts, then offsets; [2 n_blocks] = list length
     size_t block_counts_cap = 0;
     cudaEvent_t sev[5] = {};
     TrainState* train = nullptr;  // surrogate training state (sirius_cuda_train_init)
@@ -2241,7 +2255,8 @@ static int surrogate_prepare(Handle* H, const sirius_frame* frames, int n_frames
     if ((rc = ensure(H, H->d_list, H->list_cap, size_t(total))) != SIRIUS_OK) return rc;
     const int block = 256;
     const int n_blocks = int((total + block - 1) / block);
-    if ((rc = ensure(H, H->d_block_counts, H->block_counts_cap, size_t(n_blocks) + 1)) != SIRIUS_OK) return rc;
+    // per block: gated count, then audit count; [2 n_blocks] = list length
+    if ((rc = ensure(H, H->d_block_counts, H->block_counts_cap, 2 * size_t(n_blocks) + 1)) != SIRIUS_OK) return rc;
     if (!d_gate) {
         if ((rc = ensure(H, H->d_gate, H->gate_cap, size_t(total))) != SIRIUS_OK) return rc;
         d_gate = H->d_gate;
@@ -2254,7 +2269,7 @@ static int surrogate_prepare(Handle* H, const sirius_frame* frames, int n_frames
     sur_features_kernel<<<n_blocks, block, 0, st>>>(H->d_frames, H->d_sur_frames, n_frames, total, float(band), thr,
                                                     seed, H->d_feat, d_gate, H->d_block_counts);
     CK(cudaGetLastError());
-    sur_scan_kernel<<<1, 1024, 0, st>>>(H->d_block_counts, n_blocks);
+    sur_scan_kernel<<<1, 1024, 0, st>>>(H->d_block_counts, 2 * n_blocks);
     CK(cudaGetLastError());
     sur_scatter_kernel<<<n_blocks, block, 0, st>>>(d_gate, total, H->d_block_counts, H->d_list);
     CK(cudaGetLastError());
@@ -2285,7 +2300,7 @@ static int render_surrogate(Handle* H, const sirius_frame* frames, int n_frames,
     CK(cudaEventRecord(H->sev[1], st));
     unsigned n_int = 0;
     const long long n_blocks = (total + 255) / 256;
-    CK(cudaMemcpyAsync(&n_int, H->d_block_counts + n_blocks, sizeof(unsigned), cudaMemcpyDeviceToHost, st));
+    CK(cudaMemcpyAsync(&n_int, H->d_block_counts + 2 * n_blocks, sizeof(unsigned), cudaMemcpyDeviceToHost, st));
     CK(cudaStreamSynchronize(st));
     // 2. the MLP on every pixel and the shading of the ungated ones, then 3.
     // the integrator on the compacted list of gated and audit rays. (Run beside

@@ -195,13 +195,16 @@ __device__ __forceinline__ void gemm_epilogue(const GemmArgs& g, uint32_t tmem, 
         float v[16];
         tmem_ld16(tl, v);
         if (!live) return;
-        if constexpr (E == kEpiOutput) {
-            for (int j = 0; j < g.e.ny; ++j) g.e.y[row * g.e.ldy + j] = v[j] + g.e.bias[j];
-        } else if constexpr (E == kEpiDWeight) {
-            for (int j = 0; j < g.e.ng && n0 + j < g.N; ++j) atomicAdd(g.e.grad + row * g.e.ldg + n0 + j, v[j]);
-        } else if constexpr (E == kEpiDWeightT) {
-            for (int j = 0; j < g.e.ng && n0 + j < g.N; ++j)
-                atomicAdd(g.e.grad + (long long)(n0 + j) * g.e.ldg + row, v[j]);
+        // (unrolled over the 16 columns so that v stays in registers)
+#pragma unroll
+        for (int j = 0; j < 16; ++j) {
+            if constexpr (E == kEpiOutput) {
+                if (j < g.e.ny) g.e.y[row * g.e.ldy + j] = v[j] + g.e.bias[j];
+            } else if constexpr (E == kEpiDWeight) {
+                if (j < g.e.ng && n0 + j < g.N) atomicAdd(g.e.grad + row * g.e.ldg + n0 + j, v[j]);
+            } else if constexpr (E == kEpiDWeightT) {
+                if (j < g.e.ng && n0 + j < g.N) atomicAdd(g.e.grad + (long long)(n0 + j) * g.e.ldg + row, v[j]);
+            }
         }
     } else {
 #pragma unroll 1
@@ -256,7 +259,9 @@ __device__ __forceinline__ void gemm_epilogue(const GemmArgs& g, uint32_t tmem, 
                             atomicAdd(reinterpret_cast<float4*>(gr) + i,
                                       make_float4(v[4 * i], v[4 * i + 1], v[4 * i + 2], v[4 * i + 3]));
                     } else {
-                        for (int i = 0; i < 32 && n + i < g.e.ng; ++i) atomicAdd(gr + i, v[i]);
+#pragma unroll
+                        for (int i = 0; i < 32; ++i)
+                            if (n + i < g.e.ng) atomicAdd(gr + i, v[i]);
                     }
                 }
             }

@@ -2,7 +2,7 @@
 traced by the engine, with the library's own training kernels, and write its
 parameters (nn.Linear order, float32) for sirius_cuda_surrogate_load.
 
-Training set: 2^24 rays of 4096 Kerr frames with a* ~ U[0, 0.99], inclination
+Training set: 2^26 rays of 16384 Kerr frames with a* ~ U[0, 0.99], inclination
 ~ U[5, 89] deg, r_obs ~ U[20, 200] M, each a 64^2 30 deg pinhole camera (pixel
 centres with a random sub-pixel offset per frame, so alpha and beta cover the
 field of view), thin Novikov-Thorne disk r_ISCO..30 M, traced by the
@@ -102,7 +102,7 @@ def total_loss(parts):
     return parts[0] + 100.0 * (parts[1] + parts[2]) + 10.0 * parts[3]
 
 
-def train(n_rays=1 << 24, epochs=120, batch=16384, lr=2e-3, seed=0, out=DEFAULT_OUT, log=print):
+def train(n_rays=1 << 26, epochs=60, batch=32768, lr=4e-3, seed=0, out=DEFAULT_OUT, log=print):
     from sirius_b200 import abi
     from sirius_b200.engine import Engine
 
@@ -138,10 +138,10 @@ def train(n_rays=1 << 24, epochs=120, batch=16384, lr=2e-3, seed=0, out=DEFAULT_
 
 def main():
     ap = argparse.ArgumentParser()
-    ap.add_argument("--rays", type=int, default=1 << 24)
-    ap.add_argument("--epochs", type=int, default=120)
-    ap.add_argument("--batch", type=int, default=16384)
-    ap.add_argument("--lr", type=float, default=2e-3)
+    ap.add_argument("--rays", type=int, default=1 << 26)
+    ap.add_argument("--epochs", type=int, default=60)
+    ap.add_argument("--batch", type=int, default=32768)
+    ap.add_argument("--lr", type=float, default=4e-3)
     ap.add_argument("--seed", type=int, default=0)
     ap.add_argument("--out", default=DEFAULT_OUT)
     a = ap.parse_args()

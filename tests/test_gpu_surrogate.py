@@ -115,3 +115,27 @@ def test_surrogate_integrates_frames_it_does_not_cover(engine):
     img, _, gate, st = engine.render_surrogate([fr])
     assert np.all(gate == 1) and st.integrated == full.size
     np.testing.assert_array_equal(img, full)
+
+
+def test_trained_network_gains_over_the_untrained_one(engine):
+    """What training buys: the same gated render with the fitted weights and
+    with the network's initial (untrained) weights. Both integrate the same
+    ~1-2 % of the rays (the gate does not depend on the weights); the fitted
+    network brings the other pixels within the error budget, the untrained one
+    does not, so without the trained network the whole frame would have to be
+    integrated to reach that error."""
+    fr = kerr_frame(512)
+    engine.configure(render_config(abi.PRECISION_MIXED))
+    _, full, _ = engine.trace_frames([fr], results=False)
+    scale = full.max()
+    errs, fractions = {}, {}
+    rng = np.random.default_rng(11)
+    for name, params in (("trained", np.load(WEIGHTS)), ("untrained", init_params(rng))):
+        engine.surrogate_load(params)
+        img, _, gate, st = engine.render_surrogate([fr])
+        errs[name] = np.abs(img.astype(np.float64) - full) / scale
+        fractions[name] = st.integrated / st.rays
+    assert fractions["trained"] == fractions["untrained"] < 0.05
+    assert errs["trained"].mean() < 1e-3 and np.percentile(errs["trained"], 99) < 1e-2
+    assert errs["untrained"].mean() > 10 * errs["trained"].mean()
+    assert np.percentile(errs["untrained"], 99) > 5 * np.percentile(errs["trained"], 99)
