@@ -349,6 +349,40 @@ def surrogate_leg(eng, abi, np, torch, dev, stream, side=SURROGATE_SIDE, reps=3)
             "weights": "sirius_b200/data/surrogate_kerr.npy (python -m sirius_b200.surrogate_train)"}
 
 
+TRAIN_FLOP_PER_ROW = 3 * 2 * 198912 - 2 * 5 * 256  # forward, dW and dH (no dH for the input layer)
+
+
+def train_leg(eng, abi, np, torch, dev, rows=1 << 21, batch=32768, steps=64):
+    """The surrogate's training step on the tensor cores (gather, forward and
+    backward tcgen05 GEMMs, loss, Adam; one CUDA graph replay per step) over a
+    seeded synthetic training set of `rows` device-resident rows with the
+    surrogate's feature ranges; CUDA-event time of `steps` replayed steps."""
+    rng = np.random.default_rng(0)
+    X = rng.uniform(-1.0, 1.0, size=(rows, 5)).astype(np.float32)
+    hit = (np.hypot(X[:, 2], X[:, 3]) > 0.35).astype(np.float32)
+    T = np.stack([hit, hit * (0.5 * X[:, 2] - 0.2 * X[:, 0]), hit * (0.6 + 0.3 * X[:, 3] * X[:, 1]),
+                  0.2 * np.sin(3 * X[:, 2]) * X[:, 4]], 1).astype(np.float32)
+    W = rng.uniform(0.05, 1.0, size=rows).astype(np.float32)
+    dX, dT, dW = (torch.from_numpy(a).to(dev) for a in (X, T, W))
+    params = np.load(SURROGATE_WEIGHTS)
+    eng.train_init(params, abi.train_config(batch=batch, total_steps=4 * steps, max_lr=1e-4))
+    eng.train_steps(dX.data_ptr(), dT.data_ptr(), dW.data_ptr(), rows, 3)  # capture + warm-up
+    ms = eng.train_steps(dX.data_ptr(), dT.data_ptr(), dW.data_ptr(), rows, steps)
+    rows_per_s = steps * batch / (ms * 1e-3)
+    peaks = {}
+    if os.path.exists(MEASURED_PEAKS):
+        with open(MEASURED_PEAKS) as f:
+            peaks = json.load(f)
+    bf16_peak = float(peaks.get("bf16_tflops", 1590.0))
+    tflops = rows_per_s * TRAIN_FLOP_PER_ROW / 1e12
+    return {"workload": f"surrogate_mlp_training_batch{batch}", "steps": steps, "ms_per_step": ms / steps,
+            "rows_per_s": rows_per_s, "flop_per_row": TRAIN_FLOP_PER_ROW,
+            "roofline": {"bound": "tensor", "achieved": tflops, "peak": bf16_peak, "unit": "TFLOP/s",
+                         "frac": tflops / bf16_peak, "peak_source": "MEASURED_PEAKS.json bf16_tflops (burst)"
+                         if "bf16_tflops" in peaks else "fallback 1590 TFLOP/s"},
+            "data": "synthetic rows (seeded), the surrogate's feature ranges"}
+
+
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
@@ -359,6 +393,9 @@ def main():
     ap.add_argument("--surrogate-only", action="store_true",
                     help="run only the surrogate-gated leg (at --surrogate-size) and print its JSON")
     ap.add_argument("--surrogate-size", type=int, default=SURROGATE_SIDE)
+    ap.add_argument("--train-only", action="store_true",
+                    help="run only the surrogate-training leg and print its JSON")
+    ap.add_argument("--train-steps", type=int, default=64)
     ap.add_argument("--size", type=int, default=WIDTH,
                     help="frame side (default 1024, the workload; smaller sides are profiling cases)")
     args = ap.parse_args()
@@ -383,6 +420,11 @@ def main():
         dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=120))
     dev = torch.device("cuda", local)
     stream = torch.cuda.current_stream(dev)
+    if args.train_only:
+        eng = Engine(local)
+        print(json.dumps(train_leg(eng, abi, np, torch, dev, steps=args.train_steps)), flush=True)
+        eng.close()
+        return
     if args.surrogate_only:
         eng = Engine(local)
         print(json.dumps(surrogate_leg(eng, abi, np, torch, dev, stream, side=args.surrogate_size)), flush=True)
@@ -495,6 +537,7 @@ def main():
                                  "spectra_linf_rel": float(serr.max()),
                                  "spectra_p99_rel": float(np.percentile(serr, 99))}
         line["surrogate"] = surrogate_leg(eng, abi, np, torch, dev, stream)
+        line["surrogate_training"] = train_leg(eng, abi, np, torch, dev)
         line["heterogeneous_batch"] = batch_leg(eng, abi)
         line["stress_symplectic"] = stress_leg(eng, abi)
         line["cpu_baseline"] = cpu_baseline_sample()

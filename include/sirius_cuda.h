@@ -363,9 +363,10 @@ void sirius_cuda_default_train_config(sirius_train_config* config);
  * order); Adam moments and the step counter reset to zero. */
 int sirius_cuda_train_init(sirius_cuda_handle handle, const float* params, const sirius_train_config* config);
 /* n_steps optimiser steps over rows [0, n_rows): each epoch visits the rows of
- * n_rows / batch full batches in a fresh keyed permutation; synchronous on return. */
+ * n_rows / batch full batches in a fresh keyed permutation; synchronous on return.
+ * device_ms (may be NULL): CUDA-event time of the steps on the library's stream. */
 int sirius_cuda_train_steps(sirius_cuda_handle handle, const float* d_features, const float* d_targets,
-                            const float* d_weights, int64_t n_rows, int64_t n_steps);
+                            const float* d_weights, int64_t n_rows, int64_t n_steps, float* device_ms);
 /* loss parts of the current weights over rows [0, n_rows), in batches of the configured size
  * (averaged, each batch weighted by its rows) */
 int sirius_cuda_train_evaluate(sirius_cuda_handle handle, const float* d_features, const float* d_targets,

@@ -42,6 +42,8 @@ namespace {
 
 constexpr unsigned kFull = 0xffffffffu;
 
+constexpr unsigned kListSkip = 0xFFFFFFFFu;  // a list entry that names no ray
+
 struct Params {
     const FrameDev* frames;
     int n_frames;
@@ -50,7 +52,8 @@ struct Params {
     float* image;
     float* spectra;
     const sirius_camera_ray* host_rays;  // optional: explicit camera rays (device copy)
-    const unsigned* list;                 // optional: trace only these ray indices (total = list length)
+    const unsigned* list;                 // optional: trace only these ray indices (total = list length;
+                                          // kListSkip entries are padding)
     const float* flux;                    // optional: per-frame disk flux tables (mixed path), kFluxN each
     unsigned long long* queue;            // [0] ray cursor
     unsigned long long* counters;         // [0] accepted, [1] rejected, [2] fp64 steps
@@ -679,8 +682,9 @@ __global__ void __launch_bounds__(128, MINB) trace_kernel(const __grid_constant_
 
     if (!P.persistent) {
         const long long gid = (long long)blockIdx.x * blockDim.x + threadIdx.x;
-        if (gid < P.total) {
-            const long long idx = P.list ? (long long)P.list[gid] : gid;
+        const unsigned entry = (P.list && gid < P.total) ? P.list[gid] : 0u;
+        if (gid < P.total && entry != kListSkip) {
+            const long long idx = P.list ? (long long)entry : gid;
             const int frame = P.n_frames > 1 ? find_frame(P.frames, P.n_frames, idx) : 0;
             if (P.family < 0 || P.frames[frame].m.family == P.family) {
                 begin_ray<MIXED, FAM, UNI>(P, s, idx, frame, vol);
@@ -700,8 +704,9 @@ __global__ void __launch_bounds__(128, MINB) trace_kernel(const __grid_constant_
                 if (base >= (unsigned long long)P.total) exhausted = true;
                 if (!alive) {
                     const unsigned long long q = base + __popc(dead & lt_mask);
-                    if (q < (unsigned long long)P.total) {
-                        const unsigned long long idx = P.list ? (unsigned long long)P.list[q] : q;
+                    const unsigned entry = (P.list && q < (unsigned long long)P.total) ? P.list[q] : 0u;
+                    if (q < (unsigned long long)P.total && entry != kListSkip) {
+                        const unsigned long long idx = P.list ? (unsigned long long)entry : q;
                         const int frame = P.n_frames > 1 ? find_frame(P.frames, P.n_frames, (long long)idx) : 0;
                         begin_ray<MIXED, FAM, UNI>(P, s, (long long)idx, frame, vol);
                         alive = true;
@@ -818,40 +823,74 @@ __device__ __forceinline__ float seg_dist2(float px, float py, float ax, float a
     return dx * dx + dy * dy;
 }
 
-// features (a, inclination, alpha, beta, r_obs), normalised; gate: 1 = within
-// `band` of the critical curve (or a frame the MLP does not cover), 2 = audit.
+// features (a, inclination, alpha, beta, r_obs), normalised
 __global__ void sur_features_kernel(const FrameDev* frames, const SurFrameDev* sf, int n_frames, long long total,
-                                    float band, unsigned audit_threshold, unsigned seed, float* feat,
-                                    unsigned char* gate, unsigned* block_counts) {
+                                    float* feat) {
+    // the metric and the Boyer-Lindquist radius at the camera, once per block for
+    // the frame of its first pixel (a thread of another frame computes its own)
+    __shared__ double g_cam[16], r_cam;
+    __shared__ int f_cam;
     const long long idx = (long long)blockIdx.x * blockDim.x + threadIdx.x;
-    bool take = false;
-    unsigned char gate_of_thread = 0;
-    if (idx < total) {
-        const int f = n_frames > 1 ? find_frame(frames, n_frames, idx) : 0;
-        const FrameDev& F = frames[f];
-        const SurFrameDev& S = sf[f];
-        const long long pix = idx - F.ray_offset;
-        double dir[4], x[4], p[4];
-        camera_dir(F, int(pix % F.width), int(pix / F.width), dir);
+    if (threadIdx.x == 0) {
+        const long long first = (long long)blockIdx.x * blockDim.x;
+        const int f0 = n_frames > 1 ? find_frame(frames, n_frames, first) : 0;
+        f_cam = frames[f0].m.family == SIRIUS_METRIC_MORRIS_THORNE ? -1 : f0;
+        if (f_cam >= 0) {
+            double x[4];
+            camera_position_ks(frames[f0], x);
+            metric_g(frames[f0].m, x, g_cam);
+            InvForm IF;
+            inv_form(frames[f0].m, x, IF);
+            r_cam = IF.r;
+        }
+    }
+    __syncthreads();
+    if (idx >= total) return;
+    const int f = n_frames > 1 ? find_frame(frames, n_frames, idx) : 0;
+    const FrameDev& F = frames[f];
+    const SurFrameDev& S = sf[f];
+    const long long pix = idx - F.ray_offset;
+    double dir[4], x[4], p[4], r;
+    camera_dir(F, int(pix % F.width), int(pix / F.width), dir);
+    if (f == f_cam) {
+        init_state_ks(F, dir, g_cam, x, p);
+        r = r_cam;
+    } else {
         init_state(F, dir, x, p);
-        // celestial coordinates from the ray's own constants of motion:
-        // alpha = -L_z / (E sin theta_o), beta = p_theta / E
         InvForm IF;
         inv_form(F.m, x, IF);
-        const double r = IF.r, E = -p[0], L = x[1] * p[2] - x[2] * p[1];
-        const double ct = fmin(fmax(x[3] / r, -1.0), 1.0), st = sqrt(fmax(1.0 - ct * ct, 1e-30));
-        const double pth = (ct / st) * (x[1] * p[1] + x[2] * p[2]) - r * st * p[3];
-        const float alpha = float(-L / (E * S.sin_o)), beta = float(pth / E);
-        float* o = feat + idx * 5;
-        o[0] = float(2.0 * F.a_star - 1.0);
-        o[1] = float((S.theta_deg - 47.0) / 42.0);
-        o[2] = alpha / 20.f;
-        o[3] = beta / 20.f;
-        o[4] = float((F.cam_r - 110.0) / 90.0);
-        unsigned char g = 0;
+        r = IF.r;
+    }
+    // celestial coordinates from the ray's own constants of motion:
+    // alpha = -L_z / (E sin theta_o), beta = p_theta / E
+    const double E = -p[0], L = x[1] * p[2] - x[2] * p[1];
+    const double ct = fmin(fmax(x[3] / r, -1.0), 1.0), st = sqrt(fmax(1.0 - ct * ct, 1e-30));
+    const double pth = (ct / st) * (x[1] * p[1] + x[2] * p[2]) - r * st * p[3];
+    float* o = feat + idx * 5;
+    o[0] = float(2.0 * F.a_star - 1.0);
+    o[1] = float((S.theta_deg - 47.0) / 42.0);
+    o[2] = float(-L / (E * S.sin_o) / 20.0);
+    o[3] = float(pth / E / 20.0);
+    o[4] = float((F.cam_r - 110.0) / 90.0);
+}
+
+// gate per pixel from its celestial coordinates (features 2 and 3): 1 = within
+// `band` of the critical curve (or a frame the MLP does not cover), 2 = audit,
+// 0 = the MLP's pixel; and the rays to integrate counted per block and class
+// (sur_scan_kernel and sur_scatter_kernel list every gated ray before every
+// audit ray, each class in pixel order)
+__global__ void sur_gate_kernel(const FrameDev* frames, const SurFrameDev* sf, int n_frames, long long total,
+                                float band, unsigned audit_threshold, unsigned seed, const float* feat,
+                                unsigned char* gate, unsigned* block_counts) {
+    const long long idx = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+    unsigned char g = 0;
+    if (idx < total) {
+        const int f = n_frames > 1 ? find_frame(frames, n_frames, idx) : 0;
+        const SurFrameDev& S = sf[f];
         if (!S.kerr) {
             g = 1;
         } else {
+            const float alpha = feat[idx * 5 + 2] * 20.f, beta = feat[idx * 5 + 3] * 20.f;
             const float dx = alpha - S.ac, dy = beta;
             const float phi = atan2f(dy, dx);
             const int j0 = int(floorf((phi + float(kPi)) * (kCurveN / (2.f * float(kPi)))));
@@ -865,15 +904,10 @@ __global__ void sur_features_kernel(const FrameDev* frames, const SurFrameDev* s
         // audit rays come in runs of 32 consecutive pixels, so that they integrate as coherent warps
         if (!g && audit_hash((unsigned long long)idx >> 5, seed) < audit_threshold) g = 2;
         gate[idx] = g;
-        gate_of_thread = g;
-        take = g != 0;
     }
-    // rays to integrate, counted per block and class (gated, then audit: the
-    // list is built by sur_scan_kernel and sur_scatter_kernel with every gated
-    // ray before every audit ray, each class in pixel order)
     __shared__ unsigned warp_counts[2][32];
-    const unsigned m1 = __ballot_sync(kFull, take && gate_of_thread == 1);
-    const unsigned m2 = __ballot_sync(kFull, take && gate_of_thread == 2);
+    const unsigned m1 = __ballot_sync(kFull, g == 1);
+    const unsigned m2 = __ballot_sync(kFull, g == 2);
     if ((threadIdx.x & 31) == 0) {
         warp_counts[0][threadIdx.x >> 5] = __popc(m1);
         warp_counts[1][threadIdx.x >> 5] = __popc(m2);
@@ -912,8 +946,9 @@ __global__ void sur_scan_kernel(unsigned* block_counts, int n_blocks) {
     if (t == 1023) block_counts[n_blocks] = part[1023];
 }
 
-// The list of rays to integrate (same blocking as the features kernel): the
-// gated rays in pixel order, then the audit rays in pixel order.
+// The list of rays to integrate (same blocking as the gate kernel): the gated
+// rays in pixel order, kListSkip entries up to the next multiple of 32, then
+// the audit rays in pixel order (so each audit run of 32 pixels fills one warp).
 // block_offsets: class-1 offsets of the blocks, then their class-2 offsets.
 __global__ void sur_scatter_kernel(const unsigned char* gate, long long total, const unsigned* block_offsets,
                                    unsigned* list) {
@@ -927,8 +962,10 @@ __global__ void sur_scatter_kernel(const unsigned char* gate, long long total, c
         warp_base[1][warp] = __popc(m2);
     }
     __syncthreads();
+    const unsigned n1 = block_offsets[gridDim.x], pad = (32u - (n1 & 31u)) & 31u;
+    if (blockIdx.x == 0 && threadIdx.x < pad) list[n1 + threadIdx.x] = kListSkip;
     if (threadIdx.x < 2) {
-        unsigned run = block_offsets[threadIdx.x * gridDim.x + blockIdx.x];
+        unsigned run = block_offsets[threadIdx.x * gridDim.x + blockIdx.x] + (threadIdx.x == 1 ? pad : 0u);
         for (int w = 0; w < int(blockDim.x >> 5); ++w) {
             const unsigned c = warp_base[threadIdx.x][w];
             warp_base[threadIdx.x][w] = run;
@@ -1050,6 +1087,9 @@ struct Handle {
     int* d_sur_err = nullptr;
     // surrogate-gated rendering scratch
     SurFrameDev* d_sur_frames = nullptr;
+    SurFrameDev* h_sur_frames = nullptr;  // pinned staging: per-frame basics, then with the curves
+    size_t h_sur_frames_cap = 0;
+    unsigned* h_list_len = nullptr;       // pinned: gated count, gated + audit count
     size_t sur_frames_cap = 0;
     float* d_feat = nullptr;
     size_t feat_cap = 0;
@@ -1062,6 +1102,9 @@ struct Handle {
     unsigned* d_block_counts = nullptr;  // per-block gated and audit counts, then offsets; [2 n_blocks] = list length
     size_t block_counts_cap = 0;
     cudaEvent_t sev[5] = {};
+    // surrogate rendering: the gated trace (high priority) and the MLP (low priority)
+    cudaStream_t sur_stream[2] = {};
+    cudaEvent_t fev[4] = {};  // trace done, MLP done, shade done, join
     TrainState* train = nullptr;  // surrogate training state (sirius_cuda_train_init)
 };
 
@@ -1226,7 +1269,7 @@ struct LaunchScratch {
 
 int launch_trace(Handle* H, int n_frames, long long total, sirius_ray_result* d_results, float* d_image,
                  float* d_spectra, const sirius_camera_ray* d_rays, cudaStream_t st, bool timed,
-                 const LaunchScratch* scratch = nullptr, const unsigned* d_list = nullptr) {
+                 const LaunchScratch* scratch = nullptr, const unsigned* d_list = nullptr, bool flux_ready = false) {
     const sirius_trace_config& c = H->cfg;
     if (!scratch && (c.precision == SIRIUS_PRECISION_MIXED)) {
         const int rc = ensure(H, H->d_flux, H->flux_cap, size_t(n_frames) * kFluxTable);
@@ -1312,10 +1355,12 @@ int launch_trace(Handle* H, int n_frames, long long total, sirius_ray_result* d_
     P.flux = nullptr;
     int extra_launches = 0;
     if (mixed && c.enable_disk && (H->family_mask & (1 << SIRIUS_METRIC_KERR_SCHILD)) && S.flux) {
-        flux_table_kernel<<<n_frames, kFluxN, 0, st>>>(S.frames, S.flux);
-        CK(cudaGetLastError());
+        if (!flux_ready) {  // else the caller built this upload's tables ahead of this stream
+            flux_table_kernel<<<n_frames, kFluxN, 0, st>>>(S.frames, S.flux);
+            CK(cudaGetLastError());
+            extra_launches = 1;
+        }
         P.flux = S.flux;
-        extra_launches = 1;
     }
     for (int i = 0; i < n_launches; ++i) {
         P.family = launch_family[i];
@@ -1657,8 +1702,12 @@ int sirius_cuda_destroy(sirius_cuda_handle h) {
     cudaFree(H->d_surrogate); cudaFree(H->d_sur_err);
     cudaFree(H->d_sur_frames); cudaFree(H->d_feat); cudaFree(H->d_mlp_out); cudaFree(H->d_list); cudaFree(H->d_gate);
     cudaFree(H->d_block_counts);
+    if (H->h_sur_frames) cudaFreeHost(H->h_sur_frames);
+    if (H->h_list_len) cudaFreeHost(H->h_list_len);
     train_free(H->train);
     for (auto& e : H->sev) if (e) cudaEventDestroy(e);
+    for (auto& e : H->fev) if (e) cudaEventDestroy(e);
+    for (auto& q : H->sur_stream) if (q) cudaStreamDestroy(q);
     for (auto& e : H->ev) if (e) cudaEventDestroy(e);
     if (H->stream) cudaStreamDestroy(H->stream);
     delete H;
@@ -1972,7 +2021,7 @@ int sirius_cuda_surrogate_load(sirius_cuda_handle h, const float* params, int64_
     if (!H->d_surrogate) {
         if (cudaMalloc((void**)&H->d_surrogate, surrogate::kImageBytes) != cudaSuccess)
             return fail(H, SIRIUS_ERR_OUT_OF_MEMORY, "cudaMalloc surrogate weights");
-        if (cudaMalloc((void**)&H->d_sur_err, sizeof(int)) != cudaSuccess)
+        if (cudaMalloc((void**)&H->d_sur_err, 4 * sizeof(int)) != cudaSuccess)  // [0] error, [2..3] tile counter
             return fail(H, SIRIUS_ERR_OUT_OF_MEMORY, "cudaMalloc surrogate status");
         CK(cudaFuncSetAttribute(surrogate::mlp_kernel_ts, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                 surrogate::kTsSmBytes));
@@ -1990,8 +2039,10 @@ static int surrogate_launch(Handle* H, const float* d_features, long long n, flo
     const int grid = int(std::min<long long>(tiles, H->num_sms));
     // bound on any wait inside the kernel: the configured watchdog (default 30 s)
     const unsigned long long limit = (unsigned long long)(H->cfg.watchdog_ms > 0 ? H->cfg.watchdog_ms : 30000) * 1000000ull;
-    surrogate::mlp_kernel_ts<<<grid, surrogate::kThreads, surrogate::kTsSmBytes, st>>>(H->d_surrogate, d_features, n, d_out,
-                                                                               H->d_sur_err, limit);
+    unsigned long long* counter = reinterpret_cast<unsigned long long*>(H->d_sur_err + 2);
+    CK(cudaMemsetAsync(counter, 0, sizeof(unsigned long long), st));
+    surrogate::mlp_kernel_ts<<<grid, surrogate::kThreads, surrogate::kTsSmBytes, st>>>(
+        H->d_surrogate, d_features, n, d_out, H->d_sur_err, counter, limit);
     CK(cudaGetLastError());
     return SIRIUS_OK;
 }
@@ -2076,7 +2127,7 @@ int sirius_cuda_train_init(sirius_cuda_handle h, const float* params, const siri
 }
 
 int sirius_cuda_train_steps(sirius_cuda_handle h, const float* d_features, const float* d_targets,
-                            const float* d_weights, int64_t n_rows, int64_t n_steps) {
+                            const float* d_weights, int64_t n_rows, int64_t n_steps, float* device_ms) {
     Handle* H = static_cast<Handle*>(h);
     if (!H || !d_features || !d_targets || !d_weights || n_steps < 0) return SIRIUS_ERR_INVALID_ARGUMENT;
     TrainState* T = H->train;
@@ -2109,8 +2160,14 @@ int sirius_cuda_train_steps(sirius_cuda_handle h, const float* d_features, const
         T->key[2] = d_weights;
         T->key_rows = n_rows;
     }
+    for (auto& e : H->ev)
+        if (!e) CK(cudaEventCreate(&e));
+    CK(cudaEventRecord(H->ev[1], H->stream));
     for (int64_t i = 0; i < n_steps; ++i) CK(cudaGraphLaunch(T->graph, H->stream));
-    return train_check_err(H, T);
+    CK(cudaEventRecord(H->ev[2], H->stream));
+    const int rc = train_check_err(H, T);
+    if (rc == SIRIUS_OK && device_ms) CK(cudaEventElapsedTime(device_ms, H->ev[1], H->ev[2]));
+    return rc;
 }
 
 int sirius_cuda_train_evaluate(sirius_cuda_handle h, const float* d_features, const float* d_targets,
@@ -2184,7 +2241,7 @@ int sirius_cuda_train_params(sirius_cuda_handle h, float* params, int64_t* steps
 // r in [r_ph,pro, r_ph,retro] give xi = L/E, eta = Q/E^2; alpha = -xi/sin(theta_o),
 // beta = +-sqrt(eta + a^2 cos^2 theta_o - xi^2 cot^2 theta_o)), resampled at
 // kCurveN angles about its centre.
-static SurFrameDev make_sur_frame(const sirius_frame& f, const FrameDev& F) {
+static SurFrameDev make_sur_frame(const sirius_frame& f, const FrameDev& F, bool curve = true) {
     SurFrameDev S{};
     const sirius_metric& m = f.metric;
     const double x = F.cam_r * F.cam_st * F.cam_cp, y = F.cam_r * F.cam_st * F.cam_sp, z = F.cam_r * F.cam_ct;
@@ -2195,7 +2252,7 @@ static SurFrameDev make_sur_frame(const sirius_frame& f, const FrameDev& F) {
     S.sin_o = std::max(std::sin(th), 1e-6);
     S.theta_deg = th * 180.0 / kPi;
     S.kerr = (m.family == SIRIUS_METRIC_KERR_SCHILD && F.has_horizon && m.Q == 0.0 && m.Lambda == 0.0) ? 1 : 0;
-    if (!S.kerr) return S;
+    if (!S.kerr || !curve) return S;
     std::vector<std::pair<double, double>> pts;
     const double co = std::cos(th), cot = co / S.sin_o;
     if (std::fabs(a) < 1e-6 * M) {
@@ -2244,35 +2301,64 @@ static SurFrameDev make_sur_frame(const sirius_frame& f, const FrameDev& F) {
     return S;
 }
 
-// Features, gate and the list of rays to integrate for the uploaded frames.
-static int surrogate_prepare(Handle* H, const sirius_frame* frames, int n_frames, long long total,
-                             const sirius_surrogate_config* sc, unsigned char* d_gate, cudaStream_t st) {
-    std::vector<SurFrameDev> sf(n_frames);
-    for (int i = 0; i < n_frames; ++i) sf[i] = make_sur_frame(frames[i], make_frame(frames[i], H->cfg));
+// Stage 1 for the uploaded frames: the per-frame constants the features need
+// (camera inclination) and the features kernel. Its upload comes from pinned
+// memory, so the host returns at once and computes the critical curves while
+// the kernel runs.
+static int surrogate_features_launch(Handle* H, const sirius_frame* frames, int n_frames, long long total,
+                                     cudaStream_t st) {
     int rc;
+    if (H->h_sur_frames_cap < size_t(2 * n_frames)) {
+        if (H->h_sur_frames) CK(cudaFreeHost(H->h_sur_frames));
+        H->h_sur_frames = nullptr;
+        H->h_sur_frames_cap = 0;
+        CK(cudaMallocHost((void**)&H->h_sur_frames, 2 * size_t(n_frames) * sizeof(SurFrameDev)));
+        H->h_sur_frames_cap = 2 * size_t(n_frames);
+    }
     if ((rc = ensure(H, H->d_sur_frames, H->sur_frames_cap, size_t(n_frames))) != SIRIUS_OK) return rc;
     if ((rc = ensure(H, H->d_feat, H->feat_cap, size_t(total) * 5)) != SIRIUS_OK) return rc;
-    if ((rc = ensure(H, H->d_list, H->list_cap, size_t(total))) != SIRIUS_OK) return rc;
+    for (int i = 0; i < n_frames; ++i) H->h_sur_frames[i] = make_sur_frame(frames[i], make_frame(frames[i], H->cfg), false);
+    CK(cudaMemcpyAsync(H->d_sur_frames, H->h_sur_frames, n_frames * sizeof(SurFrameDev), cudaMemcpyHostToDevice, st));
+    sur_features_kernel<<<int((total + 255) / 256), 256, 0, st>>>(H->d_frames, H->d_sur_frames, n_frames, total,
+                                                                  H->d_feat);
+    CK(cudaGetLastError());
+    return SIRIUS_OK;
+}
+
+// Stage 2: the critical curves (host), the gate, and the list of rays to
+// integrate (gated rays, padding to a multiple of 32, audit rays); the two
+// list counts are copied into pinned memory (read them once the stream has
+// passed this point).
+static int surrogate_gate_launch(Handle* H, const sirius_frame* frames, int n_frames, long long total,
+                                 const sirius_surrogate_config* sc, unsigned char* d_gate, cudaStream_t st) {
+    int rc;
+    SurFrameDev* full = H->h_sur_frames + n_frames;
+    for (int i = 0; i < n_frames; ++i) full[i] = make_sur_frame(frames[i], make_frame(frames[i], H->cfg));
+    if ((rc = ensure(H, H->d_list, H->list_cap, size_t(total) + 32)) != SIRIUS_OK) return rc;
     const int block = 256;
     const int n_blocks = int((total + block - 1) / block);
-    // per block: gated count, then audit count; [2 n_blocks] = list length
+    // per block: gated count, then audit count; [2 n_blocks] = gated + audit total
     if ((rc = ensure(H, H->d_block_counts, H->block_counts_cap, 2 * size_t(n_blocks) + 1)) != SIRIUS_OK) return rc;
     if (!d_gate) {
         if ((rc = ensure(H, H->d_gate, H->gate_cap, size_t(total))) != SIRIUS_OK) return rc;
         d_gate = H->d_gate;
     }
-    CK(cudaMemcpyAsync(H->d_sur_frames, sf.data(), n_frames * sizeof(SurFrameDev), cudaMemcpyHostToDevice, st));
+    if (!H->h_list_len) CK(cudaMallocHost((void**)&H->h_list_len, 2 * sizeof(unsigned)));
+    CK(cudaMemcpyAsync(H->d_sur_frames, full, n_frames * sizeof(SurFrameDev), cudaMemcpyHostToDevice, st));
     const double band = sc ? sc->gate_band : 0.3;
     const double audit = sc ? std::clamp(sc->audit_fraction, 0.0, 1.0) : 0.01;
     const unsigned thr = unsigned(std::min(audit * 4294967296.0, 4294967295.0));
     const unsigned seed = sc ? sc->audit_seed : 0u;
-    sur_features_kernel<<<n_blocks, block, 0, st>>>(H->d_frames, H->d_sur_frames, n_frames, total, float(band), thr,
-                                                    seed, H->d_feat, d_gate, H->d_block_counts);
+    sur_gate_kernel<<<n_blocks, block, 0, st>>>(H->d_frames, H->d_sur_frames, n_frames, total, float(band), thr, seed,
+                                                H->d_feat, d_gate, H->d_block_counts);
     CK(cudaGetLastError());
     sur_scan_kernel<<<1, 1024, 0, st>>>(H->d_block_counts, 2 * n_blocks);
     CK(cudaGetLastError());
     sur_scatter_kernel<<<n_blocks, block, 0, st>>>(d_gate, total, H->d_block_counts, H->d_list);
     CK(cudaGetLastError());
+    CK(cudaMemcpyAsync(H->h_list_len, H->d_block_counts + n_blocks, sizeof(unsigned), cudaMemcpyDeviceToHost, st));
+    CK(cudaMemcpyAsync(H->h_list_len + 1, H->d_block_counts + 2 * size_t(n_blocks), sizeof(unsigned),
+                       cudaMemcpyDeviceToHost, st));
     return SIRIUS_OK;
 }
 
@@ -2296,30 +2382,46 @@ static int render_surrogate(Handle* H, const sirius_frame* frames, int n_frames,
     }
     // 1. features, gate and the compacted list of rays to integrate
     CK(cudaEventRecord(H->sev[0], st));
-    if ((rc = surrogate_prepare(H, frames, n_frames, total, sc, d_gate, st)) != SIRIUS_OK) return rc;
-    CK(cudaEventRecord(H->sev[1], st));
-    unsigned n_int = 0;
-    const long long n_blocks = (total + 255) / 256;
-    CK(cudaMemcpyAsync(&n_int, H->d_block_counts + 2 * n_blocks, sizeof(unsigned), cudaMemcpyDeviceToHost, st));
-    CK(cudaStreamSynchronize(st));
-    // 2. the MLP on every pixel and the shading of the ungated ones, then 3.
-    // the integrator on the compacted list of gated and audit rays. (Run beside
-    // the MLP, the latency-bound gated rays lose more than the overlap gains.)
-    CK(cudaMemsetAsync(H->d_sur_err, 0, sizeof(int), st));
-    if ((rc = surrogate_launch(H, H->d_feat, total, H->d_mlp_out, st)) != SIRIUS_OK) return rc;
-    CK(cudaEventRecord(H->sev[2], st));
+    if ((rc = surrogate_features_launch(H, frames, n_frames, total, st)) != SIRIUS_OK) return rc;
+    if ((rc = surrogate_gate_launch(H, frames, n_frames, total, sc, d_gate, st)) != SIRIUS_OK) return rc;
+    // 2. the integrator on the compacted list of gated and audit rays, beside
+    // 3. the MLP on every pixel and the shading of the ungated ones. The trace
+    // goes first, from a high-priority stream, so its blocks take every free
+    // slot; the MLP (low priority, tiles from a counter) fills the SMs that the
+    // trace's tail leaves idle, a few long near-critical warps. The shading
+    // writes only ungated pixels, so the two never write the same pixel.
+    if (!H->sur_stream[0]) {
+        int least = 0, greatest = 0;
+        CK(cudaDeviceGetStreamPriorityRange(&least, &greatest));
+        CK(cudaStreamCreateWithPriority(&H->sur_stream[0], cudaStreamNonBlocking, greatest));
+        CK(cudaStreamCreateWithPriority(&H->sur_stream[1], cudaStreamNonBlocking, least));
+        for (auto& e : H->fev) CK(cudaEventCreate(&e));
+    }
+    cudaStream_t s_trace = H->sur_stream[0], s_mlp = H->sur_stream[1];
     if ((rc = ensure(H, H->d_flux, H->flux_cap, size_t(n_frames) * kFluxTable)) != SIRIUS_OK) return rc;
     flux_table_kernel<<<n_frames, kFluxN, 0, st>>>(H->d_frames, H->d_flux);
     CK(cudaGetLastError());
-    sur_shade_kernel<<<int((total + 255) / 256), 256, 0, st>>>(H->d_frames, n_frames, total, H->d_mlp_out, d_gate,
-                                                               H->d_flux, d_image, d_image_mlp);
-    CK(cudaGetLastError());
-    CK(cudaEventRecord(H->sev[3], st));
+    CK(cudaMemsetAsync(H->d_sur_err, 0, sizeof(int), st));
+    CK(cudaEventRecord(H->sev[1], st));
+    CK(cudaStreamWaitEvent(s_trace, H->sev[1], 0));
+    CK(cudaStreamWaitEvent(s_mlp, H->sev[1], 0));
+    CK(cudaEventSynchronize(H->sev[1]));
+    const unsigned n_gated = H->h_list_len[0], n_int = H->h_list_len[1];
+    const long long n_list = (long long)n_int + ((32 - (n_gated & 31u)) & 31u);
     if (n_int > 0) {
-        rc = launch_trace(H, n_frames, (long long)n_int, nullptr, d_image, nullptr, nullptr, st, false, nullptr,
-                          H->d_list);
+        rc = launch_trace(H, n_frames, n_list, nullptr, d_image, nullptr, nullptr, s_trace, false, nullptr, H->d_list,
+                          true);
         if (rc != SIRIUS_OK) return rc;
     }
+    CK(cudaEventRecord(H->fev[0], s_trace));
+    if ((rc = surrogate_launch(H, H->d_feat, total, H->d_mlp_out, s_mlp)) != SIRIUS_OK) return rc;
+    CK(cudaEventRecord(H->fev[1], s_mlp));
+    sur_shade_kernel<<<int((total + 255) / 256), 256, 0, s_mlp>>>(H->d_frames, n_frames, total, H->d_mlp_out, d_gate,
+                                                                  H->d_flux, d_image, d_image_mlp);
+    CK(cudaGetLastError());
+    CK(cudaEventRecord(H->fev[2], s_mlp));
+    CK(cudaStreamWaitEvent(st, H->fev[0], 0));
+    CK(cudaStreamWaitEvent(st, H->fev[2], 0));
     CK(cudaEventRecord(H->sev[4], st));
     int err = 0, status = 0;
     CK(cudaMemcpyAsync(&err, H->d_sur_err, sizeof(int), cudaMemcpyDeviceToHost, st));
@@ -2331,13 +2433,12 @@ static int render_surrogate(Handle* H, const sirius_frame* frames, int n_frames,
         *stats = sirius_surrogate_stats{};
         stats->rays = total;
         stats->integrated = n_int;
-        float t[4] = {}, tt = 0.f;
-        for (int i = 0; i < 4; ++i) CK(cudaEventElapsedTime(&t[i], H->sev[i], H->sev[i + 1]));
+        float tt = 0.f;
+        CK(cudaEventElapsedTime(&stats->ms_features, H->sev[0], H->sev[1]));
+        CK(cudaEventElapsedTime(&stats->ms_trace, H->sev[1], H->fev[0]));   // concurrent with the MLP
+        CK(cudaEventElapsedTime(&stats->ms_mlp, H->sev[1], H->fev[1]));
+        CK(cudaEventElapsedTime(&stats->ms_shade, H->fev[1], H->fev[2]));
         CK(cudaEventElapsedTime(&tt, H->sev[0], H->sev[4]));
-        stats->ms_features = t[0];
-        stats->ms_mlp = t[1];
-        stats->ms_shade = t[2];
-        stats->ms_trace = t[3];
         stats->ms_total = tt;
     }
     return SIRIUS_OK;
@@ -2356,7 +2457,8 @@ int sirius_cuda_surrogate_features(sirius_cuda_handle h, const sirius_frame* fra
     int rc = upload_frames(H, frames, n_frames, &total);
     H->stream = keep;
     if (rc != SIRIUS_OK) return rc;
-    if ((rc = surrogate_prepare(H, frames, n_frames, total, sc, d_gate, st)) != SIRIUS_OK) return rc;
+    if ((rc = surrogate_features_launch(H, frames, n_frames, total, st)) != SIRIUS_OK) return rc;
+    if ((rc = surrogate_gate_launch(H, frames, n_frames, total, sc, d_gate, st)) != SIRIUS_OK) return rc;
     CK(cudaMemcpyAsync(d_features, H->d_feat, size_t(total) * 5 * sizeof(float), cudaMemcpyDeviceToDevice, st));
     CK(cudaStreamSynchronize(st));
     return SIRIUS_OK;

@@ -75,22 +75,27 @@ constexpr uint32_t kTmemAcc = 0, kTmemA0 = 256, kTmemA1 = 384, kTmemCols = 512;
 __device__ __forceinline__ void epilogue_half_ts(uint32_t tmem, int H, const float* bias, uint32_t a_next) {
     const int warp = threadIdx.x >> 5;
     const uint32_t lanes = uint32_t((warp & 3) * 32) << 16;
-#pragma unroll 1
+    // both 32-column loads in flight before one wait
+    const int col0 = 128 * H + 64 * (warp >> 2);
+    float v[64];
+    tmem_ld32_nowait(tmem + kTmemAcc + lanes + uint32_t(col0), v);
+    tmem_ld32_nowait(tmem + kTmemAcc + lanes + uint32_t(col0 + 32), v + 32);
+    asm volatile("tcgen05.wait::ld.sync.aligned;" ::: "memory");
+#pragma unroll
     for (int c = 0; c < 2; ++c) {
-        const int col0 = 128 * H + 64 * (warp >> 2) + 32 * c;
-        float v[32];
-        tmem_ld32(tmem + kTmemAcc + lanes + uint32_t(col0), v);
         uint32_t r[16];
 #pragma unroll
         for (int i = 0; i < 16; ++i)
-            r[i] = pack_bf16x2(silu(v[2 * i] + bias[col0 + 2 * i]), silu(v[2 * i + 1] + bias[col0 + 2 * i + 1]));
-        tmem_st16(tmem + a_next + lanes + uint32_t(col0 / 2), r);
+            r[i] = pack_bf16x2(silu(v[32 * c + 2 * i] + bias[col0 + 32 * c + 2 * i]),
+                               silu(v[32 * c + 2 * i + 1] + bias[col0 + 32 * c + 2 * i + 1]));
+        tmem_st16(tmem + a_next + lanes + uint32_t((col0 + 32 * c) / 2), r);
     }
 }
 
 __global__ void __launch_bounds__(kThreads, 1)
     mlp_kernel_ts(const unsigned char* __restrict__ wimg, const float* __restrict__ feat, long long n,
-                  float* __restrict__ out, int* err, unsigned long long wait_limit_ns) {
+                  float* __restrict__ out, int* err, unsigned long long* tile_counter,
+                  unsigned long long wait_limit_ns) {
     extern __shared__ __align__(1024) unsigned char sm[];
     unsigned char* Wbuf = sm + kTsSmWbuf;
     unsigned char* W1s = sm + kTsSmW1;
@@ -98,6 +103,7 @@ __global__ void __launch_bounds__(kThreads, 1)
     unsigned char* Xs = sm + kTsSmX;
     float* bias = reinterpret_cast<float*>(sm + kTsSmBias);
     uint32_t* tslot = reinterpret_cast<uint32_t*>(sm + kTsSmTmemSlot);
+    long long* next_s = reinterpret_cast<long long*>(sm + kTsSmTmemSlot + 8);  // the next tile to take
     const uint32_t bar_a = smem_u32(sm + kTsSmBar), bar_b = smem_u32(sm + kTsSmBar + 8),
                    bar_tma = smem_u32(sm + kTsSmBar + 16);
     const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
@@ -114,6 +120,9 @@ __global__ void __launch_bounds__(kThreads, 1)
                      "r"(kTmemCols));
         asm volatile("tcgen05.relinquish_alloc_permit.cta_group::1.sync.aligned;");
     }
+    // tiles come from a counter, so a CTA that starts late (its SM still busy
+    // with another kernel's blocks) takes fewer of them
+    if (tid == 32) *next_s = (long long)atomicAdd(tile_counter, 1ull);
     {  // resident operands: W1 | W5 (contiguous in the image and in shared memory) and the biases
         const uint4* src1 = reinterpret_cast<const uint4*>(wimg + kOffW1);
         uint4* dst1 = reinterpret_cast<uint4*>(W1s);
@@ -130,12 +139,15 @@ __global__ void __launch_bounds__(kThreads, 1)
 
     uint32_t ph_a = 0, ph_b = 0, ph_tma = 0;
     bool tma_pending = false, ok = true;
-    if (tid == 0 && blockIdx.x < ntiles) bulk_load(smem_u32(Wbuf), wimg, kBigBytes, bar_tma);
-    tma_pending = blockIdx.x < ntiles;
+    long long tile = *next_s;
+    if (tid == 0 && tile < ntiles) bulk_load(smem_u32(Wbuf), wimg, kBigBytes, bar_tma);
+    tma_pending = tile < ntiles;
     const uint32_t idesc128 = instr_desc(128), idesc16 = instr_desc(kOutPad);
 
-    for (long long tile = blockIdx.x; tile < ntiles; tile += gridDim.x) {
+    while (tile < ntiles) {
         const long long row0 = tile * kTileM;
+        __syncthreads();  // every thread has read *next_s
+        if (tid == 32) *next_s = (long long)atomicAdd(tile_counter, 1ull);
         {  // input tile: 128 rows x 16 BF16 (features 0..4, zero padding)
             const int r = tid >> 1, chunk = tid & 1;
             uint4 w = make_uint4(0, 0, 0, 0);
@@ -150,6 +162,7 @@ __global__ void __launch_bounds__(kThreads, 1)
         }
         fence_async_smem();
         __syncthreads();
+        const long long next = *next_s;
         // layer 1 (A from shared memory, K = 16): two N-halves
         if (tid == 0) {
             tc_fence_after();
@@ -209,7 +222,7 @@ __global__ void __launch_bounds__(kThreads, 1)
             ok = __syncthreads_and(ok);
             if (!ok) break;
             // Wbuf is drained: bring the next layer's weights (or layer 2's for the next tile)
-            if (L < 2 || tile + gridDim.x < ntiles) {
+            if (L < 2 || next < ntiles) {
                 if (tid == 0) bulk_load(smem_u32(Wbuf), wimg + size_t(L < 2 ? L + 1 : 0) * kBigBytes, kBigBytes, bar_tma);
                 tma_pending = true;
             }
@@ -250,6 +263,7 @@ __global__ void __launch_bounds__(kThreads, 1)
         }
         tc_fence_before();
         __syncthreads();
+        tile = next;
     }
     if (!ok) {
         if (tid == 0) atomicOr(err, 1);

@@ -156,6 +156,17 @@ __device__ __forceinline__ double null_k0(const double g[16], const double k[4])
     return fmax(kp, km);
 }
 
+// k^0 from the null condition, then p_mu = g_mu_nu k^nu.
+__device__ __forceinline__ void null_momentum(const double g[16], double k[4], double p[4]) {
+    k[0] = 0.0;
+    k[0] = null_k0(g, k);
+    for (int mu = 0; mu < 4; ++mu) {
+        double s = 0;
+        for (int nu = 0; nu < 4; ++nu) s += g[4 * mu + nu] * k[nu];
+        p[mu] = s;
+    }
+}
+
 // Initial state from a camera ray (GTRC001A.cpp:15-134 without float roundings):
 // spherical map of the camera position, spherical -> Cartesian velocity,
 // normalizeNull for k^0, p = g k.
@@ -177,13 +188,30 @@ __device__ __forceinline__ void init_state(const FrameDev& F, const double dir[4
         k[3] = vr * ct - r * vth * st;
         metric_g(F.m, x, g);
     }
-    k[0] = 0.0;
-    k[0] = null_k0(g, k);
-    for (int mu = 0; mu < 4; ++mu) {
-        double s = 0;
-        for (int nu = 0; nu < 4; ++nu) s += g[4 * mu + nu] * k[nu];
-        p[mu] = s;
-    }
+    null_momentum(g, k, p);
+}
+
+// Kerr-Schild camera position of a frame (the x of init_state's Cartesian branch).
+__device__ __forceinline__ void camera_position_ks(const FrameDev& F, double x[4]) {
+    const double r = F.cam_r, st = F.cam_st, ct = F.cam_ct, sp = F.cam_sp, cp = F.cam_cp;
+    x[0] = F.cam_t; x[1] = r * st * cp; x[2] = r * st * sp; x[3] = r * ct;
+}
+
+// init_state's Cartesian (Kerr-Schild family) branch with the metric at the
+// camera already evaluated: the same operations in the same order, for kernels
+// that start many rays from one camera.
+__device__ __forceinline__ void init_state_ks(const FrameDev& F, const double dir[4], const double g[16],
+                                              double x[4], double p[4]) {
+    const double r = F.cam_r, st = F.cam_st, ct = F.cam_ct, sp = F.cam_sp, cp = F.cam_cp;
+    const double vr = dir[1], vth = dir[2] / r;
+    double vph = dir[3] / (r * st);
+    if (fabs(st) < 1e-10) vph = 0.0;
+    double k[4];
+    camera_position_ks(F, x);
+    k[1] = vr * st * cp + r * vth * ct * cp - r * vph * st * sp;
+    k[2] = vr * st * sp + r * vth * ct * sp + r * vph * st * cp;
+    k[3] = vr * ct - r * vth * st;
+    null_momentum(g, k, p);
 }
 
 // ---------------------------------------------------------------------------

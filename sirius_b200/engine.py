@@ -73,7 +73,8 @@ def load_library(path=LIB_PATH):
     L.sirius_cuda_default_train_config.argtypes = [_P(abi.TrainConfig)]
     L.sirius_cuda_default_train_config.restype = None
     L.sirius_cuda_train_init.argtypes = [C.c_void_p, C.c_void_p, _P(abi.TrainConfig)]
-    L.sirius_cuda_train_steps.argtypes = [C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p, C.c_int64, C.c_int64]
+    L.sirius_cuda_train_steps.argtypes = [C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p, C.c_int64, C.c_int64,
+                                          _P(C.c_float)]
     L.sirius_cuda_train_evaluate.argtypes = [C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p, C.c_int64, C.c_void_p]
     L.sirius_cuda_train_gradient.argtypes = [C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p, C.c_int64, C.c_void_p,
                                              C.c_void_p]
@@ -177,8 +178,11 @@ class Engine:
         self._check(self.lib.sirius_cuda_train_init(self.h, p.ctypes.data, C.byref(config)))
 
     def train_steps(self, d_features, d_targets, d_weights, n_rows, n_steps):
-        """n_steps optimiser steps over the device-resident rows [0, n_rows)."""
-        self._check(self.lib.sirius_cuda_train_steps(self.h, d_features, d_targets, d_weights, n_rows, n_steps))
+        """n_steps optimiser steps over the device-resident rows [0, n_rows); returns their device time (ms)."""
+        ms = C.c_float()
+        self._check(self.lib.sirius_cuda_train_steps(self.h, d_features, d_targets, d_weights, n_rows, n_steps,
+                                                     C.byref(ms)))
+        return ms.value
 
     def train_evaluate(self, d_features, d_targets, d_weights, n_rows):
         """Loss parts (BCE, l_r, l_g, l_h) of the current weights over rows [0, n_rows)."""

@@ -87,7 +87,7 @@ def test_null_handle_and_bad_arguments_are_errors_not_crashes():
     assert lib.sirius_cuda_trace_frames(None, None, 0, None, None, None) == abi.ERR_INVALID_ARGUMENT
     assert lib.sirius_cuda_default_config(None) == abi.ERR_INVALID_ARGUMENT
     assert lib.sirius_cuda_train_init(None, None, None) == abi.ERR_INVALID_ARGUMENT
-    assert lib.sirius_cuda_train_steps(None, None, None, None, 0, 0) == abi.ERR_INVALID_ARGUMENT
+    assert lib.sirius_cuda_train_steps(None, None, None, None, 0, 0, None) == abi.ERR_INVALID_ARGUMENT
     assert lib.sirius_cuda_train_gradient(None, None, None, None, 128, None, None) == abi.ERR_INVALID_ARGUMENT
     h = C.c_void_p()
     rc = lib.sirius_cuda_create(999, C.byref(h))
