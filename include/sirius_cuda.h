@@ -95,6 +95,20 @@ enum sirius_projection {
                                          implementation in the reference, CMBS001A.h:68,351-362) */
 };
 
+/* Whose frame the pixel directions are given in. */
+enum sirius_observer {
+    SIRIUS_OBSERVER_STATIC = 0, /* the reference's convention (GTRC001A.cpp:15-134): the camera at
+                                   the spherical map (r sin(theta) cos(phi), ...) of its (r, theta,
+                                   phi), pixel directions as coordinate velocities there, k^0 from the
+                                   null condition; redshifts relative to a static observer */
+    SIRIUS_OBSERVER_ZAMO = 1    /* Kerr-Schild family with Lambda = 0 only: the camera at the
+                                   Kerr-Schild point whose Boyer-Lindquist coordinates are exactly (r,
+                                   theta, phi) (the oblate map, PHCT002A.h:149-169), pixel directions
+                                   as unit vectors in the orthonormal frame of the zero-angular-momentum
+                                   observer there (Bardeen 1972 tetrad; FIDO, RDOP002A.cu:2528-2604),
+                                   photon energy 1 in that frame; redshifts relative to that observer */
+};
+
 /* ---- metric parameters ---------------------------------------------------- */
 typedef struct sirius_metric {
     int32_t family;   /* enum sirius_metric_family */
@@ -111,7 +125,7 @@ typedef struct sirius_camera {
     float fov;                   /* degrees (pinhole) */
     int32_t width, height;
     int32_t projection;          /* enum sirius_projection */
-    int32_t reserved;            /* must be 0 (one sample per pixel, at the pixel centre) */
+    int32_t observer;            /* enum sirius_observer (one sample per pixel, at the pixel centre) */
 } sirius_camera;
 
 /* ---- one frame of a (possibly heterogeneous) batch ------------------------ */
@@ -267,7 +281,7 @@ int sirius_cuda_trace_frames_device(sirius_cuda_handle handle,
 /* Allocation-free form of sirius_cuda_trace_frames_device (no counterpart in the
  * reference): same arguments, same results, but the launch scratch (frame
  * descriptors, ray-queue and step counters, status word, per-frame disk flux
- * tables; 150 KB in all) lives in a static device array of the library, held
+ * tables; 160 KB in all) lives in a static device array of the library, held
  * by every GPU that loads it, so the call makes no device allocation. For
  * callers that cannot let a library allocate: a host whose own allocator
  * already holds the device memory it is given, or a frame loop that cannot

@@ -45,6 +45,8 @@ INTEGRATOR_DP45 = 0
 INTEGRATOR_SYMPLECTIC = 1
 CAMERA_PINHOLE = 0
 CAMERA_EQUIRECTANGULAR = 1
+OBSERVER_STATIC = 0  # enum sirius_observer
+OBSERVER_ZAMO = 1
 
 FLAG_NUMERICAL_FAILURE = 1
 FLAG_PHOTON_RING = 2
@@ -61,7 +63,7 @@ class Camera(C.Structure):
     _fields_ = [("t", C.c_double), ("r", C.c_double), ("theta", C.c_double), ("phi", C.c_double),
                 ("yaw", C.c_float), ("pitch", C.c_float), ("roll", C.c_float), ("fov", C.c_float),
                 ("width", C.c_int32), ("height", C.c_int32), ("projection", C.c_int32),
-                ("reserved", C.c_int32)]
+                ("observer", C.c_int32)]
 
 
 class Frame(C.Structure):
@@ -205,9 +207,9 @@ def make_metric(family=KERR_SCHILD, M=1.0, a=0.0, Q=0.0, Lambda=0.0, b0=1.0, Phi
 
 
 def make_camera(r=50.0, theta_deg=85.0, phi=0.0, fov=30.0, width=256, height=256, projection=CAMERA_PINHOLE,
-                yaw=0.0, pitch=0.0, roll=0.0):
+                yaw=0.0, pitch=0.0, roll=0.0, observer=0):
     import math
-    return Camera(0.0, r, math.radians(theta_deg), phi, yaw, pitch, roll, fov, width, height, projection, 0)
+    return Camera(0.0, r, math.radians(theta_deg), phi, yaw, pitch, roll, fov, width, height, projection, observer)
 
 
 def make_frame(metric, camera, disk_inner=0.0, disk_outer=20.0, ray_offset=0):

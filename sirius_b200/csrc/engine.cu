@@ -281,7 +281,7 @@ __device__ __noinline__ void volumetric_segment(const Params& P, const FrameDev&
     const int nq = c.vol_sub < 1 ? 1 : (c.vol_sub > 4 ? 4 : c.vol_sub);
     const float E = float(-p[0]);
     const float Lz = float(x1[1] * p[2] - x1[2] * p[1]);
-    const float nu_cam = E / float(F.sqrt_m_gtt_cam);
+    const float nu_cam = E / observer_factor<float>(F, E);
     const float rin = float(F.disk_in), rout = float(F.disk_out);
     const bool in0 = r0 >= rin && r0 <= rout, in1 = r1 >= rin && r1 <= rout;
     double fa = 0.0, fb = 1.0;
@@ -324,7 +324,7 @@ __device__ __noinline__ void volumetric_segment(const Params& P, const FrameDev&
         if (r < rin || r > rout) continue;
         const float zr = zs / (float(c.vol_hz) * r);
         if (fabsf(zr) > float(kVolCutoff)) continue;
-        const float g = kepler_g<float>(F.m, xs, ys, zs, r, E, Lz, float(F.sqrt_m_gtt_cam));
+        const float g = kepler_g<float>(F.m, xs, ys, zs, r, E, Lz, observer_factor<float>(F, E));
         if (!(g > 0.f)) continue;
         const float dl = float(h * span) * kGLw[nq - 1][s];
         const float jsp = float(c.vol_j0) / (r * r) * __expf(-0.5f * zr * zr);
@@ -416,7 +416,7 @@ __device__ __noinline__ bool record_crossing(const Params& P, const FrameDev& F,
     const double rc = CF.r;
     if (!(rc >= F.disk_in && rc <= F.disk_out)) return false;
     const double E = -p[0], Lz = x[1] * p[2] - x[2] * p[1];
-    const double g = kepler_g<double>(m, xc1, xc2, 0.0, rc, E, Lz, F.sqrt_m_gtt_cam);
+    const double g = kepler_g<double>(m, xc1, xc2, 0.0, rc, E, Lz, observer_factor<double>(F, E));
     const double Fl = P.flux ? flux_lookup(P.flux + size_t(F.flux_slot) * kFluxTable, F, rc)
                              : nt_flux(rc, F.a_star, F.isco, F.disk_in, F.disk_out);
     intensity += exp(-P.c.decay * n) * g * g * g * g * Fl;
@@ -834,7 +834,8 @@ __global__ void sur_features_kernel(const FrameDev* frames, const SurFrameDev* s
     if (threadIdx.x == 0) {
         const long long first = (long long)blockIdx.x * blockDim.x;
         const int f0 = n_frames > 1 ? find_frame(frames, n_frames, first) : 0;
-        f_cam = frames[f0].m.family == SIRIUS_METRIC_MORRIS_THORNE ? -1 : f0;
+        f_cam = (frames[f0].m.family == SIRIUS_METRIC_MORRIS_THORNE || frames[f0].observer != SIRIUS_OBSERVER_STATIC)
+                    ? -1 : f0;
         if (f_cam >= 0) {
             double x[4];
             camera_position_ks(frames[f0], x);
@@ -1143,6 +1144,22 @@ double isco_host(double a_star) {
 
 MetricDev make_metric(const sirius_metric& s) { return metric_dev(s); }
 
+// The zero-angular-momentum observer needs a Kerr-Newman metric (Kerr-Schild
+// family, Lambda = 0) and a camera outside the outer horizon, off the axis.
+int validate_observer(Handle* H, const sirius_frame& f) {
+    const sirius_camera& c = f.camera;
+    if (c.observer == SIRIUS_OBSERVER_STATIC) return SIRIUS_OK;
+    if (c.observer != SIRIUS_OBSERVER_ZAMO) return fail(H, SIRIUS_ERR_INVALID_ARGUMENT, "unknown camera observer");
+    const sirius_metric& m = f.metric;
+    if (m.family != SIRIUS_METRIC_KERR_SCHILD || std::fabs(m.Lambda) > 1e-15)
+        return fail(H, SIRIUS_ERR_UNSUPPORTED, "the ZAMO observer needs a Kerr-Schild metric with Lambda = 0");
+    const double d = m.M * m.M - m.a * m.a - m.Q * m.Q;
+    const double rp = d >= 0.0 ? m.M + std::sqrt(d) : 0.0;
+    if (!(c.r > rp) || !(c.r * c.r - 2.0 * m.M * c.r + m.a * m.a + m.Q * m.Q > 0.0))
+        return fail(H, SIRIUS_ERR_INVALID_ARGUMENT, "the ZAMO observer must sit outside the outer horizon");
+    return SIRIUS_OK;
+}
+
 int validate_metric(Handle* H, const sirius_metric& m) {
     if (m.family < 0 || m.family > 2) return fail(H, SIRIUS_ERR_INVALID_ARGUMENT, "unknown metric family");
     if (!std::isfinite(m.M) || !std::isfinite(m.a) || !std::isfinite(m.Q) || !std::isfinite(m.Lambda))
@@ -1152,6 +1169,57 @@ int validate_metric(Handle* H, const sirius_metric& m) {
     if (m.family == SIRIUS_METRIC_ALCUBIERRE && !(m.sigma > 0 && m.R > 0))
         return fail(H, SIRIUS_ERR_INVALID_ARGUMENT, "Alcubierre sigma and R must be > 0");
     return SIRIUS_OK;
+}
+
+// The zero-angular-momentum observer at Boyer-Lindquist (r, theta, phi) of a
+// Kerr-Newman metric (Bardeen 1972; the FIDO of RDOP002A.cu:2528-2604):
+//   rho^2 = r^2 + a^2 cos^2, Delta = r^2 - 2 M r + a^2 + Q^2,
+//   Sigma^2 = (r^2 + a^2)^2 - a^2 Delta sin^2, alpha = rho sqrt(Delta) / Sigma,
+//   omega = a (2 M r - Q^2) / Sigma^2, varpi = Sigma sin / rho;
+//   e_(t) = (d_t + omega d_phi) / alpha, e_(r) = sqrt(Delta) / rho d_r,
+//   e_(theta) = d_theta / rho, e_(phi) = d_phi / varpi.
+// Boyer-Lindquist to Kerr-Schild: dt' = dt + (2 M r - Q^2) / Delta dr,
+// dphi' = dphi + a / Delta dr, x = (r cos phi' - a sin phi') sin, y = (r sin phi'
+// + a cos phi') sin, z = r cos (the form whose null vector is l = (1, (r x + a y)
+// / (r^2 + a^2), (r y - a x) / (r^2 + a^2), z / r)). phi' = phi - atan2(a, r)
+// puts the camera at x = sqrt(r^2 + a^2) sin cos(phi), the oblate map of
+// PHCT002A.h:149-169. The tetrad's Kerr-Schild components are J e with J the
+// Jacobian d(t', x, y, z) / d(t, r, theta, phi) at the camera.
+static void zamo_frame(const sirius_metric& m, double t, double r, double th, double ph, FrameDev& F) {
+    const double M = m.M, a = m.a, Q2 = m.Q * m.Q;
+    const double st = std::sin(th), ct = std::cos(th);
+    const double rho2 = r * r + a * a * ct * ct, rho = std::sqrt(rho2);
+    const double Delta = r * r - 2.0 * M * r + a * a + Q2;
+    const double Sig2 = (r * r + a * a) * (r * r + a * a) - a * a * Delta * st * st, Sig = std::sqrt(Sig2);
+    const double alpha = rho * std::sqrt(Delta) / Sig, omega = a * (2.0 * M * r - Q2) / Sig2;
+    const double varpi = Sig * st / rho;
+    const double eb[4][4] = {{1.0 / alpha, 0.0, 0.0, omega / alpha},
+                             {0.0, std::sqrt(Delta) / rho, 0.0, 0.0},
+                             {0.0, 0.0, 1.0 / rho, 0.0},
+                             {0.0, 0.0, 0.0, 1.0 / varpi}};
+    const double pb = ph - std::atan2(a, r), cp = std::cos(pb), sp = std::sin(pb);
+    const double dpb = a / Delta;
+    double J[4][4] = {};
+    J[0][0] = 1.0;
+    J[0][1] = (2.0 * M * r - Q2) / Delta;
+    J[1][1] = (cp + (-r * sp - a * cp) * dpb) * st;
+    J[1][2] = (r * cp - a * sp) * ct;
+    J[1][3] = (-r * sp - a * cp) * st;
+    J[2][1] = (sp + (r * cp - a * sp) * dpb) * st;
+    J[2][2] = (r * sp + a * cp) * ct;
+    J[2][3] = (r * cp - a * sp) * st;
+    J[3][1] = ct;
+    J[3][2] = -r * st;
+    F.zx[0] = t;
+    F.zx[1] = (r * cp - a * sp) * st;
+    F.zx[2] = (r * sp + a * cp) * st;
+    F.zx[3] = r * ct;
+    for (int i = 0; i < 4; ++i)
+        for (int mu = 0; mu < 4; ++mu) {
+            double s = 0.0;
+            for (int nu = 0; nu < 4; ++nu) s += J[mu][nu] * eb[i][nu];
+            F.ze[4 * i + mu] = s;
+        }
 }
 
 FrameDev make_frame(const sirius_frame& f, const sirius_trace_config& c) {
@@ -1210,6 +1278,8 @@ FrameDev make_frame(const sirius_frame& f, const sirius_trace_config& c) {
         gtt = -(1.0 - m.vs * m.vs * fs * fs);
     }
     F.sqrt_m_gtt_cam = std::sqrt(std::max(-gtt, 1e-30));
+    F.observer = f.camera.observer;
+    if (F.observer == SIRIUS_OBSERVER_ZAMO) zamo_frame(m, f.camera.t, f.camera.r, th, f.camera.phi, F);
     return F;
 }
 
@@ -1420,7 +1490,7 @@ constexpr int kStaticMaxDevices = 64;
 }  // namespace
 
 static __device__ __align__(256) unsigned char g_static_scratch[sizeof(StaticScratch)];
-static_assert(sizeof(StaticScratch) <= 160 * 1024, "static scratch stays modest");
+static_assert(sizeof(StaticScratch) <= 168 * 1024, "static scratch stays modest");
 
 namespace {
 // The device address of g_static_scratch on `device`, resolved once per device
@@ -1740,6 +1810,7 @@ static int upload_frames(Handle* H, const sirius_frame* frames, int n, long long
             return fail(H, SIRIUS_ERR_INVALID_ARGUMENT, "camera needs width, height > 0 and r > 0");
         if (f.camera.projection != SIRIUS_CAMERA_PINHOLE && f.camera.projection != SIRIUS_CAMERA_EQUIRECTANGULAR)
             return fail(H, SIRIUS_ERR_INVALID_ARGUMENT, "unknown camera projection");
+        if ((rc = validate_observer(H, f)) != SIRIUS_OK) return rc;
         if (f.ray_offset != total)
             return fail(H, SIRIUS_ERR_INVALID_ARGUMENT, "frames must be contiguous: ray_offset[i] = sum of previous pixel counts");
         fd[i] = make_frame(f, H->cfg);
@@ -1837,6 +1908,7 @@ int sirius_cuda_trace_frames_static(sirius_cuda_handle h, const sirius_frame* d_
             return fail(H, SIRIUS_ERR_INVALID_ARGUMENT, "camera needs width, height > 0 and r > 0");
         if (f.camera.projection != SIRIUS_CAMERA_PINHOLE && f.camera.projection != SIRIUS_CAMERA_EQUIRECTANGULAR)
             return fail(H, SIRIUS_ERR_INVALID_ARGUMENT, "unknown camera projection");
+        if ((rc = validate_observer(H, f)) != SIRIUS_OK) return rc;
         if (f.ray_offset != total)
             return fail(H, SIRIUS_ERR_INVALID_ARGUMENT, "frames must be contiguous: ray_offset[i] = sum of previous pixel counts");
         fd[i] = make_frame(f, H->cfg);
@@ -2251,7 +2323,9 @@ static SurFrameDev make_sur_frame(const sirius_frame& f, const FrameDev& F, bool
     const double th = std::acos(std::clamp(z / rk, -1.0, 1.0));
     S.sin_o = std::max(std::sin(th), 1e-6);
     S.theta_deg = th * 180.0 / kPi;
-    S.kerr = (m.family == SIRIUS_METRIC_KERR_SCHILD && F.has_horizon && m.Q == 0.0 && m.Lambda == 0.0) ? 1 : 0;
+    // the MLP was fitted to static-observer Kerr frames; other frames are integrated in full
+    S.kerr = (m.family == SIRIUS_METRIC_KERR_SCHILD && F.has_horizon && m.Q == 0.0 && m.Lambda == 0.0 &&
+              F.observer == SIRIUS_OBSERVER_STATIC) ? 1 : 0;
     if (!S.kerr || !curve) return S;
     std::vector<std::pair<double, double>> pts;
     const double co = std::cos(th), cot = co / S.sin_o;

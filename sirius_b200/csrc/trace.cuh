@@ -30,7 +30,21 @@ struct FrameDev {
     // radii
     double disk_in, disk_out, r_hor, r_plus, island_r, a_star, isco, r_ph_pro;
     double sqrt_m_gtt_cam;
+    // observer (enum sirius_observer); for the zero-angular-momentum observer:
+    // the camera's Kerr-Schild position and the four tetrad vectors e_(t),
+    // e_(r), e_(theta), e_(phi) in Kerr-Schild contravariant components
+    int observer;
+    double zx[4];
+    double ze[16];  // ze[4 i + mu]: vector i, component mu
 };
+
+// The observer's energy normalisation in the redshift of an emitter: the
+// static observer sees E / sqrt(-g_tt(camera)); the zero-angular-momentum
+// observer sees frequency 1 by construction, so the factor is E itself.
+template <class T>
+__device__ __forceinline__ T observer_factor(const FrameDev& F, T E) {
+    return F.observer == SIRIUS_OBSERVER_ZAMO ? E : T(F.sqrt_m_gtt_cam);
+}
 
 struct CfgDev {
     double atol, rtol, hmin, hmax, h0, safety, grow, shrink;
@@ -171,6 +185,21 @@ __device__ __forceinline__ void null_momentum(const double g[16], double k[4], d
 // spherical map of the camera position, spherical -> Cartesian velocity,
 // normalizeNull for k^0, p = g k.
 __device__ __forceinline__ void init_state(const FrameDev& F, const double dir[4], double x[4], double p[4]) {
+    if (F.observer == SIRIUS_OBSERVER_ZAMO) {
+        // k = e_(t) + n^r e_(r) + n^theta e_(theta) + n^phi e_(phi), n = dir (a unit vector)
+        double k[4], g[16];
+        for (int mu = 0; mu < 4; ++mu) {
+            x[mu] = F.zx[mu];
+            k[mu] = F.ze[mu] + dir[1] * F.ze[4 + mu] + dir[2] * F.ze[8 + mu] + dir[3] * F.ze[12 + mu];
+        }
+        metric_g(F.m, x, g);
+        for (int mu = 0; mu < 4; ++mu) {
+            double s = 0;
+            for (int nu = 0; nu < 4; ++nu) s += g[4 * mu + nu] * k[nu];
+            p[mu] = s;
+        }
+        return;
+    }
     const double r = F.cam_r, st = F.cam_st, ct = F.cam_ct, sp = F.cam_sp, cp = F.cam_cp;
     const double vr = dir[1], vth = dir[2] / r;
     double vph = dir[3] / (r * st);
