@@ -392,6 +392,22 @@ int sirius_cuda_train_gradient(sirius_cuda_handle handle, const float* d_feature
 /* the FP32 master weights (host) and the optimiser steps taken */
 int sirius_cuda_train_params(sirius_cuda_handle handle, float* params, int64_t* steps);
 
+/* ---- image output of a headless frame buffer ---------------------------------
+ * Host functions (no handle, no device): row-major float pixels, top row first.
+ * Pixel conversions as the reference's output drivers:
+ *   write_png  PNGWriter::writeRGB / writeRGBA (OUPN001A.cpp:45-97): colour channels
+ *              through the sRGB curve to 8 bits (toSRGB8, OUPN001A.h:154-163), alpha
+ *              linear; channels 3 (RGB) or 4 (RGBA)
+ *   write_exr  EXRWriter::writeEXR (OUEW001A.cpp:17-195): OpenEXR scanline file, HALF
+ *              channels B, G, R (A, B, G, R), ZIP compression; channels 3 or 4
+ *   write_pfm  EXRWriter::writePFM (OUEW001A.h:108-124): RGB floats, bottom row first
+ *   write_ppm  EXRWriter::writePPM (OUEW001A.h:94-105): RGB through the sRGB curve
+ * SIRIUS_ERR_INVALID_ARGUMENT for bad sizes or a file that cannot be written. */
+int sirius_cuda_write_png(const char* path, int32_t width, int32_t height, int32_t channels, const float* pixels);
+int sirius_cuda_write_exr(const char* path, int32_t width, int32_t height, int32_t channels, const float* pixels);
+int sirius_cuda_write_pfm(const char* path, int32_t width, int32_t height, const float* rgb);
+int sirius_cuda_write_ppm(const char* path, int32_t width, int32_t height, const float* rgb);
+
 /* ---- batch form of GeodesicTracer::trace(const CameraRay&) (GTRC001A.h:220) ----
  * Host-generated rays through one metric; disk_inner <= 0 selects the ISCO. */
 int sirius_cuda_trace_rays(sirius_cuda_handle handle, const sirius_metric* metric,

@@ -48,7 +48,7 @@ def build(force=False, verbose=False):
     if not force and up_to_date():
         return LIB
     nvcc = shutil.which("nvcc") or "/usr/local/cuda/bin/nvcc"
-    cmd = [nvcc, *NVCC_FLAGS, "-I", os.path.join(ROOT, "include"), "-shared", "-o", LIB + ".tmp", *sources()]
+    cmd = [nvcc, *NVCC_FLAGS, "-I", os.path.join(ROOT, "include"), "-shared", "-o", LIB + ".tmp", *sources(), "-lz"]
     if verbose:
         cmd.insert(1, "-Xptxas=-v")
         print(" ".join(cmd))

@@ -26,6 +26,7 @@ EXPORTS = [
     "sirius_cuda_surrogate_infer", "sirius_cuda_surrogate_features", "sirius_cuda_render_surrogate",
     "sirius_cuda_render_surrogate_device", "sirius_cuda_default_train_config", "sirius_cuda_train_init",
     "sirius_cuda_train_steps", "sirius_cuda_train_evaluate", "sirius_cuda_train_gradient", "sirius_cuda_train_params",
+    "sirius_cuda_write_png", "sirius_cuda_write_exr", "sirius_cuda_write_pfm", "sirius_cuda_write_ppm",
 ]
 
 
@@ -79,6 +80,10 @@ def load_library(path=LIB_PATH):
     L.sirius_cuda_train_gradient.argtypes = [C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p, C.c_int64, C.c_void_p,
                                              C.c_void_p]
     L.sirius_cuda_train_params.argtypes = [C.c_void_p, C.c_void_p, _P(C.c_int64)]
+    for name in ("sirius_cuda_write_png", "sirius_cuda_write_exr"):
+        getattr(L, name).argtypes = [C.c_char_p, C.c_int32, C.c_int32, C.c_int32, C.c_void_p]
+    for name in ("sirius_cuda_write_pfm", "sirius_cuda_write_ppm"):
+        getattr(L, name).argtypes = [C.c_char_p, C.c_int32, C.c_int32, C.c_void_p]
     return L
 
 
@@ -90,6 +95,28 @@ def flop_count(metric, lib=None):
     if rc != abi.OK:
         raise SiriusError(rc, "sirius_cuda_flop_count failed")
     return a.value, b.value, c.value
+
+
+def write_image(path, pixels, fmt=None, lib=None):
+    """Write an (height, width, 3 or 4) float image (top row first) as PNG, EXR,
+    PFM or PPM (by `fmt` or the file extension) with the library's writers."""
+    lib = lib or load_library()
+    px = np.ascontiguousarray(pixels, dtype=np.float32)
+    if px.ndim != 3 or px.shape[2] not in (3, 4):
+        raise ValueError("pixels must be (height, width, 3) or (height, width, 4)")
+    h, w, c = px.shape
+    fmt = (fmt or os.path.splitext(path)[1].lstrip(".")).lower()
+    p = os.fsencode(path)
+    if fmt in ("png", "exr"):
+        rc = getattr(lib, f"sirius_cuda_write_{fmt}")(p, w, h, c, px.ctypes.data)
+    elif fmt in ("pfm", "ppm"):
+        if c != 3:
+            raise ValueError(f"{fmt} takes RGB pixels")
+        rc = getattr(lib, f"sirius_cuda_write_{fmt}")(p, w, h, px.ctypes.data)
+    else:
+        raise ValueError(f"unknown image format {fmt!r}")
+    if rc != abi.OK:
+        raise SiriusError(rc, f"writing {path}")
 
 
 def frames_array(frames):
