@@ -372,6 +372,7 @@ public:
         c.max_steps = lc.maxSteps;
         c.max_step = lc.maxStepSize;
         c.precision = SIRIUS_PRECISION_MIXED;
+        c.samples_per_pixel = std::max(1, std::min(lc.samplesPerPixel, 4096));
         if (sirius_cuda_configure(m_Handle, &c) != SIRIUS_OK) { m_LastError = sirius_cuda_get_last_error(m_Handle); return; }
         sirius_frame f{};
         f.metric.family = lc.metricFamily;

@@ -194,7 +194,14 @@ typedef struct sirius_trace_config {
                                     1..4 = persistent grid of SMs * blocks_per_sm blocks that pull rays
                                     from a queue; < 0 = persistent, occupancy-sized grid */
     int32_t watchdog_ms;         /* bound on any spin-wait inside the kernels */
-    int32_t reserved[5];
+    int32_t samples_per_pixel;   /* 0 or 1: one ray through each pixel centre. n > 1: the image and
+                                    spectra average a g x g stratified grid, g = floor(sqrt(n)), of
+                                    sub-pixel rays at ((sx + 0.5) / g, (sy + 0.5) / g) as
+                                    RenderSession::shadePixel does (SNRS001A.cpp:480-530), one
+                                    progressive pass per sub-pixel offset, summed in a fixed order;
+                                    per-ray results are then not available (NULL), and the launch
+                                    statistics count the last pass. At most 4096. */
+    int32_t reserved[4];
 } sirius_trace_config;
 
 #define SIRIUS_MAX_BINS 32

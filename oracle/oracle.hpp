@@ -654,21 +654,21 @@ inline double nt_flux(double r, double a_star, double r_in, double r_out) {
 // and the 360x180 equirectangular sky camera the engine defines (the reference's
 // Panoramic lens has no implementation, CMBS001A.h:68,351-362).
 // ---------------------------------------------------------------------------
-inline void camera_ray(const sirius_camera& cam, int px, int py, double origin[4], double dir[4]) {
+inline void camera_ray(const sirius_camera& cam, int px, int py, double origin[4], double dir[4], float u = 0.5f,
+                       float v = 0.5f) {
     origin[0] = cam.t; origin[1] = cam.r; origin[2] = cam.theta; origin[3] = cam.phi;
     dir[0] = 0.0;
     if (cam.projection == SIRIUS_CAMERA_EQUIRECTANGULAR) {
         // longitude psi in [-pi, pi) across the width, latitude chi in (-pi/2, pi/2) down the height;
         // camera-local direction (right, up, forward) = (cos chi sin psi, sin chi, cos chi cos psi).
-        const double psi = (2.0 * (px + 0.5) / cam.width - 1.0) * kPi;
-        const double chi = (1.0 - 2.0 * (py + 0.5) / cam.height) * (0.5 * kPi);
+        const double psi = (2.0 * (px + double(u)) / cam.width - 1.0) * kPi;
+        const double chi = (1.0 - 2.0 * (py + double(v)) / cam.height) * (0.5 * kPi);
         const double right = std::cos(chi) * std::sin(psi), up = std::sin(chi), fwd = std::cos(chi) * std::cos(psi);
         dir[1] = -fwd;  // forward is radially inward
         dir[2] = -up;   // up is -theta
         dir[3] = right; // right is +phi
         return;
     }
-    const float u = 0.5f, v = 0.5f;
     const float aspect = float(cam.width) / float(cam.height);
     const float tanh = std::tan(cam.fov * float(kPi) / 360.0f);
     const float pxn = (2.0f * (px + u) / cam.width - 1.0f) * aspect;

@@ -31,6 +31,8 @@ class Oracle:
         L.oracle_trace_rays.argtypes = [_P(abi.Metric), C.c_double, C.c_double, _P(abi.TraceConfig),
                                         C.c_void_p, C.c_int64, C.c_void_p, C.c_int]
         L.oracle_camera_ray.argtypes = [_P(abi.Camera), C.c_int, C.c_int, C.c_void_p, C.c_void_p]
+        L.oracle_camera_ray_uv.argtypes = [_P(abi.Camera), C.c_int, C.c_int, C.c_float, C.c_float, C.c_void_p,
+                                           C.c_void_p]
         L.oracle_metric_evaluate.argtypes = [_P(abi.Metric), C.c_void_p, C.c_int64, C.c_void_p, C.c_void_p]
         L.oracle_invert4x4.argtypes = [C.c_void_p, C.c_void_p]
         L.oracle_rhs.argtypes = [_P(abi.Metric), C.c_void_p, C.c_int64, C.c_void_p, C.c_int]
@@ -81,10 +83,11 @@ class Oracle:
         assert rc == 0
         return out
 
-    def camera_ray(self, cam, px, py):
+    def camera_ray(self, cam, px, py, u=0.5, v=0.5):
         o = np.zeros(4)
         d = np.zeros(4)
-        self.lib.oracle_camera_ray(C.byref(cam), px, py, o.ctypes.data, d.ctypes.data)
+        self.lib.oracle_camera_ray_uv(C.byref(cam), px, py, C.c_float(u), C.c_float(v), o.ctypes.data,
+                                      d.ctypes.data)
         return o, d
 
     def metric_evaluate(self, metric, pos):
@@ -215,6 +218,9 @@ class Reference:
         L.ref_camera_rays.argtypes = [C.c_double, C.c_double, C.c_double, C.c_float, C.c_int, C.c_int,
                                       C.c_float, C.c_float, C.c_float, C.c_void_p, C.c_void_p, C.c_int64,
                                       C.c_void_p, C.c_void_p]
+        L.ref_camera_rays_uv.argtypes = [C.c_double, C.c_double, C.c_double, C.c_float, C.c_int, C.c_int,
+                                         C.c_float, C.c_float, C.c_float, C.c_void_p, C.c_void_p, C.c_void_p,
+                                         C.c_void_p, C.c_int64, C.c_void_p, C.c_void_p]
         L.ref_rk45_step.argtypes = [C.c_double, C.c_double, _P(RefTracerConfig), C.c_void_p, C.c_void_p,
                                     C.c_void_p, C.c_void_p, C.c_void_p, C.c_int64]
         L.ref_trace_rays.argtypes = [C.c_double, C.c_double, _P(RefTracerConfig), C.c_void_p, C.c_void_p,
@@ -243,6 +249,19 @@ class Reference:
         d = np.zeros((n, 4))
         self.lib.ref_camera_rays(cam.r, cam.theta, cam.phi, cam.fov, cam.width, cam.height, cam.yaw, cam.pitch,
                                  cam.roll, px.ctypes.data, py.ctypes.data, n, o.ctypes.data, d.ctypes.data)
+        return o, d
+
+    def camera_rays_uv(self, cam, px, py, u, v):
+        px = np.ascontiguousarray(px, dtype=np.int32)
+        py = np.ascontiguousarray(py, dtype=np.int32)
+        u = np.ascontiguousarray(u, dtype=np.float32)
+        v = np.ascontiguousarray(v, dtype=np.float32)
+        n = len(px)
+        o = np.zeros((n, 4))
+        d = np.zeros((n, 4))
+        self.lib.ref_camera_rays_uv(cam.r, cam.theta, cam.phi, cam.fov, cam.width, cam.height, cam.yaw, cam.pitch,
+                                    cam.roll, px.ctypes.data, py.ctypes.data, u.ctypes.data, v.ctypes.data, n,
+                                    o.ctypes.data, d.ctypes.data)
         return o, d
 
     def rk45_step(self, M, a, rcfg, pos, vel, h):

@@ -145,6 +145,25 @@ int ref_camera_rays(double r, double theta, double phi, float fov, int width, in
     return 0;
 }
 
+// PinholeCamera::generateRay(x, y, u, v) with a sub-pixel position per ray
+// (the stratified samples of RenderSession::shadePixel, SNRS001A.cpp:480-497).
+int ref_camera_rays_uv(double r, double theta, double phi, float fov, int width, int height, float yaw, float pitch,
+                       float roll, const int32_t* px, const int32_t* py, const float* u, const float* v, int64_t n,
+                       double* origin, double* dir) {
+    CameraConfig cc;
+    cc.r = r; cc.theta = theta; cc.phi = phi; cc.fov = fov; cc.width = width; cc.height = height;
+    cc.yaw = yaw; cc.pitch = pitch; cc.roll = roll;
+    PinholeCamera cam(cc);
+    for (int64_t i = 0; i < n; ++i) {
+        CameraRay ray = cam.generateRay(px[i], py[i], u[i], v[i]);
+        for (int j = 0; j < 4; ++j) {
+            origin[4 * i + j] = ray.origin(j);
+            dir[4 * i + j] = ray.direction(j);
+        }
+    }
+    return 0;
+}
+
 // One Geodesic::integrateStepRK45 call per Lightray (position, velocity, h).
 // Returns success flags and terminated codes; updates pos/vel/h in place.
 int ref_rk45_step(double M, double a, const ref_tracer_config* c, double* pos, double* vel, float* h,

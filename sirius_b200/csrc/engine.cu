@@ -1000,6 +1000,16 @@ __global__ void sur_shade_kernel(const FrameDev* frames, int n_frames, long long
     if (image_mlp) image_mlp[idx] = float(I);
 }
 
+// multi-sample passes: sum += pass (the first pass copies), then out = sum * scale
+__global__ void pass_accumulate_kernel(const float* pass, float* sum, long long n, int first) {
+    const long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+    if (i < n) sum[i] = first ? pass[i] : sum[i] + pass[i];
+}
+__global__ void pass_scale_kernel(float* v, long long n, float scale) {
+    const long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+    if (i < n) v[i] *= scale;
+}
+
 __global__ void metric_kernel(MetricDev m, const double* pos, long long n, int fp32, double* g, double* dg) {
     const long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x;
     if (i >= n) return;
@@ -1084,6 +1094,10 @@ struct Handle {
     long long pending_total = 0;
     int family_mask = 0;  // bit f: a frame of the last upload is of metric family f
     FrameDev frame0{};    // the first frame of the last upload (a one-frame launch's parameter copy)
+    std::vector<FrameDev> frames_host;  // the last upload's descriptors (multi-sample passes)
+    float* d_pass_image = nullptr;      // multi-sample: one pass's image and spectra, and their sums
+    float* d_pass_spectra = nullptr;
+    size_t pass_cap = 0;
     unsigned char* d_surrogate = nullptr;  // packed surrogate weight image (surrogate::kImageBytes)
     int* d_sur_err = nullptr;
     // surrogate-gated rendering scratch
@@ -1279,6 +1293,8 @@ FrameDev make_frame(const sirius_frame& f, const sirius_trace_config& c) {
     }
     F.sqrt_m_gtt_cam = std::sqrt(std::max(-gtt, 1e-30));
     F.observer = f.camera.observer;
+    F.sub_u = 0.5f;
+    F.sub_v = 0.5f;
     if (F.observer == SIRIUS_OBSERVER_ZAMO) zamo_frame(m, f.camera.t, f.camera.r, th, f.camera.phi, F);
     return F;
 }
@@ -1307,6 +1323,8 @@ int validate_config(Handle* H, const sirius_trace_config& c) {
     if (!(c.min_step > 0) || !(c.max_step >= c.min_step) || !(c.initial_step > 0))
         return fail(H, SIRIUS_ERR_INVALID_ARGUMENT, "step limits must satisfy 0 < min_step <= max_step, initial_step > 0");
     if (c.max_steps <= 0) return fail(H, SIRIUS_ERR_INVALID_ARGUMENT, "max_steps must be > 0");
+    if (c.samples_per_pixel < 0 || c.samples_per_pixel > 4096)
+        return fail(H, SIRIUS_ERR_INVALID_ARGUMENT, "samples_per_pixel must be in 0..4096");
     if (c.enable_volumetric && (c.n_bins <= 0 || c.n_bins > SIRIUS_MAX_BINS))
         return fail(H, SIRIUS_ERR_INVALID_ARGUMENT, "n_bins must be in 1..32 when volumetric transfer is on");
     if (c.enable_volumetric && !(c.nu_min > 0 && c.nu_max >= c.nu_min && c.vol_alpha_over_j > 0 && c.vol_height_ratio > 0))
@@ -1441,6 +1459,55 @@ int launch_trace(Handle* H, int n_frames, long long total, sirius_ray_result* d_
     H->stats.grid_blocks = grid;
     H->stats.block_size = block;
     H->stats.kernel_launches = n_launches + extra_launches;
+    return SIRIUS_OK;
+}
+
+// The trace of the uploaded frames into the given outputs; with
+// samples_per_pixel > 1, one launch per sub-pixel offset of the g x g grid
+// (row by row), each into pass buffers, summed in that order and scaled by 1/g^2.
+int launch_frames(Handle* H, int n_frames, long long total, sirius_ray_result* d_results, float* d_image,
+                  float* d_spectra, cudaStream_t st, bool timed) {
+    const int spp = H->cfg.samples_per_pixel;
+    int g = 1;
+    while ((g + 1) * (g + 1) <= spp) ++g;
+    if (g == 1) return launch_trace(H, n_frames, total, d_results, d_image, d_spectra, nullptr, st, timed);
+    if (d_results) return fail(H, SIRIUS_ERR_INVALID_ARGUMENT, "per-ray results need samples_per_pixel <= 1");
+    if (!d_image && !d_spectra) return SIRIUS_OK;
+    const int nb = H->cfg.enable_volumetric ? std::min(H->cfg.n_bins, SIRIUS_MAX_BINS) : 0;
+    if (H->pass_cap < size_t(total)) {
+        cudaFree(H->d_pass_image);
+        cudaFree(H->d_pass_spectra);
+        H->d_pass_image = H->d_pass_spectra = nullptr;
+        H->pass_cap = 0;
+        CK(cudaMalloc((void**)&H->d_pass_image, size_t(total) * sizeof(float)));
+        CK(cudaMalloc((void**)&H->d_pass_spectra, size_t(total) * SIRIUS_MAX_BINS * sizeof(float)));
+        H->pass_cap = size_t(total);
+    }
+    std::vector<FrameDev> fd = H->frames_host;
+    const int blocks = int((total + 255) / 256), sblocks = int((total * std::max(nb, 1) + 255) / 256);
+    if (timed) CK(cudaEventRecord(H->ev[1], st));
+    for (int s = 0; s < g * g; ++s) {
+        const float u = (float(s % g) + 0.5f) / float(g), v = (float(s / g) + 0.5f) / float(g);
+        for (auto& f : fd) {
+            f.sub_u = u;
+            f.sub_v = v;
+        }
+        H->frame0 = fd[0];
+        CK(cudaMemcpyAsync(H->d_frames, fd.data(), fd.size() * sizeof(FrameDev), cudaMemcpyHostToDevice, st));
+        int rc = launch_trace(H, n_frames, total, nullptr, d_image ? H->d_pass_image : nullptr,
+                              (d_spectra && nb) ? H->d_pass_spectra : nullptr, nullptr, st, false);
+        if (rc != SIRIUS_OK) return rc;
+        if (d_image) pass_accumulate_kernel<<<blocks, 256, 0, st>>>(H->d_pass_image, d_image, total, s == 0);
+        if (d_spectra && nb)
+            pass_accumulate_kernel<<<sblocks, 256, 0, st>>>(H->d_pass_spectra, d_spectra, total * nb, s == 0);
+        CK(cudaGetLastError());
+    }
+    const float scale = 1.0f / float(g * g);
+    if (d_image) pass_scale_kernel<<<blocks, 256, 0, st>>>(d_image, total, scale);
+    if (d_spectra && nb) pass_scale_kernel<<<sblocks, 256, 0, st>>>(d_spectra, total * nb, scale);
+    CK(cudaGetLastError());
+    if (timed) CK(cudaEventRecord(H->ev[2], st));
+    H->frame0 = H->frames_host[0];
     return SIRIUS_OK;
 }
 
@@ -1772,6 +1839,7 @@ int sirius_cuda_destroy(sirius_cuda_handle h) {
     cudaFree(H->d_surrogate); cudaFree(H->d_sur_err);
     cudaFree(H->d_sur_frames); cudaFree(H->d_feat); cudaFree(H->d_mlp_out); cudaFree(H->d_list); cudaFree(H->d_gate);
     cudaFree(H->d_block_counts);
+    cudaFree(H->d_pass_image); cudaFree(H->d_pass_spectra);
     if (H->h_sur_frames) cudaFreeHost(H->h_sur_frames);
     if (H->h_list_len) cudaFreeHost(H->h_list_len);
     train_free(H->train);
@@ -1820,6 +1888,7 @@ static int upload_frames(Handle* H, const sirius_frame* frames, int n, long long
     H->family_mask = 0;
     for (int i = 0; i < n; ++i) H->family_mask |= 1 << frames[i].metric.family;
     H->frame0 = fd[0];
+    H->frames_host = fd;
     int rc = ensure(H, H->d_frames, H->frames_cap, size_t(n));
     if (rc != SIRIUS_OK) return rc;
     CK(cudaMemcpyAsync(H->d_frames, fd.data(), n * sizeof(FrameDev), cudaMemcpyHostToDevice, H->stream));
@@ -1841,8 +1910,8 @@ int sirius_cuda_trace_frames(sirius_cuda_handle h, const sirius_frame* frames, i
     if (results && (rc = ensure(H, H->d_results, H->results_cap, size_t(total))) != SIRIUS_OK) return rc;
     if (image && (rc = ensure(H, H->d_image, H->image_cap, size_t(total))) != SIRIUS_OK) return rc;
     if (spectra && nb && (rc = ensure(H, H->d_spectra, H->spectra_cap, size_t(total) * nb)) != SIRIUS_OK) return rc;
-    rc = launch_trace(H, n_frames, total, results ? H->d_results : nullptr, image ? H->d_image : nullptr,
-                      (spectra && nb) ? H->d_spectra : nullptr, nullptr, st, true);
+    rc = launch_frames(H, n_frames, total, results ? H->d_results : nullptr, image ? H->d_image : nullptr,
+                       (spectra && nb) ? H->d_spectra : nullptr, st, true);
     if (rc != SIRIUS_OK) return rc;
     if (results) CK(cudaMemcpyAsync(results, H->d_results, size_t(total) * sizeof(sirius_ray_result), cudaMemcpyDeviceToHost, st));
     if (image) CK(cudaMemcpyAsync(image, H->d_image, size_t(total) * sizeof(float), cudaMemcpyDeviceToHost, st));
@@ -1870,7 +1939,7 @@ int sirius_cuda_trace_frames_device(sirius_cuda_handle h, const sirius_frame* d_
     if (rc != SIRIUS_OK) return rc;
     if (total != total_rays) return fail(H, SIRIUS_ERR_INVALID_ARGUMENT, "total_rays does not match the frames");
     CK(cudaEventRecord(H->ev[0], st));
-    rc = launch_trace(H, n_frames, total, d_results, d_image, d_spectra, nullptr, st, true);
+    rc = launch_frames(H, n_frames, total, d_results, d_image, d_spectra, st, true);
     if (rc != SIRIUS_OK) return rc;
     CK(cudaEventRecord(H->ev[3], st));
     H->pending = true;
@@ -1889,6 +1958,8 @@ int sirius_cuda_trace_frames_static(sirius_cuda_handle h, const sirius_frame* d_
                                                     "SIRIUS_STATIC_MAX_FRAMES (64) frames per call");
     if (H->device < 0 || H->device >= kStaticMaxDevices)
         return fail(H, SIRIUS_ERR_INVALID_ARGUMENT, "device ordinal beyond the static scratch table");
+    if (H->cfg.samples_per_pixel > 1)
+        return fail(H, SIRIUS_ERR_UNSUPPORTED, "sirius_cuda_trace_frames_static traces one sample per pixel");
     CK(cudaSetDevice(H->device));
     StaticScratch* scratch = static_scratch(H->device);
     if (!scratch) return fail(H, SIRIUS_ERR_CUDA, "cudaGetSymbolAddress failed for the static scratch");

@@ -34,6 +34,7 @@ struct FrameDev {
     // the camera's Kerr-Schild position and the four tetrad vectors e_(t),
     // e_(r), e_(theta), e_(phi) in Kerr-Schild contravariant components
     int observer;
+    float sub_u, sub_v;  // sub-pixel position of the ray through a pixel (0.5, 0.5: the centre)
     double zx[4];
     double ze[16];  // ze[4 i + mu]: vector i, component mu
 };
@@ -127,8 +128,8 @@ __device__ double nt_flux(double r, double a, double isco, double r_in, double r
 __device__ __forceinline__ void camera_dir(const FrameDev& F, int px, int py, double dir[4]) {
     dir[0] = 0.0;
     if (F.projection == SIRIUS_CAMERA_EQUIRECTANGULAR) {
-        const double psi = (2.0 * (px + 0.5) / F.width - 1.0) * kPi;
-        const double chi = (1.0 - 2.0 * (py + 0.5) / F.height) * (0.5 * kPi);
+        const double psi = (2.0 * (px + double(F.sub_u)) / F.width - 1.0) * kPi;
+        const double chi = (1.0 - 2.0 * (py + double(F.sub_v)) / F.height) * (0.5 * kPi);
         double sc, cc, sps, cps;
         sincos(chi, &sc, &cc);
         sincos(psi, &sps, &cps);
@@ -138,8 +139,8 @@ __device__ __forceinline__ void camera_dir(const FrameDev& F, int px, int py, do
         return;
     }
     const float w = float(F.width), hgt = float(F.height);
-    const float pxn = __fmul_rn(__fsub_rn(__fdiv_rn(__fmul_rn(2.0f, __fadd_rn(float(px), 0.5f)), w), 1.0f), F.aspect);
-    const float pyn = __fsub_rn(1.0f, __fdiv_rn(__fmul_rn(2.0f, __fadd_rn(float(py), 0.5f)), hgt));
+    const float pxn = __fmul_rn(__fsub_rn(__fdiv_rn(__fmul_rn(2.0f, __fadd_rn(float(px), F.sub_u)), w), 1.0f), F.aspect);
+    const float pyn = __fsub_rn(1.0f, __fdiv_rn(__fmul_rn(2.0f, __fadd_rn(float(py), F.sub_v)), hgt));
     const float dx = __fmul_rn(pxn, F.tan_half_fov), dy = __fmul_rn(pyn, F.tan_half_fov), dz = -1.0f;
     const float rx = __fsub_rn(__fmul_rn(dx, F.cR), __fmul_rn(dy, F.sR));
     const float ry = __fadd_rn(__fmul_rn(dx, F.sR), __fmul_rn(dy, F.cR));

@@ -130,7 +130,29 @@ def main():
     # 5. AccretionDiskD::computeISCO
     spins = np.array([0.0, 0.5, 0.9, 0.998, -0.5, -0.998])
     np.savez_compressed(os.path.join(OUT, "isco.npz"), spin=spins, isco=np.array([ref.isco(s) for s in spins]))
+    camera_subpixel(ref)
     print("golden fixtures written to", OUT)
+
+
+def camera_subpixel(ref):
+    """6. PinholeCamera::generateRay(x, y, u, v) at the stratified sub-pixel positions
+    RenderSession::shadePixel uses ((s + 0.5) / g for g = 2, 3, 8) and at random (u, v)."""
+    from sirius_b200 import abi
+    rng = np.random.default_rng(20261204)
+    cam = abi.make_camera(r=20.0, theta_deg=30.0, fov=45.0, width=320, height=200, yaw=0.1, pitch=-0.2, roll=0.3)
+    px = rng.integers(0, cam.width, 256).astype(np.int32)
+    py = rng.integers(0, cam.height, 256).astype(np.int32)
+    grid = []
+    for g in (2, 3, 8):
+        s = np.arange(g, dtype=np.float32)
+        grid.append((s + np.float32(0.5)) / np.float32(g))
+    pool = np.concatenate(grid)
+    u = np.concatenate([rng.choice(pool, 128), rng.uniform(0, 1, 128)]).astype(np.float32)
+    v = np.concatenate([rng.choice(pool, 128), rng.uniform(0, 1, 128)]).astype(np.float32)
+    o, d = ref.camera_rays_uv(cam, px, py, u, v)
+    np.savez_compressed(os.path.join(OUT, "camera_uv.npz"),
+                        cam=np.array([cam.r, cam.theta, cam.phi, cam.fov, cam.width, cam.height, cam.yaw, cam.pitch,
+                                      cam.roll]), px=px, py=py, u=u, v=v, origin=o, dir=d)
 
 
 if __name__ == "__main__":

@@ -144,3 +144,14 @@ def test_live_reference_random_rays(oracle):
         np.testing.assert_array_equal(res["steps"], recs["steps_taken"])
         esc = recs["outcome"] == abi.ESCAPED
         np.testing.assert_array_equal(res["final_x"][esc], recs["final_position"][esc])
+
+
+def test_subpixel_camera_matches_reference(oracle):
+    """PinholeCamera::generateRay(x, y, u, v) (CMBS001A.h:120) at sub-pixel positions, bit for bit."""
+    d = golden("camera_uv.npz")
+    r, th, ph, fov, w, h, yaw, pitch, roll = d["cam"]
+    cam = abi.Camera(0.0, r, th, ph, yaw, pitch, roll, fov, int(w), int(h), 0, 0)
+    for i in range(len(d["px"])):
+        o, dd = oracle.camera_ray(cam, int(d["px"][i]), int(d["py"][i]), float(d["u"][i]), float(d["v"][i]))
+        np.testing.assert_array_equal(o, d["origin"][i])
+        np.testing.assert_array_equal(dd, d["dir"][i])
