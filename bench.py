@@ -349,6 +349,28 @@ def surrogate_leg(eng, abi, np, torch, dev, stream, side=SURROGATE_SIDE, reps=3)
             "weights": "sirius_b200/data/surrogate_kerr.npy (python -m sirius_b200.surrogate_train)"}
 
 
+def beam_leg(eng, abi, side=256):
+    """Beams (ray + two tangent vectors, FP64 Dormand-Prince) over the Kerr
+    a = 0.9 workload camera at side^2; host-timed call (the call synchronises),
+    with the magnification range of the escaped rays."""
+    import numpy as np
+    cfg = abi.default_config(abs_tolerance=1e-8, rel_tolerance=1e-8, min_step=1e-9, max_step=2.0, initial_step=0.1,
+                             escape_radius=1000.0, horizon_factor=1.01, max_steps=20000,
+                             precision=abi.PRECISION_FP64, enable_disk=0)
+    eng.configure(cfg)
+    fr = workload_frame(abi, side, side)
+    eng.trace_beams([fr])
+    t0 = time.perf_counter()
+    b = eng.trace_beams([fr])
+    dt = time.perf_counter() - t0
+    esc = b["outcome"] == abi.ESCAPED
+    return {"workload": f"kerr_a0.9_{side}x{side}_beams_fp64", "rays": int(b.size), "seconds": dt,
+            "mbeams_per_s": b.size / dt / 1e6, "escaped": int(esc.sum()),
+            "magnification_p50_p99": [float(np.percentile(b["magnification"][esc], 50)),
+                                      float(np.percentile(b["magnification"][esc], 99))],
+            "negative_parity_fraction": float(np.mean(b["parity"][esc] < 0)), "timing": "host clock around the call"}
+
+
 TRAIN_FLOP_PER_ROW = 3 * 2 * 198912 - 2 * 5 * 256  # forward, dW and dH (no dH for the input layer)
 
 
@@ -538,6 +560,7 @@ def main():
                                  "spectra_p99_rel": float(np.percentile(serr, 99))}
         line["surrogate"] = surrogate_leg(eng, abi, np, torch, dev, stream)
         line["surrogate_training"] = train_leg(eng, abi, np, torch, dev)
+        line["beams"] = beam_leg(eng, abi)
         line["heterogeneous_batch"] = batch_leg(eng, abi)
         line["stress_symplectic"] = stress_leg(eng, abi)
         line["cpu_baseline"] = cpu_baseline_sample()

@@ -399,6 +399,28 @@ int sirius_cuda_train_gradient(sirius_cuda_handle handle, const float* d_feature
 /* the FP32 master weights (host) and the optimiser steps taken */
 int sirius_cuda_train_params(sirius_cuda_handle handle, float* params, int64_t* steps);
 
+/* ---- beams: geodesic deviation around each pixel ray -------------------------
+ * The counterpart of BeamIntegratorD (INBI001A.h:178-363), on the engine's
+ * Hamiltonian form: each pixel's ray (FP64, Dormand-Prince 5(4) with the
+ * configured tolerances, whatever the precision setting) carries the two
+ * tangent vectors dy/du, dy/dv of its state with respect to its start in pixel
+ * coordinates (the linearised geodesic equation). For an escaped ray,
+ * magnification = |dd/du x dd/dv| / |dn/du x dn/dv|: the solid angle of the
+ * pixel in the camera frame over the solid angle it covers on the sky (d the
+ * start direction, n the escape direction); 1 in flat space. Kerr-Schild
+ * family only; host frames and results (one per pixel); synchronous. */
+typedef struct {
+    int32_t outcome;             /* SIRIUS_ESCAPED, HORIZON, DISK_HIT, MAX_STEPS or NUMERICAL_FAILURE */
+    int32_t steps;               /* accepted steps */
+    float magnification;         /* escaped rays; 0 otherwise */
+    float parity;                /* escaped rays: +1 direct image, -1 mirror-reversed; 0 otherwise */
+    float final_dir[3];          /* escaped rays: unit escape direction (Kerr-Schild Cartesian) */
+    int32_t reserved;
+} sirius_beam_result;
+
+int sirius_cuda_trace_beams(sirius_cuda_handle handle, const sirius_frame* frames, int32_t n_frames,
+                            sirius_beam_result* results);
+
 /* ---- image output of a headless frame buffer ---------------------------------
  * Host functions (no handle, no device): row-major float pixels, top row first.
  * Pixel conversions as the reference's output drivers:

@@ -686,6 +686,37 @@ inline void camera_ray(const sirius_camera& cam, int px, int py, double origin[4
     dir[3] = rx2 / len;
 }
 
+// The same pinhole and equirectangular mappings at a fractional pixel position
+// (u, v) evaluated in FP64 after the camera's FP32 constants (aspect, tan of
+// half the field of view, the rotation cosines and sines): smooth in (u, v),
+// for derivatives of the image mapping (the beam checks).
+inline void camera_ray_exact(const sirius_camera& cam, double u, double v, double origin[4], double dir[4]) {
+    origin[0] = cam.t; origin[1] = cam.r; origin[2] = cam.theta; origin[3] = cam.phi;
+    dir[0] = 0.0;
+    if (cam.projection == SIRIUS_CAMERA_EQUIRECTANGULAR) {
+        const double psi = (2.0 * u / cam.width - 1.0) * kPi;
+        const double chi = (1.0 - 2.0 * v / cam.height) * (0.5 * kPi);
+        dir[1] = -std::cos(chi) * std::cos(psi);
+        dir[2] = -std::sin(chi);
+        dir[3] = std::cos(chi) * std::sin(psi);
+        return;
+    }
+    const float aspect = float(cam.width) / float(cam.height);
+    const float tanh = std::tan(cam.fov * float(kPi) / 360.0f);
+    const double pxn = (2.0 * u / cam.width - 1.0) * double(aspect), pyn = 1.0 - 2.0 * v / cam.height;
+    const double dx = pxn * double(tanh), dy = pyn * double(tanh), dz = -1.0;
+    const double cY = std::cos(cam.yaw), sY = std::sin(cam.yaw);
+    const double cP = std::cos(cam.pitch), sP = std::sin(cam.pitch);
+    const double cR = std::cos(cam.roll), sR = std::sin(cam.roll);
+    const double rx = dx * cR - dy * sR, ry = dx * sR + dy * cR;
+    const double ry2 = ry * cP - dz * sP, rz = ry * sP + dz * cP;
+    const double rx2 = rx * cY + rz * sY, rz2 = -rx * sY + rz * cY;
+    const double len = std::sqrt(rx2 * rx2 + ry2 * ry2 + rz2 * rz2);
+    dir[1] = rz2 / len;
+    dir[2] = -ry2 / len;
+    dir[3] = rx2 / len;
+}
+
 // ---------------------------------------------------------------------------
 // Ray tracing (GeodesicTracer::trace, GTRC001A.cpp:139-592)
 // ---------------------------------------------------------------------------

@@ -86,6 +86,12 @@ int oracle_trace_rays(const sirius_metric* m, double disk_inner, double disk_out
     return 0;
 }
 
+// the camera mapping in FP64 at a fractional pixel position (u, v in pixel units)
+int oracle_camera_ray_exact(const sirius_camera* cam, double u, double v, double* origin, double* dir) {
+    camera_ray_exact(*cam, u, v, origin, dir);
+    return 0;
+}
+
 // PinholeCamera::generateRay(x, y, u, v) (CMBS001A.h:120): the ray through sub-pixel (u, v)
 int oracle_camera_ray_uv(const sirius_camera* cam, int px, int py, float u, float v, double* origin, double* dir) {
     camera_ray(*cam, px, py, origin, dir, u, v);

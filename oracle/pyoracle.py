@@ -33,6 +33,7 @@ class Oracle:
         L.oracle_camera_ray.argtypes = [_P(abi.Camera), C.c_int, C.c_int, C.c_void_p, C.c_void_p]
         L.oracle_camera_ray_uv.argtypes = [_P(abi.Camera), C.c_int, C.c_int, C.c_float, C.c_float, C.c_void_p,
                                            C.c_void_p]
+        L.oracle_camera_ray_exact.argtypes = [_P(abi.Camera), C.c_double, C.c_double, C.c_void_p, C.c_void_p]
         L.oracle_metric_evaluate.argtypes = [_P(abi.Metric), C.c_void_p, C.c_int64, C.c_void_p, C.c_void_p]
         L.oracle_invert4x4.argtypes = [C.c_void_p, C.c_void_p]
         L.oracle_rhs.argtypes = [_P(abi.Metric), C.c_void_p, C.c_int64, C.c_void_p, C.c_int]
@@ -88,6 +89,13 @@ class Oracle:
         d = np.zeros(4)
         self.lib.oracle_camera_ray_uv(C.byref(cam), px, py, C.c_float(u), C.c_float(v), o.ctypes.data,
                                       d.ctypes.data)
+        return o, d
+
+    def camera_ray_exact(self, cam, u, v):
+        """The camera mapping in FP64 at fractional pixel position (u, v)."""
+        o = np.zeros(4)
+        d = np.zeros(4)
+        self.lib.oracle_camera_ray_exact(C.byref(cam), u, v, o.ctypes.data, d.ctypes.data)
         return o, d
 
     def metric_evaluate(self, metric, pos):

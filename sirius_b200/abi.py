@@ -131,6 +131,11 @@ def surrogate_config(gate_band=0.3, audit_fraction=0.01, audit_seed=0):
     return SurrogateConfig(gate_band, audit_fraction, audit_seed)
 
 
+class BeamResult(C.Structure):
+    _fields_ = [("outcome", C.c_int32), ("steps", C.c_int32), ("magnification", C.c_float), ("parity", C.c_float),
+                ("final_dir", C.c_float * 3), ("reserved", C.c_int32)]
+
+
 class TrainConfig(C.Structure):
     _fields_ = [("batch", C.c_int32), ("reserved0", C.c_int32), ("total_steps", C.c_int64), ("max_lr", C.c_float),
                 ("warmup_fraction", C.c_float), ("beta1", C.c_float), ("beta2", C.c_float), ("eps", C.c_float),

@@ -37,6 +37,7 @@ static_assert(sizeof(sirius_camera_ray) == 64, "sirius_camera_ray layout");
 static_assert(sizeof(sirius_surrogate_config) == 40, "sirius_surrogate_config layout");
 static_assert(sizeof(sirius_surrogate_stats) == 48, "sirius_surrogate_stats layout");
 static_assert(sizeof(sirius_train_config) == 64, "sirius_train_config layout");
+static_assert(sizeof(sirius_beam_result) == 32, "sirius_beam_result layout");
 
 namespace {
 
@@ -1000,6 +1001,8 @@ __global__ void sur_shade_kernel(const FrameDev* frames, int n_frames, long long
     if (image_mlp) image_mlp[idx] = float(I);
 }
 
+#include "beam.cuh"
+
 // multi-sample passes: sum += pass (the first pass copies), then out = sum * scale
 __global__ void pass_accumulate_kernel(const float* pass, float* sum, long long n, int first) {
     const long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x;
@@ -1945,6 +1948,45 @@ int sirius_cuda_trace_frames_device(sirius_cuda_handle h, const sirius_frame* d_
     H->pending = true;
     H->pending_stream = st;
     H->pending_total = total;
+    return SIRIUS_OK;
+}
+
+int sirius_cuda_trace_beams(sirius_cuda_handle h, const sirius_frame* frames, int32_t n_frames,
+                            sirius_beam_result* results) {
+    Handle* H = static_cast<Handle*>(h);
+    if (!H || !frames || n_frames <= 0 || !results) return SIRIUS_ERR_INVALID_ARGUMENT;
+    if (!H->configured) return fail(H, SIRIUS_ERR_NOT_CONFIGURED, "sirius_cuda_configure has not been called");
+    for (int i = 0; i < n_frames; ++i)
+        if (frames[i].metric.family != SIRIUS_METRIC_KERR_SCHILD)
+            return fail(H, SIRIUS_ERR_UNSUPPORTED, "beams are traced for the Kerr-Schild family");
+    CK(cudaSetDevice(H->device));
+    long long total = 0;
+    int rc = upload_frames(H, frames, n_frames, &total);
+    if (rc != SIRIUS_OK) return rc;
+    sirius_beam_result* d_out = nullptr;
+    CK(cudaMalloc((void**)&d_out, size_t(total) * sizeof(sirius_beam_result)));
+    BeamParams B{};
+    B.frames = H->d_frames;
+    B.n_frames = n_frames;
+    B.total = total;
+    B.c = make_cfg(H->cfg);
+    B.out = d_out;
+    B.watchdog_ns = H->cfg.watchdog_ms > 0 ? (unsigned long long)H->cfg.watchdog_ms * 1000000ull : ~0ull;
+    B.status = H->d_status;
+    cudaError_t e = cudaMemsetAsync(H->d_status, 0, sizeof(int), H->stream);
+    if (e == cudaSuccess) {
+        beam_kernel<<<int((total + 63) / 64), 64, 0, H->stream>>>(B);
+        e = cudaGetLastError();
+    }
+    int status = 0;
+    if (e == cudaSuccess)
+        e = cudaMemcpyAsync(results, d_out, size_t(total) * sizeof(sirius_beam_result), cudaMemcpyDeviceToHost,
+                            H->stream);
+    if (e == cudaSuccess) e = cudaMemcpyAsync(&status, H->d_status, sizeof(int), cudaMemcpyDeviceToHost, H->stream);
+    if (e == cudaSuccess) e = cudaStreamSynchronize(H->stream);
+    cudaFree(d_out);
+    if (e != cudaSuccess) return fail(H, SIRIUS_ERR_CUDA, std::string("beam trace: ") + cudaGetErrorString(e));
+    if (status & 1) return fail(H, SIRIUS_ERR_TIMEOUT, "beam kernel stopped by its watchdog");
     return SIRIUS_OK;
 }
 

@@ -27,6 +27,7 @@ EXPORTS = [
     "sirius_cuda_render_surrogate_device", "sirius_cuda_default_train_config", "sirius_cuda_train_init",
     "sirius_cuda_train_steps", "sirius_cuda_train_evaluate", "sirius_cuda_train_gradient", "sirius_cuda_train_params",
     "sirius_cuda_write_png", "sirius_cuda_write_exr", "sirius_cuda_write_pfm", "sirius_cuda_write_ppm",
+    "sirius_cuda_trace_beams",
 ]
 
 
@@ -80,6 +81,7 @@ def load_library(path=LIB_PATH):
     L.sirius_cuda_train_gradient.argtypes = [C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p, C.c_int64, C.c_void_p,
                                              C.c_void_p]
     L.sirius_cuda_train_params.argtypes = [C.c_void_p, C.c_void_p, _P(C.c_int64)]
+    L.sirius_cuda_trace_beams.argtypes = [C.c_void_p, C.c_void_p, C.c_int32, C.c_void_p]
     for name in ("sirius_cuda_write_png", "sirius_cuda_write_exr"):
         getattr(L, name).argtypes = [C.c_char_p, C.c_int32, C.c_int32, C.c_int32, C.c_void_p]
     for name in ("sirius_cuda_write_pfm", "sirius_cuda_write_ppm"):
@@ -196,6 +198,16 @@ class Engine:
     def surrogate_infer(self, d_features, n, d_out, stream=None):
         """MLP on n x 5 device features into n x 4 device outputs."""
         self._check(self.lib.sirius_cuda_surrogate_infer(self.h, d_features, n, d_out, stream))
+
+    def trace_beams(self, frames):
+        """Beams around every pixel ray of the frames: a structured array of BeamResult
+        (outcome, steps, magnification, parity, final_dir)."""
+        arr, total = frames_array(frames)
+        out = (abi.BeamResult * total)()
+        self._check(self.lib.sirius_cuda_trace_beams(self.h, C.addressof(arr), len(frames), C.addressof(out)))
+        dt = np.dtype([("outcome", "<i4"), ("steps", "<i4"), ("magnification", "<f4"), ("parity", "<f4"),
+                       ("final_dir", "<f4", (3,)), ("reserved", "<i4")])
+        return np.frombuffer(bytes(out), dtype=dt).copy()
 
     def train_init(self, params, config):
         """Start training from params (SURROGATE_PARAMS floats): FP32 master weights, zero Adam moments."""
