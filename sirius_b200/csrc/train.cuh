@@ -29,7 +29,8 @@
 // transposed in registers (byte permutes), so the tensor core always sees the
 // K-major layout of tcgen05.cuh. One thread issues tcgen05.mma (M 128, N BN,
 // K 16) per 16 columns of the chunk and commits the chunk to its stage's
-// mbarrier; the loads of the next chunk overlap those MMAs. The weight
+// mbarrier; each thread fetches its share of the next chunk into registers
+// before those MMAs are issued, so the loads overlap them. The weight
 // gradients split K (the batch) over CTAs and add their partial tiles with
 // FP32 vector atomics. Every mbarrier wait is bounded by the device clock.
 //
@@ -125,37 +126,71 @@ __device__ __forceinline__ uint32_t word_of(const uint4& v, int w) {
     return w == 0 ? v.x : w == 1 ? v.y : w == 2 ? v.z : v.w;
 }
 
-// R rows x kw columns (kw a multiple of 16, at most 64) of an operand into the
-// K-major core-matrix layout of a 64-column stage (SBO 1024 bytes).
-__device__ __forceinline__ void load_operand(unsigned char* dst, const Operand& op, int row0, int R, int k0, int kw) {
+// An operand chunk (R rows x kw columns, kw a multiple of 16, at most 64) goes
+// into the K-major core-matrix layout of a 64-column stage (SBO 1024 bytes).
+// The copy comes in two parts, for software pipelining: fetch_operand loads
+// this thread's share of a chunk into registers (N uint4: K-major pieces,
+// or N / 8 eight-row blocks of an M-major source), stash_operand writes them
+// to shared memory. The next chunk's loads are then in flight while the
+// tensor core works on the current one.
+template <int N>
+__device__ __forceinline__ void fetch_operand(uint4 (&buf)[N], const Operand& op, int row0, int R, int k0, int kw) {
+    const uint4 zero = make_uint4(0, 0, 0, 0);
     if (op.kmajor) {
-        const int per_row = kw / 8;
-        for (int q = threadIdx.x; q < R * per_row; q += kGemmThreads) {
-            const int r = q / per_row, kg = q - r * per_row;
-            const int gr = row0 + r;
-            uint4 v = make_uint4(0, 0, 0, 0);
-            if (gr < op.rows) v = ldg16(op.p + (long long)gr * op.ld + k0 + kg * 8);
-            *reinterpret_cast<uint4*>(dst + packed_offset(r, kg * 8, kBK)) = v;
+        const int per_row = kw / 8, n = R * per_row;
+#pragma unroll
+        for (int j = 0; j < N; ++j) {
+            const int q = threadIdx.x + kGemmThreads * j;
+            buf[j] = zero;
+            if (q < n) {
+                const int r = q / per_row, kg = q - r * per_row;
+                if (row0 + r < op.rows) buf[j] = ldg16(op.p + (long long)(row0 + r) * op.ld + k0 + kg * 8);
+            }
         }
     } else {
-        const int rg_n = R / 8, kg_n = kw / 8;
-        for (int u = threadIdx.x; u < rg_n * kg_n; u += kGemmThreads) {
-            const int kg = u / rg_n, rg = u - kg * rg_n;
-            const int gr = row0 + rg * 8;
-            uint4 c[8];
+        const int rg_n = R / 8, n = rg_n * (kw / 8);
+#pragma unroll
+        for (int j = 0; j < N / 8; ++j) {
+            const int u = threadIdx.x + kGemmThreads * j;
+            const int kg = u / rg_n, gr = row0 + (u - kg * rg_n) * 8;
+            const bool live = u < n && gr < op.rows;
 #pragma unroll
             for (int i = 0; i < 8; ++i)
-                c[i] = gr < op.rows ? ldg16(op.p + (long long)(k0 + kg * 8 + i) * op.ld + gr) : make_uint4(0, 0, 0, 0);
+                buf[8 * j + i] = live ? ldg16(op.p + (long long)(k0 + kg * 8 + i) * op.ld + gr) : zero;
+        }
+    }
+}
+
+template <int N>
+__device__ __forceinline__ void stash_operand(unsigned char* dst, const uint4 (&buf)[N], const Operand& op, int R,
+                                              int kw) {
+    if (op.kmajor) {
+        const int per_row = kw / 8, n = R * per_row;
 #pragma unroll
-            for (int j = 0; j < 8; ++j) {  // core-matrix row j: element j of each of the 8 K rows
-                const int w = j >> 1;
-                const uint32_t sel = (j & 1) ? 0x7632u : 0x5410u;
+        for (int j = 0; j < N; ++j) {
+            const int q = threadIdx.x + kGemmThreads * j;
+            if (q < n) {
+                const int r = q / per_row, kg = q - r * per_row;
+                *reinterpret_cast<uint4*>(dst + packed_offset(r, kg * 8, kBK)) = buf[j];
+            }
+        }
+    } else {
+        const int rg_n = R / 8, n = rg_n * (kw / 8);
+#pragma unroll
+        for (int j = 0; j < N / 8; ++j) {
+            const int u = threadIdx.x + kGemmThreads * j;
+            if (u >= n) continue;
+            const int kg = u / rg_n, rg = u - kg * rg_n;
+#pragma unroll
+            for (int jj = 0; jj < 8; ++jj) {  // core-matrix row jj: element jj of each of the 8 K rows
+                const int w = jj >> 1;
+                const uint32_t sel = (jj & 1) ? 0x7632u : 0x5410u;
                 uint4 o;
-                o.x = __byte_perm(word_of(c[0], w), word_of(c[1], w), sel);
-                o.y = __byte_perm(word_of(c[2], w), word_of(c[3], w), sel);
-                o.z = __byte_perm(word_of(c[4], w), word_of(c[5], w), sel);
-                o.w = __byte_perm(word_of(c[6], w), word_of(c[7], w), sel);
-                *reinterpret_cast<uint4*>(dst + packed_offset(rg * 8 + j, kg * 8, kBK)) = o;
+                o.x = __byte_perm(word_of(buf[8 * j + 0], w), word_of(buf[8 * j + 1], w), sel);
+                o.y = __byte_perm(word_of(buf[8 * j + 2], w), word_of(buf[8 * j + 3], w), sel);
+                o.z = __byte_perm(word_of(buf[8 * j + 4], w), word_of(buf[8 * j + 5], w), sel);
+                o.w = __byte_perm(word_of(buf[8 * j + 6], w), word_of(buf[8 * j + 7], w), sel);
+                *reinterpret_cast<uint4*>(dst + packed_offset(rg * 8 + jj, kg * 8, kBK)) = o;
             }
         }
     }
@@ -295,6 +330,12 @@ __global__ void __launch_bounds__(kGemmThreads) gemm_kernel(const __grid_constan
     uint32_t ph = 0, pending = 0;  // per stage: wait parity, a commit not yet waited for
     bool ok = true;
     int chunk = 0;
+    constexpr int NA = 8, NB = BN >= 256 ? 16 : 8;  // this thread's share of a chunk (uint4)
+    uint4 ra[NA], rb[NB];
+    if (kbeg < kend) {
+        fetch_operand(ra, g.a, m0, kBM, kbeg, min(kBK, kend - kbeg));
+        fetch_operand(rb, g.b, n0, BN, kbeg, min(kBK, kend - kbeg));
+    }
     for (int k0 = kbeg; k0 < kend; k0 += kBK, ++chunk) {
         const int s = chunk % kStages;
         const int kw = min(kBK, kend - k0);
@@ -307,8 +348,12 @@ __global__ void __launch_bounds__(kGemmThreads) gemm_kernel(const __grid_constan
         }
         unsigned char* As = sm + s * S::Stage;
         unsigned char* Bs = As + S::A;
-        load_operand(As, g.a, m0, kBM, k0, kw);
-        load_operand(Bs, g.b, n0, BN, k0, kw);
+        stash_operand(As, ra, g.a, kBM, kw);
+        stash_operand(Bs, rb, g.b, BN, kw);
+        if (k0 + kBK < kend) {  // the next chunk's loads fly while this one multiplies
+            fetch_operand(ra, g.a, m0, kBM, k0 + kBK, min(kBK, kend - k0 - kBK));
+            fetch_operand(rb, g.b, n0, BN, k0 + kBK, min(kBK, kend - k0 - kBK));
+        }
         fence_async_smem();
         __syncthreads();
         if (tid == 0) {
