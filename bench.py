@@ -367,6 +367,43 @@ def surrogate_leg(eng, abi, np, torch, dev, stream, side=SURROGATE_SIDE, reps=3)
             "weights": "sirius_b200/data/surrogate_kerr.npy (python -m sirius_b200.surrogate_train)"}
 
 
+def graph_leg(eng, abi, torch, dev, side=128, reps=50):
+    """Small frames, where launch overhead shows: the prepared launch sequence
+    (memsets, flux tables, trace kernel) issued call by call vs replayed from a
+    captured CUDA graph; CUDA events around `reps` back-to-back frames."""
+    eng.configure(workload_config(abi, abi.PRECISION_MIXED))
+    fr = workload_frame(abi, side, side)
+    total = eng.prepare_frames([fr])
+    d_img = torch.empty(total, dtype=torch.float32, device=dev)
+    s = torch.cuda.Stream(device=dev)
+    s.wait_stream(torch.cuda.current_stream(dev))
+    ev0, ev1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    with torch.cuda.stream(s):
+        for _ in range(3):
+            eng.launch_prepared(None, d_img.data_ptr(), None, s.cuda_stream)
+        ev0.record(s)
+        for _ in range(reps):
+            eng.launch_prepared(None, d_img.data_ptr(), None, s.cuda_stream)
+        ev1.record(s)
+    torch.cuda.synchronize(dev)
+    direct = ev0.elapsed_time(ev1) / reps
+    g = torch.cuda.CUDAGraph()
+    with torch.cuda.graph(g):
+        eng.launch_prepared(None, d_img.data_ptr(), None, torch.cuda.current_stream(dev).cuda_stream)
+    g.replay()
+    torch.cuda.synchronize(dev)
+    st = torch.cuda.current_stream(dev)
+    ev0.record(st)
+    for _ in range(reps):
+        g.replay()
+    ev1.record(st)
+    torch.cuda.synchronize(dev)
+    replay = ev0.elapsed_time(ev1) / reps
+    del g
+    return {"workload": f"kerr_a0.9_{side}x{side}_mixed_prepared", "frames": reps, "ms_per_frame_direct": direct,
+            "ms_per_frame_graph": replay}
+
+
 def beam_leg(eng, abi, side=256):
     """Beams (ray + two tangent vectors, FP64 Dormand-Prince) over the Kerr
     a = 0.9 workload camera at side^2; host-timed call (the call synchronises),
@@ -579,6 +616,7 @@ def main():
         line["surrogate"] = surrogate_leg(eng, abi, np, torch, dev, stream)
         line["surrogate_training"] = train_leg(eng, abi, np, torch, dev)
         line["beams"] = beam_leg(eng, abi)
+        line["graph_replay"] = graph_leg(eng, abi, torch, dev)
         line["heterogeneous_batch"] = batch_leg(eng, abi)
         line["stress_symplectic"] = stress_leg(eng, abi)
         line["cpu_baseline"] = cpu_baseline_sample()

@@ -399,6 +399,23 @@ int sirius_cuda_train_gradient(sirius_cuda_handle handle, const float* d_feature
 /* the FP32 master weights (host) and the optimiser steps taken */
 int sirius_cuda_train_params(sirius_cuda_handle handle, float* params, int64_t* steps);
 
+/* ---- prepared frames: a launch sequence for CUDA graph capture ------------------
+ * (no counterpart in the reference) prepare_frames does the host work of a
+ * frame batch once: it validates the frames and uploads their descriptors into
+ * scratch that belongs to the prepared batch (descriptors, queue and counter
+ * words, status word, flux tables); synchronous. launch_prepared then issues
+ * the trace of those frames on `stream` as device work only (memsets and
+ * kernels: no allocation, no host synchronisation, no statistics), so a caller
+ * can capture it in a CUDA graph and replay the graph. The prepared scratch
+ * lives until the next prepare_frames or destroy; a graph captured before
+ * either of those must not be replayed after it. A captured graph renders the
+ * configuration in force when it was captured. One sample per pixel
+ * (samples_per_pixel > 1 is refused). Outputs as sirius_cuda_trace_frames_device. */
+int sirius_cuda_prepare_frames(sirius_cuda_handle handle, const sirius_frame* frames, int32_t n_frames,
+                               int64_t* total_rays);
+int sirius_cuda_launch_prepared(sirius_cuda_handle handle, sirius_ray_result* d_results, float* d_image,
+                                float* d_spectra, void* stream);
+
 /* ---- beams: geodesic deviation around each pixel ray -------------------------
  * The counterpart of BeamIntegratorD (INBI001A.h:178-363), on the engine's
  * Hamiltonian form: each pixel's ray (FP64, Dormand-Prince 5(4) with the

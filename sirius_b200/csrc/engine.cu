@@ -1066,6 +1066,16 @@ __global__ void fma_peak_kernel(T* out, int iters, T seed) {
 // ---------------------------------------------------------------------------
 // Host side
 // ---------------------------------------------------------------------------
+// Device scratch of one launch: the frame descriptors, the queue cursor and
+// counters ([0] cursor, [1..3] counters, [4] launch start), the status word and
+// room for the per-frame disk flux tables (kFluxTable floats per frame).
+struct LaunchScratch {
+    const FrameDev* frames;
+    unsigned long long* queue;
+    int* status;
+    float* flux;
+};
+
 struct TrainState;
 
 struct Handle {
@@ -1098,6 +1108,17 @@ struct Handle {
     int family_mask = 0;  // bit f: a frame of the last upload is of metric family f
     FrameDev frame0{};    // the first frame of the last upload (a one-frame launch's parameter copy)
     std::vector<FrameDev> frames_host;  // the last upload's descriptors (multi-sample passes)
+    std::vector<FrameDev> pass_frames_host;  // ... with each pass's sub-pixel offset
+    FrameDev* d_pass_frames = nullptr;
+    size_t pass_frames_cap = 0;
+    // sirius_cuda_prepare_frames: the prepared launch's own scratch (descriptors,
+    // queue and counter words, status word, flux tables), released only by the
+    // next prepare or by destroy, so a captured graph's pointers stay valid
+    unsigned char* d_prep = nullptr;
+    LaunchScratch prep{};
+    FrameDev prep_frame0{};
+    int prep_n_frames = 0, prep_family_mask = 0;
+    long long prep_total = 0;
     float* d_pass_image = nullptr;      // multi-sample: one pass's image and spectra, and their sums
     float* d_pass_spectra = nullptr;
     size_t pass_cap = 0;
@@ -1348,15 +1369,7 @@ int validate_config(Handle* H, const sirius_trace_config& c) {
 }
 
 // Launch the tracer over [0, total) of already-uploaded frames.
-// Device scratch of one launch: the frame descriptors, the queue cursor and
-// counters ([0] cursor, [1..3] counters, [4] launch start), the status word and
-// room for the per-frame disk flux tables (kFluxTable floats per frame).
-struct LaunchScratch {
-    const FrameDev* frames;
-    unsigned long long* queue;
-    int* status;
-    float* flux;
-};
+
 
 int launch_trace(Handle* H, int n_frames, long long total, sirius_ray_result* d_results, float* d_image,
                  float* d_spectra, const sirius_camera_ray* d_rays, cudaStream_t st, bool timed,
@@ -1465,18 +1478,17 @@ int launch_trace(Handle* H, int n_frames, long long total, sirius_ray_result* d_
     return SIRIUS_OK;
 }
 
-// The trace of the uploaded frames into the given outputs; with
-// samples_per_pixel > 1, one launch per sub-pixel offset of the g x g grid
-// (row by row), each into pass buffers, summed in that order and scaled by 1/g^2.
-int launch_frames(Handle* H, int n_frames, long long total, sirius_ray_result* d_results, float* d_image,
-                  float* d_spectra, cudaStream_t st, bool timed) {
-    const int spp = H->cfg.samples_per_pixel;
+int samples_grid(const sirius_trace_config& c) {
     int g = 1;
-    while ((g + 1) * (g + 1) <= spp) ++g;
-    if (g == 1) return launch_trace(H, n_frames, total, d_results, d_image, d_spectra, nullptr, st, timed);
-    if (d_results) return fail(H, SIRIUS_ERR_INVALID_ARGUMENT, "per-ray results need samples_per_pixel <= 1");
-    if (!d_image && !d_spectra) return SIRIUS_OK;
-    const int nb = H->cfg.enable_volumetric ? std::min(H->cfg.n_bins, SIRIUS_MAX_BINS) : 0;
+    while ((g + 1) * (g + 1) <= c.samples_per_pixel) ++g;
+    return g;
+}
+
+// Multi-sample pass buffers and the g x g variants of the uploaded frame
+// descriptors (one per sub-pixel offset, row by row) on the device.
+int prepare_passes(Handle* H, long long total, cudaStream_t st) {
+    const int g = samples_grid(H->cfg);
+    if (g == 1) return SIRIUS_OK;
     if (H->pass_cap < size_t(total)) {
         cudaFree(H->d_pass_image);
         cudaFree(H->d_pass_spectra);
@@ -1486,17 +1498,47 @@ int launch_frames(Handle* H, int n_frames, long long total, sirius_ray_result* d
         CK(cudaMalloc((void**)&H->d_pass_spectra, size_t(total) * SIRIUS_MAX_BINS * sizeof(float)));
         H->pass_cap = size_t(total);
     }
-    std::vector<FrameDev> fd = H->frames_host;
+    const size_t n = H->frames_host.size();
+    H->pass_frames_host.resize(size_t(g) * g * n);
+    for (int s = 0; s < g * g; ++s) {
+        const float u = (float(s % g) + 0.5f) / float(g), v = (float(s / g) + 0.5f) / float(g);
+        for (size_t i = 0; i < n; ++i) {
+            FrameDev f = H->frames_host[i];
+            f.sub_u = u;
+            f.sub_v = v;
+            H->pass_frames_host[size_t(s) * n + i] = f;
+        }
+    }
+    int rc = ensure(H, H->d_pass_frames, H->pass_frames_cap, H->pass_frames_host.size());
+    if (rc != SIRIUS_OK) return rc;
+    CK(cudaMemcpyAsync(H->d_pass_frames, H->pass_frames_host.data(), H->pass_frames_host.size() * sizeof(FrameDev),
+                       cudaMemcpyHostToDevice, st));
+    return SIRIUS_OK;
+}
+
+// The trace of the uploaded frames into the given outputs; with
+// samples_per_pixel > 1, one launch per sub-pixel offset of the g x g grid
+// (row by row), each into pass buffers, summed in that order and scaled by
+// 1/g^2. prepared: the pass descriptors are already on the device
+// (sirius_cuda_prepare_frames), so only stream work is issued.
+int launch_frames(Handle* H, int n_frames, long long total, sirius_ray_result* d_results, float* d_image,
+                  float* d_spectra, cudaStream_t st, bool timed, bool prepared = false) {
+    const int g = samples_grid(H->cfg);
+    if (g == 1) return launch_trace(H, n_frames, total, d_results, d_image, d_spectra, nullptr, st, timed);
+    if (d_results) return fail(H, SIRIUS_ERR_INVALID_ARGUMENT, "per-ray results need samples_per_pixel <= 1");
+    if (!d_image && !d_spectra) return SIRIUS_OK;
+    const int nb = H->cfg.enable_volumetric ? std::min(H->cfg.n_bins, SIRIUS_MAX_BINS) : 0;
+    if (!prepared) {
+        const int rc = prepare_passes(H, total, st);
+        if (rc != SIRIUS_OK) return rc;
+    }
+    const size_t n = size_t(n_frames);
     const int blocks = int((total + 255) / 256), sblocks = int((total * std::max(nb, 1) + 255) / 256);
     if (timed) CK(cudaEventRecord(H->ev[1], st));
     for (int s = 0; s < g * g; ++s) {
-        const float u = (float(s % g) + 0.5f) / float(g), v = (float(s / g) + 0.5f) / float(g);
-        for (auto& f : fd) {
-            f.sub_u = u;
-            f.sub_v = v;
-        }
-        H->frame0 = fd[0];
-        CK(cudaMemcpyAsync(H->d_frames, fd.data(), fd.size() * sizeof(FrameDev), cudaMemcpyHostToDevice, st));
+        H->frame0 = H->pass_frames_host[size_t(s) * n];
+        CK(cudaMemcpyAsync(H->d_frames, H->d_pass_frames + size_t(s) * n, n * sizeof(FrameDev),
+                           cudaMemcpyDeviceToDevice, st));
         int rc = launch_trace(H, n_frames, total, nullptr, d_image ? H->d_pass_image : nullptr,
                               (d_spectra && nb) ? H->d_pass_spectra : nullptr, nullptr, st, false);
         if (rc != SIRIUS_OK) return rc;
@@ -1842,7 +1884,7 @@ int sirius_cuda_destroy(sirius_cuda_handle h) {
     cudaFree(H->d_surrogate); cudaFree(H->d_sur_err);
     cudaFree(H->d_sur_frames); cudaFree(H->d_feat); cudaFree(H->d_mlp_out); cudaFree(H->d_list); cudaFree(H->d_gate);
     cudaFree(H->d_block_counts);
-    cudaFree(H->d_pass_image); cudaFree(H->d_pass_spectra);
+    cudaFree(H->d_pass_image); cudaFree(H->d_pass_spectra); cudaFree(H->d_pass_frames); cudaFree(H->d_prep);
     if (H->h_sur_frames) cudaFreeHost(H->h_sur_frames);
     if (H->h_list_len) cudaFreeHost(H->h_list_len);
     train_free(H->train);
@@ -1949,6 +1991,54 @@ int sirius_cuda_trace_frames_device(sirius_cuda_handle h, const sirius_frame* d_
     H->pending_stream = st;
     H->pending_total = total;
     return SIRIUS_OK;
+}
+
+int sirius_cuda_prepare_frames(sirius_cuda_handle h, const sirius_frame* frames, int32_t n_frames,
+                               int64_t* total_rays) {
+    Handle* H = static_cast<Handle*>(h);
+    if (!H || !frames || n_frames <= 0) return SIRIUS_ERR_INVALID_ARGUMENT;
+    if (!H->configured) return fail(H, SIRIUS_ERR_NOT_CONFIGURED, "sirius_cuda_configure has not been called");
+    if (H->cfg.samples_per_pixel > 1)
+        return fail(H, SIRIUS_ERR_UNSUPPORTED, "prepared frames trace one sample per pixel");
+    CK(cudaSetDevice(H->device));
+    long long total = 0;
+    int rc = upload_frames(H, frames, n_frames, &total);
+    if (rc != SIRIUS_OK) return rc;
+    CK(cudaStreamSynchronize(H->stream));
+    // one allocation: descriptors | queue words | status | flux tables (256-byte aligned parts)
+    auto up = [](size_t b) { return (b + 255) & ~size_t(255); };
+    const size_t o_q = up(size_t(n_frames) * sizeof(FrameDev)), o_s = o_q + up(8 * sizeof(unsigned long long)),
+                 o_f = o_s + up(sizeof(int)), bytes = o_f + size_t(n_frames) * kFluxTable * sizeof(float);
+    if (H->d_prep) CK(cudaFree(H->d_prep));
+    H->d_prep = nullptr;
+    H->prep_n_frames = 0;
+    CK(cudaMalloc((void**)&H->d_prep, bytes));
+    H->prep.frames = reinterpret_cast<FrameDev*>(H->d_prep);
+    H->prep.queue = reinterpret_cast<unsigned long long*>(H->d_prep + o_q);
+    H->prep.status = reinterpret_cast<int*>(H->d_prep + o_s);
+    H->prep.flux = reinterpret_cast<float*>(H->d_prep + o_f);
+    CK(cudaMemcpy(const_cast<FrameDev*>(H->prep.frames), H->frames_host.data(), size_t(n_frames) * sizeof(FrameDev),
+                  cudaMemcpyHostToDevice));
+    H->prep_frame0 = H->frames_host[0];
+    H->prep_n_frames = n_frames;
+    H->prep_family_mask = H->family_mask;
+    H->prep_total = total;
+    if (total_rays) *total_rays = total;
+    return SIRIUS_OK;
+}
+
+int sirius_cuda_launch_prepared(sirius_cuda_handle h, sirius_ray_result* d_results, float* d_image, float* d_spectra,
+                                void* stream) {
+    Handle* H = static_cast<Handle*>(h);
+    if (!H) return SIRIUS_ERR_INVALID_ARGUMENT;
+    if (H->prep_n_frames <= 0) return fail(H, SIRIUS_ERR_NOT_CONFIGURED, "sirius_cuda_prepare_frames has not been called");
+    if (H->cfg.samples_per_pixel > 1)
+        return fail(H, SIRIUS_ERR_UNSUPPORTED, "prepared frames trace one sample per pixel");
+    cudaStream_t st = stream ? static_cast<cudaStream_t>(stream) : cudaStreamLegacy;
+    H->frame0 = H->prep_frame0;
+    H->family_mask = H->prep_family_mask;
+    return launch_trace(H, H->prep_n_frames, H->prep_total, d_results, d_image, d_spectra, nullptr, st, false,
+                        &H->prep);
 }
 
 int sirius_cuda_trace_beams(sirius_cuda_handle h, const sirius_frame* frames, int32_t n_frames,

@@ -27,7 +27,7 @@ EXPORTS = [
     "sirius_cuda_render_surrogate_device", "sirius_cuda_default_train_config", "sirius_cuda_train_init",
     "sirius_cuda_train_steps", "sirius_cuda_train_evaluate", "sirius_cuda_train_gradient", "sirius_cuda_train_params",
     "sirius_cuda_write_png", "sirius_cuda_write_exr", "sirius_cuda_write_pfm", "sirius_cuda_write_ppm",
-    "sirius_cuda_trace_beams",
+    "sirius_cuda_trace_beams", "sirius_cuda_prepare_frames", "sirius_cuda_launch_prepared",
 ]
 
 
@@ -82,6 +82,8 @@ def load_library(path=LIB_PATH):
                                              C.c_void_p]
     L.sirius_cuda_train_params.argtypes = [C.c_void_p, C.c_void_p, _P(C.c_int64)]
     L.sirius_cuda_trace_beams.argtypes = [C.c_void_p, C.c_void_p, C.c_int32, C.c_void_p]
+    L.sirius_cuda_prepare_frames.argtypes = [C.c_void_p, C.c_void_p, C.c_int32, _P(C.c_int64)]
+    L.sirius_cuda_launch_prepared.argtypes = [C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p]
     for name in ("sirius_cuda_write_png", "sirius_cuda_write_exr"):
         getattr(L, name).argtypes = [C.c_char_p, C.c_int32, C.c_int32, C.c_int32, C.c_void_p]
     for name in ("sirius_cuda_write_pfm", "sirius_cuda_write_ppm"):
@@ -198,6 +200,17 @@ class Engine:
     def surrogate_infer(self, d_features, n, d_out, stream=None):
         """MLP on n x 5 device features into n x 4 device outputs."""
         self._check(self.lib.sirius_cuda_surrogate_infer(self.h, d_features, n, d_out, stream))
+
+    def prepare_frames(self, frames):
+        """Upload the frames for launch_prepared; returns the number of rays (pixels)."""
+        arr, _ = frames_array(frames)
+        total = C.c_int64()
+        self._check(self.lib.sirius_cuda_prepare_frames(self.h, C.addressof(arr), len(frames), C.byref(total)))
+        return total.value
+
+    def launch_prepared(self, d_results, d_image, d_spectra, stream):
+        """The trace of the prepared frames as stream work only (capturable in a CUDA graph)."""
+        self._check(self.lib.sirius_cuda_launch_prepared(self.h, d_results, d_image, d_spectra, stream))
 
     def trace_beams(self, frames):
         """Beams around every pixel ray of the frames: a structured array of BeamResult
