@@ -341,7 +341,11 @@ typedef struct {
 typedef struct {
     int64_t rays, integrated;
     float ms_features, ms_mlp, ms_shade, ms_trace, ms_total;  /* CUDA-event times of the stages */
-    int32_t reserved[3];
+    /* the audit's judgement of the surrogate: over the audit pixels (gate 2), where
+     * both the MLP's and the integrator's intensity exist, sum |I_mlp - I| / sum I
+     * and max |I_mlp - I| / max I */
+    int32_t audit_count;
+    float audit_rel_l1, audit_rel_max;
 } sirius_surrogate_stats;
 
 /* features (n x 5 floats, device) and gate (n bytes, device, may be NULL) of the frames' pixels */

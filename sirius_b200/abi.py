@@ -124,7 +124,7 @@ class SurrogateConfig(C.Structure):
 class SurrogateStats(C.Structure):
     _fields_ = [("rays", C.c_int64), ("integrated", C.c_int64), ("ms_features", C.c_float), ("ms_mlp", C.c_float),
                 ("ms_shade", C.c_float), ("ms_trace", C.c_float), ("ms_total", C.c_float),
-                ("reserved", C.c_int32 * 3)]
+                ("audit_count", C.c_int32), ("audit_rel_l1", C.c_float), ("audit_rel_max", C.c_float)]
 
 
 def surrogate_config(gate_band=0.3, audit_fraction=0.01, audit_seed=0):

@@ -983,7 +983,7 @@ __global__ void sur_scatter_kernel(const unsigned char* gate, long long total, c
 // pixel intensity from the MLP outputs: hit logit, r_1, g_1, higher orders
 // Pixels the integrator takes (gate != 0) get only the MLP copy: the
 // integrator writes their image value.
-__global__ void sur_shade_kernel(const FrameDev* frames, int n_frames, long long total, const float* out,
+__global__ void sur_shade_kernel(const FrameDev* frames, int n_frames, long long total, float* out,
                                  const unsigned char* gate, const float* flux, float* image, float* image_mlp) {
     const long long idx = (long long)blockIdx.x * blockDim.x + threadIdx.x;
     if (idx >= total) return;
@@ -997,8 +997,59 @@ __global__ void sur_shade_kernel(const FrameDev* frames, int n_frames, long long
         I = g1 * g1 * g1 * g1 * flux_lookup(flux + size_t(F.flux_slot) * kFluxTable, F, r1);
     }
     I += fmax(double(o.w), 0.0) * double(kSurHigher);
-    if (gate[idx] == 0) image[idx] = float(I);
+    const unsigned char g = gate[idx];
+    if (g == 0) image[idx] = float(I);
+    if (g == 2) out[idx * 4] = float(I);  // kept for the audit (the outputs are consumed)
     if (image_mlp) image_mlp[idx] = float(I);
+}
+
+// The audit's judgement: over the audit pixels, sum |I_mlp - I|, sum I, max
+// |I_mlp - I|, max I and their count (acc[0..4], zero on entry; the maxima as
+// the bits of non-negative floats).
+__global__ void sur_audit_kernel(const unsigned char* gate, const float* image, const float* out, long long total,
+                                 float* acc) {
+    __shared__ float red[4][32];
+    const long long idx = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+    float d = 0.f, v = 0.f, c = 0.f;
+    if (idx < total && gate[idx] == 2) {
+        v = image[idx];
+        d = fabsf(out[idx * 4] - v);
+        c = 1.f;
+    }
+    float sd = d, sv = v, md = d, mv = v, sc = c;
+    for (int o = 16; o >= 1; o >>= 1) {
+        sd += __shfl_xor_sync(kFull, sd, o);
+        sv += __shfl_xor_sync(kFull, sv, o);
+        sc += __shfl_xor_sync(kFull, sc, o);
+        md = fmaxf(md, __shfl_xor_sync(kFull, md, o));
+        mv = fmaxf(mv, __shfl_xor_sync(kFull, mv, o));
+    }
+    const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+    if (lane == 0) {
+        red[0][warp] = sd;
+        red[1][warp] = sv;
+        red[2][warp] = sc;
+        red[3][warp] = md;
+        red[0][16 + warp] = mv;
+    }
+    __syncthreads();
+    if (threadIdx.x == 0) {
+        float a = 0.f, b = 0.f, k = 0.f, m1 = 0.f, m2 = 0.f;
+        for (int w = 0; w < int(blockDim.x >> 5); ++w) {
+            a += red[0][w];
+            b += red[1][w];
+            k += red[2][w];
+            m1 = fmaxf(m1, red[3][w]);
+            m2 = fmaxf(m2, red[0][16 + w]);
+        }
+        if (k > 0.f) {
+            atomicAdd(acc, a);
+            atomicAdd(acc + 1, b);
+            atomicMax(reinterpret_cast<int*>(acc + 2), __float_as_int(m1));
+            atomicMax(reinterpret_cast<int*>(acc + 3), __float_as_int(m2));
+            atomicAdd(acc + 4, k);
+        }
+    }
 }
 
 #include "beam.cuh"
@@ -2296,7 +2347,8 @@ int sirius_cuda_surrogate_load(sirius_cuda_handle h, const float* params, int64_
     if (!H->d_surrogate) {
         if (cudaMalloc((void**)&H->d_surrogate, surrogate::kImageBytes) != cudaSuccess)
             return fail(H, SIRIUS_ERR_OUT_OF_MEMORY, "cudaMalloc surrogate weights");
-        if (cudaMalloc((void**)&H->d_sur_err, 4 * sizeof(int)) != cudaSuccess)  // [0] error, [2..3] tile counter
+        // [0] error, [2..3] MLP tile counter, [8..12] the audit's sums and maxima
+        if (cudaMalloc((void**)&H->d_sur_err, 16 * sizeof(int)) != cudaSuccess)
             return fail(H, SIRIUS_ERR_OUT_OF_MEMORY, "cudaMalloc surrogate status");
         CK(cudaFuncSetAttribute(surrogate::mlp_kernel_ts, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                 surrogate::kTsSmBytes));
@@ -2699,9 +2751,15 @@ static int render_surrogate(Handle* H, const sirius_frame* frames, int n_frames,
     CK(cudaEventRecord(H->fev[2], s_mlp));
     CK(cudaStreamWaitEvent(st, H->fev[0], 0));
     CK(cudaStreamWaitEvent(st, H->fev[2], 0));
+    float* audit = reinterpret_cast<float*>(H->d_sur_err + 8);
+    CK(cudaMemsetAsync(audit, 0, 5 * sizeof(float), st));
+    sur_audit_kernel<<<int((total + 255) / 256), 256, 0, st>>>(d_gate, d_image, H->d_mlp_out, total, audit);
+    CK(cudaGetLastError());
     CK(cudaEventRecord(H->sev[4], st));
     int err = 0, status = 0;
+    float aud[5] = {};
     CK(cudaMemcpyAsync(&err, H->d_sur_err, sizeof(int), cudaMemcpyDeviceToHost, st));
+    CK(cudaMemcpyAsync(aud, audit, sizeof(aud), cudaMemcpyDeviceToHost, st));
     CK(cudaMemcpyAsync(&status, H->d_status, sizeof(int), cudaMemcpyDeviceToHost, st));
     CK(cudaStreamSynchronize(st));
     if (err) return fail(H, SIRIUS_ERR_TIMEOUT, "surrogate MLP kernel stopped by its wait bound");
@@ -2717,6 +2775,9 @@ static int render_surrogate(Handle* H, const sirius_frame* frames, int n_frames,
         CK(cudaEventElapsedTime(&stats->ms_shade, H->fev[1], H->fev[2]));
         CK(cudaEventElapsedTime(&tt, H->sev[0], H->sev[4]));
         stats->ms_total = tt;
+        stats->audit_count = int32_t(aud[4]);
+        stats->audit_rel_l1 = aud[1] > 0.f ? aud[0] / aud[1] : 0.f;
+        stats->audit_rel_max = aud[3] > 0.f ? aud[2] / aud[3] : 0.f;
     }
     return SIRIUS_OK;
 }

@@ -103,6 +103,12 @@ def test_surrogate_render_against_the_integrator(engine):
     err = np.abs(img.astype(np.float64) - full) / full.max()
     assert err.mean() < 1e-3, err.mean()
     assert np.percentile(err, 99) < 1e-2, np.percentile(err, 99)
+    # the audit's judgement in the statistics: the MLP against the integrator on the audit pixels
+    a = gate == 2
+    d = np.abs(mimg[a].astype(np.float64) - img[a])
+    assert st.audit_count == int(a.sum())
+    np.testing.assert_allclose(st.audit_rel_l1, d.sum() / img[a].sum(dtype=np.float64), rtol=1e-4)
+    np.testing.assert_allclose(st.audit_rel_max, d.max() / img[a].max(), rtol=1e-6)
 
 
 def test_surrogate_integrates_frames_it_does_not_cover(engine):
@@ -128,14 +134,17 @@ def test_trained_network_gains_over_the_untrained_one(engine):
     engine.configure(render_config(abi.PRECISION_MIXED))
     _, full, _ = engine.trace_frames([fr], results=False)
     scale = full.max()
-    errs, fractions = {}, {}
+    errs, fractions, audits = {}, {}, {}
     rng = np.random.default_rng(11)
     for name, params in (("trained", np.load(WEIGHTS)), ("untrained", init_params(rng))):
         engine.surrogate_load(params)
         img, _, gate, st = engine.render_surrogate([fr])
         errs[name] = np.abs(img.astype(np.float64) - full) / scale
         fractions[name] = st.integrated / st.rays
+        audits[name] = st.audit_rel_l1
     assert fractions["trained"] == fractions["untrained"] < 0.05
+    # the 1 % audit sees the difference on its own
+    assert audits["untrained"] > 10 * audits["trained"], audits
     assert errs["trained"].mean() < 1e-3 and np.percentile(errs["trained"], 99) < 1e-2
     assert errs["untrained"].mean() > 10 * errs["trained"].mean()
     assert np.percentile(errs["untrained"], 99) > 5 * np.percentile(errs["trained"], 99)
