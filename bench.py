@@ -360,6 +360,8 @@ def surrogate_leg(eng, abi, np, torch, dev, stream, side=SURROGATE_SIDE, reps=3)
                                  "integrate_gated_and_audit are measured from that point"},
             "error_vs_fp64": {"image_linf_rel": float(err.max()), "image_p99_rel": float(np.percentile(err, 99)),
                               "image_mean_rel": float(err.mean())},
+            "audit_judgement": {"pixels": int(stats.audit_count), "rel_l1": float(stats.audit_rel_l1),
+                                "rel_max": float(stats.audit_rel_max)},
             "mlp_roofline": {"bound": "tensor", "kernel_ms": mlp_alone, "achieved": flops / (mlp_alone * 1e-3) / 1e12,
                              "peak": bf16_peak, "unit": "TFLOP/s", "frac": flops / (mlp_alone * 1e-3) / 1e12 / bf16_peak,
                              "peak_source": "MEASURED_PEAKS.json bf16_tflops (burst)" if peaks else "fallback",

@@ -522,7 +522,7 @@ __device__ __forceinline__ int advance(const Params& P, Ray<MIXED>& s, float& ma
     if (cross) {
         const double hs = hermite_root(s.x[3], xn[3], double(s.k[3]), double(k7[3]), hstep) * hstep;
         if constexpr (MIXED) {
-            if (island) locate_equator<double, FAM>(m, c, s.x, s.p, hs, xc1, xc2);
+            if (island) locate_equator<double, FAM, true>(m, c, s.x, s.p, hs, xc1, xc2);
             else locate_equator_f32<FAM>(m, c, s.x, s.p, s.k, hs, xc1, xc2);
         } else {
             locate_equator<double, FAM>(m, c, s.x, s.p, hs, xc1, xc2);
@@ -1416,6 +1416,8 @@ int validate_config(Handle* H, const sirius_trace_config& c) {
         return fail(H, SIRIUS_ERR_INVALID_ARGUMENT, "block_size must be 0, 32, 64 or 128");
     if (c.refill_threshold < 0 || c.refill_threshold > 32)
         return fail(H, SIRIUS_ERR_INVALID_ARGUMENT, "refill_threshold must be in 0..32");
+    if (c.register_blocks < 0 || c.register_blocks > 4)
+        return fail(H, SIRIUS_ERR_INVALID_ARGUMENT, "register_blocks must be in 0..4");
     return SIRIUS_OK;
 }
 
@@ -1458,9 +1460,12 @@ int launch_trace(Handle* H, int n_frames, long long total, sirius_ray_result* d_
     // launches (a list of gated rays) spread over more SMs with smaller blocks
     const int block = (c.block_size == 32 || c.block_size == 64) ? c.block_size : 128;
     const size_t shmem = size_t(2) * P.c.nbins * block * sizeof(float);
-    // register budget: blocks_per_sm in 1..4 selects the kernel compiled for that
-    // many resident 128-thread blocks per SM (fewer registers, possibly spills)
-    const int minb = c.blocks_per_sm > 0 ? std::min(c.blocks_per_sm, 4) : kDefaultMinBlocks;
+    // register budget: the kernel compiled for blocks_per_sm (persistent) or
+    // register_blocks (one thread per ray) resident 128-thread blocks per SM
+    // (fewer registers, possibly spills)
+    const int minb = c.blocks_per_sm > 0    ? std::min(c.blocks_per_sm, 4)
+                     : c.register_blocks > 0 ? c.register_blocks
+                                             : kDefaultMinBlocks;
     // the families present: one family -> its specialised kernel; several ->
     // one launch per family (each thread skips the rays of other families), so
     // a ray's result never depends on what else shares the batch; the
@@ -2289,14 +2294,17 @@ int sirius_cuda_autotune(sirius_cuda_handle h, const sirius_frame* frames, int32
     if (rc != SIRIUS_OK) return rc;
     if ((rc = ensure(H, H->d_image, H->image_cap, size_t(total))) != SIRIUS_OK) return rc;
     const sirius_trace_config base = H->cfg;
-    // (blocks/SM, threshold): (0, -) is the one-thread-per-ray launch
-    const int candidates[][2] = {{0, 1}, {1, 1}, {2, 1}, {3, 1}, {4, 1}, {2, 4}, {2, 8}, {3, 4}};
+    // (blocks/SM, threshold, register blocks): blocks/SM 0 is the one-thread-per-ray
+    // launch at the register budget of 2 or 3 resident blocks
+    const int candidates[][3] = {{0, 1, 2}, {0, 1, 3}, {1, 1, 0}, {2, 1, 0}, {3, 1, 0},
+                                 {4, 1, 0}, {2, 4, 0}, {2, 8, 0}, {3, 4, 0}};
     double best = 1e300;
     sirius_trace_config best_cfg = base;
     for (const auto& cand : candidates) {
         H->cfg = base;
         H->cfg.blocks_per_sm = cand[0];
         H->cfg.refill_threshold = cand[1];
+        H->cfg.register_blocks = cand[2];
         CK(cudaEventRecord(H->ev[0], H->stream));
         rc = launch_trace(H, n_frames, total, nullptr, H->d_image, nullptr, nullptr, H->stream, true);
         if (rc != SIRIUS_OK) { H->cfg = base; return rc; }

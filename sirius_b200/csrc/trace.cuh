@@ -408,16 +408,24 @@ __device__ __forceinline__ double dp45_attempt_lowreg(const MetricDev& m, const 
 // sub-steps from the step's start state (x0, p0) with f(x0, p0) recomputed in
 // T, the sub-step length corrected by Newton on z(l) (dz/dl = k^z), seeded by
 // the cubic Hermite root; two sub-steps and a final first-order correction.
-template <class T, int FAM = kAnyFamily>
+// LOWREG (FP64 only) takes the sub-steps with the local-array attempt, for the
+// mixed path's rare FP64 steps: with the register-resident attempt this one
+// function set the mixed kernel's register count.
+template <class T, int FAM = kAnyFamily, bool LOWREG = false>
 __device__ __noinline__ void locate_equator(const MetricDev& m, const CfgDev& c, const double x0[4],
                                             const double p0[4], double hs, double& xc1, double& xc2) {
+    static_assert(!LOWREG || sizeof(T) == sizeof(double), "the low-register attempt is FP64");
     T xk[4], pk[4], k0[8], k7[8];
     for (int i = 0; i < 4; ++i) { xk[i] = T(x0[i]); pk[i] = T(p0[i]); }
     rhs<T, FAM>(m, xk, pk, k0, k0 + 4);
     double xn[4], pn[4];
-    dp45_attempt<T, FAM>(m, c, x0, p0, hs, k0, xn, pn, k7);
+    auto attempt = [&](double hh) {
+        if constexpr (LOWREG) dp45_attempt_lowreg<FAM>(m, c, x0, p0, hh, k0, xn, pn, k7);
+        else dp45_attempt<T, FAM>(m, c, x0, p0, hh, k0, xn, pn, k7);
+    };
+    attempt(hs);
     hs -= xn[3] / double(k7[3]);
-    dp45_attempt<T, FAM>(m, c, x0, p0, hs, k0, xn, pn, k7);
+    attempt(hs);
     const double dl = -xn[3] / double(k7[3]);
     xc1 = xn[1] + dl * double(k7[1]);
     xc2 = xn[2] + dl * double(k7[2]);
