@@ -201,10 +201,10 @@ typedef struct sirius_trace_config {
                                     progressive pass per sub-pixel offset, summed in a fixed order;
                                     per-ray results are then not available (NULL), and the launch
                                     statistics count the last pass. At most 4096. */
-    int32_t register_blocks;     /* one-thread-per-ray launch: the trace kernel compiled for this many
-                                    resident 128-thread blocks per SM, i.e. its register budget
-                                    (0 = 2: up to 255 registers; 3: 168; 4: 128, with spills).
-                                    The persistent launch takes its budget from blocks_per_sm. */
+    int32_t max_registers;       /* one-thread-per-ray launch: the register cap of the trace kernel,
+                                    0 or 255 (default; 8 warps per SM), 168 (12) or 128 (16); the
+                                    lower caps spill. The persistent launch takes its budget from
+                                    blocks_per_sm. */
     int32_t reserved[3];
 } sirius_trace_config;
 

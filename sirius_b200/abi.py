@@ -91,7 +91,7 @@ class TraceConfig(C.Structure):
                 ("island_factor", C.c_double), ("critical_band", C.c_double), ("symplectic_step", C.c_double),
                 ("symplectic_order", C.c_int32), ("block_size", C.c_int32),
                 ("refill_threshold", C.c_int32), ("blocks_per_sm", C.c_int32),
-                ("watchdog_ms", C.c_int32), ("samples_per_pixel", C.c_int32), ("register_blocks", C.c_int32),
+                ("watchdog_ms", C.c_int32), ("samples_per_pixel", C.c_int32), ("max_registers", C.c_int32),
                 ("reserved", C.c_int32 * 3)]
 
 

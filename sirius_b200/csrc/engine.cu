@@ -660,8 +660,8 @@ __device__ __forceinline__ int advance(const Params& P, Ray<MIXED>& s, float& ma
 }
 
 // Persistent tracer. Dynamic shared memory: 2 * nbins floats per thread (volumetric bins).
-template <bool MIXED, int MINB, int FAM, bool UNI>
-__global__ void __launch_bounds__(128, MINB) trace_kernel(const __grid_constant__ Params P) {
+template <bool MIXED, int FAM, bool UNI>
+__device__ __forceinline__ void trace_body(const Params& P) {
     extern __shared__ float smem[];
     float* vol = (P.c.enable_vol && P.c.nbins > 0) ? smem + threadIdx.x : nullptr;
     const int lane = threadIdx.x & 31;
@@ -756,6 +756,13 @@ __global__ void __launch_bounds__(128, MINB) trace_kernel(const __grid_constant_
         atomicAdd(&P.counters[1], rej0);
         atomicAdd(&P.counters[2], f64);
     }
+}
+
+// The tracer compiled for MINB resident 128-thread blocks per SM (MINB 2: up to
+// 255 registers, 3: 168, 4: 128).
+template <bool MIXED, int MINB, int FAM, bool UNI>
+__global__ void __launch_bounds__(128, MINB) trace_kernel(const __grid_constant__ Params P) {
+    trace_body<MIXED, FAM, UNI>(P);
 }
 
 using TraceFn = void (*)(Params);
@@ -1416,8 +1423,8 @@ int validate_config(Handle* H, const sirius_trace_config& c) {
         return fail(H, SIRIUS_ERR_INVALID_ARGUMENT, "block_size must be 0, 32, 64 or 128");
     if (c.refill_threshold < 0 || c.refill_threshold > 32)
         return fail(H, SIRIUS_ERR_INVALID_ARGUMENT, "refill_threshold must be in 0..32");
-    if (c.register_blocks < 0 || c.register_blocks > 4)
-        return fail(H, SIRIUS_ERR_INVALID_ARGUMENT, "register_blocks must be in 0..4");
+    if (c.max_registers != 0 && c.max_registers != 128 && c.max_registers != 168 && c.max_registers != 255)
+        return fail(H, SIRIUS_ERR_INVALID_ARGUMENT, "max_registers must be 0, 128, 168 or 255");
     return SIRIUS_OK;
 }
 
@@ -1460,12 +1467,13 @@ int launch_trace(Handle* H, int n_frames, long long total, sirius_ray_result* d_
     // launches (a list of gated rays) spread over more SMs with smaller blocks
     const int block = (c.block_size == 32 || c.block_size == 64) ? c.block_size : 128;
     const size_t shmem = size_t(2) * P.c.nbins * block * sizeof(float);
-    // register budget: the kernel compiled for blocks_per_sm (persistent) or
-    // register_blocks (one thread per ray) resident 128-thread blocks per SM
-    // (fewer registers, possibly spills)
-    const int minb = c.blocks_per_sm > 0    ? std::min(c.blocks_per_sm, 4)
-                     : c.register_blocks > 0 ? c.register_blocks
-                                             : kDefaultMinBlocks;
+    // register budget: the kernel compiled for blocks_per_sm resident 128-thread
+    // blocks per SM (persistent), or for max_registers (one thread per ray);
+    // fewer registers, possibly spills
+    const int minb = c.blocks_per_sm > 0      ? std::min(c.blocks_per_sm, 4)
+                     : c.max_registers == 128 ? 4
+                     : c.max_registers == 168 ? 3
+                                              : kDefaultMinBlocks;
     // the families present: one family -> its specialised kernel; several ->
     // one launch per family (each thread skips the rays of other families), so
     // a ray's result never depends on what else shares the batch; the
@@ -2294,17 +2302,17 @@ int sirius_cuda_autotune(sirius_cuda_handle h, const sirius_frame* frames, int32
     if (rc != SIRIUS_OK) return rc;
     if ((rc = ensure(H, H->d_image, H->image_cap, size_t(total))) != SIRIUS_OK) return rc;
     const sirius_trace_config base = H->cfg;
-    // (blocks/SM, threshold, register blocks): blocks/SM 0 is the one-thread-per-ray
-    // launch at the register budget of 2 or 3 resident blocks
-    const int candidates[][3] = {{0, 1, 2}, {0, 1, 3}, {1, 1, 0}, {2, 1, 0}, {3, 1, 0},
-                                 {4, 1, 0}, {2, 4, 0}, {2, 8, 0}, {3, 4, 0}};
+    // (blocks/SM, threshold, register cap): blocks/SM 0 is the one-thread-per-ray
+    // launch at a register cap (0: 255)
+    const int candidates[][3] = {{0, 1, 0}, {0, 1, 168}, {1, 1, 0}, {2, 1, 0}, {3, 1, 0},
+                                 {4, 1, 0}, {2, 4, 0},   {2, 8, 0}, {3, 4, 0}};
     double best = 1e300;
     sirius_trace_config best_cfg = base;
     for (const auto& cand : candidates) {
         H->cfg = base;
         H->cfg.blocks_per_sm = cand[0];
         H->cfg.refill_threshold = cand[1];
-        H->cfg.register_blocks = cand[2];
+        H->cfg.max_registers = cand[2];
         CK(cudaEventRecord(H->ev[0], H->stream));
         rc = launch_trace(H, n_frames, total, nullptr, H->d_image, nullptr, nullptr, H->stream, true);
         if (rc != SIRIUS_OK) { H->cfg = base; return rc; }
