@@ -34,8 +34,8 @@ N_BINS = 16
 MEASURED_PEAKS = os.path.join(ROOT, "MEASURED_PEAKS.json")
 # DRAM bytes (read + write) per ray of the trace kernel, from one ncu capture of
 # the 256^2 case of this workload (profiles/trace_kernel_mixed_kerr256_full.md):
-# (1.55 + 0.81) MB / 65,536 rays; traffic grows with the ray count.
-TRAFFIC_BYTES_PER_RAY = 36.0
+# (0.86 + 0.06) MB / 65,536 rays; traffic grows with the ray count.
+TRAFFIC_BYTES_PER_RAY = 14.1
 
 
 def inclination_deg(seed=SEED):

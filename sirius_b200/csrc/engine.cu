@@ -114,7 +114,7 @@ struct Ray {
 // Delta (Q + (L - a E)^2), Delta = r^2 - 2 M r + a^2 + Q_e^2: a double root marks
 // the critical curve. Returns min R / (E^2 r^4) over the photon region
 // r in [1.0001 r_+, 4.5 M] (48 samples).
-__device__ __noinline__ double radial_potential_gap(const MetricDev& m, double rp, double E, double L, double Q) {
+__device__ __forceinline__ double radial_potential_gap(const MetricDev& m, double rp, double E, double L, double Q) {
     double best = 1e300;
     const double r0 = 1.0001 * rp, r1 = 4.5 * m.M;
     for (int i = 0; i < 48; ++i) {
@@ -155,7 +155,7 @@ __device__ void invariants(const MetricDev& m, const InvForm& F, const double x[
 }
 
 template <bool MIXED, int FAM, bool UNI>
-__device__ __noinline__ void begin_ray(const Params& P, Ray<MIXED>& s, long long idx, int frame, float* vol) {
+__device__ __forceinline__ void begin_ray(const Params& P, Ray<MIXED>& s, long long idx, int frame, float* vol) {
     using K = typename Ray<MIXED>::K;
     s.idx = idx;
     s.frame = frame;
@@ -212,7 +212,7 @@ __device__ __noinline__ void begin_ray(const Params& P, Ray<MIXED>& s, long long
 }
 
 template <bool MIXED, bool UNI>
-__device__ __noinline__ void end_ray(const Params& P, const Ray<MIXED>& s, int outcome, float magnification, int flags,
+__device__ __forceinline__ void end_ray(const Params& P, const Ray<MIXED>& s, int outcome, float magnification, int flags,
                                      const float* vol) {
     const FrameDev& F = frame_of<UNI>(P, s.frame);
     if (P.image) P.image[s.idx] = float(s.intensity);
@@ -275,7 +275,7 @@ __device__ __forceinline__ float ks_r(const MetricDev& m, float x, float y, floa
 // I_b += T_b S (1 - e^-dtau), T_b = e^-tau_b,
 //   j = j0 r^-2 exp(-z^2/(2 (h_z r)^2)) nu_em^-s, alpha = c_a j,
 //   dtau = alpha (nu_cam/g) dl, S = g^3 / c_a.  (vol: [2b] = I_b, [2b+1] = T_b, stride blockDim)
-__device__ __noinline__ void volumetric_segment(const Params& P, const FrameDev& F, const double x0[4],
+__device__ __forceinline__ void volumetric_segment(const Params& P, const FrameDev& F, const double x0[4],
                                                 const double x1[4], const float k0[4], const float k1[4],
                                                 const double p[4], double h, float r0, float r1, float* vol) {
     const CfgDev& c = P.c;
@@ -408,7 +408,7 @@ __device__ __forceinline__ double flux_lookup(const float* t, const FrameDev& F,
     return flux_cubic(t, x);
 }
 
-__device__ __noinline__ bool record_crossing(const Params& P, const FrameDev& F, long long idx, int n, double xc1,
+__device__ __forceinline__ bool record_crossing(const Params& P, const FrameDev& F, long long idx, int n, double xc1,
                                              double xc2, const double x[4], const double p[4], double& intensity) {
     const MetricDev& m = F.m;
     const double xc[4] = {0.0, xc1, xc2, 0.0};
@@ -435,7 +435,7 @@ __device__ __noinline__ bool record_crossing(const Params& P, const FrameDev& F,
 // attempt in FP64; the derivative at the candidate point returned in float for
 // the FP32 steps that may follow.
 template <int FAM>
-__device__ __noinline__ double island_attempt(const MetricDev& m, const CfgDev& c, const double x[4],
+__device__ __forceinline__ double island_attempt(const MetricDev& m, const CfgDev& c, const double x[4],
                                               const double p[4], double h, double xn[4], double pn[4], float k7f[8]) {
     double k1[8], k7[8];
     rhs<double, FAM>(m, x, p, k1, k1 + 4);
@@ -447,7 +447,7 @@ __device__ __noinline__ double island_attempt(const MetricDev& m, const CfgDev& 
 
 // f(x, p) of the current state in the storage precision of the path.
 template <bool MIXED, int FAM>
-__device__ __noinline__ void refresh_derivative(const MetricDev& m, Ray<MIXED>& s) {
+__device__ __forceinline__ void refresh_derivative(const MetricDev& m, Ray<MIXED>& s) {
     using K = typename Ray<MIXED>::K;
     K xk[4], pk[4];
     for (int i = 0; i < 4; ++i) { xk[i] = K(s.x[i]); pk[i] = K(s.p[i]); }

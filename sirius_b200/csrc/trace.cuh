@@ -409,10 +409,10 @@ __device__ __forceinline__ double dp45_attempt_lowreg(const MetricDev& m, const 
 // T, the sub-step length corrected by Newton on z(l) (dz/dl = k^z), seeded by
 // the cubic Hermite root; two sub-steps and a final first-order correction.
 // LOWREG (FP64 only) takes the sub-steps with the local-array attempt, for the
-// mixed path's rare FP64 steps: with the register-resident attempt this one
-// function set the mixed kernel's register count.
+// mixed path's rare FP64 steps: with the register-resident attempt, the 48 FP64
+// stage accumulators of this rare path set the mixed kernel's register count.
 template <class T, int FAM = kAnyFamily, bool LOWREG = false>
-__device__ __noinline__ void locate_equator(const MetricDev& m, const CfgDev& c, const double x0[4],
+__device__ __forceinline__ void locate_equator(const MetricDev& m, const CfgDev& c, const double x0[4],
                                             const double p0[4], double hs, double& xc1, double& xc2) {
     static_assert(!LOWREG || sizeof(T) == sizeof(double), "the low-register attempt is FP64");
     T xk[4], pk[4], k0[8], k7[8];
@@ -436,7 +436,7 @@ __device__ __noinline__ void locate_equator(const MetricDev& m, const CfgDev& c,
 // correction along k. FP32 stages bound the location at ~1e-7 relative, which a
 // second sub-step would not improve.
 template <int FAM = kAnyFamily>
-__device__ __noinline__ void locate_equator_f32(const MetricDev& m, const CfgDev& c, const double x0[4],
+__device__ __forceinline__ void locate_equator_f32(const MetricDev& m, const CfgDev& c, const double x0[4],
                                                 const double p0[4], const float k0[8], double hs, double& xc1,
                                                 double& xc2) {
     double xn[4], pn[4];
@@ -472,7 +472,7 @@ __constant__ double kYoshida[3][15] = {
      0.29906418130365, -0.57386247111608, 0.19075471029623, -0.40910082580003, 0.74167036435061}};
 
 template <class T, int FAM = kAnyFamily>
-__device__ __noinline__ void symplectic_step(const MetricDev& m, int order, double h, double x[4], double p[4]) {
+__device__ __forceinline__ void symplectic_step(const MetricDev& m, int order, double h, double x[4], double p[4]) {
     const int row = order >= 8 ? 2 : (order >= 6 ? 1 : 0);
     const int n = row == 2 ? 15 : (row == 1 ? 7 : 3);
 #pragma unroll 1
