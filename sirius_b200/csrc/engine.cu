@@ -766,7 +766,8 @@ __global__ void __launch_bounds__(128, MINB) trace_kernel(const __grid_constant_
 }
 
 using TraceFn = void (*)(Params);
-constexpr int kDefaultMinBlocks = 2;
+constexpr int kDefaultMinBlocks = 2;       // FP64 path: up to 255 registers
+constexpr int kDefaultMinBlocksMixed = 4;  // mixed path: 128 registers
 
 template <bool MIXED, int FAM, bool UNI>
 TraceFn pick_minb(int minb) {
@@ -1469,10 +1470,15 @@ int launch_trace(Handle* H, int n_frames, long long total, sirius_ray_result* d_
     const size_t shmem = size_t(2) * P.c.nbins * block * sizeof(float);
     // register budget: the kernel compiled for blocks_per_sm resident 128-thread
     // blocks per SM (persistent), or for max_registers (one thread per ray);
-    // fewer registers, possibly spills
+    // fewer registers, possibly spills. The default per precision was measured
+    // on the 1024^2 bench frame: the mixed kernel is fastest at 128 registers
+    // (16 warps per SM; 38.9 ms against 41.5 ms at 255), the FP64 kernel at 255
+    // (63.0 ms against 78.0 ms at 128).
     const int minb = c.blocks_per_sm > 0      ? std::min(c.blocks_per_sm, 4)
                      : c.max_registers == 128 ? 4
                      : c.max_registers == 168 ? 3
+                     : c.max_registers == 255 ? 2
+                     : mixed                  ? kDefaultMinBlocksMixed
                                               : kDefaultMinBlocks;
     // the families present: one family -> its specialised kernel; several ->
     // one launch per family (each thread skips the rays of other families), so
@@ -2304,8 +2310,8 @@ int sirius_cuda_autotune(sirius_cuda_handle h, const sirius_frame* frames, int32
     const sirius_trace_config base = H->cfg;
     // (blocks/SM, threshold, register cap): blocks/SM 0 is the one-thread-per-ray
     // launch at a register cap (0: 255)
-    const int candidates[][3] = {{0, 1, 0}, {0, 1, 168}, {1, 1, 0}, {2, 1, 0}, {3, 1, 0},
-                                 {4, 1, 0}, {2, 4, 0},   {2, 8, 0}, {3, 4, 0}};
+    const int candidates[][3] = {{0, 1, 0}, {0, 1, 255}, {0, 1, 168}, {0, 1, 128}, {1, 1, 0}, {2, 1, 0},
+                                 {3, 1, 0}, {4, 1, 0},   {2, 4, 0},   {2, 8, 0},   {3, 4, 0}};
     double best = 1e300;
     sirius_trace_config best_cfg = base;
     for (const auto& cand : candidates) {

@@ -292,20 +292,21 @@ def test_watchdog_bounds_a_launch(engine):
 
 def test_register_budgets_agree(engine):
     """max_registers selects the trace kernel compiled for a register cap (255,
-    168 or 128). The cap changes spills, not arithmetic: FP64 images are
-    bit-identical; the mixed path's FP32 contractions may round differently, so
-    its images agree within the FP32 right-hand side's error budget."""
+    168 or 128; 0 is the precision's default, 128 mixed and 255 FP64). The cap
+    changes spills, not arithmetic: FP64 images are bit-identical; the mixed
+    path's FP32 contractions may round differently, so its images agree within
+    the FP32 right-hand side's error budget."""
     fr = kerr_frame(w=96, h=96)
     for prec in (abi.PRECISION_FP64, abi.PRECISION_MIXED):
         imgs = {}
-        for cap in (0, 168, 128):
+        for cap in (0, 255, 168, 128):
             engine.configure(workload(prec, max_registers=cap))
             _, imgs[cap], _ = engine.trace_frames([fr], results=False)
-        for cap in (168, 128):
+        for cap in (0, 168, 128):
             if prec == abi.PRECISION_FP64:
-                np.testing.assert_array_equal(imgs[cap], imgs[0])
+                np.testing.assert_array_equal(imgs[cap], imgs[255])
             else:
-                err = np.abs(imgs[cap].astype(np.float64) - imgs[0]) / imgs[0].max()
+                err = np.abs(imgs[cap].astype(np.float64) - imgs[255]) / imgs[255].max()
                 assert err.max() <= 1e-4, err.max()
     with pytest.raises(Exception) as e:
         engine.configure(workload(abi.PRECISION_MIXED, max_registers=5))
@@ -316,5 +317,5 @@ def test_autotune_and_peaks(engine):
     engine.configure(workload(abi.PRECISION_MIXED))
     cfg = engine.autotune([kerr_frame(w=128, h=128)])
     assert 0 <= cfg.blocks_per_sm <= 4 and 1 <= cfg.refill_threshold <= 32
-    assert cfg.max_registers in (0, 168)
+    assert cfg.max_registers in (0, 255, 168, 128)
     assert engine.fma_peak(1) > 1e13 and engine.fma_peak(0) > 5e12
