@@ -202,10 +202,12 @@ typedef struct sirius_trace_config {
                                     per-ray results are then not available (NULL), and the launch
                                     statistics count the last pass. At most 4096. */
     int32_t max_registers;       /* one-thread-per-ray launch: the register cap of the trace kernel,
-                                    255 (8 warps per SM), 168 (12) or 128 (16; these two spill);
-                                    0 = the precision's default, 128 for mixed and 255 for FP64
-                                    (the fastest on the 1024^2 bench frame). The persistent
-                                    launch takes its budget from blocks_per_sm. */
+                                    255 (8 warps per SM), 168 (12) or 128 (16; these two spill).
+                                    0 = measured default: 128 for mixed DP45, else 255 (FP64,
+                                    symplectic). The budgets' FP32 roundings differ, so mixed
+                                    images at different caps agree to ~1e-5 of the peak, not
+                                    bit for bit. The persistent launch takes its budget from
+                                    blocks_per_sm. */
     int32_t reserved[3];
 } sirius_trace_config;
 

@@ -766,8 +766,8 @@ __global__ void __launch_bounds__(128, MINB) trace_kernel(const __grid_constant_
 }
 
 using TraceFn = void (*)(Params);
-constexpr int kDefaultMinBlocks = 2;       // FP64 path: up to 255 registers
-constexpr int kDefaultMinBlocksMixed = 4;  // mixed path: 128 registers
+constexpr int kDefaultMinBlocks = 2;       // up to 255 registers
+constexpr int kDefaultMinBlocksMixed = 4;  // 128 registers: mixed DP45
 
 template <bool MIXED, int FAM, bool UNI>
 TraceFn pick_minb(int minb) {
@@ -1470,15 +1470,18 @@ int launch_trace(Handle* H, int n_frames, long long total, sirius_ray_result* d_
     const size_t shmem = size_t(2) * P.c.nbins * block * sizeof(float);
     // register budget: the kernel compiled for blocks_per_sm resident 128-thread
     // blocks per SM (persistent), or for max_registers (one thread per ray);
-    // fewer registers, possibly spills. The default per precision was measured
-    // on the 1024^2 bench frame: the mixed kernel is fastest at 128 registers
-    // (16 warps per SM; 38.9 ms against 41.5 ms at 255), the FP64 kernel at 255
-    // (63.0 ms against 78.0 ms at 128).
+    // fewer registers, possibly spills. The default was measured: the mixed DP45
+    // kernel runs fastest at 128 registers (16 warps per SM; 1024^2 bench frame
+    // 38.9 ms against 41.5 ms at 255); FP64 (63.0 ms against 78.0 ms at 128) and
+    // the symplectic integrator keep 255. The choice depends on the configuration
+    // only, never on the launch's size or contents: the budgets' FP32 roundings
+    // differ, and a ray's result must not depend on what else shares its launch.
+    const bool wide = mixed && c.integrator == SIRIUS_INTEGRATOR_DP45;
     const int minb = c.blocks_per_sm > 0      ? std::min(c.blocks_per_sm, 4)
                      : c.max_registers == 128 ? 4
                      : c.max_registers == 168 ? 3
                      : c.max_registers == 255 ? 2
-                     : mixed                  ? kDefaultMinBlocksMixed
+                     : wide                   ? kDefaultMinBlocksMixed
                                               : kDefaultMinBlocks;
     // the families present: one family -> its specialised kernel; several ->
     // one launch per family (each thread skips the rays of other families), so
