@@ -33,9 +33,9 @@ SEED = 0
 N_BINS = 16
 MEASURED_PEAKS = os.path.join(ROOT, "MEASURED_PEAKS.json")
 # DRAM bytes (read + write) per ray of the trace kernel, from one ncu capture of
-# the 256^2 case of this workload (profiles/trace_kernel_mixed_kerr256_full.md):
-# (0.86 + 0.06) MB / 65,536 rays; traffic grows with the ray count.
-TRAFFIC_BYTES_PER_RAY = 14.1
+# the 512^2 case of this workload (profiles/trace_kernel_mixed_kerr512_full.md):
+# (4.35 + 5.63) MB / 262,144 rays; traffic grows with the ray count.
+TRAFFIC_BYTES_PER_RAY = 38.1
 
 
 def inclination_deg(seed=SEED):
@@ -475,6 +475,8 @@ def main():
     ap.add_argument("--train-only", action="store_true",
                     help="run only the surrogate-training leg and print its JSON")
     ap.add_argument("--train-steps", type=int, default=64)
+    ap.add_argument("--max-registers", type=int, default=0,
+                    help="register cap of the mixed trace kernel (0: the library default, 128)")
     ap.add_argument("--size", type=int, default=WIDTH,
                     help="frame side (default 1024, the workload; smaller sides are profiling cases)")
     args = ap.parse_args()
@@ -510,7 +512,9 @@ def main():
         eng.close()
         return
 
-    eng = Engine(local, config=workload_config(abi, abi.PRECISION_MIXED))
+    main_cfg = workload_config(abi, abi.PRECISION_MIXED)
+    main_cfg.max_registers = args.max_registers
+    eng = Engine(local, config=main_cfg)
     frame = workload_frame(abi, args.size, args.size)
     frames = (abi.Frame * 1)(frame)
     frames[0].ray_offset = 0
