@@ -431,18 +431,45 @@ __device__ __forceinline__ bool record_crossing(const Params& P, const FrameDev&
     return true;
 }
 
-// The FP64 island attempt of the mixed path: f(x, p) recomputed in FP64, a DP45
-// attempt in FP64; the derivative at the candidate point returned in float for
-// the FP32 steps that may follow.
+// The FP64 island of the mixed path is large and rare, so it stays out of line
+// (less code in the hot loop). Its arguments and results travel by value: an
+// array passed by address would pin the caller's ray state in local memory.
+struct Vec4v {
+    double v[4];
+};
+struct IslandStep {
+    double xn[4], pn[4];
+    float k7[8];
+    double err;
+};
+struct CrossXY {
+    double x, y;
+};
+
+__device__ __forceinline__ Vec4v vec4v(const double a[4]) { return Vec4v{{a[0], a[1], a[2], a[3]}}; }
+
+// The FP64 island attempt: f(x, p) recomputed in FP64, a DP45 attempt in FP64;
+// the derivative at the candidate point returned in float for the FP32 steps
+// that may follow.
 template <int FAM>
-__device__ __forceinline__ double island_attempt(const MetricDev& m, const CfgDev& c, const double x[4],
-                                              const double p[4], double h, double xn[4], double pn[4], float k7f[8]) {
+__device__ __noinline__ IslandStep island_attempt(const MetricDev& m, const CfgDev& c, const Vec4v x, const Vec4v p,
+                                                  double h) {
+    IslandStep o;
     double k1[8], k7[8];
-    rhs<double, FAM>(m, x, p, k1, k1 + 4);
-    const double err = dp45_attempt_lowreg<FAM>(m, c, x, p, h, k1, xn, pn, k7);
+    rhs<double, FAM>(m, x.v, p.v, k1, k1 + 4);
+    o.err = dp45_attempt_lowreg<FAM>(m, c, x.v, p.v, h, k1, o.xn, o.pn, k7);
 #pragma unroll
-    for (int i = 0; i < 8; ++i) k7f[i] = float(k7[i]);
-    return err;
+    for (int i = 0; i < 8; ++i) o.k7[i] = float(k7[i]);
+    return o;
+}
+
+// The equatorial crossing of an accepted island step, located in FP64.
+template <int FAM>
+__device__ __noinline__ CrossXY island_crossing(const MetricDev& m, const CfgDev& c, const Vec4v x, const Vec4v p,
+                                                double hs) {
+    CrossXY o;
+    locate_equator<double, FAM, true>(m, c, x.v, p.v, hs, o.x, o.y);
+    return o;
 }
 
 // f(x, p) of the current state in the storage precision of the path.
@@ -493,8 +520,16 @@ __device__ __forceinline__ int advance(const Params& P, Ray<MIXED>& s, float& ma
         rhs<K>(m, xk, pk, k7, k7 + 4);
         err = 0.0;
     } else if constexpr (MIXED) {
-        if (island) err = island_attempt<FAM>(m, c, s.x, s.p, s.h, xn, pn, k7);
-        else err = dp45_attempt<float, FAM>(m, c, s.x, s.p, s.h, s.k, xn, pn, k7);
+        if (island) {
+            const IslandStep o = island_attempt<FAM>(m, c, vec4v(s.x), vec4v(s.p), s.h);
+#pragma unroll
+            for (int i = 0; i < 4; ++i) { xn[i] = o.xn[i]; pn[i] = o.pn[i]; }
+#pragma unroll
+            for (int i = 0; i < 8; ++i) k7[i] = o.k7[i];
+            err = o.err;
+        } else {
+            err = dp45_attempt<float, FAM>(m, c, s.x, s.p, s.h, s.k, xn, pn, k7);
+        }
     } else {
         err = dp45_attempt<double, FAM>(m, c, s.x, s.p, s.h, s.k, xn, pn, k7);
     }
@@ -522,7 +557,11 @@ __device__ __forceinline__ int advance(const Params& P, Ray<MIXED>& s, float& ma
     if (cross) {
         const double hs = hermite_root(s.x[3], xn[3], double(s.k[3]), double(k7[3]), hstep) * hstep;
         if constexpr (MIXED) {
-            if (island) locate_equator<double, FAM, true>(m, c, s.x, s.p, hs, xc1, xc2);
+            if (island) {
+                const CrossXY o = island_crossing<FAM>(m, c, vec4v(s.x), vec4v(s.p), hs);
+                xc1 = o.x;
+                xc2 = o.y;
+            }
             else locate_equator_f32<FAM>(m, c, s.x, s.p, s.k, hs, xc1, xc2);
         } else {
             locate_equator<double, FAM>(m, c, s.x, s.p, hs, xc1, xc2);
