@@ -1515,12 +1515,12 @@ int launch_trace(Handle* H, int n_frames, long long total, sirius_ray_result* d_
     // the symplectic integrator keep 255. The choice depends on the configuration
     // only, never on the launch's size or contents: the budgets' FP32 roundings
     // differ, and a ray's result must not depend on what else shares its launch.
-    const bool wide = mixed && c.integrator == SIRIUS_INTEGRATOR_DP45;
+    const bool mixed_dp45 = mixed && c.integrator == SIRIUS_INTEGRATOR_DP45;
     const int minb = c.blocks_per_sm > 0      ? std::min(c.blocks_per_sm, 4)
                      : c.max_registers == 128 ? 4
                      : c.max_registers == 168 ? 3
                      : c.max_registers == 255 ? 2
-                     : wide                   ? kDefaultMinBlocksMixed
+                     : mixed_dp45             ? kDefaultMinBlocksMixed
                                               : kDefaultMinBlocks;
     // the families present: one family -> its specialised kernel; several ->
     // one launch per family (each thread skips the rays of other families), so
