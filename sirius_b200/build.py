@@ -7,6 +7,7 @@ import os
 import shutil
 import subprocess
 import sys
+from concurrent.futures import ThreadPoolExecutor
 
 HERE = os.path.dirname(os.path.abspath(__file__))
 ROOT = os.path.dirname(HERE)
@@ -23,7 +24,7 @@ NVCC_FLAGS = [
 
 
 def sources():
-    srcs = [os.path.join(CSRC, "engine.cu")]
+    srcs = sorted(os.path.join(CSRC, f) for f in os.listdir(CSRC) if f.endswith(".cu"))
     if os.path.isdir(HOST):
         srcs += sorted(os.path.join(HOST, f) for f in os.listdir(HOST) if f.endswith(".cpp"))
     return srcs
@@ -45,14 +46,31 @@ def up_to_date():
 
 
 def build(force=False, verbose=False):
+    """Compile every translation unit to an object in parallel, then link."""
     if not force and up_to_date():
         return LIB
     nvcc = shutil.which("nvcc") or "/usr/local/cuda/bin/nvcc"
-    cmd = [nvcc, *NVCC_FLAGS, "-I", os.path.join(ROOT, "include"), "-shared", "-o", LIB + ".tmp", *sources(), "-lz"]
-    if verbose:
-        cmd.insert(1, "-Xptxas=-v")
-        print(" ".join(cmd))
-    subprocess.run(cmd, check=True)
+    objdir = os.path.join(HERE, "_build")
+    os.makedirs(objdir, exist_ok=True)
+    inc = ["-I", os.path.join(ROOT, "include")]
+
+    def compile_one(src):
+        obj = os.path.join(objdir, os.path.basename(src) + ".o")
+        cmd = [nvcc, *NVCC_FLAGS, *inc, "-c", "-o", obj, src]
+        if verbose and src.endswith(".cu"):
+            cmd.insert(1, "-Xptxas=-v")
+        r = subprocess.run(cmd, capture_output=True, text=True)
+        if verbose or r.returncode:
+            sys.stderr.write(r.stderr)
+        if r.returncode:
+            raise subprocess.CalledProcessError(r.returncode, cmd)
+        return obj
+
+    srcs = sources()
+    with ThreadPoolExecutor(max_workers=min(len(srcs), os.cpu_count() or 1)) as ex:
+        objs = list(ex.map(compile_one, srcs))
+    subprocess.run([nvcc, "-gencode", "arch=compute_100a,code=sm_100a", "-shared", "-o", LIB + ".tmp", *objs, "-lz"],
+                   check=True)
     os.replace(LIB + ".tmp", LIB)
     return LIB
 

@@ -1,16 +1,17 @@
-// engine.cu — the B200 geodesic engine: kernels and the C ABI (include/sirius_cuda.h).
+// engine.cu — the B200 geodesic engine: host side, the C ABI (include/sirius_cuda.h)
+// and the kernels around the tracer.
 //
-// Kernels
-//   trace_kernel<MIXED>   persistent ray tracer. Each warp keeps 32 live rays;
-//                         when the live count falls below a threshold the
-//                         dead lanes are refilled from a global ray queue with
-//                         one atomicAdd per warp (ballot + popc prefix), so
-//                         rays with wildly different step counts do not idle
-//                         lanes. MIXED=false is the all-FP64 integrator (also
-//                         launched non-persistently as the plain baseline).
+// Kernels here
+//   flux_table_kernel     per-frame Page-Thorne flux tables of the mixed path.
+//   sur_* kernels         surrogate-gated rendering (features, gate, compaction,
+//                         shading, audit judgement).
+//   beam_kernel           geodesic deviation around each pixel ray (beam.cuh).
 //   metric_kernel         IMetric::evaluate for a batch of points.
 //   dp45_step_kernel      one Geodesic::integrateStepRK45 attempt per state.
 //   fma_peak_kernel       FP32/FP64 FMA-chain microbenchmark (roofline peak).
+// The trace kernels themselves (tracer.cuh) are instantiated in
+// trace_ks_mixed.cu, trace_ks_fp64.cu and trace_families.cu; the surrogate MLP
+// and its training kernels in surrogate.cuh and train.cuh.
 #include <cuda_runtime.h>
 
 #include <algorithm>
@@ -24,7 +25,7 @@
 #include <type_traits>
 #include <vector>
 
-#include "trace.cuh"
+#include "tracer.cuh"
 #include "surrogate.cuh"
 #include "train.cuh"
 
@@ -39,341 +40,9 @@ static_assert(sizeof(sirius_surrogate_stats) == 48, "sirius_surrogate_stats layo
 static_assert(sizeof(sirius_train_config) == 64, "sirius_train_config layout");
 static_assert(sizeof(sirius_beam_result) == 32, "sirius_beam_result layout");
 
+using namespace sirius::eng;
+
 namespace {
-
-constexpr unsigned kFull = 0xffffffffu;
-
-constexpr unsigned kListSkip = 0xFFFFFFFFu;  // a list entry that names no ray
-
-struct Params {
-    const FrameDev* frames;
-    int n_frames;
-    long long total;
-    sirius_ray_result* results;
-    float* image;
-    float* spectra;
-    const sirius_camera_ray* host_rays;  // optional: explicit camera rays (device copy)
-    const unsigned* list;                 // optional: trace only these ray indices (total = list length;
-                                          // kListSkip entries are padding)
-    const float* flux;                    // optional: per-frame disk flux tables (mixed path), kFluxN each
-    unsigned long long* queue;            // [0] ray cursor
-    unsigned long long* counters;         // [0] accepted, [1] rejected, [2] fp64 steps
-    int* status;                          // [0] watchdog flag
-    int persistent;
-    int refill_threshold;
-    int family;                           // >= 0: trace only the rays of frames of this family
-    unsigned long long* clock0;           // launch start on the device clock (first warp stamps it)
-    unsigned long long watchdog_ns;       // globaltimer bound for the whole launch, per warp
-    CfgDev c;
-    FrameDev f0;                          // the frame of a one-frame launch (read from the parameter bank)
-};
-
-// The frame of ray state s: a one-frame launch (UNI) reads it, metric included,
-// from the kernel's parameter bank, whose constants the arithmetic takes as
-// operands instead of loading them from global memory.
-template <bool UNI>
-__device__ __forceinline__ const FrameDev& frame_of(const Params& P, int frame) {
-    if constexpr (UNI) return P.f0;
-    else return P.frames[frame];
-}
-
-__device__ __forceinline__ unsigned long long globaltimer() {
-    unsigned long long t;
-    asm volatile("mov.u64 %0, %globaltimer;" : "=l"(t));
-    return t;
-}
-
-__device__ __forceinline__ int find_frame(const FrameDev* frames, int n, long long idx) {
-    int lo = 0, hi = n - 1;
-    while (lo < hi) {
-        const int mid = (lo + hi + 1) >> 1;
-        if (frames[mid].ray_offset <= idx) lo = mid; else hi = mid - 1;
-    }
-    return lo;
-}
-
-// Per-ray state held in registers between steps. K is the storage type of the
-// first-same-as-last derivative f(x, p): float on the mixed path (the FP64
-// island recomputes it in FP64), double on the all-FP64 path.
-template <bool MIXED>
-struct Ray {
-    using K = typename std::conditional<MIXED, float, double>::type;
-    double x[4], p[4];
-    K k[8];
-    double h;
-    double intensity;
-    float min_r, null_max, tphi, prev_z;
-    float prev_r;  // r at the start of the step (volumetric early-out)
-    int steps, rejected, attempts, ncross, eq, fp64_steps;
-    int frame;
-    int crit;  // mixed path: the ray skims the photon region, every step in FP64
-    long long idx;
-};
-
-// Kerr-Newman radial potential of a null ray, R(r) = ((r^2+a^2) E - a L)^2 -
-// Delta (Q + (L - a E)^2), Delta = r^2 - 2 M r + a^2 + Q_e^2: a double root marks
-// the critical curve. Returns min R / (E^2 r^4) over the photon region
-// r in [1.0001 r_+, 4.5 M] (48 samples).
-__device__ __forceinline__ double radial_potential_gap(const MetricDev& m, double rp, double E, double L, double Q) {
-    double best = 1e300;
-    const double r0 = 1.0001 * rp, r1 = 4.5 * m.M;
-    for (int i = 0; i < 48; ++i) {
-        const double r = r0 + (r1 - r0) * (i / 47.0);
-        const double A = (r * r + m.a2) * E - m.a * L;
-        const double D = r * r - 2.0 * m.M * r + m.a2 + m.Q2;
-        const double La = L - m.a * E;
-        const double R = (A * A - D * (Q + La * La)) / (E * E * r * r * r * r);
-        best = fmin(best, R);
-    }
-    return best;
-}
-
-__device__ __forceinline__ void write_default_crossings(sirius_ray_result* R) {
-#pragma unroll
-    for (int i = 0; i < SIRIUS_MAX_CROSSINGS; ++i) {
-        R->disk_r[i] = 0.f; R->disk_phi[i] = 0.f; R->disk_g[i] = 1.f; R->disk_flux[i] = 0.f;
-    }
-}
-
-__device__ void invariants(const MetricDev& m, const InvForm& F, const double x[4], const double p[4], float& E,
-                           float& Lz, float& Q) {
-    E = float(-p[0]);
-    if (m.family == SIRIUS_METRIC_MORRIS_THORNE) {
-        const double s = sin(x[2]), c = cos(x[2]);
-        Lz = float(p[3]);
-        Q = float(p[2] * p[2] + c * c * p[3] * p[3] / (s * s));
-        return;
-    }
-    const double L = x[1] * p[2] - x[2] * p[1];
-    Lz = float(L);
-    const double r = F.r;
-    const double ct = fmin(fmax(x[3] / r, -1.0), 1.0);
-    const double st = sqrt(fmax(1.0 - ct * ct, 1e-30));
-    const double pth = (ct / st) * (x[1] * p[1] + x[2] * p[2]) - r * st * p[3];
-    const double e = -p[0];
-    Q = float(pth * pth + ct * ct * (-m.a2 * e * e + L * L / (st * st)));
-}
-
-template <bool MIXED, int FAM, bool UNI>
-__device__ __forceinline__ void begin_ray(const Params& P, Ray<MIXED>& s, long long idx, int frame, float* vol) {
-    using K = typename Ray<MIXED>::K;
-    s.idx = idx;
-    s.frame = frame;
-    const FrameDev& F = frame_of<UNI>(P, s.frame);
-    double dir[4];
-    if (P.host_rays) {
-        const sirius_camera_ray& cr = P.host_rays[idx];
-        for (int i = 0; i < 4; ++i) dir[i] = cr.direction[i];
-    } else {
-        const long long pix = idx - F.ray_offset;
-        camera_dir(F, int(pix % F.width), int(pix / F.width), dir);
-    }
-    init_state(F, dir, s.x, s.p);
-    K xk[4], pk[4];
-    for (int i = 0; i < 4; ++i) { xk[i] = K(s.x[i]); pk[i] = K(s.p[i]); }
-    rhs<K, FAM>(F.m, xk, pk, s.k, s.k + 4);
-    s.h = P.c.h0;
-    s.intensity = 0.0;
-    s.min_r = 1e10f;
-    s.null_max = 0.f;
-    s.tphi = 0.f;
-    s.prev_z = float(s.x[3]);
-    s.prev_r = float(ks_radius(F.m, s.x));
-    s.steps = s.rejected = s.attempts = s.ncross = s.eq = s.fp64_steps = 0;
-    s.crit = 0;
-    if (MIXED && F.gate && P.c.crit_band > 0.0) {
-        InvForm GF;
-        inv_form(F.m, s.x, GF);
-        float E, L, Q;
-        invariants(F.m, GF, s.x, s.p, E, L, Q);
-        s.crit = fabs(radial_potential_gap(F.m, F.r_plus, double(E), double(L), double(Q))) < P.c.crit_band;
-    }
-    if (P.results) {
-        sirius_ray_result* R = P.results + idx;
-        write_default_crossings(R);
-        InvForm IF;
-        inv_form(F.m, s.x, IF);
-        float E, L, Q;
-        invariants(F.m, IF, s.x, s.p, E, L, Q);
-        R->E0 = E; R->Lz0 = L; R->Carter0 = Q;
-        // impact parameter heuristic (GTRC001A.cpp:208-233)
-        float b = 0.f;
-        if (!is_family<FAM>(F.m, SIRIUS_METRIC_MORRIS_THORNE)) {
-            const double k1 = double(s.k[1]), k2 = double(s.k[2]), k3 = double(s.k[3]);
-            const double R0 = sqrt(s.x[1] * s.x[1] + s.x[2] * s.x[2] + s.x[3] * s.x[3]);
-            const double vm = sqrt(k1 * k1 + k2 * k2 + k3 * k3);
-            const double vrad = (k1 * s.x[1] + k2 * s.x[2] + k3 * s.x[3]) / R0;
-            b = float(R0 * sqrt(fmax(vm * vm - vrad * vrad, 0.0)) / fmax(vm, 1e-10));
-        }
-        R->impact_parameter = b;
-    }
-    if (vol)
-        for (int b = 0; b < P.c.nbins; ++b) { vol[2 * b * blockDim.x] = 0.f; vol[(2 * b + 1) * blockDim.x] = 1.f; }
-}
-
-template <bool MIXED, bool UNI>
-__device__ __forceinline__ void end_ray(const Params& P, const Ray<MIXED>& s, int outcome, float magnification, int flags,
-                                     const float* vol) {
-    const FrameDev& F = frame_of<UNI>(P, s.frame);
-    if (P.image) P.image[s.idx] = float(s.intensity);
-    if (P.spectra && vol)
-        for (int b = 0; b < P.c.nbins; ++b) P.spectra[s.idx * P.c.nbins + b] = vol[2 * b * blockDim.x];
-    if (!P.results) return;
-    sirius_ray_result* R = P.results + s.idx;
-    InvForm IF;
-    inv_form(F.m, s.x, IF);
-    float E, L, Q;
-    invariants(F.m, IF, s.x, s.p, E, L, Q);
-    R->outcome = outcome;
-    R->steps = s.steps;
-    R->rejected = s.rejected;
-    R->n_crossings = s.ncross;
-    for (int i = 0; i < 4; ++i) {
-        R->final_x[i] = s.x[i];
-        R->final_p[i] = s.p[i];
-        R->final_k[i] = float(s.k[i]);
-    }
-    R->equatorial_crossings = s.eq;
-    R->image_order = s.eq >= 1 ? (s.eq + 1) / 2 : 0;
-    R->total_phi_change = s.tphi;
-    R->min_radius = s.min_r;
-    R->intensity = float(s.intensity);
-    R->E = E; R->Lz = L; R->Carter = Q;
-    R->null_drift_max = s.null_max;
-    R->null_final = float(fabs(inv_apply(F.m, IF, s.p, s.p)));
-    R->magnification = magnification;
-    float tmin = 1.f;
-    if (vol)
-        for (int b = 0; b < P.c.nbins; ++b) tmin = fminf(tmin, vol[(2 * b + 1) * blockDim.x]);
-    R->optical_depth = tmin > 0.f ? -logf(tmin) : 1e30f;
-    R->fp64_steps = s.fp64_steps;
-    R->flags = flags;
-}
-
-// A point of the step's cubic Hermite interpolant at parameter q in [0, 1].
-__device__ __forceinline__ void hermite_xyz(const double x0[4], const double x1[4], const float k0[4],
-                                            const float k1[4], double h, double q, float& xs, float& ys, float& zs) {
-    const double q2 = q * q, q3 = q2 * q;
-    const double h00 = 2.0 * q3 - 3.0 * q2 + 1.0, h10 = (q3 - 2.0 * q2 + q) * h, h01 = -2.0 * q3 + 3.0 * q2,
-                 h11 = (q3 - q2) * h;
-    xs = float(h00 * x0[1] + h10 * k0[1] + h01 * x1[1] + h11 * k1[1]);
-    ys = float(h00 * x0[2] + h10 * k0[2] + h01 * x1[2] + h11 * k1[2]);
-    zs = float(h00 * x0[3] + h10 * k0[3] + h01 * x1[3] + h11 * k1[3]);
-}
-
-__device__ __forceinline__ float ks_r(const MetricDev& m, float x, float y, float z) {
-    const float a2 = float(m.a2), R2 = x * x + y * y + z * z, Rm2 = R2 - a2;
-    const float sd = sqrtf(fmaxf(Rm2 * Rm2 + 4.f * a2 * z * z, 1e-20f));
-    return sqrtf(fmaxf(0.5f * (Rm2 + sd), 1e-10f));
-}
-
-// Volumetric transfer over the accepted segment x0 -> x1 (affine length h):
-// Gauss-Legendre points on the step's cubic Hermite interpolant (the reference
-// marches the chord with midpoints, GTRC001A.cpp:943-958) over the part of the
-// step inside the emitting annulus r_in <= r <= r_out (its edges, where j jumps,
-// are located by bisection), camera-first accumulation per bin:
-// I_b += T_b S (1 - e^-dtau), T_b = e^-tau_b,
-//   j = j0 r^-2 exp(-z^2/(2 (h_z r)^2)) nu_em^-s, alpha = c_a j,
-//   dtau = alpha (nu_cam/g) dl, S = g^3 / c_a.  (vol: [2b] = I_b, [2b+1] = T_b, stride blockDim)
-__device__ __forceinline__ void volumetric_segment(const Params& P, const FrameDev& F, const double x0[4],
-                                                const double x1[4], const float k0[4], const float k1[4],
-                                                const double p[4], double h, float r0, float r1, float* vol) {
-    const CfgDev& c = P.c;
-    const int nq = c.vol_sub < 1 ? 1 : (c.vol_sub > 4 ? 4 : c.vol_sub);
-    const float E = float(-p[0]);
-    const float Lz = float(x1[1] * p[2] - x1[2] * p[1]);
-    const float nu_cam = E / observer_factor<float>(F, E);
-    const float rin = float(F.disk_in), rout = float(F.disk_out);
-    const bool in0 = r0 >= rin && r0 <= rout, in1 = r1 >= rin && r1 <= rout;
-    double fa = 0.0, fb = 1.0;
-    if (in0 != in1) {
-        // the annulus edge on the step's Hermite interpolant: regula falsi
-        // (Illinois) on r(q) - edge over [0, 1], three evaluations
-        const float edge = in0 ? (r1 < rin ? rin : rout) : (r0 < rin ? rin : rout);
-        double qa = 0.0, qb = 1.0, ga = double(r0) - edge, gb = double(r1) - edge;
-        int side = 0;
-        for (int it = 0; it < 3; ++it) {
-            const double q = (qa * gb - qb * ga) / (gb - ga);
-            float xs, ys, zs;
-            hermite_xyz(x0, x1, k0, k1, h, q, xs, ys, zs);
-            const double g = double(ks_r(F.m, xs, ys, zs)) - edge;
-            if ((g < 0.0) == (ga < 0.0)) {
-                qa = q; ga = g;
-                if (side == -1) gb *= 0.5;
-                side = -1;
-            } else {
-                qb = q; gb = g;
-                if (side == 1) ga *= 0.5;
-                side = 1;
-            }
-        }
-        const double qe = (qa * gb - qb * ga) / (gb - ga);
-        if (in0) fb = qe;
-        else fa = qe;
-    }
-    const double span = fb - fa;
-    // per Gauss-Legendre point: optical depth per unit nu^-s and source function
-    float dt0[4], S[4];
-#pragma unroll
-    for (int s = 0; s < 4; ++s) {
-        dt0[s] = 0.f;
-        S[s] = 0.f;
-        if (s >= nq) continue;
-        float xs, ys, zs;
-        hermite_xyz(x0, x1, k0, k1, h, fa + span * double(kGLx[nq - 1][s]), xs, ys, zs);
-        const float r = ks_r(F.m, xs, ys, zs);
-        if (r < rin || r > rout) continue;
-        const float zr = zs / (float(c.vol_hz) * r);
-        if (fabsf(zr) > float(kVolCutoff)) continue;
-        const float g = kepler_g<float>(F.m, xs, ys, zs, r, E, Lz, observer_factor<float>(F, E));
-        if (!(g > 0.f)) continue;
-        const float dl = float(h * span) * kGLw[nq - 1][s];
-        const float jsp = float(c.vol_j0) / (r * r) * __expf(-0.5f * zr * zr);
-        const float gs = __powf(g, float(c.vol_s));  // nu_em^-s = (g/nu_b)^s
-        dt0[s] = float(c.vol_aoj) * jsp * gs * (nu_cam / g) * dl;
-        S[s] = g * g * g / float(c.vol_aoj);
-    }
-    if (dt0[0] == 0.f && dt0[1] == 0.f && dt0[2] == 0.f && dt0[3] == 0.f) return;
-    for (int b = 0; b < c.nbins; ++b) {
-        float& I = vol[2 * b * blockDim.x];
-        float& Tr = vol[(2 * b + 1) * blockDim.x];  // transmittance e^-tau to the camera
-        float Ib = I, Tb = Tr;
-        const float cb = c.nu_pow[b];
-#pragma unroll
-        for (int s = 0; s < 4; ++s) {
-            const float dtau = dt0[s] * cb;
-            // 1 - e^-x by its series while x is small (no special-function unit needed)
-            const float om = dtau < 1e-3f ? dtau * (1.f - dtau * (0.5f - dtau * (1.f / 6.f))) : 1.f - __expf(-dtau);
-            Ib += Tb * S[s] * om;
-            Tb *= 1.f - om;
-        }
-        I = Ib;
-        Tr = Tb;
-    }
-}
-
-// A disk crossing at the event-located point (xc1, xc2, 0): BL radius, exact
-// redshift with the ray's conserved E and L_z (from the state x, p), flux.
-// Returns true when the crossing lies on the disk (GTRC001A.cpp:468-555).
-// Per-frame table of the Page-Thorne flux for the mixed path: kFluxN samples
-// at u = sqrt((r - r_in) / (r_out - r_in)) in [0, 1] (F ~ (r - r_ISCO) near the
-// inner edge is smooth in u), read by cubic Lagrange interpolation, followed by
-// kFluxN cell flags. The flux as the reference defines it switches to an
-// approximate form where the full expression is not positive (PHAD001A.h:321-361),
-// which leaves a kink; a cell whose interpolant misses the exact flux at its
-// midpoint by more than 1e-6 (relative) is flagged, and a crossing there
-// evaluates the 16-point quadrature itself, as the FP64 path does everywhere.
-constexpr int kFluxN = 256;
-constexpr int kFluxTable = 2 * kFluxN;  // floats per frame: samples, then cell flags
-
-__device__ __forceinline__ double flux_cubic(const float* t, double x) {
-    int j = int(x) - 1;
-    j = j < 0 ? 0 : (j > kFluxN - 4 ? kFluxN - 4 : j);
-    const double f = x - j;  // position within the samples j..j+3, in [0, 3]
-    const double w0 = -(f - 1.0) * (f - 2.0) * (f - 3.0) / 6.0, w1 = f * (f - 2.0) * (f - 3.0) / 2.0,
-                 w2 = -f * (f - 1.0) * (f - 3.0) / 2.0, w3 = f * (f - 1.0) * (f - 2.0) / 6.0;
-    return w0 * t[j] + w1 * t[j + 1] + w2 * t[j + 2] + w3 * t[j + 3];
-}
 
 // One block of kFluxN threads per frame.
 __global__ void __launch_bounds__(kFluxN) flux_table_kernel(const FrameDev* frames, float* table) {
@@ -400,445 +69,16 @@ __global__ void __launch_bounds__(kFluxN) flux_table_kernel(const FrameDev* fram
     t[kFluxN + j] = flag;
 }
 
-__device__ __forceinline__ double flux_lookup(const float* t, const FrameDev& F, double r) {
-    const double u = sqrt(fmin(fmax((r - F.disk_in) / (F.disk_out - F.disk_in), 0.0), 1.0));
-    const double x = u * (kFluxN - 1);
-    const int cell = min(int(x), kFluxN - 2);
-    if (t[kFluxN + cell] != 0.f) return nt_flux(r, F.a_star, F.isco, F.disk_in, F.disk_out);
-    return flux_cubic(t, x);
-}
-
-__device__ __forceinline__ bool record_crossing(const Params& P, const FrameDev& F, long long idx, int n, double xc1,
-                                             double xc2, const double x[4], const double p[4], double& intensity) {
-    const MetricDev& m = F.m;
-    const double xc[4] = {0.0, xc1, xc2, 0.0};
-    InvForm CF;
-    inv_form(m, xc, CF);
-    const double rc = CF.r;
-    if (!(rc >= F.disk_in && rc <= F.disk_out)) return false;
-    const double E = -p[0], Lz = x[1] * p[2] - x[2] * p[1];
-    const double g = kepler_g<double>(m, xc1, xc2, 0.0, rc, E, Lz, observer_factor<double>(F, E));
-    const double Fl = P.flux ? flux_lookup(P.flux + size_t(F.flux_slot) * kFluxTable, F, rc)
-                             : nt_flux(rc, F.a_star, F.isco, F.disk_in, F.disk_out);
-    intensity += exp(-P.c.decay * n) * g * g * g * g * Fl;
-    if (P.results) {
-        sirius_ray_result* R = P.results + idx;
-        R->disk_r[n] = float(rc);
-        R->disk_phi[n] = float(atan2(xc2, xc1));
-        R->disk_g[n] = float(g);
-        R->disk_flux[n] = float(Fl);
-    }
-    return true;
-}
-
-// The FP64 island of the mixed path is large and rare, so it stays out of line
-// (less code in the hot loop). Its arguments and results travel by value: an
-// array passed by address would pin the caller's ray state in local memory.
-struct Vec4v {
-    double v[4];
-};
-struct IslandStep {
-    double xn[4], pn[4];
-    float k7[8];
-    double err;
-};
-struct CrossXY {
-    double x, y;
-};
-
-__device__ __forceinline__ Vec4v vec4v(const double a[4]) { return Vec4v{{a[0], a[1], a[2], a[3]}}; }
-
-// The FP64 island attempt: f(x, p) recomputed in FP64, a DP45 attempt in FP64;
-// the derivative at the candidate point returned in float for the FP32 steps
-// that may follow.
-template <int FAM>
-__device__ __noinline__ IslandStep island_attempt(const MetricDev& m, const CfgDev& c, const Vec4v x, const Vec4v p,
-                                                  double h) {
-    IslandStep o;
-    double k1[8], k7[8];
-    rhs<double, FAM>(m, x.v, p.v, k1, k1 + 4);
-    o.err = dp45_attempt_lowreg<FAM>(m, c, x.v, p.v, h, k1, o.xn, o.pn, k7);
-#pragma unroll
-    for (int i = 0; i < 8; ++i) o.k7[i] = float(k7[i]);
-    return o;
-}
-
-// The equatorial crossing of an accepted island step, located in FP64.
-template <int FAM>
-__device__ __noinline__ CrossXY island_crossing(const MetricDev& m, const CfgDev& c, const Vec4v x, const Vec4v p,
-                                                double hs) {
-    CrossXY o;
-    locate_equator<double, FAM, true>(m, c, x.v, p.v, hs, o.x, o.y);
-    return o;
-}
-
-// f(x, p) of the current state in the storage precision of the path.
-template <bool MIXED, int FAM>
-__device__ __forceinline__ void refresh_derivative(const MetricDev& m, Ray<MIXED>& s) {
-    using K = typename Ray<MIXED>::K;
-    K xk[4], pk[4];
-    for (int i = 0; i < 4; ++i) { xk[i] = K(s.x[i]); pk[i] = K(s.p[i]); }
-    rhs<K, FAM>(m, xk, pk, s.k, s.k + 4);
-}
-
-// One iteration of the ray state machine: a DP45 attempt, and on acceptance
-// the termination checks. Returns -1 while the ray continues, else its outcome.
-template <bool MIXED, int FAM, bool UNI>
-__device__ __forceinline__ int advance(const Params& P, Ray<MIXED>& s, float& magnification, int& flags, float* vol) {
-    using K = typename Ray<MIXED>::K;
-    const FrameDev& F = frame_of<UNI>(P, s.frame);
-    const MetricDev& m = F.m;
-    const CfgDev& c = P.c;
-    double xn[4], pn[4];
-    K k7[8];
-    bool island = true;
-    double err;
-    if constexpr (MIXED) {
-        // FP64 island: inside island_factor * r_ph (retrograde) or near the horizon
-        const double R2 = s.x[1] * s.x[1] + s.x[2] * s.x[2] + s.x[3] * s.x[3];
-        island = s.crit ||
-                 (is_family<FAM>(m, SIRIUS_METRIC_MORRIS_THORNE) ? (s.x[1] < F.island_r)
-                                                                 : (R2 < F.island_r * F.island_r));
-    }
-    const bool symp = c.integrator == SIRIUS_INTEGRATOR_SYMPLECTIC;
-    if (symp) {
-        // fixed d-lambda, shrunk near the horizon as SymplecticIntegratorD::integrate
-        // does (h0 min(1, ((r - r_+)/r_+)^2), PHSI001A.h:260-263); always accepted
-        double hs = c.symp_step;
-        if (F.has_horizon) {
-            const double q = (ks_radius(m, s.x) - F.r_plus) / F.r_plus;
-            hs = fmax(c.hmin, hs * fmin(1.0, q * q));
-        }
-        s.h = hs;
-#pragma unroll
-        for (int i = 0; i < 4; ++i) { xn[i] = s.x[i]; pn[i] = s.p[i]; }
-        if (MIXED && !island) symplectic_step<float, FAM>(m, c.symp_order, hs, xn, pn);
-        else symplectic_step<double, FAM>(m, c.symp_order, hs, xn, pn);
-        K xk[4], pk[4];
-#pragma unroll
-        for (int i = 0; i < 4; ++i) { xk[i] = K(xn[i]); pk[i] = K(pn[i]); }
-        rhs<K>(m, xk, pk, k7, k7 + 4);
-        err = 0.0;
-    } else if constexpr (MIXED) {
-        if (island) {
-            const IslandStep o = island_attempt<FAM>(m, c, vec4v(s.x), vec4v(s.p), s.h);
-#pragma unroll
-            for (int i = 0; i < 4; ++i) { xn[i] = o.xn[i]; pn[i] = o.pn[i]; }
-#pragma unroll
-            for (int i = 0; i < 8; ++i) k7[i] = o.k7[i];
-            err = o.err;
-        } else {
-            err = dp45_attempt<float, FAM>(m, c, s.x, s.p, s.h, s.k, xn, pn, k7);
-        }
-    } else {
-        err = dp45_attempt<double, FAM>(m, c, s.x, s.p, s.h, s.k, xn, pn, k7);
-    }
-    ++s.attempts;
-    if (!(err <= 1.0)) {
-        ++s.rejected;
-        s.h = MIXED ? optimal_step_fast(s.h, isfinite(err) ? err : 1e10, c)
-                    : optimal_step(s.h, isfinite(err) ? err : 1e10, c);
-        if (c.enable_vol && c.enable_disk && F.has_horizon && is_family<FAM>(m, SIRIUS_METRIC_KERR_SCHILD)) {
-            InvForm RF;
-            inv_form(m, s.x, RF);
-            s.h = fmax(c.hmin, fmin(s.h, volume_step_cap(RF.r, s.x[3], double(s.k[1]), double(s.k[2]),
-                                                         double(s.k[3]), c.vol_hz, F.disk_in, F.disk_out)));
-        }
-        if (s.h <= c.hmin) { ++s.steps; return SIRIUS_STEP_UNDERFLOW; }
-        if (s.attempts > c.max_steps * 64 + 1024) return SIRIUS_STEP_UNDERFLOW;
-        return -1;
-    }
-    // accepted
-    const double hstep = s.h;
-    const bool disk_on = is_family<FAM>(m, SIRIUS_METRIC_KERR_SCHILD) && c.enable_disk && F.has_horizon;
-    // equatorial crossing inside the step: locate it from the step's start state
-    double xc1 = 0.0, xc2 = 0.0;
-    const bool cross = disk_on && (s.x[3] * xn[3] < 0.0);
-    if (cross) {
-        const double hs = hermite_root(s.x[3], xn[3], double(s.k[3]), double(k7[3]), hstep) * hstep;
-        if constexpr (MIXED) {
-            if (island) {
-                const CrossXY o = island_crossing<FAM>(m, c, vec4v(s.x), vec4v(s.p), hs);
-                xc1 = o.x;
-                xc2 = o.y;
-            }
-            else locate_equator_f32<FAM>(m, c, s.x, s.p, s.k, hs, xc1, xc2);
-        } else {
-            locate_equator<double, FAM>(m, c, s.x, s.p, hs, xc1, xc2);
-        }
-    }
-    double x0[4];
-    float k0f[4];
-#pragma unroll
-    for (int i = 0; i < 4; ++i) { x0[i] = s.x[i]; k0f[i] = float(s.k[i]); }
-    if (!symp) s.h = MIXED ? optimal_step_fast(s.h, err, c) : optimal_step(s.h, err, c);
-    ++s.steps;
-    if (MIXED && island) ++s.fp64_steps;
-    bool bad = false;
-#pragma unroll
-    for (int i = 0; i < 4; ++i) bad |= !isfinite(xn[i]) || !isfinite(pn[i]) || !isfinite(double(k7[i]));
-#pragma unroll
-    for (int i = 0; i < 4; ++i) { s.x[i] = xn[i]; s.p[i] = pn[i]; }
-#pragma unroll
-    for (int i = 0; i < 8; ++i) s.k[i] = k7[i];
-    if (bad) { flags |= SIRIUS_FLAG_NUMERICAL_FAILURE; return SIRIUS_NUMERICAL_FAILURE; }
-
-    // constraint re-projection (E, L_z and Carter preserving); the mixed path
-    // forms only the null value in FP64 (Kerr-Schild without Lambda)
-    double rr;
-    const bool project = c.proj_period > 0 && (s.steps % c.proj_period) == 0;
-    const bool ks_fast = MIXED && is_family<FAM>(m, SIRIUS_METRIC_KERR_SCHILD) && !m.has_lambda;
-    if (project) {
-        double pb[4];
-#pragma unroll
-        for (int i = 0; i < 4; ++i) pb[i] = s.p[i];
-        double before;
-        if (ks_fast) {
-            before = project_null_ks_mixed(m, s.x, s.p, rr);
-        } else {
-            InvForm IF;
-            inv_form(m, s.x, IF);
-            rr = IF.r;
-            before = project_null(m, IF, s.p);
-        }
-        s.null_max = fmaxf(s.null_max, float(fabs(before)));
-        // a projection that moved p beyond what the stored f(x, p) resolves
-        // (1e-10 relative in FP64, 1e-6 with FP32 storage) makes it stale: recompute it
-        double dp = 0.0, pm = 0.0;
-#pragma unroll
-        for (int i = 0; i < 4; ++i) {
-            dp = fmax(dp, fabs(s.p[i] - pb[i]));
-            pm = fmax(pm, fabs(s.p[i]));
-        }
-        if (dp > (MIXED ? 1e-6 : 1e-10) * pm) refresh_derivative<MIXED, FAM>(m, s);
-    } else if (ks_fast) {
-        rr = ks_radius(m, s.x);
-    } else {
-        InvForm IF;
-        inv_form(m, s.x, IF);
-        rr = IF.r;
-    }
-    if (float(rr) < s.min_r) s.min_r = float(rr);
-    if (disk_on && c.enable_vol && !symp)
-        s.h = fmax(c.hmin, fmin(s.h, volume_step_cap(rr, s.x[3], double(s.k[1]), double(s.k[2]), double(s.k[3]),
-                                                     c.vol_hz, F.disk_in, F.disk_out)));
-    const bool mt = is_family<FAM>(m, SIRIUS_METRIC_MORRIS_THORNE);
-
-    // winding: equatorial crossings and |d phi| (GTRC001A.cpp:294-309)
-    if (!mt) {
-        const float cz = float(s.x[3]);
-        if (s.prev_z * cz < 0.f) ++s.eq;
-        s.prev_z = cz;
-        const float cr = float(x0[1] * s.x[2] - x0[2] * s.x[1]);
-        const float dt = float(x0[1] * s.x[1] + x0[2] * s.x[2]);
-        s.tphi += fabsf(atan2f(cr, dt));
-    }
-    // spiral early-out (GTRC001A.cpp:322-352)
-    const int sidx = s.steps - 1;
-    if (c.spiral && !mt && (sidx % 100) == 0 && sidx > 100) {
-        const float ratio = s.min_r / float(F.r_ph_pro);
-        if (ratio < 1.5f && ratio > 0.9f && s.tphi > 2.f * float(kPi)) {
-            const double k1 = double(s.k[1]), k2 = double(s.k[2]), k3 = double(s.k[3]);
-            const double Reu = sqrt(s.x[1] * s.x[1] + s.x[2] * s.x[2] + s.x[3] * s.x[3]);
-            const double vrad = (s.x[1] * k1 + s.x[2] * k2 + s.x[3] * k3) / Reu;
-            const double vt = sqrt(k1 * k1 + k2 * k2 + k3 * k3);
-            if (fabs(vrad) / fmax(vt, 1e-10) < 0.3) return s.ncross > 0 ? SIRIUS_DISK_HIT : SIRIUS_SPIRALING;
-        }
-    }
-    // horizon
-    if (F.r_hor > 0.0 && rr < F.r_hor) return SIRIUS_HORIZON;
-    // throat
-    if (mt && s.x[1] <= 1.001 * m.b0 * 1.0001) return SIRIUS_THROAT;
-    // escape
-    {
-        const double Resc = mt ? s.x[1] : sqrt(s.x[1] * s.x[1] + s.x[2] * s.x[2] + s.x[3] * s.x[3]);
-        if (Resc > c.escape_r) {
-            const double vrad = mt ? double(s.k[1])
-                                   : (s.x[1] * double(s.k[1]) + s.x[2] * double(s.k[2]) + s.x[3] * double(s.k[3]));
-            if (vrad > 0.0) {
-                const float ratio = s.min_r / float(F.r_ph_pro);
-                if (ratio < 1.5f) {
-                    flags |= SIRIUS_FLAG_PHOTON_RING;
-                    magnification = ratio > 1.f ? fminf(1.f + 2.f / fmaxf(ratio - 1.f, 0.1f), 20.f) : 20.f;
-                }
-                return s.ncross > 0 ? SIRIUS_DISK_HIT : SIRIUS_ESCAPED;
-            }
-        }
-    }
-    if (!disk_on) return s.steps >= c.max_steps ? (s.ncross > 0 ? SIRIUS_DISK_HIT : SIRIUS_MAX_STEPS) : -1;
-    if (c.enable_vol && vol) {
-        // steps that cannot reach the emitting region skip the segment (the
-        // step cap keeps a step that starts outside it from jumping in)
-        const float r0 = s.prev_r, r1 = float(rr), rin = float(F.disk_in), rout = float(F.disk_out);
-        const float zc = float(kVolCutoff * c.vol_hz), z0 = float(x0[3]), z1 = float(s.x[3]);
-        const bool beyond = (r0 > rout && r1 > rout) ||
-                            (z0 * z1 > 0.f && fabsf(z0) > zc * fminf(fmaxf(r0, rin), rout) &&
-                             fabsf(z1) > zc * fminf(fmaxf(r1, rin), rout));
-        if (!beyond) {
-            float k1f[4];
-#pragma unroll
-            for (int i = 0; i < 4; ++i) k1f[i] = float(s.k[i]);
-            volumetric_segment(P, F, x0, s.x, k0f, k1f, s.p, hstep, r0, r1, vol);
-        }
-    }
-    s.prev_r = float(rr);
-    // thin-disk crossing (GTRC001A.h:404-431, GTRC001A.cpp:468-555)
-    if (cross && s.ncross < SIRIUS_MAX_CROSSINGS) {
-        if (record_crossing(P, F, s.idx, s.ncross, xc1, xc2, s.x, s.p, s.intensity)) {
-            ++s.ncross;
-            const float ratio = s.min_r / float(F.r_ph_pro);
-            if (ratio < 1.5f) {
-                flags |= SIRIUS_FLAG_PHOTON_RING;
-                magnification = ratio > 1.f ? fminf(1.f + 2.f / fmaxf(ratio - 1.f, 0.05f), 100.f) : 100.f;
-            }
-            if (s.ncross >= SIRIUS_MAX_CROSSINGS) return SIRIUS_DISK_HIT;
-        }
-    }
-    if (s.steps >= c.max_steps) return s.ncross > 0 ? SIRIUS_DISK_HIT : SIRIUS_MAX_STEPS;
-    return -1;
-}
-
-// Persistent tracer. Dynamic shared memory: 2 * nbins floats per thread (volumetric bins).
-template <bool MIXED, int FAM, bool UNI>
-__device__ __forceinline__ void trace_body(const Params& P) {
-    extern __shared__ float smem[];
-    float* vol = (P.c.enable_vol && P.c.nbins > 0) ? smem + threadIdx.x : nullptr;
-    const int lane = threadIdx.x & 31;
-    const unsigned lt_mask = (1u << lane) - 1u;
-    Ray<MIXED> s;
-    bool alive = false;
-    float magnification = 1.f;
-    int flags = 0;
-    unsigned long long acc = 0, rej0 = 0, f64 = 0;
-    bool exhausted = false;
-    // the watchdog bounds the whole launch: every warp measures from the first warp's start
-    unsigned long long t_start = 0;
-    if (lane == 0) {
-        const unsigned long long now = globaltimer();
-        const unsigned long long first = atomicCAS(P.clock0, 0ull, now);
-        t_start = first ? first : now;
-    }
-    t_start = __shfl_sync(kFull, t_start, 0);
-
-    if (!P.persistent) {
-        const long long gid = (long long)blockIdx.x * blockDim.x + threadIdx.x;
-        const unsigned entry = (P.list && gid < P.total) ? P.list[gid] : 0u;
-        if (gid < P.total && entry != kListSkip) {
-            const long long idx = P.list ? (long long)entry : gid;
-            const int frame = P.n_frames > 1 ? find_frame(P.frames, P.n_frames, idx) : 0;
-            if (P.family < 0 || P.frames[frame].m.family == P.family) {
-                begin_ray<MIXED, FAM, UNI>(P, s, idx, frame, vol);
-                alive = true;
-            }
-        }
-        exhausted = true;
-    }
-    for (unsigned iter = 0;; ++iter) {
-        if (P.persistent && !exhausted) {
-            const unsigned dead = __ballot_sync(kFull, !alive);
-            const int nlive = 32 - __popc(dead);
-            if (dead && nlive < P.refill_threshold) {
-                unsigned long long base = 0;
-                if (lane == 0) base = atomicAdd(P.queue, (unsigned long long)__popc(dead));
-                base = __shfl_sync(kFull, base, 0);
-                if (base >= (unsigned long long)P.total) exhausted = true;
-                if (!alive) {
-                    const unsigned long long q = base + __popc(dead & lt_mask);
-                    const unsigned entry = (P.list && q < (unsigned long long)P.total) ? P.list[q] : 0u;
-                    if (q < (unsigned long long)P.total && entry != kListSkip) {
-                        const unsigned long long idx = P.list ? (unsigned long long)entry : q;
-                        const int frame = P.n_frames > 1 ? find_frame(P.frames, P.n_frames, (long long)idx) : 0;
-                        begin_ray<MIXED, FAM, UNI>(P, s, (long long)idx, frame, vol);
-                        alive = true;
-                        magnification = 1.f;
-                        flags = 0;
-                    }
-                }
-            }
-        }
-        if ((iter & 255u) == 0) {
-            int stop = 0;
-            if (lane == 0) {
-                if (globaltimer() - t_start > P.watchdog_ns) atomicOr(P.status, 1);
-                stop = *((volatile int*)P.status) & 1;
-            }
-            stop = __shfl_sync(kFull, stop, 0);
-            if (stop) {
-                // watchdog: abandon the remaining queue and close the live rays
-                exhausted = true;
-                if (alive) { end_ray<MIXED, UNI>(P, s, SIRIUS_MAX_STEPS, magnification, flags, vol); alive = false; }
-            }
-        }
-        if (__ballot_sync(kFull, alive) == 0) {
-            if (!P.persistent || exhausted) break;
-            continue;
-        }
-        if (alive) {
-            const int out = advance<MIXED, FAM, UNI>(P, s, magnification, flags, vol);
-            if (out >= 0) {
-                end_ray<MIXED, UNI>(P, s, out, magnification, flags, vol);
-                acc += s.steps;
-                rej0 += s.rejected;
-                f64 += s.fp64_steps;
-                alive = false;
-            }
-        }
-    }
-    // warp-aggregated counters
-    for (int o = 16; o > 0; o >>= 1) {
-        acc += __shfl_down_sync(kFull, acc, o);
-        rej0 += __shfl_down_sync(kFull, rej0, o);
-        f64 += __shfl_down_sync(kFull, f64, o);
-    }
-    if (lane == 0) {
-        atomicAdd(&P.counters[0], acc);
-        atomicAdd(&P.counters[1], rej0);
-        atomicAdd(&P.counters[2], f64);
-    }
-}
-
-// The tracer compiled for MINB resident 128-thread blocks per SM (MINB 2: up to
-// 255 registers, 3: 168, 4: 128).
-template <bool MIXED, int MINB, int FAM, bool UNI>
-__global__ void __launch_bounds__(128, MINB) trace_kernel(const __grid_constant__ Params P) {
-    trace_body<MIXED, FAM, UNI>(P);
-}
-
-using TraceFn = void (*)(Params);
 constexpr int kDefaultMinBlocks = 2;       // up to 255 registers
 constexpr int kDefaultMinBlocksMixed = 4;  // 128 registers: mixed DP45
-
-template <bool MIXED, int FAM, bool UNI>
-TraceFn pick_minb(int minb) {
-    switch (minb) {
-        case 1: return trace_kernel<MIXED, 1, FAM, UNI>;
-        case 3: return trace_kernel<MIXED, 3, FAM, UNI>;
-        case 4: return trace_kernel<MIXED, 4, FAM, UNI>;
-        default: return trace_kernel<MIXED, 2, FAM, UNI>;
-    }
-}
 
 // A kernel specialised for one metric family carries only that family's
 // right-hand side (a smaller loop body and register set); kAnyFamily
 // dispatches per ray. The Kerr-Schild kernels come in every register budget,
 // and for one-frame launches (uni) with the frame in the parameter bank.
 TraceFn pick_kernel(bool mixed, int minb, int fam, bool uni = false) {
-    switch (fam) {
-        case SIRIUS_METRIC_KERR_SCHILD:
-            if (uni)
-                return mixed ? pick_minb<true, SIRIUS_METRIC_KERR_SCHILD, true>(minb)
-                             : pick_minb<false, SIRIUS_METRIC_KERR_SCHILD, true>(minb);
-            return mixed ? pick_minb<true, SIRIUS_METRIC_KERR_SCHILD, false>(minb)
-                         : pick_minb<false, SIRIUS_METRIC_KERR_SCHILD, false>(minb);
-        case SIRIUS_METRIC_MORRIS_THORNE:
-            return mixed ? trace_kernel<true, 2, SIRIUS_METRIC_MORRIS_THORNE, false>
-                         : trace_kernel<false, 2, SIRIUS_METRIC_MORRIS_THORNE, false>;
-        case SIRIUS_METRIC_ALCUBIERRE:
-            return mixed ? trace_kernel<true, 2, SIRIUS_METRIC_ALCUBIERRE, false>
-                         : trace_kernel<false, 2, SIRIUS_METRIC_ALCUBIERRE, false>;
-        default:
-            return mixed ? trace_kernel<true, 2, kAnyFamily, false> : trace_kernel<false, 2, kAnyFamily, false>;
-    }
+    if (fam == SIRIUS_METRIC_KERR_SCHILD) return mixed ? pick_ks_mixed(minb, uni) : pick_ks_fp64(minb, uni);
+    return pick_family(mixed, fam);
 }
 
 // ---------------------------------------------------------------------------

@@ -89,7 +89,7 @@ __device__ __forceinline__ double pt_dOm(double r, double a) {
     return -3.0 * sqrt(r) / (2.0 * den * den);
 }
 
-__device__ double nt_flux(double r, double a, double isco, double r_in, double r_out) {
+static __device__ double nt_flux(double r, double a, double isco, double r_in, double r_out) {
     const double gx[8] = {0.0950125098376374, 0.2816035507792589, 0.4580167776572274, 0.6178762444026438,
                           0.7554044083550030, 0.8656312023878318, 0.9445750230732326, 0.9894009349916499};
     const double gw[8] = {0.1894506104550685, 0.1826034150449236, 0.1691565193950025, 0.1495959888165767,
@@ -266,8 +266,8 @@ struct DPTable {
      {T(35.0 / 384.0 - 5179.0 / 57600.0), T(0), T(500.0 / 1113.0 - 7571.0 / 16695.0),                              \
       T(125.0 / 192.0 - 393.0 / 640.0), T(-2187.0 / 6784.0 + 92097.0 / 339200.0), T(11.0 / 84.0 - 187.0 / 2100.0),  \
       T(-1.0 / 40.0)}}
-__constant__ DPTable<float> kDPf = SIRIUS_DP45_TABLE(float);
-__constant__ DPTable<double> kDPd = SIRIUS_DP45_TABLE(double);
+static __constant__ DPTable<float> kDPf = SIRIUS_DP45_TABLE(float);
+static __constant__ DPTable<double> kDPd = SIRIUS_DP45_TABLE(double);
 
 template <class T>
 __device__ __forceinline__ const DPTable<T>& dp_table();
@@ -463,7 +463,7 @@ __device__ __forceinline__ double optimal_step(double h, double err, const CfgDe
 // (k = g^{-1} p, f = 1/2 d g k k). The three phases share one RHS call site;
 // the right-hand sides run in T, the state accumulates in FP64.
 // ---------------------------------------------------------------------------
-__constant__ double kYoshida[3][15] = {
+static __constant__ double kYoshida[3][15] = {
     {1.3512071919596576, -1.7024143839193153, 1.3512071919596576},
     {0.78451361047756, 0.23557321335936, -1.17767998417887, 1.31518632068391, -1.17767998417887,
      0.23557321335936, 0.78451361047756},
@@ -512,12 +512,12 @@ __device__ __forceinline__ double optimal_step_fast(double h, double err, const 
 
 // Gauss-Legendre points and weights on [0, 1] for n = 1..4 (Abramowitz & Stegun
 // 25.4), ordered along the step: the volumetric quadrature of one step.
-__constant__ float kGLx[4][4] = {{0.5f, 0, 0, 0},
+static __constant__ float kGLx[4][4] = {{0.5f, 0, 0, 0},
                                  {0.21132486540518713f, 0.78867513459481287f, 0, 0},
                                  {0.11270166537925831f, 0.5f, 0.88729833462074169f, 0},
                                  {0.069431844202973713f, 0.33000947820757187f, 0.66999052179242813f,
                                   0.93056815579702629f}};
-__constant__ float kGLw[4][4] = {{1.0f, 0, 0, 0},
+static __constant__ float kGLw[4][4] = {{1.0f, 0, 0, 0},
                                  {0.5f, 0.5f, 0, 0},
                                  {0.27777777777777778f, 0.44444444444444444f, 0.27777777777777778f, 0},
                                  {0.17392742256872693f, 0.32607257743127307f, 0.32607257743127307f,
