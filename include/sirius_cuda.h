@@ -32,7 +32,7 @@
 extern "C" {
 #endif
 
-#define SIRIUS_CUDA_ABI_VERSION 1
+#define SIRIUS_CUDA_ABI_VERSION 2
 
 /* ---- status codes --------------------------------------------------------- */
 enum sirius_status {
@@ -135,6 +135,14 @@ typedef struct sirius_frame {
     double disk_inner;           /* <= 0: use the prograde ISCO of the frame's (M,a) */
     double disk_outer;
     int64_t ray_offset;          /* first ray/pixel index of this frame in the batch outputs */
+    /* Row window: trace only camera rows [row_begin, row_begin + row_count) of the
+     * width x height image (row_count 0: every row, row_begin 0). Each ray is the
+     * one the full frame traces through that pixel, so a frame split into row
+     * blocks across devices reassembles the full frame bit for bit (the tile
+     * distribution of ACMG001A.h:256). The frame then holds width * row_count
+     * rays, output (y - row_begin) * width + x. */
+    int32_t row_begin;
+    int32_t row_count;
 } sirius_frame;
 
 /* ---- a host-generated camera ray (CameraRay, CMBS001A.h:26-32) -------------- */
@@ -234,14 +242,17 @@ typedef struct sirius_ray_result {
     float total_phi_change;
     float min_radius;
     float intensity;             /* bolometric: sum_n exp(-decay n) g_n^4 F(r_n) (+ volumetric) */
-    float E, Lz, Carter;         /* conserved quantities at termination (p_t, KS azimuthal, Carter Q) */
-    float E0, Lz0, Carter0;      /* ... at initialisation */
+    int32_t fp64_steps;          /* accepted steps taken on the FP64 island path (mixed precision) */
+    /* conserved quantities (computeConservedQuantities, MTTP001A.h:114-132), evaluated in
+     * FP64 from the FP64 state: E = -p_t, L_z = x p_y - y p_x (the Kerr-Schild azimuthal
+     * momentum), Carter Q = p_theta^2 + cos^2(theta) (-a^2 E^2 + L_z^2 / sin^2(theta)) */
+    double E, Lz, Carter;        /* at termination */
+    double E0, Lz0, Carter0;     /* at initialisation */
     float null_drift_max;        /* max over accepted steps of |g^{mu nu} p_mu p_nu| before re-projection */
     float null_final;            /* |g^{mu nu} p_mu p_nu| of the returned state */
     float impact_parameter;
     float magnification;
     float optical_depth;
-    int32_t fp64_steps;          /* accepted steps taken on the FP64 island path (mixed precision) */
     int32_t flags;               /* SIRIUS_FLAG_* bits */
 } sirius_ray_result;
 
@@ -301,12 +312,17 @@ int sirius_cuda_trace_frames_device(sirius_cuda_handle handle,
  * already holds the device memory it is given, or a frame loop that cannot
  * afford the implicit device-wide synchronisation of cudaMalloc/cudaFree.
  * Limits: at most SIRIUS_STATIC_MAX_FRAMES frames per call (more is rejected
- * with SIRIUS_ERR_INVALID_ARGUMENT). The counters and status word must start a
- * launch at zero; the call zeroes them on `stream` itself. The scratch is one
- * per device: overlapping calls on one device (other streams, handles or host
- * threads) race on it and must be serialised by the caller. The scratch address
+ * with SIRIUS_ERR_INVALID_ARGUMENT). Each call copies the frame descriptors to
+ * the host and synchronises `stream` before it launches; it returns while its
+ * kernels still run. The counters and status word must start a launch at zero;
+ * the call zeroes them on `stream` itself. The scratch is one per device, and
+ * every call rewrites it: calls whose kernels overlap on one device race on
+ * it. A host-side lock is not enough, because a call returns before its kernels
+ * end: order successive calls on the device, on one stream, or with an event
+ * recorded after call N that call N+1's stream waits on. The scratch address
  * is resolved on the first call per device; make that first call before any
- * stream capture. sirius_cuda_last_stats does not describe these launches. */
+ * stream capture. sirius_cuda_last_stats does not describe these launches: the
+ * handle's statistics keep describing its last traced call. */
 #define SIRIUS_STATIC_MAX_FRAMES 64
 int sirius_cuda_trace_frames_static(sirius_cuda_handle handle,
                                     const sirius_frame* d_frames, int32_t n_frames,

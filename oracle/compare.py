@@ -1,0 +1,99 @@
+"""Per-output error report of an engine trace against the CPU oracle.
+
+TEST INFRASTRUCTURE ONLY — imported by tests/ and by the CPU-baseline leg of
+bench.py, as the checker; never by the product package.
+
+The outputs compared are the ones the task's accuracy bars name (null-constraint
+drift, conserved E / L_z / Carter Q, terminal position and direction, outcome
+agreement, disk crossings, image intensity). Rays whose histories split at
+rounding level between the two integrations are counted and left out of the
+per-ray comparisons: a different outcome, a different number of disk crossings
+or equatorial crossings (a grazing ray that one integration sends just inside
+the horizon or the disk edge and the other just outside). Everything else is
+compared ray by ray, and the maxima are over every compared ray.
+
+Conserved quantities (computeConservedQuantities, MTTP001A.h:114-132):
+  drift      |X_final - X_initial| / max(|X_initial|, floor) per ray of the engine,
+             with floor = 1e-3 x the median |X_initial| of the frame (L_z and Q
+             vanish on some rays, where a relative drift is meaningless);
+  vs_oracle  |X_engine - X_oracle| / max(|X_oracle|, floor) at termination.
+"""
+import numpy as np
+
+
+def _stats(v):
+    v = np.asarray(v, dtype=np.float64)
+    if v.size == 0:
+        return {"max": 0.0, "p99": 0.0, "n": 0}
+    return {"max": float(v.max()), "p99": float(np.percentile(v, 99)), "n": int(v.size)}
+
+
+def _rel(a, b, x0):
+    floor = 1e-3 * float(np.median(np.abs(x0))) if x0.size else 0.0
+    floor = max(floor, 1e-300)
+    return np.abs(a - b) / np.maximum(np.abs(x0), floor)
+
+
+def split_histories(res, ref):
+    """Rays whose histories split at rounding level: outcome, disk crossings or
+    equatorial crossings differ."""
+    return ((res["outcome"] != ref["outcome"]) | (res["n_crossings"] != ref["n_crossings"]) |
+            (res["equatorial_crossings"] != ref["equatorial_crossings"]))
+
+
+def report(res, img, ref, spectra=None, ref_bins=None):
+    """Errors of an engine trace (results res, image img, optional spectra) against
+    the oracle's trace of the same pixels (ref, ref_bins). Images are compared
+    relative to the oracle image's peak, spectra per bin relative to the bin's peak."""
+    n = len(ref)
+    split = split_histories(res, ref)
+    same = ~split
+    out = {"rays": int(n), "outcome_agreement": float((res["outcome"] == ref["outcome"]).mean()),
+           "split_histories": int(split.sum())}
+    # null constraint |g^{mu nu} p_mu p_nu| of the engine: the largest value met before a
+    # re-projection, and the returned state's
+    out["null_before_projection"] = _stats(res["null_drift_max"])
+    out["null_final"] = _stats(res["null_final"])
+    # conserved quantities
+    for name in ("E", "Lz", "Carter"):
+        x0 = res[name + "0"].astype(np.float64)
+        out[name] = {"drift": _stats(_rel(res[name], res[name + "0"], x0)),
+                     "vs_oracle": _stats(_rel(res[name][same], ref[name][same], ref[name][same]))}
+    # terminal position (relative to the oracle's radius) and direction (angle between
+    # the spatial parts of k, radians)
+    xg = res["final_x"][same, 1:].astype(np.float64)
+    xo = ref["final_x"][same, 1:].astype(np.float64)
+    out["terminal_position"] = _stats(np.linalg.norm(xg - xo, axis=1) / np.maximum(np.linalg.norm(xo, axis=1), 1e-30))
+    kg = res["final_k"][same, 1:].astype(np.float64)
+    ko = ref["final_k"][same, 1:].astype(np.float64)
+    cos = np.sum(kg * ko, 1) / np.maximum(np.linalg.norm(kg, axis=1) * np.linalg.norm(ko, axis=1), 1e-300)
+    out["terminal_direction_rad"] = _stats(np.arccos(np.clip(cos, -1.0, 1.0)))
+    # disk crossings (first crossing of rays that both trace onto the disk)
+    hit = same & (ref["n_crossings"] > 0)
+    out["disk_r"] = _stats(np.abs(res["disk_r"][hit, 0] - ref["disk_r"][hit, 0]) / ref["disk_r"][hit, 0])
+    out["disk_g"] = _stats(np.abs(res["disk_g"][hit, 0] - ref["disk_g"][hit, 0]) /
+                           np.maximum(np.abs(ref["disk_g"][hit, 0]), 1e-30))
+    # image intensity, relative to the oracle image's peak: every compared ray, and every ray
+    scale = max(float(np.abs(ref["intensity"]).max()), 1e-300)
+    err = np.abs(np.asarray(img, dtype=np.float64) - ref["intensity"]) / scale
+    out["image"] = _stats(err[same])
+    out["image_all_rays"] = _stats(err)
+    if spectra is not None and ref_bins is not None and ref_bins.size:
+        bscale = np.maximum(np.abs(ref_bins).max(axis=0, keepdims=True), 1e-300)
+        serr = np.abs(np.asarray(spectra, dtype=np.float64) - ref_bins) / bscale
+        out["spectra"] = _stats(serr[same].ravel())
+    return out
+
+
+def summary(rep):
+    """One line per output: max and p99."""
+    lines = [f"rays {rep['rays']}, outcome agreement {rep['outcome_agreement']:.5f}, "
+             f"split histories {rep['split_histories']}"]
+    for k, v in rep.items():
+        if isinstance(v, dict) and "max" in v:
+            lines.append(f"{k}: max {v['max']:.3e} p99 {v['p99']:.3e}")
+        elif isinstance(v, dict):
+            for kk, vv in v.items():
+                lines.append(f"{k}.{kk}: max {vv['max']:.3e} p99 {vv['p99']:.3e}")
+    return "\n".join(lines)
+

@@ -1051,7 +1051,7 @@ void trace_ray(const TraceContext& ctx, const double origin[4], const double dir
     init_state(ctx, origin, dir, x, p, k);
     R E0, L0, Q0;
     invariants(m, x, p, E0, L0, Q0);
-    res.E0 = float(E0); res.Lz0 = float(L0); res.Carter0 = float(Q0);
+    res.E0 = double(E0); res.Lz0 = double(L0); res.Carter0 = double(Q0);
 
     const bool ks = m.family == SIRIUS_METRIC_KERR_SCHILD;
     const bool mt = m.family == SIRIUS_METRIC_MORRIS_THORNE;
@@ -1385,14 +1385,14 @@ void trace_ray(const TraceContext& ctx, const double origin[4], const double dir
         for (int i = 0; i < 4; ++i) res.final_p[i] = double(pp[i]);
         R E, L, Q;
         invariants(m, x, pp, E, L, Q);
-        res.E = float(E); res.Lz = float(L); res.Carter = float(Q);
+        res.E = double(E); res.Lz = double(L); res.Carter = double(Q);
         res.null_final = float(std::abs(double(inner(g1, k, k))));
         res.intensity = float(intensity + vol_acc);
         res.optical_depth = float(vol_tau);
     } else {
         R E, L, Q;
         invariants(m, x, p, E, L, Q);
-        res.E = float(E); res.Lz = float(L); res.Carter = float(Q);
+        res.E = double(E); res.Lz = double(L); res.Carter = double(Q);
         res.null_final = float(std::abs(double(null_value(m, x, p))));
         res.intensity = float(intensity);
         double taumax = 0;

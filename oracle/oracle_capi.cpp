@@ -23,12 +23,14 @@ void trace_pixels(const sirius_frame& f, const sirius_trace_config& cfg, int64_t
     ctx.disk_inner = f.disk_inner > 0 ? f.disk_inner : isco(astar) * f.metric.M;
     ctx.disk_outer = f.disk_outer;
     const int nb = std::min(cfg.n_bins, SIRIUS_MAX_BINS);
+    // pixel indices are relative to the frame's row window (row_count 0: the whole image)
+    const int64_t row0 = f.row_count > 0 ? f.row_begin : 0;
     std::atomic<int64_t> next{0};
     auto worker = [&]() {
         for (;;) {
             const int64_t i = next.fetch_add(1);
             if (i >= count) break;
-            const int64_t pix = first + i;
+            const int64_t pix = row0 * f.camera.width + first + i;
             const int px = int(pix % f.camera.width), py = int(pix / f.camera.width);
             double o[4], d[4];
             camera_ray(f.camera, px, py, o, d);
@@ -51,7 +53,8 @@ int oracle_sizeof_result() { return int(sizeof(sirius_ray_result)); }
 int oracle_sizeof_config() { return int(sizeof(sirius_trace_config)); }
 int oracle_sizeof_frame() { return int(sizeof(sirius_frame)); }
 
-// Trace pixels [first, first+count) of one frame (row-major pixel index).
+// Trace pixels [first, first+count) of one frame (row-major pixel index within
+// the frame's row window).
 // precision: 0 = double, 1 = long double.
 int oracle_trace_frame(const sirius_frame* f, const sirius_trace_config* cfg, int64_t first, int64_t count,
                        sirius_ray_result* out, double* bins, int threads, int precision) {

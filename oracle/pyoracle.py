@@ -64,9 +64,8 @@ class Oracle:
         assert L.oracle_sizeof_frame() == C.sizeof(abi.Frame)
 
     def trace_frame(self, frame, cfg, first=0, count=None, threads=1, long_double=False):
-        w, h = frame.camera.width, frame.camera.height
         if count is None:
-            count = w * h - first
+            count = abi.frame_rays(frame) - first
         out = np.zeros(count, dtype=abi.result_dtype())
         nb = max(cfg.n_bins, 0)
         bins = np.zeros((count, max(nb, 1)), dtype=np.float64)

@@ -5,7 +5,7 @@ field offset here against the compiled library.
 """
 import ctypes as C
 
-ABI_VERSION = 1
+ABI_VERSION = 2
 MAX_BINS = 32
 MAX_CROSSINGS = 4
 STATIC_MAX_FRAMES = 64  # SIRIUS_STATIC_MAX_FRAMES
@@ -68,7 +68,8 @@ class Camera(C.Structure):
 
 class Frame(C.Structure):
     _fields_ = [("metric", Metric), ("camera", Camera), ("disk_inner", C.c_double),
-                ("disk_outer", C.c_double), ("ray_offset", C.c_int64)]
+                ("disk_outer", C.c_double), ("ray_offset", C.c_int64),
+                ("row_begin", C.c_int32), ("row_count", C.c_int32)]
 
 
 class CameraRay(C.Structure):
@@ -103,11 +104,12 @@ class RayResult(C.Structure):
                 ("disk_flux", C.c_float * 4),
                 ("equatorial_crossings", C.c_int32), ("image_order", C.c_int32),
                 ("total_phi_change", C.c_float), ("min_radius", C.c_float), ("intensity", C.c_float),
-                ("E", C.c_float), ("Lz", C.c_float), ("Carter", C.c_float),
-                ("E0", C.c_float), ("Lz0", C.c_float), ("Carter0", C.c_float),
+                ("fp64_steps", C.c_int32),
+                ("E", C.c_double), ("Lz", C.c_double), ("Carter", C.c_double),
+                ("E0", C.c_double), ("Lz0", C.c_double), ("Carter0", C.c_double),
                 ("null_drift_max", C.c_float), ("null_final", C.c_float),
                 ("impact_parameter", C.c_float), ("magnification", C.c_float), ("optical_depth", C.c_float),
-                ("fp64_steps", C.c_int32), ("flags", C.c_int32)]
+                ("flags", C.c_int32)]
 
 
 class LaunchStats(C.Structure):
@@ -218,5 +220,11 @@ def make_camera(r=50.0, theta_deg=85.0, phi=0.0, fov=30.0, width=256, height=256
     return Camera(0.0, r, math.radians(theta_deg), phi, yaw, pitch, roll, fov, width, height, projection, observer)
 
 
-def make_frame(metric, camera, disk_inner=0.0, disk_outer=20.0, ray_offset=0):
-    return Frame(metric, camera, disk_inner, disk_outer, ray_offset)
+def make_frame(metric, camera, disk_inner=0.0, disk_outer=20.0, ray_offset=0, row_begin=0, row_count=0):
+    return Frame(metric, camera, disk_inner, disk_outer, ray_offset, row_begin, row_count)
+
+
+def frame_rays(frame):
+    """Rays of a frame: width x its row window (row_count 0: every row)."""
+    rows = frame.camera.height if frame.row_count <= 0 else frame.row_count
+    return frame.camera.width * rows

@@ -111,7 +111,7 @@ __global__ void __launch_bounds__(64) beam_kernel(const __grid_constant__ BeamPa
     const CfgDev& c = B.c;
     const MetricDev& m = F.m;
     const long long pix = idx - F.ray_offset;
-    const double u0 = double(pix % F.width) + 0.5, v0 = double(pix / F.width) + 0.5;
+    const double u0 = double(pix % F.width) + 0.5, v0 = double(F.row0 + pix / F.width) + 0.5;
     // start: the ray, its tangents along u and v, and the pixel's solid angle
     double Y[24];
     beam_start(F, u0, v0, Y);

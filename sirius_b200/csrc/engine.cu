@@ -33,7 +33,8 @@ using namespace sirius;
 
 static_assert(sizeof(sirius_metric) == 80, "sirius_metric layout");
 static_assert(sizeof(sirius_camera) == 64, "sirius_camera layout");
-static_assert(sizeof(sirius_frame) == 168, "sirius_frame layout");
+static_assert(sizeof(sirius_frame) == 176, "sirius_frame layout");
+static_assert(sizeof(sirius_ray_result) == 256, "sirius_ray_result layout");
 static_assert(sizeof(sirius_camera_ray) == 64, "sirius_camera_ray layout");
 static_assert(sizeof(sirius_surrogate_config) == 40, "sirius_surrogate_config layout");
 static_assert(sizeof(sirius_surrogate_stats) == 48, "sirius_surrogate_stats layout");
@@ -140,7 +141,7 @@ __global__ void sur_features_kernel(const FrameDev* frames, const SurFrameDev* s
     const SurFrameDev& S = sf[f];
     const long long pix = idx - F.ray_offset;
     double dir[4], x[4], p[4], r;
-    camera_dir(F, int(pix % F.width), int(pix / F.width), dir);
+    camera_dir(F, int(pix % F.width), F.row0 + int(pix / F.width), dir);
     if (f == f_cam) {
         init_state_ks(F, dir, g_cam, x, p);
         r = r_cam;
@@ -520,6 +521,11 @@ double isco_host(double a_star) {
 
 MetricDev make_metric(const sirius_metric& s) { return metric_dev(s); }
 
+// Rays of a frame: its row window (row_count rows), or the whole image.
+long long frame_rays(const sirius_frame& f) {
+    return (long long)f.camera.width * (f.row_count > 0 ? f.row_count : f.camera.height);
+}
+
 // The zero-angular-momentum observer needs a Kerr-Newman metric (Kerr-Schild
 // family, Lambda = 0) and a camera outside the outer horizon, off the axis.
 int validate_observer(Handle* H, const sirius_frame& f) {
@@ -545,6 +551,21 @@ int validate_metric(Handle* H, const sirius_metric& m) {
     if (m.family == SIRIUS_METRIC_ALCUBIERRE && !(m.sigma > 0 && m.R > 0))
         return fail(H, SIRIUS_ERR_INVALID_ARGUMENT, "Alcubierre sigma and R must be > 0");
     return SIRIUS_OK;
+}
+
+// A frame's camera, projection, observer and row window.
+int validate_frame(Handle* H, const sirius_frame& f) {
+    int rc = validate_metric(H, f.metric);
+    if (rc != SIRIUS_OK) return rc;
+    if (f.camera.width <= 0 || f.camera.height <= 0 || !(f.camera.r > 0))
+        return fail(H, SIRIUS_ERR_INVALID_ARGUMENT, "camera needs width, height > 0 and r > 0");
+    if (f.camera.projection != SIRIUS_CAMERA_PINHOLE && f.camera.projection != SIRIUS_CAMERA_EQUIRECTANGULAR)
+        return fail(H, SIRIUS_ERR_INVALID_ARGUMENT, "unknown camera projection");
+    if (f.row_count < 0 || f.row_begin < 0 || (f.row_count == 0 && f.row_begin != 0) ||
+        (long long)f.row_begin + f.row_count > f.camera.height)
+        return fail(H, SIRIUS_ERR_INVALID_ARGUMENT,
+                    "row window must satisfy 0 <= row_begin, row_begin + row_count <= height (row_count 0: the whole frame)");
+    return validate_observer(H, f);
 }
 
 // The zero-angular-momentum observer at Boyer-Lindquist (r, theta, phi) of a
@@ -604,7 +625,8 @@ FrameDev make_frame(const sirius_frame& f, const sirius_trace_config& c) {
     F.ray_offset = f.ray_offset;
     F.width = f.camera.width;
     F.height = f.camera.height;
-    F.n_rays = (long long)f.camera.width * f.camera.height;
+    F.row0 = f.row_count > 0 ? f.row_begin : 0;
+    F.n_rays = frame_rays(f);
     F.projection = f.camera.projection;
     // camera (CameraConfig, CMBS001A.h:37-58); theta clamp of initializeLightray (GTRC001A.cpp:25)
     const double th = std::clamp(f.camera.theta, 0.01, kPi - 0.01);
@@ -1269,13 +1291,8 @@ static int upload_frames(Handle* H, const sirius_frame* frames, int n, long long
     long long total = 0;
     for (int i = 0; i < n; ++i) {
         const sirius_frame& f = frames[i];
-        int rc = validate_metric(H, f.metric);
+        int rc = validate_frame(H, f);
         if (rc != SIRIUS_OK) return rc;
-        if (f.camera.width <= 0 || f.camera.height <= 0 || !(f.camera.r > 0))
-            return fail(H, SIRIUS_ERR_INVALID_ARGUMENT, "camera needs width, height > 0 and r > 0");
-        if (f.camera.projection != SIRIUS_CAMERA_PINHOLE && f.camera.projection != SIRIUS_CAMERA_EQUIRECTANGULAR)
-            return fail(H, SIRIUS_ERR_INVALID_ARGUMENT, "unknown camera projection");
-        if ((rc = validate_observer(H, f)) != SIRIUS_OK) return rc;
         if (f.ray_offset != total)
             return fail(H, SIRIUS_ERR_INVALID_ARGUMENT, "frames must be contiguous: ray_offset[i] = sum of previous pixel counts");
         fd[i] = make_frame(f, H->cfg);
@@ -1457,13 +1474,8 @@ int sirius_cuda_trace_frames_static(sirius_cuda_handle h, const sirius_frame* d_
     int mask = 0;
     for (int i = 0; i < n_frames; ++i) {
         const sirius_frame& f = hf[i];
-        int rc = validate_metric(H, f.metric);
+        int rc = validate_frame(H, f);
         if (rc != SIRIUS_OK) return rc;
-        if (f.camera.width <= 0 || f.camera.height <= 0 || !(f.camera.r > 0))
-            return fail(H, SIRIUS_ERR_INVALID_ARGUMENT, "camera needs width, height > 0 and r > 0");
-        if (f.camera.projection != SIRIUS_CAMERA_PINHOLE && f.camera.projection != SIRIUS_CAMERA_EQUIRECTANGULAR)
-            return fail(H, SIRIUS_ERR_INVALID_ARGUMENT, "unknown camera projection");
-        if ((rc = validate_observer(H, f)) != SIRIUS_OK) return rc;
         if (f.ray_offset != total)
             return fail(H, SIRIUS_ERR_INVALID_ARGUMENT, "frames must be contiguous: ray_offset[i] = sum of previous pixel counts");
         fd[i] = make_frame(f, H->cfg);
@@ -1474,10 +1486,20 @@ int sirius_cuda_trace_frames_static(sirius_cuda_handle h, const sirius_frame* d_
     if (total != total_rays) return fail(H, SIRIUS_ERR_INVALID_ARGUMENT, "total_rays does not match the frames");
     // a pageable source: the copy has been staged when cudaMemcpyAsync returns
     CK(cudaMemcpyAsync(scratch->frames, fd, n_frames * sizeof(FrameDev), cudaMemcpyHostToDevice, st));
+    // the launch reads the family mask and the one-frame parameter copy from the
+    // handle; the handle's own upload and the statistics of its last traced call
+    // are left as they were
+    const int saved_mask = H->family_mask;
+    const FrameDev saved_frame0 = H->frame0;
+    const sirius_launch_stats saved_stats = H->stats;
     H->family_mask = mask;
     H->frame0 = fd[0];
     const LaunchScratch ls{scratch->frames, scratch->queue, &scratch->status, scratch->flux};
-    return launch_trace(H, n_frames, total, d_results, d_image, d_spectra, nullptr, st, false, &ls);
+    const int rc = launch_trace(H, n_frames, total, d_results, d_image, d_spectra, nullptr, st, false, &ls);
+    H->family_mask = saved_mask;
+    H->frame0 = saved_frame0;
+    H->stats = saved_stats;
+    return rc;
 }
 
 int sirius_cuda_trace_rays(sirius_cuda_handle h, const sirius_metric* metric, double disk_inner, double disk_outer,
@@ -2123,7 +2145,7 @@ int sirius_cuda_render_surrogate(sirius_cuda_handle h, const sirius_frame* frame
     if (!H || !frames || n_frames <= 0 || !image) return SIRIUS_ERR_INVALID_ARGUMENT;
     CK(cudaSetDevice(H->device));
     long long total = 0;
-    for (int i = 0; i < n_frames; ++i) total += (long long)frames[i].camera.width * frames[i].camera.height;
+    for (int i = 0; i < n_frames; ++i) total += frame_rays(frames[i]);
     int rc;
     if ((rc = ensure(H, H->d_image, H->image_cap, size_t(total) * (image_mlp ? 2 : 1))) != SIRIUS_OK) return rc;
     if ((rc = ensure(H, H->d_gate, H->gate_cap, size_t(total))) != SIRIUS_OK) return rc;

@@ -24,6 +24,7 @@ struct FrameDev {
     long long ray_offset, n_rays;
     int width, height, projection, has_horizon, gate;
     int flux_slot;  // index of this frame's disk flux table (its position in the launch)
+    int row0;       // first camera row of the frame's row window (pixel row of its ray 0)
     // camera
     double cam_t, cam_r, cam_st, cam_ct, cam_sp, cam_cp, cam_th, cam_ph;
     float aspect, tan_half_fov, cY, sY, cP, sP, cR, sR;

@@ -112,23 +112,23 @@ __device__ __forceinline__ void write_default_crossings(sirius_ray_result* R) {
     }
 }
 
-static __device__ void invariants(const MetricDev& m, const InvForm& F, const double x[4], const double p[4], float& E,
-                           float& Lz, float& Q) {
-    E = float(-p[0]);
+static __device__ void invariants(const MetricDev& m, const InvForm& F, const double x[4], const double p[4], double& E,
+                           double& Lz, double& Q) {
+    E = -p[0];
     if (m.family == SIRIUS_METRIC_MORRIS_THORNE) {
         const double s = sin(x[2]), c = cos(x[2]);
-        Lz = float(p[3]);
-        Q = float(p[2] * p[2] + c * c * p[3] * p[3] / (s * s));
+        Lz = p[3];
+        Q = p[2] * p[2] + c * c * p[3] * p[3] / (s * s);
         return;
     }
     const double L = x[1] * p[2] - x[2] * p[1];
-    Lz = float(L);
+    Lz = L;
     const double r = F.r;
     const double ct = fmin(fmax(x[3] / r, -1.0), 1.0);
     const double st = sqrt(fmax(1.0 - ct * ct, 1e-30));
     const double pth = (ct / st) * (x[1] * p[1] + x[2] * p[2]) - r * st * p[3];
     const double e = -p[0];
-    Q = float(pth * pth + ct * ct * (-m.a2 * e * e + L * L / (st * st)));
+    Q = pth * pth + ct * ct * (-m.a2 * e * e + L * L / (st * st));
 }
 
 template <bool MIXED, int FAM, bool UNI>
@@ -143,7 +143,7 @@ __device__ __forceinline__ void begin_ray(const Params& P, Ray<MIXED>& s, long l
         for (int i = 0; i < 4; ++i) dir[i] = cr.direction[i];
     } else {
         const long long pix = idx - F.ray_offset;
-        camera_dir(F, int(pix % F.width), int(pix / F.width), dir);
+        camera_dir(F, int(pix % F.width), F.row0 + int(pix / F.width), dir);
     }
     init_state(F, dir, s.x, s.p);
     K xk[4], pk[4];
@@ -161,16 +161,16 @@ __device__ __forceinline__ void begin_ray(const Params& P, Ray<MIXED>& s, long l
     if (MIXED && F.gate && P.c.crit_band > 0.0) {
         InvForm GF;
         inv_form(F.m, s.x, GF);
-        float E, L, Q;
+        double E, L, Q;
         invariants(F.m, GF, s.x, s.p, E, L, Q);
-        s.crit = fabs(radial_potential_gap(F.m, F.r_plus, double(E), double(L), double(Q))) < P.c.crit_band;
+        s.crit = fabs(radial_potential_gap(F.m, F.r_plus, E, L, Q)) < P.c.crit_band;
     }
     if (P.results) {
         sirius_ray_result* R = P.results + idx;
         write_default_crossings(R);
         InvForm IF;
         inv_form(F.m, s.x, IF);
-        float E, L, Q;
+        double E, L, Q;
         invariants(F.m, IF, s.x, s.p, E, L, Q);
         R->E0 = E; R->Lz0 = L; R->Carter0 = Q;
         // impact parameter heuristic (GTRC001A.cpp:208-233)
@@ -199,7 +199,7 @@ __device__ __forceinline__ void end_ray(const Params& P, const Ray<MIXED>& s, in
     sirius_ray_result* R = P.results + s.idx;
     InvForm IF;
     inv_form(F.m, s.x, IF);
-    float E, L, Q;
+    double E, L, Q;
     invariants(F.m, IF, s.x, s.p, E, L, Q);
     R->outcome = outcome;
     R->steps = s.steps;

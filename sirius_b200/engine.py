@@ -129,7 +129,7 @@ def frames_array(frames):
     off = 0
     for f in arr:
         f.ray_offset = off
-        off += f.camera.width * f.camera.height
+        off += abi.frame_rays(f)
     return arr, off
 
 

@@ -43,7 +43,8 @@ def test_struct_layouts_match_c(oracle):
     # static_asserts in engine.cu
     assert C.sizeof(abi.Metric) == 80
     assert C.sizeof(abi.Camera) == 64
-    assert C.sizeof(abi.Frame) == 168
+    assert C.sizeof(abi.Frame) == 176
+    assert C.sizeof(abi.RayResult) == 256
     assert C.sizeof(abi.CameraRay) == 64
     assert C.sizeof(abi.SurrogateConfig) == 40
     assert C.sizeof(abi.SurrogateStats) == 48
