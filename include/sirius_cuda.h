@@ -216,7 +216,15 @@ typedef struct sirius_trace_config {
                                     images at different caps agree to ~1e-5 of the peak, not
                                     bit for bit. The persistent launch takes its budget from
                                     blocks_per_sm. */
-    int32_t reserved[3];
+    int32_t rays_per_thread;     /* one-thread-per-ray launch of mixed-precision DP45 over Kerr-Schild
+                                    frames: 2 = each thread carries two neighbouring rays whose FP32
+                                    arithmetic runs as packed pairs (f32x2); 1 = one ray per thread;
+                                    0 = the measured default. Other configurations trace one ray
+                                    per thread. The two forms round differently (FP32 contraction
+                                    order), so their images agree to ~1e-5 of the peak, not bit
+                                    for bit; within one form a ray's result does not depend on its
+                                    pairing. */
+    int32_t reserved[2];
 } sirius_trace_config;
 
 #define SIRIUS_MAX_BINS 32

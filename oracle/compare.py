@@ -12,6 +12,17 @@ or equatorial crossings (a grazing ray that one integration sends just inside
 the horizon or the disk edge and the other just outside). Everything else is
 compared ray by ray, and the maxima are over every compared ray.
 
+Null constraint: |g^{mu nu} p_mu p_nu| as the engine returns it, absolute (the
+camera normalises E to O(1)) and relative to sum_mu p_mu^2.
+
+Terminal state, over the rays that escape in both traces (final coordinate
+radius beyond the escape radius): the escape direction is the angle between the
+spatial parts of the final covariant momenta (FP64 in both records); the
+terminal position is the final point's offset across the ray (the component of
+the position difference perpendicular to the escape direction) relative to its
+radius, since the two integrations stop at different points along the same
+asymptotic line.
+
 Conserved quantities (computeConservedQuantities, MTTP001A.h:114-132):
   drift      |X_final - X_initial| / max(|X_initial|, floor) per ray of the engine,
              with floor = 1e-3 x the median |X_initial| of the frame (L_z and Q
@@ -41,10 +52,12 @@ def split_histories(res, ref):
             (res["equatorial_crossings"] != ref["equatorial_crossings"]))
 
 
-def report(res, img, ref, spectra=None, ref_bins=None):
+def report(res, img, ref, spectra=None, ref_bins=None, escape_radius=None):
     """Errors of an engine trace (results res, image img, optional spectra) against
     the oracle's trace of the same pixels (ref, ref_bins). Images are compared
-    relative to the oracle image's peak, spectra per bin relative to the bin's peak."""
+    relative to the oracle image's peak, spectra per bin relative to the bin's peak.
+    escape_radius (None: the smallest final radius of the oracle's escaped rays)
+    selects the escaped rays of the terminal-state comparison."""
     n = len(ref)
     split = split_histories(res, ref)
     same = ~split
@@ -54,20 +67,29 @@ def report(res, img, ref, spectra=None, ref_bins=None):
     # re-projection, and the returned state's
     out["null_before_projection"] = _stats(res["null_drift_max"])
     out["null_final"] = _stats(res["null_final"])
+    p2 = np.sum(res["final_p"].astype(np.float64) ** 2, axis=1)
+    out["null_final_relative"] = _stats(res["null_final"] / np.maximum(p2, 1e-300))
     # conserved quantities
     for name in ("E", "Lz", "Carter"):
         x0 = res[name + "0"].astype(np.float64)
         out[name] = {"drift": _stats(_rel(res[name], res[name + "0"], x0)),
                      "vs_oracle": _stats(_rel(res[name][same], ref[name][same], ref[name][same]))}
-    # terminal position (relative to the oracle's radius) and direction (angle between
-    # the spatial parts of k, radians)
-    xg = res["final_x"][same, 1:].astype(np.float64)
-    xo = ref["final_x"][same, 1:].astype(np.float64)
-    out["terminal_position"] = _stats(np.linalg.norm(xg - xo, axis=1) / np.maximum(np.linalg.norm(xo, axis=1), 1e-30))
-    kg = res["final_k"][same, 1:].astype(np.float64)
-    ko = ref["final_k"][same, 1:].astype(np.float64)
-    cos = np.sum(kg * ko, 1) / np.maximum(np.linalg.norm(kg, axis=1) * np.linalg.norm(ko, axis=1), 1e-300)
-    out["terminal_direction_rad"] = _stats(np.arccos(np.clip(cos, -1.0, 1.0)))
+    # terminal state of the rays that escape in both traces
+    rg = np.linalg.norm(res["final_x"][:, 1:].astype(np.float64), axis=1)
+    ro = np.linalg.norm(ref["final_x"][:, 1:].astype(np.float64), axis=1)
+    if escape_radius is None:
+        esc0 = ref["outcome"] == 0
+        escape_radius = float(ro[esc0].min()) if esc0.any() else np.inf
+    esc = same & (rg >= escape_radius) & (ro >= escape_radius)
+    out["escaped_compared"] = int(esc.sum())
+    pg = res["final_p"][esc, 1:].astype(np.float64)
+    po = ref["final_p"][esc, 1:].astype(np.float64)
+    ng = pg / np.linalg.norm(pg, axis=1, keepdims=True)
+    no = po / np.linalg.norm(po, axis=1, keepdims=True)
+    out["escape_direction_rad"] = _stats(np.arctan2(np.linalg.norm(np.cross(ng, no), axis=1), np.sum(ng * no, 1)))
+    dx = res["final_x"][esc, 1:].astype(np.float64) - ref["final_x"][esc, 1:].astype(np.float64)
+    perp = dx - np.sum(dx * no, 1, keepdims=True) * no
+    out["terminal_position"] = _stats(np.linalg.norm(perp, axis=1) / ro[esc])
     # disk crossings (first crossing of rays that both trace onto the disk)
     hit = same & (ref["n_crossings"] > 0)
     out["disk_r"] = _stats(np.abs(res["disk_r"][hit, 0] - ref["disk_r"][hit, 0]) / ref["disk_r"][hit, 0])
@@ -88,7 +110,7 @@ def report(res, img, ref, spectra=None, ref_bins=None):
 def summary(rep):
     """One line per output: max and p99."""
     lines = [f"rays {rep['rays']}, outcome agreement {rep['outcome_agreement']:.5f}, "
-             f"split histories {rep['split_histories']}"]
+             f"split histories {rep['split_histories']}, escaped rays compared {rep['escaped_compared']}"]
     for k, v in rep.items():
         if isinstance(v, dict) and "max" in v:
             lines.append(f"{k}: max {v['max']:.3e} p99 {v['p99']:.3e}")

@@ -93,7 +93,7 @@ class TraceConfig(C.Structure):
                 ("symplectic_order", C.c_int32), ("block_size", C.c_int32),
                 ("refill_threshold", C.c_int32), ("blocks_per_sm", C.c_int32),
                 ("watchdog_ms", C.c_int32), ("samples_per_pixel", C.c_int32), ("max_registers", C.c_int32),
-                ("reserved", C.c_int32 * 3)]
+                ("rays_per_thread", C.c_int32), ("reserved", C.c_int32 * 2)]
 
 
 class RayResult(C.Structure):

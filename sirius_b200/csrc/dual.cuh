@@ -34,6 +34,11 @@ __device__ __forceinline__ double rcp_(double x) { return 1.0 / x; }
 __device__ __forceinline__ float sqrt_(float x) { return sqrtf(x); }
 __device__ __forceinline__ double sqrt_(double x) { return sqrt(x); }
 __device__ __forceinline__ float rsqrt_(float x) { return rsqrtf(x); }
+// Square root of a positive argument. FP32: x * rsqrt(x), two instructions with
+// single-precision relative accuracy (the correctly rounded sqrtf is a longer
+// sequence with a special-case branch); FP64: sqrt.
+__device__ __forceinline__ float sqrtp_(float x) { return x * rsqrtf(x); }
+__device__ __forceinline__ double sqrtp_(double x) { return sqrt(x); }
 __device__ __forceinline__ double rsqrt_(double x) { return 1.0 / sqrt(x); }
 __device__ __forceinline__ float exp_(float x) { return __expf(x); }
 __device__ __forceinline__ double exp_(double x) { return exp(x); }
@@ -45,6 +50,8 @@ inline double rcp_(double x) { return 1.0 / x; }
 inline float sqrt_(float x) { return std::sqrt(x); }
 inline double sqrt_(double x) { return std::sqrt(x); }
 inline float rsqrt_(float x) { return 1.0f / std::sqrt(x); }
+inline float sqrtp_(float x) { return std::sqrt(x); }
+inline double sqrtp_(double x) { return std::sqrt(x); }
 inline double rsqrt_(double x) { return 1.0 / std::sqrt(x); }
 inline float exp_(float x) { return std::exp(x); }
 inline double exp_(double x) { return std::exp(x); }

@@ -72,13 +72,15 @@ __global__ void __launch_bounds__(kFluxN) flux_table_kernel(const FrameDev* fram
 
 constexpr int kDefaultMinBlocks = 2;       // up to 255 registers
 constexpr int kDefaultMinBlocksMixed = 4;  // 128 registers: mixed DP45
+constexpr int kDefaultRaysPerThread = 1;   // rays per thread of mixed DP45 over Kerr-Schild frames
 
 // A kernel specialised for one metric family carries only that family's
 // right-hand side (a smaller loop body and register set); kAnyFamily
 // dispatches per ray. The Kerr-Schild kernels come in every register budget,
 // and for one-frame launches (uni) with the frame in the parameter bank.
-TraceFn pick_kernel(bool mixed, int minb, int fam, bool uni = false) {
-    if (fam == SIRIUS_METRIC_KERR_SCHILD) return mixed ? pick_ks_mixed(minb, uni) : pick_ks_fp64(minb, uni);
+TraceFn pick_kernel(bool mixed, int minb, int fam, bool symp, bool uni = false) {
+    if (fam == SIRIUS_METRIC_KERR_SCHILD)
+        return mixed ? pick_ks_mixed(minb, uni, symp) : pick_ks_fp64(minb, uni, symp);
     return pick_family(mixed, fam);
 }
 
@@ -694,10 +696,12 @@ CfgDev make_cfg(const sirius_trace_config& c) {
     d.vol_j0 = c.vol_j0; d.vol_aoj = c.vol_alpha_over_j; d.vol_hz = c.vol_height_ratio; d.vol_s = c.vol_spectral_index;
     d.integrator = c.integrator; d.symp_order = c.symplectic_order; d.symp_step = c.symplectic_step;
     d.crit_band = c.critical_band;
+    d.npair = (d.nbins + 1) / 2;
     for (int b = 0; b < d.nbins; ++b) {
         const double nu = d.nbins == 1 ? c.nu_min : c.nu_min * std::pow(c.nu_max / c.nu_min, double(b) / (d.nbins - 1));
-        d.nu[b] = float(nu);
-        d.nu_pow[b] = float(std::pow(nu, -c.vol_spectral_index));
+        const float w = float(std::pow(nu, -c.vol_spectral_index));
+        if (b & 1) d.nu_pow2[b / 2].y = w;
+        else d.nu_pow2[b / 2] = make_float2(w, 0.f);
     }
     return d;
 }
@@ -727,6 +731,8 @@ int validate_config(Handle* H, const sirius_trace_config& c) {
         return fail(H, SIRIUS_ERR_INVALID_ARGUMENT, "refill_threshold must be in 0..32");
     if (c.max_registers != 0 && c.max_registers != 128 && c.max_registers != 168 && c.max_registers != 255)
         return fail(H, SIRIUS_ERR_INVALID_ARGUMENT, "max_registers must be 0, 128, 168 or 255");
+    if (c.rays_per_thread < 0 || c.rays_per_thread > 2)
+        return fail(H, SIRIUS_ERR_INVALID_ARGUMENT, "rays_per_thread must be 0, 1 or 2");
     return SIRIUS_OK;
 }
 
@@ -768,7 +774,7 @@ int launch_trace(Handle* H, int n_frames, long long total, sirius_ray_result* d_
     // 32, 64 or 128 threads per block (__launch_bounds__ allows 128): small
     // launches (a list of gated rays) spread over more SMs with smaller blocks
     const int block = (c.block_size == 32 || c.block_size == 64) ? c.block_size : 128;
-    const size_t shmem = size_t(2) * P.c.nbins * block * sizeof(float);
+    const size_t shmem = size_t(2) * P.c.npair * block * sizeof(float2);
     // register budget: the kernel compiled for blocks_per_sm resident 128-thread
     // blocks per SM (persistent), or for max_registers (one thread per ray);
     // fewer registers, possibly spills. The default was measured: the mixed DP45
@@ -777,7 +783,8 @@ int launch_trace(Handle* H, int n_frames, long long total, sirius_ray_result* d_
     // the symplectic integrator keep 255. The choice depends on the configuration
     // only, never on the launch's size or contents: the budgets' FP32 roundings
     // differ, and a ray's result must not depend on what else shares its launch.
-    const bool mixed_dp45 = mixed && c.integrator == SIRIUS_INTEGRATOR_DP45;
+    const bool symp = c.integrator == SIRIUS_INTEGRATOR_SYMPLECTIC;
+    const bool mixed_dp45 = mixed && !symp;
     const int minb = c.blocks_per_sm > 0      ? std::min(c.blocks_per_sm, 4)
                      : c.max_registers == 128 ? 4
                      : c.max_registers == 168 ? 3
@@ -795,20 +802,34 @@ int launch_trace(Handle* H, int n_frames, long long total, sirius_ray_result* d_
     TraceFn launch_fn[3];
     int launch_family[3], n_launches = 0;
     if (n_fams == 1) {
-        launch_fn[0] = pick_kernel(mixed, minb, fams[0], n_frames == 1);
+        launch_fn[0] = pick_kernel(mixed, minb, fams[0], symp, n_frames == 1);
         launch_family[0] = -1;
         n_launches = 1;
     } else if (!P.persistent) {
         for (int i = 0; i < n_fams; ++i) {
-            launch_fn[i] = pick_kernel(mixed, minb, fams[i]);
+            launch_fn[i] = pick_kernel(mixed, minb, fams[i], symp);
             launch_family[i] = fams[i];
         }
         n_launches = n_fams;
     } else {
-        launch_fn[0] = pick_kernel(mixed, minb, kAnyFamily);
+        launch_fn[0] = pick_kernel(mixed, minb, kAnyFamily, symp);
         launch_family[0] = -1;
         n_launches = 1;
     }
+    // two rays per thread (packed FP32 pairs): mixed DP45 over Kerr-Schild frames,
+    // one-thread-per-ray launch shape, rays generated on the device
+    const int rpt = c.rays_per_thread > 0 ? c.rays_per_thread : kDefaultRaysPerThread;
+    const bool pair = rpt == 2 && mixed_dp45 && !P.persistent && !d_rays && n_fams == 1 &&
+                      fams[0] == SIRIUS_METRIC_KERR_SCHILD;
+    if (pair) {
+        const int pminb = c.max_registers == 168 ? 3 : 2;
+        launch_fn[0] = pick_ks_mixed_pair(pminb, n_frames == 1);
+    }
+    const int rays_per_block = pair ? 2 * block : block;
+    const size_t shmem_launch = pair ? 2 * shmem : shmem;
+    if (shmem_launch > 48 * 1024)
+        CK(cudaFuncSetAttribute((const void*)launch_fn[0], cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                int(shmem_launch)));
     int grid;
     if (P.persistent) {
         int per_sm = c.blocks_per_sm;
@@ -821,7 +842,7 @@ int launch_trace(Handle* H, int n_frames, long long total, sirius_ray_result* d_
         const long long need = (total + block - 1) / block;
         if (grid > need) grid = int(std::max<long long>(need, 1));
     } else {
-        grid = int((total + block - 1) / block);
+        grid = int((total + rays_per_block - 1) / rays_per_block);
     }
     // [0] queue cursor, [1..3] counters, [4] launch start: all start at zero
     CK(cudaMemsetAsync(S.queue, 0, 5 * sizeof(unsigned long long), st));
@@ -842,7 +863,7 @@ int launch_trace(Handle* H, int n_frames, long long total, sirius_ray_result* d_
     }
     for (int i = 0; i < n_launches; ++i) {
         P.family = launch_family[i];
-        launch_fn[i]<<<grid, block, shmem, st>>>(P);
+        launch_fn[i]<<<grid, block, shmem_launch, st>>>(P);
         CK(cudaGetLastError());
     }
     if (timed) CK(cudaEventRecord(H->ev[2], st));

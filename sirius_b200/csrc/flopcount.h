@@ -42,6 +42,7 @@ inline bool operator<=(Counted a, Counted b) { return a.v <= b.v; }
 inline bool operator>=(Counted a, Counted b) { return a.v >= b.v; }
 inline Counted rcp_(Counted a) { return tick(1.0 / a.v); }
 inline Counted sqrt_(Counted a) { return tick(std::sqrt(a.v)); }
+inline Counted sqrtp_(Counted a) { return tick(std::sqrt(a.v)); }
 inline Counted rsqrt_(Counted a) { return tick(1.0 / std::sqrt(a.v)); }
 inline Counted exp_(Counted a) { return tick(std::exp(a.v)); }
 inline Counted tanh_(Counted a) { return tick(std::tanh(a.v)); }

@@ -64,9 +64,9 @@ SIRIUS_HD __forceinline__ void ks_pieces(const MetricDev& m, T x, T y, T z, KSPi
     const T R2 = x * x + y * y + z * z;
     const T Rm2 = R2 - a2;
     const T disc = tmax(Rm2 * Rm2 + T(4) * a2 * z * z, T(1e-20));
-    const T sd = sqrt_(disc);
+    const T sd = sqrtp_(disc);
     const T r2 = tmax((Rm2 + sd) * T(0.5), T(1e-10));
-    const T r = sqrt_(r2);
+    const T r = sqrtp_(r2);
     const T isd = rcp_(sd);
     const T ir = rcp_(r);
     const D3<T> rd = dwith(r, r * x * isd, r * y * isd, z * (r2 + a2) * isd * ir);

@@ -55,8 +55,8 @@ struct CfgDev {
     int integrator, symp_order;
     double symp_step, crit_band;
     double vol_j0, vol_aoj, vol_hz, vol_s;
-    float nu[SIRIUS_MAX_BINS];       // bin frequencies
-    float nu_pow[SIRIUS_MAX_BINS];   // nu^-s
+    int npair;                       // bin pairs, (nbins + 1) / 2
+    float2 nu_pow2[SIRIUS_MAX_BINS / 2];  // nu^-s of bins (2j, 2j + 1); 0 pads an odd last pair
 };
 
 // ---------------------------------------------------------------------------
@@ -90,7 +90,7 @@ __device__ __forceinline__ double pt_dOm(double r, double a) {
     return -3.0 * sqrt(r) / (2.0 * den * den);
 }
 
-static __device__ double nt_flux(double r, double a, double isco, double r_in, double r_out) {
+static __device__ __noinline__ double nt_flux(double r, double a, double isco, double r_in, double r_out) {
     const double gx[8] = {0.0950125098376374, 0.2816035507792589, 0.4580167776572274, 0.6178762444026438,
                           0.7554044083550030, 0.8656312023878318, 0.9445750230732326, 0.9894009349916499};
     const double gw[8] = {0.1894506104550685, 0.1826034150449236, 0.1691565193950025, 0.1495959888165767,
@@ -352,7 +352,8 @@ __device__ __forceinline__ double dp45_attempt(const MetricDev& m, const CfgDev&
             en += e * e;
         }
     }
-    return double(sqrt_(T(0.25) * en));
+    if constexpr (sizeof(T) == sizeof(double)) return sqrt(0.25 * en);
+    else return double(sqrtp_(tmax(T(0.25) * en, T(1e-30))));  // 1e-15 when the estimate vanishes
 }
 
 // The same DP45 attempt in FP64 with the stage derivatives in a thread-local
@@ -540,6 +541,14 @@ __device__ __forceinline__ double volume_step_cap(double r, double z, double vx,
     return fmax(0.5 * H, dist) / fmax(v, 1e-3);
 }
 
+// The same cap in FP32 for the mixed path (a step-size bound needs a few digits).
+__device__ __forceinline__ float volume_step_cap_f(float r, float z, float vx, float vy, float vz, float hz,
+                                                   float r_in, float r_out) {
+    const float H = hz * fminf(fmaxf(r, r_in), r_out);
+    const float dist = fmaxf(fmaxf(r_in - r, r - r_out), fabsf(z) - float(kVolCutoff) * H);
+    return fmaxf(0.5f * H, dist) * rsqrtf(fmaxf(vx * vx + vy * vy + vz * vz, 1e-6f));
+}
+
 // Cubic Hermite interpolation of z over the accepted step; bisection for z = 0.
 __device__ __forceinline__ double hermite_root(double z0, double z1, double dz0, double dz1, double h) {
     double lo = 0.0, hi = 1.0, flo = z0;
@@ -565,7 +574,7 @@ __device__ __forceinline__ T kepler_g(const MetricDev& m, T x, T y, T z, T rbl, 
     T gtt = -T(1) + H;
     if (m.has_lambda) gtt -= T(m.lam3) * (x * x + y * y + z * z);
     const T gtp = H * lxi, gpp = x * x + y * y + H * lxi * lxi;
-    const T Om = T(m.sqrtM) * rcp_(rbl * sqrt_(rbl) + T(m.a) * T(m.sqrtM));
+    const T Om = T(m.sqrtM) * rcp_(rbl * sqrtp_(rbl) + T(m.a) * T(m.sqrtM));
     const T n = -(gtt + T(2) * Om * gtp + Om * Om * gpp);
     if (!(n > T(0))) return T(0);
     const T ut = rsqrt_(n);

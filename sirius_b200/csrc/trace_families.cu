@@ -9,13 +9,13 @@ namespace eng {
 TraceFn pick_family(bool mixed, int fam) {
     switch (fam) {
         case SIRIUS_METRIC_MORRIS_THORNE:
-            return mixed ? trace_kernel<true, 2, SIRIUS_METRIC_MORRIS_THORNE, false>
-                         : trace_kernel<false, 2, SIRIUS_METRIC_MORRIS_THORNE, false>;
+            return mixed ? trace_kernel<true, 2, SIRIUS_METRIC_MORRIS_THORNE, false, kAnyIntegrator>
+                         : trace_kernel<false, 2, SIRIUS_METRIC_MORRIS_THORNE, false, kAnyIntegrator>;
         case SIRIUS_METRIC_ALCUBIERRE:
-            return mixed ? trace_kernel<true, 2, SIRIUS_METRIC_ALCUBIERRE, false>
-                         : trace_kernel<false, 2, SIRIUS_METRIC_ALCUBIERRE, false>;
+            return mixed ? trace_kernel<true, 2, SIRIUS_METRIC_ALCUBIERRE, false, kAnyIntegrator>
+                         : trace_kernel<false, 2, SIRIUS_METRIC_ALCUBIERRE, false, kAnyIntegrator>;
         default:
-            return mixed ? trace_kernel<true, 2, kAnyFamily, false> : trace_kernel<false, 2, kAnyFamily, false>;
+            return mixed ? trace_kernel<true, 2, kAnyFamily, false, kAnyIntegrator> : trace_kernel<false, 2, kAnyFamily, false, kAnyIntegrator>;
     }
 }
 

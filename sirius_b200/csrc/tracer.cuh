@@ -14,6 +14,7 @@
 
 #include <type_traits>
 
+#include "packed.cuh"
 #include "trace.cuh"
 
 namespace sirius {
@@ -132,7 +133,7 @@ static __device__ void invariants(const MetricDev& m, const InvForm& F, const do
 }
 
 template <bool MIXED, int FAM, bool UNI>
-__device__ __forceinline__ void begin_ray(const Params& P, Ray<MIXED>& s, long long idx, int frame, float* vol) {
+__device__ __forceinline__ void begin_ray(const Params& P, Ray<MIXED>& s, long long idx, int frame, float2* vol) {
     using K = typename Ray<MIXED>::K;
     s.idx = idx;
     s.frame = frame;
@@ -185,16 +186,22 @@ __device__ __forceinline__ void begin_ray(const Params& P, Ray<MIXED>& s, long l
         R->impact_parameter = b;
     }
     if (vol)
-        for (int b = 0; b < P.c.nbins; ++b) { vol[2 * b * blockDim.x] = 0.f; vol[(2 * b + 1) * blockDim.x] = 1.f; }
+        for (int j = 0; j < P.c.npair; ++j) {
+            vol[j * blockDim.x] = p2(0.f);
+            vol[(P.c.npair + j) * blockDim.x] = p2(1.f);
+        }
 }
 
 template <bool MIXED, bool UNI>
 __device__ __forceinline__ void end_ray(const Params& P, const Ray<MIXED>& s, int outcome, float magnification, int flags,
-                                     const float* vol) {
+                                     const float2* vol) {
     const FrameDev& F = frame_of<UNI>(P, s.frame);
     if (P.image) P.image[s.idx] = float(s.intensity);
     if (P.spectra && vol)
-        for (int b = 0; b < P.c.nbins; ++b) P.spectra[s.idx * P.c.nbins + b] = vol[2 * b * blockDim.x];
+        for (int b = 0; b < P.c.nbins; ++b) {
+            const float2 I = vol[(b >> 1) * blockDim.x];
+            P.spectra[s.idx * P.c.nbins + b] = (b & 1) ? I.y : I.x;
+        }
     if (!P.results) return;
     sirius_ray_result* R = P.results + s.idx;
     InvForm IF;
@@ -221,7 +228,10 @@ __device__ __forceinline__ void end_ray(const Params& P, const Ray<MIXED>& s, in
     R->magnification = magnification;
     float tmin = 1.f;
     if (vol)
-        for (int b = 0; b < P.c.nbins; ++b) tmin = fminf(tmin, vol[(2 * b + 1) * blockDim.x]);
+        for (int b = 0; b < P.c.nbins; ++b) {
+            const float2 T = vol[(P.c.npair + (b >> 1)) * blockDim.x];
+            tmin = fminf(tmin, (b & 1) ? T.y : T.x);
+        }
     R->optical_depth = tmin > 0.f ? -logf(tmin) : 1e30f;
     R->fp64_steps = s.fp64_steps;
     R->flags = flags;
@@ -240,21 +250,38 @@ __device__ __forceinline__ void hermite_xyz(const double x0[4], const double x1[
 
 __device__ __forceinline__ float ks_r(const MetricDev& m, float x, float y, float z) {
     const float a2 = float(m.a2), R2 = x * x + y * y + z * z, Rm2 = R2 - a2;
-    const float sd = sqrtf(fmaxf(Rm2 * Rm2 + 4.f * a2 * z * z, 1e-20f));
-    return sqrtf(fmaxf(0.5f * (Rm2 + sd), 1e-10f));
+    const float sd = sqrtp_(fmaxf(Rm2 * Rm2 + 4.f * a2 * z * z, 1e-20f));
+    return sqrtp_(fmaxf(0.5f * (Rm2 + sd), 1e-10f));
+}
+
+// A point of the step's cubic Hermite interpolant at parameter q in [0, 1], in
+// FP32 relative to the step's start: x(q) = x0 + h10 k0 + h01 (x1 - x0) + h11 k1
+// (the mixed path; the step is short against |x0|, so the offset carries the
+// digits that matter).
+__device__ __forceinline__ void hermite_xyz_f(const float x0[3], const float dx[3], const float k0[4],
+                                              const float k1[4], float h, float q, float& xs, float& ys, float& zs) {
+    const float q2 = q * q, q3 = q2 * q;
+    const float h10 = (q3 - 2.f * q2 + q) * h, h01 = 3.f * q2 - 2.f * q3, h11 = (q3 - q2) * h;
+    xs = x0[0] + (h10 * k0[1] + h01 * dx[0] + h11 * k1[1]);
+    ys = x0[1] + (h10 * k0[2] + h01 * dx[1] + h11 * k1[2]);
+    zs = x0[2] + (h10 * k0[3] + h01 * dx[2] + h11 * k1[3]);
 }
 
 // Volumetric transfer over the accepted segment x0 -> x1 (affine length h):
 // Gauss-Legendre points on the step's cubic Hermite interpolant (the reference
 // marches the chord with midpoints, GTRC001A.cpp:943-958) over the part of the
 // step inside the emitting annulus r_in <= r <= r_out (its edges, where j jumps,
-// are located by bisection), camera-first accumulation per bin:
+// are located by regula falsi), camera-first accumulation per bin:
 // I_b += T_b S (1 - e^-dtau), T_b = e^-tau_b,
 //   j = j0 r^-2 exp(-z^2/(2 (h_z r)^2)) nu_em^-s, alpha = c_a j,
-//   dtau = alpha (nu_cam/g) dl, S = g^3 / c_a.  (vol: [2b] = I_b, [2b+1] = T_b, stride blockDim)
+//   dtau = alpha (nu_cam/g) dl, S = g^3 / c_a.
+// The bins are updated in pairs with packed FP32 arithmetic: vol[j * blockDim]
+// holds (I_2j, I_2j+1), vol[(npair + j) * blockDim] (T_2j, T_2j+1). MIXED
+// evaluates the interpolant in FP32 (hermite_xyz_f); the FP64 path in FP64.
+template <bool MIXED>
 __device__ __forceinline__ void volumetric_segment(const Params& P, const FrameDev& F, const double x0[4],
                                                 const double x1[4], const float k0[4], const float k1[4],
-                                                const double p[4], double h, float r0, float r1, float* vol) {
+                                                const double p[4], double h, float r0, float r1, float2* vol) {
     const CfgDev& c = P.c;
     const int nq = c.vol_sub < 1 ? 1 : (c.vol_sub > 4 ? 4 : c.vol_sub);
     const float E = float(-p[0]);
@@ -262,6 +289,15 @@ __device__ __forceinline__ void volumetric_segment(const Params& P, const FrameD
     const float nu_cam = E / observer_factor<float>(F, E);
     const float rin = float(F.disk_in), rout = float(F.disk_out);
     const bool in0 = r0 >= rin && r0 <= rout, in1 = r1 >= rin && r1 <= rout;
+    float xf0[3], dxf[3];
+    if constexpr (MIXED) {
+#pragma unroll
+        for (int i = 0; i < 3; ++i) { xf0[i] = float(x0[i + 1]); dxf[i] = float(x1[i + 1] - x0[i + 1]); }
+    }
+    auto point = [&](double q, float& xs, float& ys, float& zs) {
+        if constexpr (MIXED) hermite_xyz_f(xf0, dxf, k0, k1, float(h), float(q), xs, ys, zs);
+        else hermite_xyz(x0, x1, k0, k1, h, q, xs, ys, zs);
+    };
     double fa = 0.0, fb = 1.0;
     if (in0 != in1) {
         // the annulus edge on the step's Hermite interpolant: regula falsi
@@ -272,7 +308,7 @@ __device__ __forceinline__ void volumetric_segment(const Params& P, const FrameD
         for (int it = 0; it < 3; ++it) {
             const double q = (qa * gb - qb * ga) / (gb - ga);
             float xs, ys, zs;
-            hermite_xyz(x0, x1, k0, k1, h, q, xs, ys, zs);
+            point(q, xs, ys, zs);
             const double g = double(ks_r(F.m, xs, ys, zs)) - edge;
             if ((g < 0.0) == (ga < 0.0)) {
                 qa = q; ga = g;
@@ -289,15 +325,14 @@ __device__ __forceinline__ void volumetric_segment(const Params& P, const FrameD
         else fa = qe;
     }
     const double span = fb - fa;
-    // per Gauss-Legendre point: optical depth per unit nu^-s and source function
-    float dt0[4], S[4];
-#pragma unroll
-    for (int s = 0; s < 4; ++s) {
-        dt0[s] = 0.f;
-        S[s] = 0.f;
-        if (s >= nq) continue;
+    // the Gauss-Legendre points in step order, each applied to every bin pair
+    // (a point outside the emitting region, or with no redshift, leaves the bins
+    // as they are)
+    const unsigned bd = blockDim.x;
+#pragma unroll 1
+    for (int s = 0; s < nq; ++s) {
         float xs, ys, zs;
-        hermite_xyz(x0, x1, k0, k1, h, fa + span * double(kGLx[nq - 1][s]), xs, ys, zs);
+        point(fa + span * double(kGLx[nq - 1][s]), xs, ys, zs);
         const float r = ks_r(F.m, xs, ys, zs);
         if (r < rin || r > rout) continue;
         const float zr = zs / (float(c.vol_hz) * r);
@@ -307,25 +342,22 @@ __device__ __forceinline__ void volumetric_segment(const Params& P, const FrameD
         const float dl = float(h * span) * kGLw[nq - 1][s];
         const float jsp = float(c.vol_j0) / (r * r) * __expf(-0.5f * zr * zr);
         const float gs = __powf(g, float(c.vol_s));  // nu_em^-s = (g/nu_b)^s
-        dt0[s] = float(c.vol_aoj) * jsp * gs * (nu_cam / g) * dl;
-        S[s] = g * g * g / float(c.vol_aoj);
-    }
-    if (dt0[0] == 0.f && dt0[1] == 0.f && dt0[2] == 0.f && dt0[3] == 0.f) return;
-    for (int b = 0; b < c.nbins; ++b) {
-        float& I = vol[2 * b * blockDim.x];
-        float& Tr = vol[(2 * b + 1) * blockDim.x];  // transmittance e^-tau to the camera
-        float Ib = I, Tb = Tr;
-        const float cb = c.nu_pow[b];
-#pragma unroll
-        for (int s = 0; s < 4; ++s) {
-            const float dtau = dt0[s] * cb;
+        // optical depth per unit nu^-s and source function of the point
+        const float2 dt0 = p2(float(c.vol_aoj) * jsp * gs * (nu_cam / g) * dl);
+        const float2 S = p2(g * g * g / float(c.vol_aoj));
+#pragma unroll 1
+        for (int j = 0; j < c.npair; ++j) {
+            float2 I = vol[j * bd];
+            float2 T = vol[(c.npair + j) * bd];  // transmittance e^-tau to the camera
+            const float2 dtau = mul2(dt0, c.nu_pow2[j]);
             // 1 - e^-x by its series while x is small (no special-function unit needed)
-            const float om = dtau < 1e-3f ? dtau * (1.f - dtau * (0.5f - dtau * (1.f / 6.f))) : 1.f - __expf(-dtau);
-            Ib += Tb * S[s] * om;
-            Tb *= 1.f - om;
+            const float2 u = fma2(dtau, p2(-1.f / 6.f), p2(0.5f));
+            float2 om = mul2(dtau, fma2(neg2(dtau), u, p2(1.f)));
+            if (!(dtau.x < 1e-3f)) om.x = 1.f - __expf(-dtau.x);
+            if (!(dtau.y < 1e-3f)) om.y = 1.f - __expf(-dtau.y);
+            vol[j * bd] = fma2(mul2(T, S), om, I);
+            vol[(c.npair + j) * bd] = fma2(neg2(T), om, T);
         }
-        I = Ib;
-        Tr = Tb;
     }
 }
 
@@ -361,19 +393,26 @@ __device__ __forceinline__ double flux_lookup(const float* t, const FrameDev& F,
     return flux_cubic(t, x);
 }
 
-__device__ __forceinline__ bool record_crossing(const Params& P, const FrameDev& F, long long idx, int n, double xc1,
-                                             double xc2, const double x[4], const double p[4], double& intensity) {
+struct Vec4v {
+    double v[4];
+};
+
+// (out of line: rare, and its flux fallback is long)
+static __device__ __noinline__ double record_crossing(const Params& P, const FrameDev& F, long long idx, int n, double xc1,
+                                               double xc2, const Vec4v xv, const Vec4v pv) {
+    const double* x = xv.v;
+    const double* p = pv.v;
     const MetricDev& m = F.m;
     const double xc[4] = {0.0, xc1, xc2, 0.0};
     InvForm CF;
     inv_form(m, xc, CF);
     const double rc = CF.r;
-    if (!(rc >= F.disk_in && rc <= F.disk_out)) return false;
+    if (!(rc >= F.disk_in && rc <= F.disk_out)) return -1.0;
     const double E = -p[0], Lz = x[1] * p[2] - x[2] * p[1];
     const double g = kepler_g<double>(m, xc1, xc2, 0.0, rc, E, Lz, observer_factor<double>(F, E));
     const double Fl = P.flux ? flux_lookup(P.flux + size_t(F.flux_slot) * kFluxTable, F, rc)
                              : nt_flux(rc, F.a_star, F.isco, F.disk_in, F.disk_out);
-    intensity += exp(-P.c.decay * n) * g * g * g * g * Fl;
+    const double dI = exp(-P.c.decay * n) * g * g * g * g * Fl;
     if (P.results) {
         sirius_ray_result* R = P.results + idx;
         R->disk_r[n] = float(rc);
@@ -381,15 +420,12 @@ __device__ __forceinline__ bool record_crossing(const Params& P, const FrameDev&
         R->disk_g[n] = float(g);
         R->disk_flux[n] = float(Fl);
     }
-    return true;
+    return dI;
 }
 
 // The FP64 island of the mixed path is large and rare, so it stays out of line
 // (less code in the hot loop). Its arguments and results travel by value: an
 // array passed by address would pin the caller's ray state in local memory.
-struct Vec4v {
-    double v[4];
-};
 struct IslandStep {
     double xn[4], pn[4];
     float k7[8];
@@ -425,6 +461,19 @@ __device__ __noinline__ CrossXY island_crossing(const MetricDev& m, const CfgDev
     return o;
 }
 
+// The mixed path's equatorial crossing, located from the step's start state
+// with one FP32 sub-step (out of line: it carries its own DP45 attempt).
+struct K8f {
+    float v[8];
+};
+template <int FAM>
+__device__ __noinline__ CrossXY crossing_f32(const MetricDev& m, const CfgDev& c, const Vec4v x, const Vec4v p,
+                                             const K8f k, double hs) {
+    CrossXY o;
+    locate_equator_f32<FAM>(m, c, x.v, p.v, k.v, hs, o.x, o.y);
+    return o;
+}
+
 // f(x, p) of the current state in the storage precision of the path.
 template <bool MIXED, int FAM>
 __device__ __forceinline__ void refresh_derivative(const MetricDev& m, Ray<MIXED>& s) {
@@ -434,10 +483,35 @@ __device__ __forceinline__ void refresh_derivative(const MetricDev& m, Ray<MIXED
     rhs<K, FAM>(m, xk, pk, s.k, s.k + 4);
 }
 
+// INT selects the integrator at compile time (SIRIUS_INTEGRATOR_DP45 or
+// _SYMPLECTIC: the kernel carries one), or kAnyIntegrator (the configuration's).
+constexpr int kAnyIntegrator = -1;
+template <int INT>
+__device__ __forceinline__ bool is_symplectic(const CfgDev& c) {
+    if constexpr (INT == kAnyIntegrator) return c.integrator == SIRIUS_INTEGRATOR_SYMPLECTIC;
+    else return INT == SIRIUS_INTEGRATOR_SYMPLECTIC;
+}
+
+template <bool MIXED, int FAM, bool UNI, int INT>
+__device__ __forceinline__ int advance_post(const Params& P, Ray<MIXED>& s, bool island, const double xn[4],
+                                            const double pn[4], const typename Ray<MIXED>::K k7[8], double err,
+                                            float& magnification, int& flags, float2* vol);
+
+// The volumetric step cap at radius r, height z, spatial velocity k[1..3]: FP32
+// on the mixed path, FP64 on the FP64 path.
+template <bool MIXED, class K>
+__device__ __forceinline__ double vol_cap(double r, double z, const K k[8], double hz, double r_in, double r_out) {
+    if constexpr (MIXED)
+        return double(volume_step_cap_f(float(r), float(z), float(k[1]), float(k[2]), float(k[3]), float(hz),
+                                        float(r_in), float(r_out)));
+    else
+        return volume_step_cap(r, z, double(k[1]), double(k[2]), double(k[3]), hz, r_in, r_out);
+}
+
 // One iteration of the ray state machine: a DP45 attempt, and on acceptance
 // the termination checks. Returns -1 while the ray continues, else its outcome.
-template <bool MIXED, int FAM, bool UNI>
-__device__ __forceinline__ int advance(const Params& P, Ray<MIXED>& s, float& magnification, int& flags, float* vol) {
+template <bool MIXED, int FAM, bool UNI, int INT>
+__device__ __forceinline__ int advance(const Params& P, Ray<MIXED>& s, float& magnification, int& flags, float2* vol) {
     using K = typename Ray<MIXED>::K;
     const FrameDev& F = frame_of<UNI>(P, s.frame);
     const MetricDev& m = F.m;
@@ -453,7 +527,7 @@ __device__ __forceinline__ int advance(const Params& P, Ray<MIXED>& s, float& ma
                  (is_family<FAM>(m, SIRIUS_METRIC_MORRIS_THORNE) ? (s.x[1] < F.island_r)
                                                                  : (R2 < F.island_r * F.island_r));
     }
-    const bool symp = c.integrator == SIRIUS_INTEGRATOR_SYMPLECTIC;
+    const bool symp = is_symplectic<INT>(c);
     if (symp) {
         // fixed d-lambda, shrunk near the horizon as SymplecticIntegratorD::integrate
         // does (h0 min(1, ((r - r_+)/r_+)^2), PHSI001A.h:260-263); always accepted
@@ -486,6 +560,23 @@ __device__ __forceinline__ int advance(const Params& P, Ray<MIXED>& s, float& ma
     } else {
         err = dp45_attempt<double, FAM>(m, c, s.x, s.p, s.h, s.k, xn, pn, k7);
     }
+    return advance_post<MIXED, FAM, UNI, INT>(P, s, island, xn, pn, k7, err, magnification, flags, vol);
+}
+
+// The rest of one iteration after the attempt: on rejection the step-size
+// update; on acceptance the event location of a disk crossing, the constraint
+// re-projection and the termination checks (GeodesicTracer::trace's order,
+// GTRC001A.cpp:264-556), the volumetric segment and the crossing record.
+// (xn, pn, k7, err) is the attempt from s's state; island: it ran in FP64.
+template <bool MIXED, int FAM, bool UNI, int INT>
+__device__ __forceinline__ int advance_post(const Params& P, Ray<MIXED>& s, bool island, const double xn[4],
+                                            const double pn[4], const typename Ray<MIXED>::K k7[8], double err,
+                                            float& magnification, int& flags, float2* vol) {
+    using K = typename Ray<MIXED>::K;
+    const FrameDev& F = frame_of<UNI>(P, s.frame);
+    const MetricDev& m = F.m;
+    const CfgDev& c = P.c;
+    const bool symp = is_symplectic<INT>(c);
     ++s.attempts;
     if (!(err <= 1.0)) {
         ++s.rejected;
@@ -494,8 +585,7 @@ __device__ __forceinline__ int advance(const Params& P, Ray<MIXED>& s, float& ma
         if (c.enable_vol && c.enable_disk && F.has_horizon && is_family<FAM>(m, SIRIUS_METRIC_KERR_SCHILD)) {
             InvForm RF;
             inv_form(m, s.x, RF);
-            s.h = fmax(c.hmin, fmin(s.h, volume_step_cap(RF.r, s.x[3], double(s.k[1]), double(s.k[2]),
-                                                         double(s.k[3]), c.vol_hz, F.disk_in, F.disk_out)));
+            s.h = fmax(c.hmin, fmin(s.h, vol_cap<MIXED>(RF.r, s.x[3], s.k, c.vol_hz, F.disk_in, F.disk_out)));
         }
         if (s.h <= c.hmin) { ++s.steps; return SIRIUS_STEP_UNDERFLOW; }
         if (s.attempts > c.max_steps * 64 + 1024) return SIRIUS_STEP_UNDERFLOW;
@@ -515,7 +605,14 @@ __device__ __forceinline__ int advance(const Params& P, Ray<MIXED>& s, float& ma
                 xc1 = o.x;
                 xc2 = o.y;
             }
-            else locate_equator_f32<FAM>(m, c, s.x, s.p, s.k, hs, xc1, xc2);
+            else {
+                K8f k0;
+#pragma unroll
+                for (int i = 0; i < 8; ++i) k0.v[i] = float(s.k[i]);
+                const CrossXY o = crossing_f32<FAM>(m, c, vec4v(s.x), vec4v(s.p), k0, hs);
+                xc1 = o.x;
+                xc2 = o.y;
+            }
         } else {
             locate_equator<double, FAM>(m, c, s.x, s.p, hs, xc1, xc2);
         }
@@ -527,9 +624,10 @@ __device__ __forceinline__ int advance(const Params& P, Ray<MIXED>& s, float& ma
     if (!symp) s.h = MIXED ? optimal_step_fast(s.h, err, c) : optimal_step(s.h, err, c);
     ++s.steps;
     if (MIXED && island) ++s.fp64_steps;
-    bool bad = false;
-#pragma unroll
-    for (int i = 0; i < 4; ++i) bad |= !isfinite(xn[i]) || !isfinite(pn[i]) || !isfinite(double(k7[i]));
+    // a NaN or infinity in any component survives the sums (inf - inf is NaN)
+    const double sx = ((xn[0] + xn[1]) + (xn[2] + xn[3])) + ((pn[0] + pn[1]) + (pn[2] + pn[3]));
+    const K sk = (k7[0] + k7[1]) + (k7[2] + k7[3]);
+    const bool bad = !isfinite(sx) || !isfinite(sk);
 #pragma unroll
     for (int i = 0; i < 4; ++i) { s.x[i] = xn[i]; s.p[i] = pn[i]; }
 #pragma unroll
@@ -573,18 +671,20 @@ __device__ __forceinline__ int advance(const Params& P, Ray<MIXED>& s, float& ma
     }
     if (float(rr) < s.min_r) s.min_r = float(rr);
     if (disk_on && c.enable_vol && !symp)
-        s.h = fmax(c.hmin, fmin(s.h, volume_step_cap(rr, s.x[3], double(s.k[1]), double(s.k[2]), double(s.k[3]),
-                                                     c.vol_hz, F.disk_in, F.disk_out)));
+        s.h = fmax(c.hmin, fmin(s.h, vol_cap<MIXED>(rr, s.x[3], s.k, c.vol_hz, F.disk_in, F.disk_out)));
     const bool mt = is_family<FAM>(m, SIRIUS_METRIC_MORRIS_THORNE);
 
-    // winding: equatorial crossings and |d phi| (GTRC001A.cpp:294-309)
+    // winding: equatorial crossings and |d phi| (GTRC001A.cpp:294-309); the
+    // azimuth sum feeds the spiral check and the per-ray record only
     if (!mt) {
         const float cz = float(s.x[3]);
         if (s.prev_z * cz < 0.f) ++s.eq;
         s.prev_z = cz;
-        const float cr = float(x0[1] * s.x[2] - x0[2] * s.x[1]);
-        const float dt = float(x0[1] * s.x[1] + x0[2] * s.x[2]);
-        s.tphi += fabsf(atan2f(cr, dt));
+        if (c.spiral || P.results) {
+            const float cr = float(x0[1] * s.x[2] - x0[2] * s.x[1]);
+            const float dt = float(x0[1] * s.x[1] + x0[2] * s.x[2]);
+            s.tphi += fabsf(atan2f(cr, dt));
+        }
     }
     // spiral early-out (GTRC001A.cpp:322-352)
     const int sidx = s.steps - 1;
@@ -604,8 +704,8 @@ __device__ __forceinline__ int advance(const Params& P, Ray<MIXED>& s, float& ma
     if (mt && s.x[1] <= 1.001 * m.b0 * 1.0001) return SIRIUS_THROAT;
     // escape
     {
-        const double Resc = mt ? s.x[1] : sqrt(s.x[1] * s.x[1] + s.x[2] * s.x[2] + s.x[3] * s.x[3]);
-        if (Resc > c.escape_r) {
+        const double R2e = mt ? s.x[1] * fabs(s.x[1]) : s.x[1] * s.x[1] + s.x[2] * s.x[2] + s.x[3] * s.x[3];
+        if (R2e > c.escape_r * c.escape_r) {
             const double vrad = mt ? double(s.k[1])
                                    : (s.x[1] * double(s.k[1]) + s.x[2] * double(s.k[2]) + s.x[3] * double(s.k[3]));
             if (vrad > 0.0) {
@@ -631,13 +731,15 @@ __device__ __forceinline__ int advance(const Params& P, Ray<MIXED>& s, float& ma
             float k1f[4];
 #pragma unroll
             for (int i = 0; i < 4; ++i) k1f[i] = float(s.k[i]);
-            volumetric_segment(P, F, x0, s.x, k0f, k1f, s.p, hstep, r0, r1, vol);
+            volumetric_segment<MIXED>(P, F, x0, s.x, k0f, k1f, s.p, hstep, r0, r1, vol);
         }
     }
     s.prev_r = float(rr);
     // thin-disk crossing (GTRC001A.h:404-431, GTRC001A.cpp:468-555)
     if (cross && s.ncross < SIRIUS_MAX_CROSSINGS) {
-        if (record_crossing(P, F, s.idx, s.ncross, xc1, xc2, s.x, s.p, s.intensity)) {
+        const double dI = record_crossing(P, F, s.idx, s.ncross, xc1, xc2, vec4v(s.x), vec4v(s.p));
+        if (dI >= 0.0) {
+            s.intensity += dI;
             ++s.ncross;
             const float ratio = s.min_r / float(F.r_ph_pro);
             if (ratio < 1.5f) {
@@ -651,11 +753,11 @@ __device__ __forceinline__ int advance(const Params& P, Ray<MIXED>& s, float& ma
     return -1;
 }
 
-// Persistent tracer. Dynamic shared memory: 2 * nbins floats per thread (volumetric bins).
-template <bool MIXED, int FAM, bool UNI>
+// Persistent tracer. Dynamic shared memory: 2 * npair float2 per thread (volumetric bin pairs).
+template <bool MIXED, int FAM, bool UNI, int INT>
 __device__ __forceinline__ void trace_body(const Params& P) {
     extern __shared__ float smem[];
-    float* vol = (P.c.enable_vol && P.c.nbins > 0) ? smem + threadIdx.x : nullptr;
+    float2* vol = (P.c.enable_vol && P.c.nbins > 0) ? reinterpret_cast<float2*>(smem) + threadIdx.x : nullptr;
     const int lane = threadIdx.x & 31;
     const unsigned lt_mask = (1u << lane) - 1u;
     Ray<MIXED> s;
@@ -727,7 +829,7 @@ __device__ __forceinline__ void trace_body(const Params& P) {
             continue;
         }
         if (alive) {
-            const int out = advance<MIXED, FAM, UNI>(P, s, magnification, flags, vol);
+            const int out = advance<MIXED, FAM, UNI, INT>(P, s, magnification, flags, vol);
             if (out >= 0) {
                 end_ray<MIXED, UNI>(P, s, out, magnification, flags, vol);
                 acc += s.steps;
@@ -752,9 +854,9 @@ __device__ __forceinline__ void trace_body(const Params& P) {
 
 // The tracer compiled for MINB resident 128-thread blocks per SM (MINB 2: up to
 // 255 registers, 3: 168, 4: 128).
-template <bool MIXED, int MINB, int FAM, bool UNI>
+template <bool MIXED, int MINB, int FAM, bool UNI, int INT>
 __global__ void __launch_bounds__(128, MINB) trace_kernel(const __grid_constant__ Params P) {
-    trace_body<MIXED, FAM, UNI>(P);
+    trace_body<MIXED, FAM, UNI, INT>(P);
 }
 
 using TraceFn = void (*)(Params);
@@ -762,9 +864,12 @@ using TraceFn = void (*)(Params);
 // The trace kernel for a register budget (minb resident 128-thread blocks per
 // SM: 1 or 2 = up to 255 registers, 3 = 168, 4 = 128) and a launch form
 // (uni: one frame, read from the parameter bank).
-TraceFn pick_ks_mixed(int minb, bool uni);  // Kerr-Schild family, mixed precision
-TraceFn pick_ks_fp64(int minb, bool uni);   // Kerr-Schild family, FP64
+// Kerr-Schild family, mixed precision / FP64; symp: the symplectic integrator (else DP45)
+TraceFn pick_ks_mixed(int minb, bool uni, bool symp);
+TraceFn pick_ks_fp64(int minb, bool uni, bool symp);
 TraceFn pick_family(bool mixed, int fam);   // Morris-Thorne, Alcubierre, or any family (kAnyFamily)
+// Kerr-Schild family, mixed precision, two rays per thread (minb 2: 255 registers, 3: 168)
+TraceFn pick_ks_mixed_pair(int minb, bool uni);
 
 }  // namespace eng
 }  // namespace sirius

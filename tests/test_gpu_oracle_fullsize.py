@@ -67,8 +67,11 @@ def test_config2_mixed_1024_vs_oracle(engine, oracle_config2):
     ref, bins = oracle_config2
     engine.configure(config2(abi.PRECISION_MIXED))
     res, img, spc = engine.trace_frames([frame2()], spectra=True)
-    rep = compare.report(res, img, ref, spc, bins)
+    rep = compare.report(res, img, ref, spc, bins, escape_radius=200.0)
     check(rep, image_max=1e-4, null_max=1e-8, split_max=200)
+    # escape direction: the FP32 right-hand side against the FP64 integration (the
+    # FP64 oracle's own sensitivity to its tolerance, 1e-8 -> 1e-9, is ~5e-5 rad here)
+    assert rep["escape_direction_rad"]["p99"] <= 1e-4, rep["escape_direction_rad"]
     # L_z and Carter Q: conserved by the flow and by the projection; the drift is the
     # integration error (DP45 at 1e-8; the reference's own bar is 1e-4, TSDG003A.cpp)
     assert rep["Lz"]["drift"]["p99"] <= 1e-6 and rep["Carter"]["drift"]["p99"] <= 1e-5
@@ -79,10 +82,10 @@ def test_config2_fp64_1024_vs_oracle(engine, oracle_config2):
     ref, bins = oracle_config2
     engine.configure(config2(abi.PRECISION_FP64))
     res, img, spc = engine.trace_frames([frame2()], spectra=True)
-    rep = compare.report(res, img, ref, spc, bins)
+    rep = compare.report(res, img, ref, spc, bins, escape_radius=200.0)
     check(rep, image_max=1e-7, null_max=1e-12, split_max=200)
     assert rep["image"]["p99"] <= 1e-10
-    assert rep["terminal_direction_rad"]["p99"] <= 1e-8
+    assert rep["escape_direction_rad"]["max"] <= 1e-7, rep["escape_direction_rad"]
 
 
 def test_config1_schwarzschild_256_fp64_vs_oracle(engine, oracle):
@@ -94,8 +97,9 @@ def test_config1_schwarzschild_256_fp64_vs_oracle(engine, oracle):
     engine.configure(cfg)
     res, img, _ = engine.trace_frames([fr])
     ref, _ = oracle.trace_frame(fr, cfg, threads=THREADS)
-    rep = compare.report(res, img, ref)
+    rep = compare.report(res, img, ref, escape_radius=1000.0)
     check(rep, image_max=1e-7, null_max=1e-12, split_max=20)
+    assert rep["escape_direction_rad"]["max"] <= 1e-7, rep["escape_direction_rad"]
     assert set(np.unique(ref["outcome"])) <= {abi.ESCAPED, abi.HORIZON, abi.DISK_HIT}
 
 
@@ -116,12 +120,15 @@ def test_config3_family_mixed_128_vs_oracle(engine, oracle, name, metric, cam, r
     engine.configure(abi.default_config(precision=abi.PRECISION_MIXED, **base))
     res, img, _ = engine.trace_frames([fr])
     ref, _ = oracle.trace_frame(fr, abi.default_config(precision=abi.PRECISION_FP64, **base), threads=THREADS)
-    rep = compare.report(res, img, ref)
+    rep = compare.report(res, img, ref, escape_radius=200.0)
     print(name)
     check(rep, image_max=1e-4, agree_min=0.995)
-    # the escape direction of every ray whose history agrees
-    assert rep["terminal_direction_rad"]["max"] <= 1e-4, rep["terminal_direction_rad"]
-    assert rep["null_final"]["max"] <= (1e-8 if metric.family == abi.KERR_SCHILD else 1e-10)
+    # the escape direction of every escaped ray whose history agrees
+    assert rep["escape_direction_rad"]["p99"] <= 1e-4, rep["escape_direction_rad"]
+    assert rep["escape_direction_rad"]["max"] <= 1e-2, rep["escape_direction_rad"]
+    # null constraint of the returned state, relative to |p|^2 (the Alcubierre wall
+    # accelerates rays to |p| ~ 1e2)
+    assert rep["null_final_relative"]["max"] <= 1e-8, rep["null_final_relative"]
 
 
 def test_row_window_equals_slice_of_full_frame(engine):
