@@ -113,6 +113,77 @@ SIRIUS_HD __forceinline__ void ks_rhs(const MetricDev& m, const T x[4], const T 
     }
 }
 
+// The same right-hand side with the forward-mode tangents of ks_pieces
+// propagated term by term: the coordinate seeds dx = (1, 0, 0), ... have zero
+// components, and an IEEE product with a zero cannot be dropped at compile time
+// (inf * 0 is NaN), so the generic dual arithmetic pays for every one of them.
+// Here only the non-zero terms are formed:
+//   dr  = (r x, r y, z (r^2 + a^2) / r) / sqrt(disc)
+//   d(1/(r^2 + a^2)) = -2 r / (r^2 + a^2)^2 dr
+//   d l1 = (x dr + (r, a, 0)) / (r^2 + a^2) + (r x + a y) d(1/(r^2 + a^2)), l2 alike
+//   d l3 = (0, 0, 1) / r - z / r^2 dr
+//   d H  = ((2 M r^2 + 2 r (2 M r - Q^2) - H 4 r^3) dr - H (0, 0, 2 a^2 z)) / fden
+// with num = (2 M r - Q^2) r^2, fden = r^4 + a^2 z^2, H = num / fden.
+template <class T>
+SIRIUS_HD __forceinline__ void ks_rhs_fast(const MetricDev& m, const T x[4], const T p[4], T k[4], T f[4]) {
+    const T a = T(m.a), a2 = T(m.a2);
+    const T X = x[1], Y = x[2], Z = x[3];
+    const T zz = Z * Z;
+    const T R2 = X * X + Y * Y + zz;
+    const T Rm2 = R2 - a2;
+    const T a2zz = a2 * zz;
+    const T disc = tmax(Rm2 * Rm2 + T(4) * a2zz, T(1e-20));
+    const T sd = sqrtp_(disc);
+    const T r2 = tmax((Rm2 + sd) * T(0.5), T(1e-10));
+    const T r = sqrtp_(r2);
+    const T isd = rcp_(sd), ir = rcp_(r);
+    const T den = r2 + a2;
+    const T risd = r * isd;
+    const T rx = risd * X, ry = risd * Y, rz = Z * den * isd * ir;
+    const T iden = rcp_(den);
+    const T gi = -T(2) * r * iden * iden;
+    const T n1 = r * X + a * Y, n2 = r * Y - a * X;
+    const T l1 = n1 * iden, l2 = n2 * iden;
+    const T n1g = n1 * gi, n2g = n2 * gi;
+    const T l1d0 = (X * rx + r) * iden + n1g * rx, l1d1 = (X * ry + a) * iden + n1g * ry,
+            l1d2 = X * rz * iden + n1g * rz;
+    const T l2d0 = (Y * rx - a) * iden + n2g * rx, l2d1 = (Y * ry + r) * iden + n2g * ry,
+            l2d2 = Y * rz * iden + n2g * rz;
+    const T l3 = Z * ir;
+    const T zi2 = -l3 * ir;
+    const T l3d0 = zi2 * rx, l3d1 = zi2 * ry, l3d2 = zi2 * rz + ir;
+    const T q = T(2.0 * m.M) * r - T(m.Q2);
+    const T fden = r2 * r2 + a2zz;
+    const T ifd = rcp_(fden);
+    const T H = q * r2 * ifd;
+    const T w = (T(2.0 * m.M) * r2 + T(2) * r * q - H * T(4) * r2 * r) * ifd;
+    const T Hd0 = w * rx, Hd1 = w * ry, Hd2 = w * rz - H * ifd * T(2) * a2 * Z;
+    // k = g^{-1} p = eta p - H l# (l# . p), l# = (-1, l1, l2, l3)
+    const T lp = -p[0] + l1 * p[1] + l2 * p[2] + l3 * p[3];
+    const T Hlp = H * lp;
+    k[0] = -p[0] + Hlp;
+    k[1] = p[1] - l1 * Hlp;
+    k[2] = p[2] - l2 * Hlp;
+    k[3] = p[3] - l3 * Hlp;
+    if (m.has_lambda) {
+        const T c = T(m.lam3) * R2;
+        const T w0 = -T(1) - H, w1 = H * l1, w2 = H * l2, w3 = H * l3;
+        const T s = c * (w0 * p[0] + w1 * p[1] + w2 * p[2] + w3 * p[3]) * rcp_(T(1) + c * (T(1) + H));
+        k[0] += s * w0; k[1] += s * w1; k[2] += s * w2; k[3] += s * w3;
+    }
+    // dp_lambda = 1/2 dH (l.k)^2 + H (l.k)(dl.k) [- Lambda x_lambda (k^0)^2 / 3]
+    const T lk = k[0] + l1 * k[1] + l2 * k[2] + l3 * k[3];
+    const T hlk = T(0.5) * lk;
+    f[0] = T(0);
+    f[1] = lk * (Hd0 * hlk + H * (l1d0 * k[1] + l2d0 * k[2] + l3d0 * k[3]));
+    f[2] = lk * (Hd1 * hlk + H * (l1d1 * k[1] + l2d1 * k[2] + l3d1 * k[3]));
+    f[3] = lk * (Hd2 * hlk + H * (l1d2 * k[1] + l2d2 * k[2] + l3d2 * k[3]));
+    if (m.has_lambda) {
+        const T qq = T(m.lam3) * k[0] * k[0];
+        f[1] -= qq * X; f[2] -= qq * Y; f[3] -= qq * Z;
+    }
+}
+
 // ---------------------------------------------------------------------------
 // Morris-Thorne (PHMT101A.h:195-345), chart (t, r, theta, phi); r clamped to
 // >= 1.001 b0 as the reference does (:293); g diagonal.
@@ -182,10 +253,10 @@ constexpr int kAnyFamily = -1;
 
 template <class T, int FAM = kAnyFamily>
 SIRIUS_HD __forceinline__ void rhs(const MetricDev& m, const T x[4], const T p[4], T k[4], T f[4]) {
-    if constexpr (FAM == SIRIUS_METRIC_KERR_SCHILD) ks_rhs(m, x, p, k, f);
+    if constexpr (FAM == SIRIUS_METRIC_KERR_SCHILD) ks_rhs_fast(m, x, p, k, f);
     else if constexpr (FAM == SIRIUS_METRIC_MORRIS_THORNE) mt_rhs(m, x, p, k, f);
     else if constexpr (FAM == SIRIUS_METRIC_ALCUBIERRE) alc_rhs(m, x, p, k, f);
-    else if (m.family == SIRIUS_METRIC_KERR_SCHILD) ks_rhs(m, x, p, k, f);
+    else if (m.family == SIRIUS_METRIC_KERR_SCHILD) ks_rhs_fast(m, x, p, k, f);
     else if (m.family == SIRIUS_METRIC_MORRIS_THORNE) mt_rhs(m, x, p, k, f);
     else alc_rhs(m, x, p, k, f);
 }

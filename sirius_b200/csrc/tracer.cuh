@@ -325,36 +325,47 @@ __device__ __forceinline__ void volumetric_segment(const Params& P, const FrameD
         else fa = qe;
     }
     const double span = fb - fa;
-    // the Gauss-Legendre points in step order, each applied to every bin pair
-    // (a point outside the emitting region, or with no redshift, leaves the bins
-    // as they are)
     const unsigned bd = blockDim.x;
-#pragma unroll 1
-    for (int s = 0; s < nq; ++s) {
+    auto one_minus_exp = [&](float2 dtau) {
+        // 1 - e^-x by its series while x is small (no special-function unit needed)
+        const float2 u = fma2(dtau, p2(-1.f / 6.f), p2(0.5f));
+        float2 om = mul2(dtau, fma2(neg2(dtau), u, p2(1.f)));
+        const float ex = 1.f - __expf(-dtau.x), ey = 1.f - __expf(-dtau.y);
+        om.x = dtau.x < 1e-3f ? om.x : ex;
+        om.y = dtau.y < 1e-3f ? om.y : ey;
+        return om;
+    };
+    auto point_at = [&](int s, float& dts, float& Ss) {
+        dts = 0.f;
+        Ss = 0.f;
         float xs, ys, zs;
         point(fa + span * double(kGLx[nq - 1][s]), xs, ys, zs);
         const float r = ks_r(F.m, xs, ys, zs);
-        if (r < rin || r > rout) continue;
+        if (r < rin || r > rout) return;
         const float zr = zs / (float(c.vol_hz) * r);
-        if (fabsf(zr) > float(kVolCutoff)) continue;
+        if (fabsf(zr) > float(kVolCutoff)) return;
         const float g = kepler_g<float>(F.m, xs, ys, zs, r, E, Lz, observer_factor<float>(F, E));
-        if (!(g > 0.f)) continue;
+        if (!(g > 0.f)) return;
         const float dl = float(h * span) * kGLw[nq - 1][s];
         const float jsp = float(c.vol_j0) / (r * r) * __expf(-0.5f * zr * zr);
         const float gs = __powf(g, float(c.vol_s));  // nu_em^-s = (g/nu_b)^s
-        // optical depth per unit nu^-s and source function of the point
-        const float2 dt0 = p2(float(c.vol_aoj) * jsp * gs * (nu_cam / g) * dl);
-        const float2 S = p2(g * g * g / float(c.vol_aoj));
+        dts = float(c.vol_aoj) * jsp * gs * (nu_cam / g) * dl;
+        Ss = g * g * g / float(c.vol_aoj);
+    };
+    // the Gauss-Legendre points in step order, each applied to every bin pair
+    // (a point outside the emitting region, or with no redshift, leaves the bins
+    // as they are)
+#pragma unroll 1
+    for (int s = 0; s < nq; ++s) {
+        float dts, Ss;
+        point_at(s, dts, Ss);
+        if (dts == 0.f) continue;
+        const float2 dt0 = p2(dts), S = p2(Ss);
 #pragma unroll 1
         for (int j = 0; j < c.npair; ++j) {
-            float2 I = vol[j * bd];
-            float2 T = vol[(c.npair + j) * bd];  // transmittance e^-tau to the camera
-            const float2 dtau = mul2(dt0, c.nu_pow2[j]);
-            // 1 - e^-x by its series while x is small (no special-function unit needed)
-            const float2 u = fma2(dtau, p2(-1.f / 6.f), p2(0.5f));
-            float2 om = mul2(dtau, fma2(neg2(dtau), u, p2(1.f)));
-            if (!(dtau.x < 1e-3f)) om.x = 1.f - __expf(-dtau.x);
-            if (!(dtau.y < 1e-3f)) om.y = 1.f - __expf(-dtau.y);
+            const float2 I = vol[j * bd];
+            const float2 T = vol[(c.npair + j) * bd];  // transmittance e^-tau to the camera
+            const float2 om = one_minus_exp(mul2(dt0, c.nu_pow2[j]));
             vol[j * bd] = fma2(mul2(T, S), om, I);
             vol[(c.npair + j) * bd] = fma2(neg2(T), om, T);
         }
@@ -596,7 +607,22 @@ __device__ __forceinline__ int advance_post(const Params& P, Ray<MIXED>& s, bool
     const bool disk_on = is_family<FAM>(m, SIRIUS_METRIC_KERR_SCHILD) && c.enable_disk && F.has_horizon;
     // equatorial crossing inside the step: locate it from the step's start state
     double xc1 = 0.0, xc2 = 0.0;
-    const bool cross = disk_on && (s.x[3] * xn[3] < 0.0);
+    bool cross = disk_on && (s.x[3] * xn[3] < 0.0);
+    if (cross) {
+        // a crossing that cannot land on the disk needs no location: the chord's
+        // crossing point lies within three step lengths of the trajectory's, so
+        // Boyer-Lindquist radii (r^2 = x^2 + y^2 - a^2 at z = 0) outside
+        // [r_in, r_out] by that margin would fail the disk test in any case
+        const float t = float(s.x[3] / (s.x[3] - xn[3]));
+        const float dx = float(xn[1] - s.x[1]), dy = float(xn[2] - s.x[2]), dz = float(xn[3] - s.x[3]);
+        const float cx = float(s.x[1]) + t * dx, cy = float(s.x[2]) + t * dy;
+        const float rho = sqrtp_(fmaxf(cx * cx + cy * cy, 1e-30f));
+        const float L3 = 3.f * sqrtp_(fmaxf(dx * dx + dy * dy + dz * dz, 1e-30f));
+        const float a2 = float(m.a2), rhi = rho + L3, rlo = fmaxf(rho - L3, 0.f);
+        if (rlo * rlo - a2 > float(F.disk_out) * float(F.disk_out) * 1.0001f ||
+            rhi * rhi - a2 < float(F.disk_in) * float(F.disk_in) * 0.9999f)
+            cross = false;
+    }
     if (cross) {
         const double hs = hermite_root(s.x[3], xn[3], double(s.k[3]), double(k7[3]), hstep) * hstep;
         if constexpr (MIXED) {
