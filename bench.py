@@ -13,7 +13,10 @@ The reference arm (--impl reference) runs the reference's own CPU tracer
 all host threads.
 
 Usage: python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference]
-Under torchrun each rank renders its own frame (weak scaling, no data collective).
+Under torchrun the frame is split into contiguous row blocks, one per rank (each
+rank traces its block's row window); every step ends with the gather of the image
+rows to rank 0, the one exchange of a split frame (strong scaling: value = the
+frame's rays over the slowest rank's device time).
 """
 import argparse
 import ctypes as C
@@ -141,78 +144,148 @@ def run_reference(args):
     def run_sample(n):
         stride = max(npix // n, 1)
         t0 = time.perf_counter()
+        recs = []
         if kind == "reference":
             # rows sampled with a stride; each call traces a contiguous block of one row
             rows = max(n // WIDTH, 1)
             row_stride = max(HEIGHT // rows, 1)
             for r in range(rows):
-                ref.trace_frame(1.0, 0.9, rcfg, fr.camera, (r * row_stride) * WIDTH, WIDTH, threads=threads,
-                                keep=False)
+                recs.append(ref.trace_frame(1.0, 0.9, rcfg, fr.camera, (r * row_stride) * WIDTH, WIDTH,
+                                            threads=threads))
             n_done = rows * WIDTH
         else:
             orc = Oracle()
             rows = max(n // WIDTH, 1)
             row_stride = max(HEIGHT // rows, 1)
             for r in range(rows):
-                orc.trace_frame(fr, cfg, (r * row_stride) * WIDTH, WIDTH, threads=threads)
+                recs.append(orc.trace_frame(fr, cfg, (r * row_stride) * WIDTH, WIDTH, threads=threads)[0])
             n_done = rows * WIDTH
-        return time.perf_counter() - t0, n_done
+        return time.perf_counter() - t0, n_done, recs
 
-    dt, n = run_sample(WIDTH)
+    dt, n, _ = run_sample(WIDTH)
     rate = n / dt
     n_step = int(min(max(rate * 4.0, WIDTH), npix))
-    times, counts = [], []
+    times, counts, recs = [], [], []
     for i in range(args.warmup + args.steps):
-        dt, n = run_sample(n_step)
+        dt, n, rr = run_sample(n_step)
         if i >= args.warmup:
             times.append(dt)
             counts.append(n)
+            recs += rr
+    import numpy as np
+    allrec = np.concatenate(recs)
+    steps_field = "steps_taken" if kind == "reference" else "steps"
     value = sum(counts) / sum(times) / 1e6
     sample = (f"{counts[0]} pixels per step ({counts[0] // WIDTH} full rows evenly spaced over the 1024^2 frame), "
               f"RenderSession-style atomic pixel queue, {threads} threads, the reference's TracerConfig with the "
               f"workload's tolerances (thin disk; its gray volumetric march replaces the disk, so it is off)")
     line = {"metric": "Mrays/s", "value": value, "unit": "Mrays/s", "impl": "reference", "n_gpus": args.gpus,
             "steps": args.steps, "warmup": args.warmup, "ms_per_step": 1e3 * sum(times) / len(times),
-            "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f64",
+            "higher_is_better": True, "scaling": "strong", "vs_baseline": None, "dtype": "f64",
             "data": "synthetic (seeded camera frame)", "config": workload_desc(),
-            "cpu_baseline": {"value": value, "unit": "Mrays/s", "cores": threads, "kind": kind, "sample": sample},
+            "cpu_baseline": {"value": value, "unit": "Mrays/s", "cores": threads, "kind": kind, "sample": sample,
+                             "cpu_model": cpu_model(), "steps_per_ray": float(allrec[steps_field].mean()),
+                             "outcome_mix": outcome_mix(allrec["outcome"], {0: "escaped", 1: "horizon", 2: "disk",
+                                                                            3: "max_steps", 4: "spiraling"})},
             "e2e": {"value": value, "unit": "Mrays/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
     print(json.dumps(line), flush=True)
 
 
 # -------------------------------------------------------------------- ours --
-def cpu_baseline_sample(seconds=12.0):
-    """The reference tracer (or the oracle port) on the box's host cores, rank 0 at N = 1."""
+def cpu_model():
+    try:
+        with open("/proc/cpuinfo") as f:
+            for ln in f:
+                if ln.startswith("model name"):
+                    return ln.split(":", 1)[1].strip()
+    except OSError:
+        pass
+    return "unknown"
+
+
+def outcome_mix(outcomes, names):
+    """Counts of each outcome (names: value -> label)."""
+    import numpy as np
+    vals, counts = np.unique(np.asarray(outcomes), return_counts=True)
+    return {names.get(int(v), str(int(v))): int(c) for v, c in zip(vals, counts)}
+
+
+SAMPLE_ROWS = [(i * 97) % HEIGHT for i in range(HEIGHT)]  # rows spread over the frame, in sampling order
+
+
+def cpu_baseline_sample(gpu_res, gpu_img, gpu_spc, seconds=12.0):
+    """The two CPU numbers on the box's host cores (rank 0, N = 1), each on whole
+    rows of the 1024^2 frame spread over its height for about `seconds`:
+      reference  the reference's own tracer (oracle/_ref, GeodesicTracer) in
+                 RenderSession's pattern; thin disk (its gray volumetric march
+                 replaces the disk), stop-on-reject as written;
+      oracle     the FP64 restatement in engine semantics (retry on reject, the
+                 full workload: NT disk and 16-bin volumetric transfer).
+    The oracle's rows also judge the GPU frame (gpu_res, gpu_img, gpu_spc: the
+    mixed-precision trace of the full frame): error_vs_oracle, max and p99 of every
+    output over those rows (oracle/compare.py)."""
+    import numpy as np
+
+    from oracle import compare
     from oracle.pyoracle import Oracle, Reference, ref_available, ref_config_from
     from sirius_b200 import abi
     cfg = workload_config(abi, abi.PRECISION_FP64)
     fr = workload_frame(abi)
     threads = os.cpu_count() or 1
+    names = {abi.ESCAPED: "escaped", abi.HORIZON: "horizon", abi.DISK_HIT: "disk", abi.MAX_STEPS: "max_steps",
+             abi.SPIRALING: "spiraling", abi.NUMERICAL_FAILURE: "numerical_failure",
+             abi.STEP_UNDERFLOW: "step_underflow"}
+    out = {}
+    orc = Oracle()
     if ref_available():
         ref = Reference()
-        rcfg = ref_config_from(cfg, float(Oracle().isco(0.9)), 30.0)
+        rcfg = ref_config_from(cfg, float(orc.isco(0.9)), 30.0)
         rcfg.enable_volumetric = 0
-        kind = "reference"
-
-        def row(r):
-            ref.trace_frame(1.0, 0.9, rcfg, fr.camera, r * WIDTH, WIDTH, threads=threads, keep=False)
-    else:
-        orc = Oracle()
-        kind = "port"
-
-        def row(r):
-            orc.trace_frame(fr, cfg, r * WIDTH, WIDTH, threads=threads)
+        recs, rows = [], 0
+        t0 = time.perf_counter()
+        while time.perf_counter() - t0 < seconds and rows < HEIGHT:
+            recs.append(ref.trace_frame(1.0, 0.9, rcfg, fr.camera, SAMPLE_ROWS[rows] * WIDTH, WIDTH, threads=threads))
+            rows += 1
+        dt = time.perf_counter() - t0
+        r = np.concatenate(recs)
+        out["cpu_baseline"] = {
+            "value": rows * WIDTH / dt / 1e6, "unit": "Mrays/s", "cores": threads, "kind": "reference",
+            "cpu_model": cpu_model(), "steps_per_ray": float(r["steps_taken"].mean()),
+            "outcome_mix": outcome_mix(r["outcome"], {0: "escaped", 1: "horizon", 2: "disk", 3: "max_steps",
+                                                      4: "spiraling"}),
+            "sample": f"{rows} full rows ({rows * WIDTH} rays) of the 1024^2 frame spread over its height, {dt:.1f} s, "
+                      f"RenderSession-style pixel queue over {threads} threads; thin disk only (the reference's gray "
+                      f"volumetric march replaces its disk); a rejected step ends a ray as MAX_STEPS "
+                      f"(GTRC001A.cpp:272-277), so max_steps counts the rays stop-on-reject cut short"}
+    res_o, bins_o, rows_o = [], [], []
     t0 = time.perf_counter()
-    rows = 0
-    order = [(i * 97) % HEIGHT for i in range(HEIGHT)]  # rows spread over the frame
-    while time.perf_counter() - t0 < seconds and rows < HEIGHT:
-        row(order[rows])
-        rows += 1
+    while time.perf_counter() - t0 < seconds and len(rows_o) < HEIGHT:
+        row = SAMPLE_ROWS[len(rows_o)]
+        a, b = orc.trace_frame(fr, cfg, row * WIDTH, WIDTH, threads=threads)
+        res_o.append(a)
+        bins_o.append(b)
+        rows_o.append(row)
     dt = time.perf_counter() - t0
-    return {"value": rows * WIDTH / dt / 1e6, "unit": "Mrays/s", "cores": threads, "kind": kind,
-            "sample": f"{rows} full rows ({rows * WIDTH} rays) of the 1024^2 frame spread over its height, "
-                      f"{dt:.1f} s, RenderSession-style pixel queue over {threads} threads; thin disk only "
-                      f"(the reference's gray volumetric march replaces its disk)"}
+    ro = np.concatenate(res_o)
+    bo = np.concatenate(bins_o)
+    oracle_line = {"value": len(rows_o) * WIDTH / dt / 1e6, "unit": "Mrays/s", "cores": threads, "kind": "port",
+                   "cpu_model": cpu_model(), "steps_per_ray": float(ro["steps"].mean()),
+                   "rejected_per_ray": float(ro["rejected"].mean()), "outcome_mix": outcome_mix(ro["outcome"], names),
+                   "sample": f"{len(rows_o)} full rows ({len(rows_o) * WIDTH} rays) of the 1024^2 frame, {dt:.1f} s, "
+                             f"atomic pixel queue over {threads} threads; the full workload (NT disk + 16-bin "
+                             f"volumetric), engine semantics (retry on reject)"}
+    if "cpu_baseline" not in out:
+        out["cpu_baseline"] = oracle_line
+    else:
+        out["cpu_baseline_oracle"] = oracle_line
+    idx = np.concatenate([np.arange(r * WIDTH, (r + 1) * WIDTH) for r in rows_o])
+    rep = compare.report(gpu_res[idx], gpu_img[idx], ro, gpu_spc[idx], bo, escape_radius=200.0)
+    rep["rows"] = len(rows_o)
+    rep["note"] = ("mixed-precision GPU frame against the FP64 oracle on the oracle's sampled rows; image errors "
+                   "relative to the sample's peak, spectra per bin; maxima over the rays whose histories agree "
+                   "(split_histories counts the others)")
+    out["error_vs_oracle"] = rep
+    return out
 
 
 def batch_frames(abi, seed=3, n=96):
@@ -490,7 +563,7 @@ def main():
 
     from sirius_b200 import abi
     from sirius_b200.engine import Engine, flop_count
-    from sirius_b200.shard import max_over_ranks
+    from sirius_b200.shard import gather_rows, max_over_ranks, row_block
 
     world = int(os.environ.get("WORLD_SIZE", "1"))
     rank = int(os.environ.get("RANK", "0"))
@@ -515,10 +588,18 @@ def main():
     main_cfg = workload_config(abi, abi.PRECISION_MIXED)
     main_cfg.max_registers = args.max_registers
     eng = Engine(local, config=main_cfg)
+    full_frame = workload_frame(abi, args.size, args.size)
+    # the frame is split across ranks as contiguous row blocks (strong scaling);
+    # each rank traces its block's row window, and the image rows are gathered to
+    # rank 0 every step (the one exchange of a split frame)
+    r0, r1 = row_block(args.size, rank, world)
     frame = workload_frame(abi, args.size, args.size)
+    if world > 1:
+        frame.row_begin, frame.row_count = r0, r1 - r0
     frames = (abi.Frame * 1)(frame)
     frames[0].ray_offset = 0
-    total = args.size * args.size
+    total = abi.frame_rays(frame)
+    frame_total = args.size * args.size
     fbytes = bytes(frames)
     d_frames = torch.frombuffer(bytearray(fbytes), dtype=torch.uint8).to(dev)
     d_image = torch.empty(total, dtype=torch.float32, device=dev)
@@ -528,6 +609,8 @@ def main():
     def step():
         eng.trace_frames_device(d_frames.data_ptr(), 1, total, None, d_image.data_ptr(), d_spectra.data_ptr(),
                                 stream.cuda_stream)
+        if world > 1:
+            gather_rows(d_image, args.size, args.size, dist, dev)
 
     for _ in range(max(args.warmup, 3)):
         step()
@@ -556,9 +639,9 @@ def main():
     torch.cuda.synchronize()
     clk = clocks.stop()
     step_ms = [a.elapsed_time(b) for a, b in ev]
-    # device time of the K steps, the maximum over ranks (each rank renders its own frame)
+    # device time of the K steps, the maximum over ranks (each rank traces its row block)
     t_total = max_over_ranks(sum(step_ms), dist if world > 1 else None, dev)
-    value = world * total * args.steps / (t_total * 1e-3) / 1e6
+    value = frame_total * args.steps / (t_total * 1e-3) / 1e6
 
     # end to end through the host entry point: frame descriptor H2D, image + spectra D2H (pinned)
     h_img = torch.empty(total, dtype=torch.float32, pin_memory=True)
@@ -572,7 +655,7 @@ def main():
     for _ in range(args.steps):
         eng.trace_frames_into(C.addressof(fr_arr), 1, None, h_img.data_ptr(), h_spc.data_ptr())
     t_e2e = max_over_ranks(time.perf_counter() - t0, dist if world > 1 else None, dev)
-    e2e = world * total * args.steps / t_e2e / 1e6
+    e2e = frame_total * args.steps / t_e2e / 1e6
 
     # roofline of the trace kernel: algorithmic operations / kernel time vs the measured FP32 SIMT peak
     rhs_f, att_f, acc_f = flop_count(frame.metric)
@@ -583,7 +666,7 @@ def main():
     peak64 = eng.fma_peak(0) / 1e12
 
     line = {"metric": "Mrays/s", "value": value, "unit": "Mrays/s", "n_gpus": world, "steps": args.steps,
-            "warmup": args.warmup, "ms_per_step": t_total / args.steps, "higher_is_better": True, "scaling": "weak",
+            "warmup": args.warmup, "ms_per_step": t_total / args.steps, "higher_is_better": True, "scaling": "strong",
             "vs_baseline": None, "dtype": "f32+f64",
             "data": "synthetic (seeded camera frame; no dataset)", "config": workload_desc(args.size),
             "e2e": {"value": e2e, "unit": "Mrays/s", "h2d_bytes_per_step": C.sizeof(abi.Frame),
@@ -599,6 +682,8 @@ def main():
             "fp64_island_step_fraction": fp64 / max(accepted, 1), "clocks": clk}
 
     if rank == 0 and world == 1 and not args.no_extras:
+        # the mixed frame with per-ray records (untimed), for the error report against the oracle
+        res_mixed, _, _ = eng.trace_frames([full_frame], results=True, spectra=False)
         # the plain FP64 GPU integrator on the same frame (one thread per ray), and the error vs it
         img_mixed = d_image.cpu().numpy().astype(np.float64)
         spc_mixed = d_spectra.cpu().numpy().reshape(total, N_BINS).astype(np.float64)
@@ -625,7 +710,7 @@ def main():
         line["graph_replay"] = graph_leg(eng, abi, torch, dev)
         line["heterogeneous_batch"] = batch_leg(eng, abi)
         line["stress_symplectic"] = stress_leg(eng, abi)
-        line["cpu_baseline"] = cpu_baseline_sample()
+        line.update(cpu_baseline_sample(res_mixed, img_mixed, spc_mixed))
     if rank == 0:
         print(json.dumps(line), flush=True)
     eng.close()

@@ -52,12 +52,32 @@ def split_histories(res, ref):
             (res["equatorial_crossings"] != ref["equatorial_crossings"]))
 
 
-def report(res, img, ref, spectra=None, ref_bins=None, escape_radius=None):
+def _cartesian(res, spherical):
+    """Final positions and spatial momentum directions in Cartesian components.
+    Spherical states (t, r, theta, phi; the Morris-Thorne chart) are mapped with
+    the orthonormal spherical frame: (p_r, p_theta / r, p_phi / (r sin theta))
+    rotated onto (x, y, z) (the far-field direction of an escaped ray)."""
+    x = res["final_x"].astype(np.float64)
+    p = res["final_p"].astype(np.float64)
+    if not spherical:
+        return x[:, 1:], p[:, 1:]
+    r, th, ph = x[:, 1], x[:, 2], x[:, 3]
+    st, ct, sp, cp = np.sin(th), np.cos(th), np.sin(ph), np.cos(ph)
+    pos = np.stack([r * st * cp, r * st * sp, r * ct], 1)
+    er = np.stack([st * cp, st * sp, ct], 1)
+    et = np.stack([ct * cp, ct * sp, -st], 1)
+    ep = np.stack([-sp, cp, np.zeros_like(sp)], 1)
+    pr, pt, pp = p[:, 1], p[:, 2] / np.maximum(r, 1e-30), p[:, 3] / np.maximum(r * np.abs(st), 1e-30)
+    return pos, pr[:, None] * er + pt[:, None] * et + pp[:, None] * ep
+
+
+def report(res, img, ref, spectra=None, ref_bins=None, escape_radius=None, spherical=False):
     """Errors of an engine trace (results res, image img, optional spectra) against
     the oracle's trace of the same pixels (ref, ref_bins). Images are compared
     relative to the oracle image's peak, spectra per bin relative to the bin's peak.
     escape_radius (None: the smallest final radius of the oracle's escaped rays)
-    selects the escaped rays of the terminal-state comparison."""
+    selects the escaped rays of the terminal-state comparison; spherical: the
+    states are in the (t, r, theta, phi) chart."""
     n = len(ref)
     split = split_histories(res, ref)
     same = ~split
@@ -75,19 +95,21 @@ def report(res, img, ref, spectra=None, ref_bins=None, escape_radius=None):
         out[name] = {"drift": _stats(_rel(res[name], res[name + "0"], x0)),
                      "vs_oracle": _stats(_rel(res[name][same], ref[name][same], ref[name][same]))}
     # terminal state of the rays that escape in both traces
-    rg = np.linalg.norm(res["final_x"][:, 1:].astype(np.float64), axis=1)
-    ro = np.linalg.norm(ref["final_x"][:, 1:].astype(np.float64), axis=1)
+    xg_all, pg_all = _cartesian(res, spherical)
+    xo_all, po_all = _cartesian(ref, spherical)
+    rg = np.linalg.norm(xg_all, axis=1)
+    ro = np.linalg.norm(xo_all, axis=1)
     if escape_radius is None:
         esc0 = ref["outcome"] == 0
         escape_radius = float(ro[esc0].min()) if esc0.any() else np.inf
     esc = same & (rg >= escape_radius) & (ro >= escape_radius)
     out["escaped_compared"] = int(esc.sum())
-    pg = res["final_p"][esc, 1:].astype(np.float64)
-    po = ref["final_p"][esc, 1:].astype(np.float64)
+    pg = pg_all[esc]
+    po = po_all[esc]
     ng = pg / np.linalg.norm(pg, axis=1, keepdims=True)
     no = po / np.linalg.norm(po, axis=1, keepdims=True)
     out["escape_direction_rad"] = _stats(np.arctan2(np.linalg.norm(np.cross(ng, no), axis=1), np.sum(ng * no, 1)))
-    dx = res["final_x"][esc, 1:].astype(np.float64) - ref["final_x"][esc, 1:].astype(np.float64)
+    dx = xg_all[esc] - xo_all[esc]
     perp = dx - np.sum(dx * no, 1, keepdims=True) * no
     out["terminal_position"] = _stats(np.linalg.norm(perp, axis=1) / ro[esc])
     # disk crossings (first crossing of rays that both trace onto the disk)

