@@ -281,7 +281,9 @@ __device__ __forceinline__ const DPTable<double>& dp_table<double>() { return kD
 // the FP32 bulk; double: FP64). The state stays in FP64; stage inputs are
 // x + h acc where acc = sum_j a_sj k_j accumulates in T in a sliding window, so
 // the six right-hand sides share one call site (a compact loop body keeps the
-// instruction stream in cache). On entry k1 = f(x, p); on exit (xn, pn) is the
+// instruction stream in cache). The p_0 component is not accumulated: every
+// family's metric is static, so dp_0/dl = 0 and p_0 (the conserved -E) carries
+// through the attempt unchanged. On entry k1 = f(x, p); on exit (xn, pn) is the
 // fifth-order solution and k7 = f(xn, pn) (first same as last). Returns the
 // scaled RMS error of the position components (computeRK45ErrorNorm,
 // PHGD001A.cpp:508-517).
@@ -311,7 +313,8 @@ __device__ __forceinline__ double dp45_attempt(const MetricDev& m, const CfgDev&
         for (int s = 0; s < 6; ++s) {
             const T a = D.A[j][s];
 #pragma unroll
-            for (int i = 0; i < 8; ++i) acc[s][i] += a * kc[i];
+            for (int i = 0; i < 8; ++i)
+                if (i != 4) acc[s][i] += a * kc[i];
         }
         const T e = D.E[j];
 #pragma unroll
@@ -321,20 +324,24 @@ __device__ __forceinline__ double dp45_attempt(const MetricDev& m, const CfgDev&
 #pragma unroll
             for (int i = 0; i < 4; ++i) {
                 xn[i] = x[i] + h * double(acc[0][i]);
-                pn[i] = p[i] + h * double(acc[0][4 + i]);
+                pn[i] = i == 0 ? p[0] : p[i] + h * double(acc[0][4 + i]);
                 xs[i] = T(xn[i]);
                 ps[i] = T(pn[i]);
             }
         } else {
 #pragma unroll
-            for (int i = 0; i < 4; ++i) { xs[i] = X[i] + ht * acc[0][i]; ps[i] = X[4 + i] + ht * acc[0][4 + i]; }
+            for (int i = 0; i < 4; ++i) {
+                xs[i] = X[i] + ht * acc[0][i];
+                ps[i] = i == 0 ? X[4] : X[4 + i] + ht * acc[0][4 + i];
+            }
         }
         rhs<T, FAM>(m, xs, ps, kc, kc + 4);
         // slide the window: the next stage's input moves to slot 0
 #pragma unroll
         for (int s = 0; s < 5; ++s)
 #pragma unroll
-            for (int i = 0; i < 8; ++i) acc[s][i] = acc[s + 1][i];
+            for (int i = 0; i < 8; ++i)
+                if (i != 4) acc[s][i] = acc[s + 1][i];
 #pragma unroll
         for (int i = 0; i < 8; ++i) acc[5][i] = T(0);
     }
