@@ -678,6 +678,10 @@ FrameDev make_frame(const sirius_frame& f, const sirius_trace_config& c) {
         gtt = -(1.0 - m.vs * m.vs * fs * fs);
     }
     F.sqrt_m_gtt_cam = std::sqrt(std::max(-gtt, 1e-30));
+    F.fsqrt_m_gtt_cam = float(F.sqrt_m_gtt_cam);
+    F.fdisk_in = float(F.disk_in);
+    F.fdisk_out = float(F.disk_out);
+    F.fr_ph_pro = float(F.r_ph_pro);
     F.observer = f.camera.observer;
     F.sub_u = 0.5f;
     F.sub_v = 0.5f;
@@ -696,6 +700,9 @@ CfgDev make_cfg(const sirius_trace_config& c) {
     d.vol_j0 = c.vol_j0; d.vol_aoj = c.vol_alpha_over_j; d.vol_hz = c.vol_height_ratio; d.vol_s = c.vol_spectral_index;
     d.integrator = c.integrator; d.symp_order = c.symplectic_order; d.symp_step = c.symplectic_step;
     d.crit_band = c.critical_band;
+    d.fatol = float(d.atol); d.frtol = float(d.rtol); d.fsafety = float(d.safety); d.fgrow = float(d.grow);
+    d.fshrink = float(d.shrink); d.fvol_j0 = float(d.vol_j0); d.fvol_aoj = float(d.vol_aoj);
+    d.fvol_hz = float(d.vol_hz); d.fvol_s = float(d.vol_s);
     d.npair = (d.nbins + 1) / 2;
     for (int b = 0; b < d.nbins; ++b) {
         const double nu = d.nbins == 1 ? c.nu_min : c.nu_min * std::pow(c.nu_max / c.nu_min, double(b) / (d.nbins - 1));

@@ -28,7 +28,15 @@ struct MetricDev {
     int has_lambda;        // |Lambda| > 1e-15 (PHMT100A.h:365)
     double b0, Phi0, gtt_mt;  // Morris-Thorne: g_tt = -exp(2 Phi0)
     double vs, sigma, Rb, inv_2tanhsR;  // Alcubierre
+    // FP32 copies for the single-precision paths (rounded once on the host)
+    float fa, fa2, fM2, fQ2, flam3, fsqrtM;
 };
+
+// A launch constant in precision T: the FP32 copy for float, else the double.
+template <class T>
+SIRIUS_HD __forceinline__ T cst(double d, float) { return T(d); }
+template <>
+SIRIUS_HD __forceinline__ float cst<float>(double, float f) { return f; }
 
 // Host: the per-metric constants the device code reads.
 inline MetricDev metric_dev(const sirius_metric& s) {
@@ -41,6 +49,8 @@ inline MetricDev metric_dev(const sirius_metric& s) {
     m.b0 = s.b0; m.Phi0 = s.Phi0; m.gtt_mt = -std::exp(2.0 * s.Phi0);
     m.vs = s.vs; m.sigma = s.sigma; m.Rb = s.R;
     m.inv_2tanhsR = (s.sigma * s.R != 0.0) ? 1.0 / (2.0 * std::tanh(s.sigma * s.R)) : 0.0;
+    m.fa = float(m.a); m.fa2 = float(m.a2); m.fM2 = float(2.0 * m.M); m.fQ2 = float(m.Q2);
+    m.flam3 = float(m.lam3); m.fsqrtM = float(m.sqrtM);
     return m;
 }
 
@@ -126,7 +136,7 @@ SIRIUS_HD __forceinline__ void ks_rhs(const MetricDev& m, const T x[4], const T 
 // with num = (2 M r - Q^2) r^2, fden = r^4 + a^2 z^2, H = num / fden.
 template <class T>
 SIRIUS_HD __forceinline__ void ks_rhs_fast(const MetricDev& m, const T x[4], const T p[4], T k[4], T f[4]) {
-    const T a = T(m.a), a2 = T(m.a2);
+    const T a = cst<T>(m.a, m.fa), a2 = cst<T>(m.a2, m.fa2);
     const T X = x[1], Y = x[2], Z = x[3];
     const T zz = Z * Z;
     const T R2 = X * X + Y * Y + zz;
@@ -152,11 +162,12 @@ SIRIUS_HD __forceinline__ void ks_rhs_fast(const MetricDev& m, const T x[4], con
     const T l3 = Z * ir;
     const T zi2 = -l3 * ir;
     const T l3d0 = zi2 * rx, l3d1 = zi2 * ry, l3d2 = zi2 * rz + ir;
-    const T q = T(2.0 * m.M) * r - T(m.Q2);
+    const T M2 = cst<T>(2.0 * m.M, m.fM2);
+    const T q = M2 * r - cst<T>(m.Q2, m.fQ2);
     const T fden = r2 * r2 + a2zz;
     const T ifd = rcp_(fden);
     const T H = q * r2 * ifd;
-    const T w = (T(2.0 * m.M) * r2 + T(2) * r * q - H * T(4) * r2 * r) * ifd;
+    const T w = (M2 * r2 + T(2) * r * q - H * T(4) * r2 * r) * ifd;
     const T Hd0 = w * rx, Hd1 = w * ry, Hd2 = w * rz - H * ifd * T(2) * a2 * Z;
     // k = g^{-1} p = eta p - H l# (l# . p), l# = (-1, l1, l2, l3)
     const T lp = -p[0] + l1 * p[1] + l2 * p[2] + l3 * p[3];
@@ -166,7 +177,7 @@ SIRIUS_HD __forceinline__ void ks_rhs_fast(const MetricDev& m, const T x[4], con
     k[2] = p[2] - l2 * Hlp;
     k[3] = p[3] - l3 * Hlp;
     if (m.has_lambda) {
-        const T c = T(m.lam3) * R2;
+        const T c = cst<T>(m.lam3, m.flam3) * R2;
         const T w0 = -T(1) - H, w1 = H * l1, w2 = H * l2, w3 = H * l3;
         const T s = c * (w0 * p[0] + w1 * p[1] + w2 * p[2] + w3 * p[3]) * rcp_(T(1) + c * (T(1) + H));
         k[0] += s * w0; k[1] += s * w1; k[2] += s * w2; k[3] += s * w3;
@@ -179,7 +190,7 @@ SIRIUS_HD __forceinline__ void ks_rhs_fast(const MetricDev& m, const T x[4], con
     f[2] = lk * (Hd1 * hlk + H * (l1d1 * k[1] + l2d1 * k[2] + l3d1 * k[3]));
     f[3] = lk * (Hd2 * hlk + H * (l1d2 * k[1] + l2d2 * k[2] + l3d2 * k[3]));
     if (m.has_lambda) {
-        const T qq = T(m.lam3) * k[0] * k[0];
+        const T qq = cst<T>(m.lam3, m.flam3) * k[0] * k[0];
         f[1] -= qq * X; f[2] -= qq * Y; f[3] -= qq * Z;
     }
 }

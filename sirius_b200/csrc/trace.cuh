@@ -31,6 +31,7 @@ struct FrameDev {
     // radii
     double disk_in, disk_out, r_hor, r_plus, island_r, a_star, isco, r_ph_pro;
     double sqrt_m_gtt_cam;
+    float fsqrt_m_gtt_cam, fdisk_in, fdisk_out, fr_ph_pro;  // FP32 copies
     // observer (enum sirius_observer); for the zero-angular-momentum observer:
     // the camera's Kerr-Schild position and the four tetrad vectors e_(t),
     // e_(r), e_(theta), e_(phi) in Kerr-Schild contravariant components
@@ -45,7 +46,7 @@ struct FrameDev {
 // observer sees frequency 1 by construction, so the factor is E itself.
 template <class T>
 __device__ __forceinline__ T observer_factor(const FrameDev& F, T E) {
-    return F.observer == SIRIUS_OBSERVER_ZAMO ? E : T(F.sqrt_m_gtt_cam);
+    return F.observer == SIRIUS_OBSERVER_ZAMO ? E : cst<T>(F.sqrt_m_gtt_cam, F.fsqrt_m_gtt_cam);
 }
 
 struct CfgDev {
@@ -55,6 +56,8 @@ struct CfgDev {
     int integrator, symp_order;
     double symp_step, crit_band;
     double vol_j0, vol_aoj, vol_hz, vol_s;
+    // FP32 copies for the single-precision paths
+    float fatol, frtol, fsafety, fgrow, fshrink, fvol_j0, fvol_aoj, fvol_hz, fvol_s;
     int npair;                       // bin pairs, (nbins + 1) / 2
     float2 nu_pow2[SIRIUS_MAX_BINS / 2];  // nu^-s of bins (2j, 2j + 1); 0 pads an odd last pair
 };
@@ -355,7 +358,7 @@ __device__ __forceinline__ double dp45_attempt(const MetricDev& m, const CfgDev&
             const double e = h * double(ex) / (c.atol + c.rtol * fabs(xn[i]));
             en += e * e;
         } else {  // the estimate needs a few digits only
-            const float e = ht * ex * rcp_(float(c.atol) + float(c.rtol) * fabsf(float(xn[i])));
+            const float e = ht * ex * rcp_(c.fatol + c.frtol * fabsf(float(xn[i])));
             en += e * e;
         }
     }
@@ -514,8 +517,8 @@ __device__ __forceinline__ double ks_radius(const MetricDev& m, const double x[4
 // Step control in FP32 for the mixed path (the factor needs a few digits only).
 __device__ __forceinline__ double optimal_step_fast(double h, double err, const CfgDev& c) {
     if (err < 1e-15) return fmin(h * c.grow, c.hmax);
-    float fac = float(c.safety) * exp2f(-0.2f * __log2f(float(err)));
-    fac = fmaxf(float(c.shrink), fminf(float(c.grow), fac));
+    float fac = c.fsafety * exp2f(-0.2f * __log2f(float(err)));
+    fac = fmaxf(c.fshrink, fminf(c.fgrow, fac));
     return fmax(c.hmin, fmin(c.hmax, h * double(fac)));
 }
 
@@ -574,14 +577,15 @@ __device__ __forceinline__ double hermite_root(double z0, double z1, double dz0,
 // rbl is the Kerr-Schild r of (x, y, z): H and l follow from it without derivatives.
 template <class T>
 __device__ __forceinline__ T kepler_g(const MetricDev& m, T x, T y, T z, T rbl, T E, T Lz, T sqrt_m_gtt_cam) {
-    const T r2 = rbl * rbl, iden = rcp_(r2 + T(m.a2));
-    const T l1 = (rbl * x + T(m.a) * y) * iden, l2 = (rbl * y - T(m.a) * x) * iden;
-    const T H = (T(2.0 * m.M) * rbl - T(m.Q2)) * r2 * rcp_(r2 * r2 + T(m.a2) * z * z);
+    const T a = cst<T>(m.a, m.fa), a2 = cst<T>(m.a2, m.fa2), sqrtM = cst<T>(m.sqrtM, m.fsqrtM);
+    const T r2 = rbl * rbl, iden = rcp_(r2 + a2);
+    const T l1 = (rbl * x + a * y) * iden, l2 = (rbl * y - a * x) * iden;
+    const T H = (cst<T>(2.0 * m.M, m.fM2) * rbl - cst<T>(m.Q2, m.fQ2)) * r2 * rcp_(r2 * r2 + a2 * z * z);
     const T lxi = -y * l1 + x * l2;
     T gtt = -T(1) + H;
-    if (m.has_lambda) gtt -= T(m.lam3) * (x * x + y * y + z * z);
+    if (m.has_lambda) gtt -= cst<T>(m.lam3, m.flam3) * (x * x + y * y + z * z);
     const T gtp = H * lxi, gpp = x * x + y * y + H * lxi * lxi;
-    const T Om = T(m.sqrtM) * rcp_(rbl * sqrtp_(rbl) + T(m.a) * T(m.sqrtM));
+    const T Om = sqrtM * rcp_(rbl * sqrtp_(rbl) + a * sqrtM);
     const T n = -(gtt + T(2) * Om * gtp + Om * Om * gpp);
     if (!(n > T(0))) return T(0);
     const T ut = rsqrt_(n);

@@ -249,7 +249,7 @@ __device__ __forceinline__ void hermite_xyz(const double x0[4], const double x1[
 }
 
 __device__ __forceinline__ float ks_r(const MetricDev& m, float x, float y, float z) {
-    const float a2 = float(m.a2), R2 = x * x + y * y + z * z, Rm2 = R2 - a2;
+    const float a2 = m.fa2, R2 = x * x + y * y + z * z, Rm2 = R2 - a2;
     const float sd = sqrtp_(fmaxf(Rm2 * Rm2 + 4.f * a2 * z * z, 1e-20f));
     return sqrtp_(fmaxf(0.5f * (Rm2 + sd), 1e-10f));
 }
@@ -287,7 +287,7 @@ __device__ __forceinline__ void volumetric_segment(const Params& P, const FrameD
     const float E = float(-p[0]);
     const float Lz = float(x1[1] * p[2] - x1[2] * p[1]);
     const float nu_cam = E / observer_factor<float>(F, E);
-    const float rin = float(F.disk_in), rout = float(F.disk_out);
+    const float rin = F.fdisk_in, rout = F.fdisk_out;
     const bool in0 = r0 >= rin && r0 <= rout, in1 = r1 >= rin && r1 <= rout;
     float xf0[3], dxf[3];
     if constexpr (MIXED) {
@@ -342,15 +342,15 @@ __device__ __forceinline__ void volumetric_segment(const Params& P, const FrameD
         point(fa + span * double(kGLx[nq - 1][s]), xs, ys, zs);
         const float r = ks_r(F.m, xs, ys, zs);
         if (r < rin || r > rout) return;
-        const float zr = zs / (float(c.vol_hz) * r);
+        const float zr = zs / (c.fvol_hz * r);
         if (fabsf(zr) > float(kVolCutoff)) return;
         const float g = kepler_g<float>(F.m, xs, ys, zs, r, E, Lz, observer_factor<float>(F, E));
         if (!(g > 0.f)) return;
         const float dl = float(h * span) * kGLw[nq - 1][s];
-        const float jsp = float(c.vol_j0) / (r * r) * __expf(-0.5f * zr * zr);
-        const float gs = __powf(g, float(c.vol_s));  // nu_em^-s = (g/nu_b)^s
-        dts = float(c.vol_aoj) * jsp * gs * (nu_cam / g) * dl;
-        Ss = g * g * g / float(c.vol_aoj);
+        const float jsp = c.fvol_j0 / (r * r) * __expf(-0.5f * zr * zr);
+        const float gs = __powf(g, c.fvol_s);  // nu_em^-s = (g/nu_b)^s
+        dts = c.fvol_aoj * jsp * gs * (nu_cam / g) * dl;
+        Ss = g * g * g / c.fvol_aoj;
     };
     // the Gauss-Legendre points in step order, each applied to every bin pair
     // (a point outside the emitting region, or with no redshift, leaves the bins
@@ -511,12 +511,12 @@ __device__ __forceinline__ int advance_post(const Params& P, Ray<MIXED>& s, bool
 // The volumetric step cap at radius r, height z, spatial velocity k[1..3]: FP32
 // on the mixed path, FP64 on the FP64 path.
 template <bool MIXED, class K>
-__device__ __forceinline__ double vol_cap(double r, double z, const K k[8], double hz, double r_in, double r_out) {
+__device__ __forceinline__ double vol_cap(double r, double z, const K k[8], const CfgDev& c, const FrameDev& F) {
     if constexpr (MIXED)
-        return double(volume_step_cap_f(float(r), float(z), float(k[1]), float(k[2]), float(k[3]), float(hz),
-                                        float(r_in), float(r_out)));
+        return double(volume_step_cap_f(float(r), float(z), float(k[1]), float(k[2]), float(k[3]), c.fvol_hz,
+                                        F.fdisk_in, F.fdisk_out));
     else
-        return volume_step_cap(r, z, double(k[1]), double(k[2]), double(k[3]), hz, r_in, r_out);
+        return volume_step_cap(r, z, double(k[1]), double(k[2]), double(k[3]), c.vol_hz, F.disk_in, F.disk_out);
 }
 
 // One iteration of the ray state machine: a DP45 attempt, and on acceptance
@@ -596,7 +596,7 @@ __device__ __forceinline__ int advance_post(const Params& P, Ray<MIXED>& s, bool
         if (c.enable_vol && c.enable_disk && F.has_horizon && is_family<FAM>(m, SIRIUS_METRIC_KERR_SCHILD)) {
             InvForm RF;
             inv_form(m, s.x, RF);
-            s.h = fmax(c.hmin, fmin(s.h, vol_cap<MIXED>(RF.r, s.x[3], s.k, c.vol_hz, F.disk_in, F.disk_out)));
+            s.h = fmax(c.hmin, fmin(s.h, vol_cap<MIXED>(RF.r, s.x[3], s.k, c, F)));
         }
         if (s.h <= c.hmin) { ++s.steps; return SIRIUS_STEP_UNDERFLOW; }
         if (s.attempts > c.max_steps * 64 + 1024) return SIRIUS_STEP_UNDERFLOW;
@@ -618,9 +618,8 @@ __device__ __forceinline__ int advance_post(const Params& P, Ray<MIXED>& s, bool
         const float cx = float(s.x[1]) + t * dx, cy = float(s.x[2]) + t * dy;
         const float rho = sqrtp_(fmaxf(cx * cx + cy * cy, 1e-30f));
         const float L3 = 3.f * sqrtp_(fmaxf(dx * dx + dy * dy + dz * dz, 1e-30f));
-        const float a2 = float(m.a2), rhi = rho + L3, rlo = fmaxf(rho - L3, 0.f);
-        if (rlo * rlo - a2 > float(F.disk_out) * float(F.disk_out) * 1.0001f ||
-            rhi * rhi - a2 < float(F.disk_in) * float(F.disk_in) * 0.9999f)
+        const float a2 = m.fa2, rhi = rho + L3, rlo = fmaxf(rho - L3, 0.f);
+        if (rlo * rlo - a2 > F.fdisk_out * F.fdisk_out * 1.0001f || rhi * rhi - a2 < F.fdisk_in * F.fdisk_in * 0.9999f)
             cross = false;
     }
     if (cross) {
@@ -697,7 +696,7 @@ __device__ __forceinline__ int advance_post(const Params& P, Ray<MIXED>& s, bool
     }
     if (float(rr) < s.min_r) s.min_r = float(rr);
     if (disk_on && c.enable_vol && !symp)
-        s.h = fmax(c.hmin, fmin(s.h, vol_cap<MIXED>(rr, s.x[3], s.k, c.vol_hz, F.disk_in, F.disk_out)));
+        s.h = fmax(c.hmin, fmin(s.h, vol_cap<MIXED>(rr, s.x[3], s.k, c, F)));
     const bool mt = is_family<FAM>(m, SIRIUS_METRIC_MORRIS_THORNE);
 
     // winding: equatorial crossings and |d phi| (GTRC001A.cpp:294-309); the
@@ -715,7 +714,7 @@ __device__ __forceinline__ int advance_post(const Params& P, Ray<MIXED>& s, bool
     // spiral early-out (GTRC001A.cpp:322-352)
     const int sidx = s.steps - 1;
     if (c.spiral && !mt && (sidx % 100) == 0 && sidx > 100) {
-        const float ratio = s.min_r / float(F.r_ph_pro);
+        const float ratio = s.min_r / F.fr_ph_pro;
         if (ratio < 1.5f && ratio > 0.9f && s.tphi > 2.f * float(kPi)) {
             const double k1 = double(s.k[1]), k2 = double(s.k[2]), k3 = double(s.k[3]);
             const double Reu = sqrt(s.x[1] * s.x[1] + s.x[2] * s.x[2] + s.x[3] * s.x[3]);
@@ -735,7 +734,7 @@ __device__ __forceinline__ int advance_post(const Params& P, Ray<MIXED>& s, bool
             const double vrad = mt ? double(s.k[1])
                                    : (s.x[1] * double(s.k[1]) + s.x[2] * double(s.k[2]) + s.x[3] * double(s.k[3]));
             if (vrad > 0.0) {
-                const float ratio = s.min_r / float(F.r_ph_pro);
+                const float ratio = s.min_r / F.fr_ph_pro;
                 if (ratio < 1.5f) {
                     flags |= SIRIUS_FLAG_PHOTON_RING;
                     magnification = ratio > 1.f ? fminf(1.f + 2.f / fmaxf(ratio - 1.f, 0.1f), 20.f) : 20.f;
@@ -748,7 +747,7 @@ __device__ __forceinline__ int advance_post(const Params& P, Ray<MIXED>& s, bool
     if (c.enable_vol && vol) {
         // steps that cannot reach the emitting region skip the segment (the
         // step cap keeps a step that starts outside it from jumping in)
-        const float r0 = s.prev_r, r1 = float(rr), rin = float(F.disk_in), rout = float(F.disk_out);
+        const float r0 = s.prev_r, r1 = float(rr), rin = F.fdisk_in, rout = F.fdisk_out;
         const float zc = float(kVolCutoff * c.vol_hz), z0 = float(x0[3]), z1 = float(s.x[3]);
         const bool beyond = (r0 > rout && r1 > rout) ||
                             (z0 * z1 > 0.f && fabsf(z0) > zc * fminf(fmaxf(r0, rin), rout) &&
@@ -767,7 +766,7 @@ __device__ __forceinline__ int advance_post(const Params& P, Ray<MIXED>& s, bool
         if (dI >= 0.0) {
             s.intensity += dI;
             ++s.ncross;
-            const float ratio = s.min_r / float(F.r_ph_pro);
+            const float ratio = s.min_r / F.fr_ph_pro;
             if (ratio < 1.5f) {
                 flags |= SIRIUS_FLAG_PHOTON_RING;
                 magnification = ratio > 1.f ? fminf(1.f + 2.f / fmaxf(ratio - 1.f, 0.05f), 100.f) : 100.f;
