@@ -370,10 +370,11 @@ def surrogate_config(abi, precision):
                               precision=precision, enable_disk=1, enable_volumetric=0, critical_band=0.0)
 
 
-def surrogate_leg(eng, abi, np, torch, dev, stream, side=SURROGATE_SIDE, reps=3):
+def surrogate_leg(eng, abi, np, torch, dev, stream, side=SURROGATE_SIDE, reps=3, inner_gate=0.0):
     """Surrogate-gated rendering of the Kerr a = 0.9 frame at side^2 (gate +-0.3 M
-    around the critical curve, 1 % audit rays) against the plain FP64 integrator
-    on the same frame; CUDA events on the launch stream around whole calls."""
+    around the critical curve, the inner-disk gate r_1 < 2.5 r_in from a coarse
+    MLP pass on 8 x 8 pixel cells, 1 % audit rays) against the plain FP64
+    integrator on the same frame; CUDA events on the launch stream around whole calls."""
     params = np.load(SURROGATE_WEIGHTS)
     eng.surrogate_load(params)
     frame = workload_frame(abi, side, side)
@@ -387,12 +388,14 @@ def surrogate_leg(eng, abi, np, torch, dev, stream, side=SURROGATE_SIDE, reps=3)
         fp64_ms.append(eng.stats().kernel_ms)
     eng.configure(surrogate_config(abi, abi.PRECISION_MIXED))
     ev0, ev1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    sc = abi.surrogate_config(inner_gate=inner_gate)
     for _ in range(2):
-        eng.render_surrogate_device([frame], d_img.data_ptr(), None, d_gate.data_ptr(), stream=stream.cuda_stream)
+        eng.render_surrogate_device([frame], d_img.data_ptr(), None, d_gate.data_ptr(), config=sc,
+                                    stream=stream.cuda_stream)
     times, stats = [], None
     for _ in range(reps):
         ev0.record(stream)
-        stats = eng.render_surrogate_device([frame], d_img.data_ptr(), None, d_gate.data_ptr(),
+        stats = eng.render_surrogate_device([frame], d_img.data_ptr(), None, d_gate.data_ptr(), config=sc,
                                             stream=stream.cuda_stream)
         ev1.record(stream)
         torch.cuda.synchronize()
@@ -425,7 +428,9 @@ def surrogate_leg(eng, abi, np, torch, dev, stream, side=SURROGATE_SIDE, reps=3)
     bf16_peak = float(peaks.get("bf16_tflops", 1590.0))
     return {"workload": f"kerr_a0.9_{side}x{side}_nt_disk_surrogate_gated", "mrays_per_s": n / (ms * 1e-3) / 1e6,
             "ms_per_frame": ms, "fp64_plain_ms": t64, "speedup_vs_fp64_plain": t64 / ms,
-            "gate_band_m": 0.3, "audit_fraction": 0.01, "gated_fraction": float(np.mean(gate == 1)),
+            "gate_band_m": 0.3, "inner_gate_r_in": 2.5 if inner_gate == 0.0 else (None if inner_gate < 0 else inner_gate),
+            "coarse_stride": 8, "coarse_mlp_rows": int(stats.coarse_rays),
+            "audit_fraction": 0.01, "gated_fraction": float(np.mean(gate == 1)),
             "audit_fraction_measured": float(np.mean(gate == 2)), "integrated_rays": int(stats.integrated),
             "stage_ms": {"features_gate": stats.ms_features, "mlp_end": stats.ms_mlp, "shade": stats.ms_shade,
                          "integrate_gated_and_audit": stats.ms_trace,
@@ -704,7 +709,10 @@ def main():
         line["error_vs_fp64"] = {"image_linf_rel": float(err.max()), "image_p99_rel": float(np.percentile(err, 99)),
                                  "spectra_linf_rel": float(serr.max()),
                                  "spectra_p99_rel": float(np.percentile(serr, 99))}
+        # the library's default gates (critical-curve band and inner-disk gate), and the
+        # critical-curve band alone (faster, with the network's worst case at the inner edge)
         line["surrogate"] = surrogate_leg(eng, abi, np, torch, dev, stream)
+        line["surrogate_band_only"] = surrogate_leg(eng, abi, np, torch, dev, stream, inner_gate=-1.0)
         line["surrogate_training"] = train_leg(eng, abi, np, torch, dev)
         line["beams"] = beam_leg(eng, abi)
         line["graph_replay"] = graph_leg(eng, abi, torch, dev)

@@ -361,12 +361,23 @@ int sirius_cuda_surrogate_infer(sirius_cuda_handle handle, const float* d_featur
  * chosen by a hash seeded with audit_seed), and
  * every ray of a frame that is not charge- and Lambda-free Kerr are integrated
  * instead (the configured integrator, compacted into one launch) and overwrite
- * their pixels. gate (optional): per pixel 0 = MLP, 1 = gated, 2 = audit. */
+ * their pixels. gate (optional): per pixel 0 = MLP, 1 = gated, 2 = audit.
+ * The inner-disk gate: the MLP first runs on a coarse grid (every
+ * coarse_stride-th pixel in each direction, the cell centres); every pixel whose
+ * coarse cell or a neighbouring one predicts a disk hit at r_1 < inner_gate *
+ * r_in is integrated too. There the flux rises steeply from zero at the inner
+ * edge, so a small error of the network's r_1 is a large error of the pixel.
+ * audit_budget > 0: when the audit finds max |I_mlp - I| / max I above it, the
+ * frame is rendered once more with the critical-curve band and inner_gate 1.5
+ * times wider (sirius_surrogate_stats.rerendered). */
 typedef struct {
     double gate_band;          /* half width of the gate around the critical curve, M (0.3) */
     double audit_fraction;     /* fraction of ungated rays also integrated (0.01) */
     uint32_t audit_seed;
-    int32_t reserved[5];
+    float inner_gate;          /* r_1 bound of the inner-disk gate in units of r_in: 0 = 2.5, < 0 = off */
+    int32_t coarse_stride;     /* pixels per coarse cell side of the inner-disk gate: 0 = 8 */
+    float audit_budget;        /* 0: the audit only reports */
+    int32_t reserved[2];
 } sirius_surrogate_config;
 
 typedef struct {
@@ -377,6 +388,8 @@ typedef struct {
      * and max |I_mlp - I| / max I */
     int32_t audit_count;
     float audit_rel_l1, audit_rel_max;
+    int32_t rerendered;        /* 1: the audit exceeded audit_budget and the frame was rendered again */
+    int32_t coarse_rays;       /* MLP rows of the inner-disk gate's coarse pass */
 } sirius_surrogate_stats;
 
 /* features (n x 5 floats, device) and gate (n bytes, device, may be NULL) of the frames' pixels */

@@ -121,17 +121,21 @@ class LaunchStats(C.Structure):
 
 class SurrogateConfig(C.Structure):
     _fields_ = [("gate_band", C.c_double), ("audit_fraction", C.c_double), ("audit_seed", C.c_uint32),
-                ("reserved", C.c_int32 * 5)]
+                ("inner_gate", C.c_float), ("coarse_stride", C.c_int32), ("audit_budget", C.c_float),
+                ("reserved", C.c_int32 * 2)]
 
 
 class SurrogateStats(C.Structure):
     _fields_ = [("rays", C.c_int64), ("integrated", C.c_int64), ("ms_features", C.c_float), ("ms_mlp", C.c_float),
                 ("ms_shade", C.c_float), ("ms_trace", C.c_float), ("ms_total", C.c_float),
-                ("audit_count", C.c_int32), ("audit_rel_l1", C.c_float), ("audit_rel_max", C.c_float)]
+                ("audit_count", C.c_int32), ("audit_rel_l1", C.c_float), ("audit_rel_max", C.c_float),
+                ("rerendered", C.c_int32), ("coarse_rays", C.c_int32)]
 
 
-def surrogate_config(gate_band=0.3, audit_fraction=0.01, audit_seed=0):
-    return SurrogateConfig(gate_band, audit_fraction, audit_seed)
+def surrogate_config(gate_band=0.3, audit_fraction=0.01, audit_seed=0, inner_gate=0.0, coarse_stride=0,
+                     audit_budget=0.0):
+    """sirius_surrogate_config (inner_gate 0: 2.5 r_in, < 0: off; coarse_stride 0: 8; audit_budget 0: report only)."""
+    return SurrogateConfig(gate_band, audit_fraction, audit_seed, inner_gate, coarse_stride, audit_budget)
 
 
 class BeamResult(C.Structure):

@@ -37,7 +37,7 @@ static_assert(sizeof(sirius_frame) == 176, "sirius_frame layout");
 static_assert(sizeof(sirius_ray_result) == 256, "sirius_ray_result layout");
 static_assert(sizeof(sirius_camera_ray) == 64, "sirius_camera_ray layout");
 static_assert(sizeof(sirius_surrogate_config) == 40, "sirius_surrogate_config layout");
-static_assert(sizeof(sirius_surrogate_stats) == 48, "sirius_surrogate_stats layout");
+static_assert(sizeof(sirius_surrogate_stats) == 56, "sirius_surrogate_stats layout");
 static_assert(sizeof(sirius_train_config) == 64, "sirius_train_config layout");
 static_assert(sizeof(sirius_beam_result) == 32, "sirius_beam_result layout");
 
@@ -90,6 +90,8 @@ TraceFn pick_kernel(bool mixed, int minb, int fam, bool symp, bool uni = false) 
 // of gated (near-critical) and audit rays, which overwrite their pixels.
 // ---------------------------------------------------------------------------
 constexpr int kCurveN = 256;      // critical-curve points per frame, ordered by angle about its centre
+constexpr double kInnerGateDefault = 2.5;  // inner-disk gate: r_1 < 2.5 r_in
+constexpr int kCoarseStrideDefault = 8;    // inner-disk gate: 8 x 8 pixels per coarse cell
 constexpr float kSurRScale = 15.f;   // MLP output 1: r_1 = 15 (1 + o_1)
 constexpr float kSurHigher = 1e-3f;  // MLP output 3: higher-order intensity / 1e-3
 
@@ -98,7 +100,31 @@ struct SurFrameDev {
     float ac;                     // centre (alpha_c, 0) of the critical curve
     int kerr;                     // 1: Kerr frame (no charge, no Lambda) the MLP covers; 0: integrate every ray
     float ca[kCurveN], cb[kCurveN];
+    // inner-disk gate: the frame's coarse cells (cw x ch, row-major from coarse_offset)
+    long long coarse_offset;
+    int cw, ch;
+    float r1_max;                 // inner_gate * r_in (0: off)
 };
+
+// The inner-disk gate's coarse pass: the features of each coarse cell's centre
+// pixel (stride s), cells of all frames concatenated.
+__global__ void sur_coarse_gather_kernel(const FrameDev* frames, const SurFrameDev* sf, int n_frames, int stride,
+                                         long long n_coarse, const float* feat, float* cfeat) {
+    const long long c = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+    if (c >= n_coarse) return;
+    int f = 0;
+    while (f + 1 < n_frames && sf[f + 1].coarse_offset <= c) ++f;
+    const SurFrameDev& S = sf[f];
+    const FrameDev& F = frames[f];
+    const long long cc = c - S.coarse_offset;
+    const int cx = int(cc % S.cw), cy = int(cc / S.cw);
+    const long long rows = F.n_rays / F.width;
+    const int x = min(cx * stride + stride / 2, F.width - 1);
+    const long long y = min((long long)cy * stride + stride / 2, rows - 1);
+    const long long idx = F.ray_offset + y * F.width + x;
+#pragma unroll
+    for (int k = 0; k < 5; ++k) cfeat[c * 5 + k] = feat[idx * 5 + k];
+}
 
 __device__ __forceinline__ unsigned audit_hash(unsigned long long idx, unsigned seed) {
     unsigned long long z = idx * 0x9E3779B97F4A7C15ull + seed;
@@ -173,7 +199,7 @@ __global__ void sur_features_kernel(const FrameDev* frames, const SurFrameDev* s
 // audit ray, each class in pixel order)
 __global__ void sur_gate_kernel(const FrameDev* frames, const SurFrameDev* sf, int n_frames, long long total,
                                 float band, unsigned audit_threshold, unsigned seed, const float* feat,
-                                unsigned char* gate, unsigned* block_counts) {
+                                int stride, const float* cout, unsigned char* gate, unsigned* block_counts) {
     const long long idx = (long long)blockIdx.x * blockDim.x + threadIdx.x;
     unsigned char g = 0;
     if (idx < total) {
@@ -192,6 +218,20 @@ __global__ void sur_gate_kernel(const FrameDev* frames, const SurFrameDev* sf, i
                 d2 = fminf(d2, seg_dist2(alpha, beta, S.ca[a], S.cb[a], S.ca[b], S.cb[b]));
             }
             if (d2 < band * band) g = 1;
+            // inner-disk gate: the coarse cell of the pixel or a neighbouring one
+            // predicts a disk hit inside r1_max
+            if (!g && S.r1_max > 0.f) {
+                const FrameDev& F = frames[f];
+                const long long pix = idx - F.ray_offset;
+                const int cx = int(pix % F.width) / stride, cy = int(pix / F.width / stride);
+                for (int dy = -1; dy <= 1 && !g; ++dy)
+                    for (int dx2 = -1; dx2 <= 1; ++dx2) {
+                        const int ux = cx + dx2, uy = cy + dy;
+                        if (ux < 0 || uy < 0 || ux >= S.cw || uy >= S.ch) continue;
+                        const float* o = cout + (S.coarse_offset + (long long)uy * S.cw + ux) * 4;
+                        if (o[0] > 0.f && kSurRScale * (1.f + o[1]) < S.r1_max) { g = 1; break; }
+                    }
+            }
         }
         // audit rays come in runs of 32 consecutive pixels, so that they integrate as coherent warps
         if (!g && audit_hash((unsigned long long)idx >> 5, seed) < audit_threshold) g = 2;
@@ -477,6 +517,11 @@ struct Handle {
     size_t mlp_out_cap = 0;
     unsigned* d_list = nullptr;
     size_t list_cap = 0;
+    float* d_coarse_feat = nullptr;  // the inner-disk gate's coarse features and MLP outputs
+    size_t coarse_feat_cap = 0;
+    float* d_coarse_out = nullptr;
+    size_t coarse_out_cap = 0;
+    long long last_coarse = 0;
     unsigned char* d_gate = nullptr;
     size_t gate_cap = 0;
     unsigned* d_block_counts = nullptr;  // per-block gated and audit counts, then offsets; [2 n_blocks] = list length
@@ -1285,6 +1330,7 @@ int sirius_cuda_destroy(sirius_cuda_handle h) {
     cudaFree(H->d_rays); cudaFree(H->d_queue); cudaFree(H->d_status);
     cudaFree(H->d_surrogate); cudaFree(H->d_sur_err);
     cudaFree(H->d_sur_frames); cudaFree(H->d_feat); cudaFree(H->d_mlp_out); cudaFree(H->d_list); cudaFree(H->d_gate);
+    cudaFree(H->d_coarse_feat); cudaFree(H->d_coarse_out);
     cudaFree(H->d_block_counts);
     cudaFree(H->d_pass_image); cudaFree(H->d_pass_spectra); cudaFree(H->d_pass_frames); cudaFree(H->d_prep);
     if (H->h_sur_frames) cudaFreeHost(H->h_sur_frames);
@@ -2027,13 +2073,38 @@ static int surrogate_gate_launch(Handle* H, const sirius_frame* frames, int n_fr
         d_gate = H->d_gate;
     }
     if (!H->h_list_len) CK(cudaMallocHost((void**)&H->h_list_len, 2 * sizeof(unsigned)));
-    CK(cudaMemcpyAsync(H->d_sur_frames, full, n_frames * sizeof(SurFrameDev), cudaMemcpyHostToDevice, st));
     const double band = sc ? sc->gate_band : 0.3;
     const double audit = sc ? std::clamp(sc->audit_fraction, 0.0, 1.0) : 0.01;
     const unsigned thr = unsigned(std::min(audit * 4294967296.0, 4294967295.0));
     const unsigned seed = sc ? sc->audit_seed : 0u;
+    // the inner-disk gate's coarse MLP pass (after the descriptors above reach the device)
+    const double inner = sc ? (sc->inner_gate == 0.f ? kInnerGateDefault : double(sc->inner_gate)) : kInnerGateDefault;
+    const int stride = (sc && sc->coarse_stride > 0) ? sc->coarse_stride : kCoarseStrideDefault;
+    long long n_coarse = 0;
+    if (inner > 0.0) {
+        for (int i = 0; i < n_frames; ++i) {
+            const FrameDev F = make_frame(frames[i], H->cfg);
+            const long long rows = F.n_rays / F.width;
+            full[i].coarse_offset = n_coarse;
+            full[i].cw = (F.width + stride - 1) / stride;
+            full[i].ch = int((rows + stride - 1) / stride);
+            full[i].r1_max = full[i].kerr ? float(inner * F.disk_in) : 0.f;
+            n_coarse += (long long)full[i].cw * full[i].ch;
+        }
+    }
+    CK(cudaMemcpyAsync(H->d_sur_frames, full, n_frames * sizeof(SurFrameDev), cudaMemcpyHostToDevice, st));
+    if (n_coarse > 0) {
+        if ((rc = ensure(H, H->d_coarse_feat, H->coarse_feat_cap, size_t(n_coarse) * 5)) != SIRIUS_OK) return rc;
+        if ((rc = ensure(H, H->d_coarse_out, H->coarse_out_cap, size_t(n_coarse) * 4)) != SIRIUS_OK) return rc;
+        sur_coarse_gather_kernel<<<int((n_coarse + 255) / 256), 256, 0, st>>>(H->d_frames, H->d_sur_frames, n_frames,
+                                                                            stride, n_coarse, H->d_feat,
+                                                                            H->d_coarse_feat);
+        CK(cudaGetLastError());
+        if ((rc = surrogate_launch(H, H->d_coarse_feat, n_coarse, H->d_coarse_out, st)) != SIRIUS_OK) return rc;
+    }
+    H->last_coarse = n_coarse;
     sur_gate_kernel<<<n_blocks, block, 0, st>>>(H->d_frames, H->d_sur_frames, n_frames, total, float(band), thr, seed,
-                                                H->d_feat, d_gate, H->d_block_counts);
+                                                H->d_feat, stride, H->d_coarse_out, d_gate, H->d_block_counts);
     CK(cudaGetLastError());
     sur_scan_kernel<<<1, 1024, 0, st>>>(H->d_block_counts, 2 * n_blocks);
     CK(cudaGetLastError());
@@ -2045,9 +2116,9 @@ static int surrogate_gate_launch(Handle* H, const sirius_frame* frames, int n_fr
     return SIRIUS_OK;
 }
 
-static int render_surrogate(Handle* H, const sirius_frame* frames, int n_frames, const sirius_surrogate_config* sc,
-                            float* d_image, float* d_image_mlp, unsigned char* d_gate, cudaStream_t st,
-                            sirius_surrogate_stats* stats) {
+static int render_surrogate_pass(Handle* H, const sirius_frame* frames, int n_frames,
+                                 const sirius_surrogate_config* sc, float* d_image, float* d_image_mlp,
+                                 unsigned char* d_gate, cudaStream_t st, sirius_surrogate_stats* stats) {
     if (!H->d_surrogate) return fail(H, SIRIUS_ERR_NOT_CONFIGURED, "no surrogate weights loaded");
     for (auto& e : H->sev)
         if (!e) CK(cudaEventCreate(&e));
@@ -2063,7 +2134,9 @@ static int render_surrogate(Handle* H, const sirius_frame* frames, int n_frames,
         if ((rc = ensure(H, H->d_gate, H->gate_cap, size_t(total))) != SIRIUS_OK) return rc;
         d_gate = H->d_gate;
     }
-    // 1. features, gate and the compacted list of rays to integrate
+    // 1. features, the inner-disk gate's coarse MLP pass, the gate and the
+    // compacted list of rays to integrate
+    CK(cudaMemsetAsync(H->d_sur_err, 0, sizeof(int), st));
     CK(cudaEventRecord(H->sev[0], st));
     if ((rc = surrogate_features_launch(H, frames, n_frames, total, st)) != SIRIUS_OK) return rc;
     if ((rc = surrogate_gate_launch(H, frames, n_frames, total, sc, d_gate, st)) != SIRIUS_OK) return rc;
@@ -2084,7 +2157,6 @@ static int render_surrogate(Handle* H, const sirius_frame* frames, int n_frames,
     if ((rc = ensure(H, H->d_flux, H->flux_cap, size_t(n_frames) * kFluxTable)) != SIRIUS_OK) return rc;
     flux_table_kernel<<<n_frames, kFluxN, 0, st>>>(H->d_frames, H->d_flux);
     CK(cudaGetLastError());
-    CK(cudaMemsetAsync(H->d_sur_err, 0, sizeof(int), st));
     CK(cudaEventRecord(H->sev[1], st));
     CK(cudaStreamWaitEvent(s_trace, H->sev[1], 0));
     CK(cudaStreamWaitEvent(s_mlp, H->sev[1], 0));
@@ -2132,7 +2204,33 @@ static int render_surrogate(Handle* H, const sirius_frame* frames, int n_frames,
         stats->audit_count = int32_t(aud[4]);
         stats->audit_rel_l1 = aud[1] > 0.f ? aud[0] / aud[1] : 0.f;
         stats->audit_rel_max = aud[3] > 0.f ? aud[2] / aud[3] : 0.f;
+        stats->coarse_rays = int32_t(std::min<long long>(H->last_coarse, 0x7fffffff));
     }
+    return SIRIUS_OK;
+}
+
+// The render and the audit's judgement of it: above the caller's budget, one
+// more render with the critical-curve band and the inner-disk gate widened.
+static int render_surrogate(Handle* H, const sirius_frame* frames, int n_frames, const sirius_surrogate_config* sc,
+                            float* d_image, float* d_image_mlp, unsigned char* d_gate, cudaStream_t st,
+                            sirius_surrogate_stats* stats) {
+    sirius_surrogate_stats first{};
+    int rc = render_surrogate_pass(H, frames, n_frames, sc, d_image, d_image_mlp, d_gate, st, &first);
+    if (rc != SIRIUS_OK) return rc;
+    if (sc && sc->audit_budget > 0.f && first.audit_rel_max > sc->audit_budget) {
+        sirius_surrogate_config wide = *sc;
+        wide.gate_band = 1.5 * sc->gate_band;
+        const float inner = sc->inner_gate == 0.f ? float(kInnerGateDefault) : sc->inner_gate;
+        wide.inner_gate = inner > 0.f ? 1.5f * inner : inner;
+        sirius_surrogate_stats second{};
+        rc = render_surrogate_pass(H, frames, n_frames, &wide, d_image, d_image_mlp, d_gate, st, &second);
+        if (rc != SIRIUS_OK) return rc;
+        second.rerendered = 1;
+        second.ms_total += first.ms_total;
+        if (stats) *stats = second;
+        return SIRIUS_OK;
+    }
+    if (stats) *stats = first;
     return SIRIUS_OK;
 }
 

@@ -47,7 +47,7 @@ def test_struct_layouts_match_c(oracle):
     assert C.sizeof(abi.RayResult) == 256
     assert C.sizeof(abi.CameraRay) == 64
     assert C.sizeof(abi.SurrogateConfig) == 40
-    assert C.sizeof(abi.SurrogateStats) == 48
+    assert C.sizeof(abi.SurrogateStats) == 56
     assert C.sizeof(abi.TrainConfig) == 64
     dt = abi.result_dtype()
     for name, _ in abi.RayResult._fields_:

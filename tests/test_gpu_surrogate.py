@@ -88,7 +88,10 @@ def render_config(prec):
 def test_surrogate_render_against_the_integrator(engine):
     """Surrogate-gated frame vs the same frame fully integrated: the gated and
     audit pixels are the integrator's own values (bit for bit); the rest come
-    from the MLP within the surrogate's error budget."""
+    from the MLP within the surrogate's error budget, which holds for the worst
+    pixel too: L-infinity <= 1e-2 and p99 <= 1e-3 of the frame peak (the
+    inner-disk gate takes the pixels where the flux rises steeply from the
+    inner edge, which the network's radius cannot resolve)."""
     engine.surrogate_load(np.load(WEIGHTS))
     fr = kerr_frame(512)
     engine.configure(render_config(abi.PRECISION_MIXED))
@@ -99,10 +102,15 @@ def test_surrogate_render_against_the_integrator(engine):
     np.testing.assert_array_equal(img[taken], full[taken])
     np.testing.assert_array_equal(img[~taken], mimg[~taken])
     assert 0.004 < np.mean(gate == 2) < 0.02      # 1 % audit, in runs of 32 pixels
-    assert 0.001 < np.mean(gate == 1) < 0.05      # the +-0.3 M band around the critical curve
+    # the +-0.3 M band around the critical curve and the inner-disk gate
+    assert 0.001 < np.mean(gate == 1) < 0.08, np.mean(gate == 1)
+    assert st.coarse_rays == 64 * 64  # 8 x 8 pixel cells
     err = np.abs(img.astype(np.float64) - full) / full.max()
-    assert err.mean() < 1e-3, err.mean()
-    assert np.percentile(err, 99) < 1e-2, np.percentile(err, 99)
+    print("surrogate 512^2: L-inf %.3e p99 %.3e mean %.3e gated %.4f" % (err.max(), np.percentile(err, 99), err.mean(),
+                                                                           np.mean(gate == 1)))
+    assert err.mean() < 1e-4, err.mean()
+    assert np.percentile(err, 99) < 1e-3, np.percentile(err, 99)
+    assert err.max() < 1e-2, err.max()
     # the audit's judgement in the statistics: the MLP against the integrator on the audit pixels
     a = gate == 2
     d = np.abs(mimg[a].astype(np.float64) - img[a])
@@ -136,9 +144,11 @@ def test_trained_network_gains_over_the_untrained_one(engine):
     scale = full.max()
     errs, fractions, audits = {}, {}, {}
     rng = np.random.default_rng(11)
+    # the critical-curve gate alone (the inner-disk gate reads the network's own outputs)
+    cfg = abi.surrogate_config(inner_gate=-1.0)
     for name, params in (("trained", np.load(WEIGHTS)), ("untrained", init_params(rng))):
         engine.surrogate_load(params)
-        img, _, gate, st = engine.render_surrogate([fr])
+        img, _, gate, st = engine.render_surrogate([fr], config=cfg)
         errs[name] = np.abs(img.astype(np.float64) - full) / scale
         fractions[name] = st.integrated / st.rays
         audits[name] = st.audit_rel_l1
@@ -148,3 +158,21 @@ def test_trained_network_gains_over_the_untrained_one(engine):
     assert errs["trained"].mean() < 1e-3 and np.percentile(errs["trained"], 99) < 1e-2
     assert errs["untrained"].mean() > 10 * errs["trained"].mean()
     assert np.percentile(errs["untrained"], 99) > 5 * np.percentile(errs["trained"], 99)
+
+
+def test_audit_over_budget_renders_again_with_wider_gates(engine):
+    """The audit acts: with a budget below the audit's measured error, the frame
+    is rendered once more with the critical-curve band and the inner-disk gate
+    1.5 times wider; more pixels are integrated, and those are the integrator's."""
+    engine.surrogate_load(np.load(WEIGHTS))
+    fr = kerr_frame(256)
+    engine.configure(render_config(abi.PRECISION_MIXED))
+    _, full, _ = engine.trace_frames([fr], results=False)
+    img0, _, gate0, st0 = engine.render_surrogate([fr])
+    assert st0.rerendered == 0
+    img1, _, gate1, st1 = engine.render_surrogate([fr], config=abi.surrogate_config(audit_budget=1e-9))
+    assert st1.rerendered == 1
+    assert st1.integrated > st0.integrated
+    assert np.all(gate1[gate0 == 1] == 1)
+    taken = gate1 != 0
+    np.testing.assert_array_equal(img1[taken], full[taken])

@@ -109,7 +109,7 @@ def test_gate_matches_the_analytic_critical_curve(engine, oracle, a, theta, fov)
                              precision=abi.PRECISION_MIXED, enable_disk=1, enable_volumetric=0,
                              critical_band=0.0)
     engine.configure(cfg)
-    _, _, gate, st = engine.render_surrogate([fr], config=abi.surrogate_config(gate_band=BAND, audit_fraction=0.0))
+    _, _, gate, st = engine.render_surrogate([fr], config=abi.surrogate_config(gate_band=BAND, audit_fraction=0.0, inner_gate=-1.0))
     al, be, theta_o = celestial(oracle, fr, cfg)
     curve = critical_curve(a, 1.0, theta_o)
     dist, _ = cKDTree(curve).query(np.stack([al, be], axis=1))
