@@ -528,9 +528,10 @@ int sirius_cuda_dp45_step(sirius_cuda_handle handle, const sirius_metric* metric
 /* ---- statistics of the last trace call ---------------------------------------- */
 int sirius_cuda_last_stats(sirius_cuda_handle handle, sirius_launch_stats* out_stats);
 
-/* ---- autotuner: times the one-thread-per-ray launch and the persistent launch
- * (blocks/SM x refill threshold) on the given frames and stores the best
- * setting in the handle's configuration.
+/* ---- autotuner: times the one-thread-per-ray launch (register caps; one ray or
+ * two packed rays per thread) and the persistent launch (blocks/SM x refill
+ * threshold) on the given frames and stores the best setting in the handle's
+ * configuration.
  * The chosen values are written to *out_config (may be NULL). ---------------- */
 int sirius_cuda_autotune(sirius_cuda_handle handle, const sirius_frame* frames, int32_t n_frames,
                          sirius_trace_config* out_config);

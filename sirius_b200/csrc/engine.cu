@@ -1686,17 +1686,23 @@ int sirius_cuda_autotune(sirius_cuda_handle h, const sirius_frame* frames, int32
     if (rc != SIRIUS_OK) return rc;
     if ((rc = ensure(H, H->d_image, H->image_cap, size_t(total))) != SIRIUS_OK) return rc;
     const sirius_trace_config base = H->cfg;
-    // (blocks/SM, threshold, register cap): blocks/SM 0 is the one-thread-per-ray
-    // launch at a register cap (0: 255)
-    const int candidates[][3] = {{0, 1, 0}, {0, 1, 255}, {0, 1, 168}, {0, 1, 128}, {1, 1, 0}, {2, 1, 0},
-                                 {3, 1, 0}, {4, 1, 0},   {2, 4, 0},   {2, 8, 0},   {3, 4, 0}};
+    // (blocks/SM, threshold, register cap, rays per thread): blocks/SM 0 is the
+    // one-thread-per-ray launch at a register cap (0: the default), with one ray
+    // or two packed rays per thread (mixed DP45 over Kerr-Schild frames)
+    const int candidates[][4] = {{0, 1, 0, 1},   {0, 1, 255, 1}, {0, 1, 168, 1}, {0, 1, 128, 1}, {0, 1, 255, 2},
+                                 {0, 1, 168, 2}, {1, 1, 0, 1},   {2, 1, 0, 1},   {3, 1, 0, 1},   {4, 1, 0, 1},
+                                 {2, 4, 0, 1},   {2, 8, 0, 1},   {3, 4, 0, 1}};
+    const bool pairs = base.precision == SIRIUS_PRECISION_MIXED && base.integrator == SIRIUS_INTEGRATOR_DP45 &&
+                       H->family_mask == (1 << SIRIUS_METRIC_KERR_SCHILD);
     double best = 1e300;
     sirius_trace_config best_cfg = base;
     for (const auto& cand : candidates) {
+        if (cand[3] == 2 && !pairs) continue;
         H->cfg = base;
         H->cfg.blocks_per_sm = cand[0];
         H->cfg.refill_threshold = cand[1];
         H->cfg.max_registers = cand[2];
+        H->cfg.rays_per_thread = cand[3];
         CK(cudaEventRecord(H->ev[0], H->stream));
         rc = launch_trace(H, n_frames, total, nullptr, H->d_image, nullptr, nullptr, H->stream, true);
         if (rc != SIRIUS_OK) { H->cfg = base; return rc; }

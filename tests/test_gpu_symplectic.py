@@ -7,6 +7,7 @@ import os
 import numpy as np
 import pytest
 
+from oracle import compare
 from sirius_b200 import abi
 
 pytestmark = pytest.mark.gpu
@@ -36,23 +37,27 @@ def test_equirectangular_camera_rays(engine, oracle):
     np.testing.assert_allclose(res["Lz0"], ref["Lz0"], rtol=1e-5, atol=1e-6)
 
 
-@pytest.mark.parametrize("prec,tol", [(abi.PRECISION_FP64, 1e-6), (abi.PRECISION_MIXED, 2e-3)])
-def test_symplectic_frame_matches_oracle(engine, oracle, prec, tol):
-    fr = stress_frame()
+# (precision, image L-infinity bar over the rays whose histories agree, spectra bar)
+@pytest.mark.parametrize("prec,img_max,spec_max", [(abi.PRECISION_FP64, 1e-5, 1e-4),
+                                                   (abi.PRECISION_MIXED, 1e-3, 1e-2)])
+def test_symplectic_frame_matches_oracle(engine, oracle, prec, img_max, spec_max):
+    """A 64 x 32 crop of the sky map: per-output errors against the FP64 oracle
+    (the same Yoshida-4 scheme in FP64), maxima over the rays whose histories
+    agree. Fixed d-lambda = 0.01 over ~6,000 steps per ray: the FP32 right-hand
+    side's rounding accumulates along the orbit, which sets the mixed bars."""
+    fr = stress_frame(64, 32)
     engine.configure(stress_config(prec))
     res, img, spc = engine.trace_frames([fr], spectra=True)
     ref, bins = oracle.trace_frame(fr, stress_config(abi.PRECISION_FP64), threads=THREADS)
-    agree = res["outcome"] == ref["outcome"]
-    assert agree.mean() >= 0.98
-    scale = max(float(ref["intensity"].max()), 1e-30)
-    err = np.abs(img.astype(np.float64) - ref["intensity"]) / scale
-    assert np.percentile(err, 99) <= tol, np.percentile(err, 99)
-    sscale = bins.max(axis=0, keepdims=True) + 1e-30
-    serr = np.abs(spc[agree] - bins[agree]) / sscale
-    # the device accumulates the transfer in FP32 in both precision modes
-    assert np.percentile(serr, 99) <= max(10 * tol, 1e-4), np.percentile(serr, 99)
-    np.testing.assert_allclose(res["E"], res["E0"], rtol=1e-6)
-    assert np.median(res["null_final"]) < 1e-6
+    rep = compare.report(res, img, ref, spc, bins, escape_radius=60.0)
+    print("symplectic", prec)
+    print(compare.summary(rep))
+    assert rep["outcome_agreement"] >= 0.98
+    assert rep["image"]["max"] <= img_max, rep["image"]
+    assert rep["spectra"]["max"] <= spec_max, rep["spectra"]
+    assert rep["E"]["drift"]["max"] <= 1e-12
+    # re-projection every 8 steps: the returned state is at most 7 steps past one
+    assert rep["null_final"]["max"] <= 1e-5, rep["null_final"]
 
 
 def test_symplectic_rejects_bad_order(engine):
