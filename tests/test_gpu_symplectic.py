@@ -38,13 +38,16 @@ def test_equirectangular_camera_rays(engine, oracle):
 
 
 # (precision, image L-infinity bar over the rays whose histories agree, spectra bar)
-@pytest.mark.parametrize("prec,img_max,spec_max", [(abi.PRECISION_FP64, 1e-5, 1e-4),
-                                                   (abi.PRECISION_MIXED, 1e-3, 1e-2)])
+@pytest.mark.parametrize("prec,img_max,spec_max", [(abi.PRECISION_FP64, 1e-7, 5e-4),
+                                                   (abi.PRECISION_MIXED, 1e-5, 5e-4)])
 def test_symplectic_frame_matches_oracle(engine, oracle, prec, img_max, spec_max):
     """A 64 x 32 crop of the sky map: per-output errors against the FP64 oracle
     (the same Yoshida-4 scheme in FP64), maxima over the rays whose histories
-    agree. Fixed d-lambda = 0.01 over ~6,000 steps per ray: the FP32 right-hand
-    side's rounding accumulates along the orbit, which sets the mixed bars."""
+    agree. The spectra accumulate in FP32 on the device in both precision modes.
+    The null constraint and L_z drift are the scheme's own (the reference's
+    leapfrog drifts with dH/dp at the old position, PHSI001A.h:430-455, and the
+    re-projection runs every 8 steps): the device's returned states carry the
+    oracle's values of both."""
     fr = stress_frame(64, 32)
     engine.configure(stress_config(prec))
     res, img, spc = engine.trace_frames([fr], spectra=True)
@@ -56,8 +59,11 @@ def test_symplectic_frame_matches_oracle(engine, oracle, prec, img_max, spec_max
     assert rep["image"]["max"] <= img_max, rep["image"]
     assert rep["spectra"]["max"] <= spec_max, rep["spectra"]
     assert rep["E"]["drift"]["max"] <= 1e-12
-    # re-projection every 8 steps: the returned state is at most 7 steps past one
-    assert rep["null_final"]["max"] <= 1e-5, rep["null_final"]
+    assert rep["Lz"]["vs_oracle"]["max"] <= 1e-5 and rep["Carter"]["vs_oracle"]["max"] <= 1e-5
+    # re-projection every 8 steps: the returned state is at most 7 steps past one,
+    # and its null value is the oracle's
+    oracle_null = float(np.abs(ref["null_final"]).max())
+    assert rep["null_final"]["max"] <= 1.01 * oracle_null + 1e-12, (rep["null_final"], oracle_null)
 
 
 def test_symplectic_rejects_bad_order(engine):
