@@ -37,8 +37,8 @@ N_BINS = 16
 MEASURED_PEAKS = os.path.join(ROOT, "MEASURED_PEAKS.json")
 # DRAM bytes (read + write) per ray of the trace kernel, from one ncu capture of
 # the 512^2 case of this workload (profiles/trace_kernel_mixed_kerr512_full.md):
-# (4.35 + 5.63) MB / 262,144 rays; traffic grows with the ray count.
-TRAFFIC_BYTES_PER_RAY = 38.1
+# (4.04 + 1.85) MB / 262,144 rays; traffic grows with the ray count.
+TRAFFIC_BYTES_PER_RAY = 22.5
 
 
 def inclination_deg(seed=SEED):
@@ -316,13 +316,19 @@ def batch_frames(abi, seed=3, n=96):
     return frames
 
 
-def batch_leg(eng, abi):
+def batch_leg(eng, abi, rank=0, world=1, dist=None, dev=None):
     """All 96 frames in one launch (persistent queue, generic kernel) and as
-    per-family launches (one thread per ray), mixed precision, thin disk."""
-    frames = batch_frames(abi)
-    total = sum(f.camera.width * f.camera.height for f in frames)
+    per-family launches (one thread per ray), mixed precision, thin disk. Under
+    torchrun each rank takes whole frames round robin (shard.frames_for_rank) and
+    the device time is the maximum over ranks; every rank runs both variants."""
+    from sirius_b200.shard import frames_for_rank, max_over_ranks
+    all_frames = batch_frames(abi)
+    frames = frames_for_rank(all_frames, rank, world)
+    total = sum(f.camera.width * f.camera.height for f in all_frames)
+    mine = sum(f.camera.width * f.camera.height for f in frames)
     out = {"workload": "96 seeded frames: Kerr-Newman / Kerr-de Sitter / Morris-Thorne / Alcubierre, "
-                       "sides U{128..1024}", "rays": total}
+                       "sides U{128..1024}", "rays": total,
+           "split": f"whole frames round robin over {world} rank(s)" if world > 1 else "one GPU"}
     for name, bps in (("persistent_one_launch", -1), ("per_family_launches", 0)):
         cfg = workload_config(abi, abi.PRECISION_MIXED)
         cfg.enable_volumetric = 0
@@ -331,8 +337,9 @@ def batch_leg(eng, abi):
         eng.trace_frames(frames, results=False, image=True)
         eng.trace_frames(frames, results=False, image=True)
         st = eng.stats()
-        out[name] = {"kernel_ms": st.kernel_ms, "mrays_per_s": total / (st.kernel_ms * 1e-3) / 1e6,
-                     "kernel_launches": st.kernel_launches, "steps_per_ray": st.accepted_steps / total}
+        ms = max_over_ranks(st.kernel_ms, dist if world > 1 else None, dev)
+        out[name] = {"kernel_ms": ms, "mrays_per_s": total / (ms * 1e-3) / 1e6,
+                     "kernel_launches": st.kernel_launches, "steps_per_ray": st.accepted_steps / max(mine, 1)}
     return out
 
 
@@ -548,6 +555,31 @@ def train_leg(eng, abi, np, torch, dev, rows=1 << 21, batch=32768, steps=64):
             "data": "synthetic rows (seeded), the surrogate's feature ranges"}
 
 
+def profile_target(target, side, Engine, abi, np):
+    """One call of one leg on the workload's camera at side x side, untimed: the
+    program ncu captures for the kernel summaries."""
+    eng = Engine(0)
+    frame = workload_frame(abi, side, side)
+    if target in ("trace-mixed", "trace-fp64"):
+        eng.configure(workload_config(abi, abi.PRECISION_MIXED if target == "trace-mixed" else abi.PRECISION_FP64))
+        eng.trace_frames([frame], results=False)
+        st = eng.stats()
+        # a first call: its time includes the one-time module load, so none is printed
+        print(target, side, f"rays={st.rays}", f"steps_per_ray={st.accepted_steps / st.rays:.1f}")
+    elif target == "beams":
+        eng.configure(abi.default_config(abs_tolerance=1e-8, rel_tolerance=1e-8, min_step=1e-9, max_step=2.0,
+                                         initial_step=0.1, escape_radius=1000.0, horizon_factor=1.01,
+                                         max_steps=20000, precision=abi.PRECISION_FP64, enable_disk=0))
+        b = eng.trace_beams([frame])
+        print(target, side, b.size, float(b["magnification"].mean()))
+    else:
+        eng.surrogate_load(np.load(SURROGATE_WEIGHTS))
+        eng.configure(surrogate_config(abi, abi.PRECISION_MIXED))
+        _, _, _, st = eng.render_surrogate([frame])
+        print(target, side, f"rays={st.rays}", f"integrated={st.integrated}")
+    eng.close()
+
+
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
@@ -565,6 +597,8 @@ def main():
                     help="register cap of the mixed trace kernel (0: the library default, 128)")
     ap.add_argument("--size", type=int, default=WIDTH,
                     help="frame side (default 1024, the workload; smaller sides are profiling cases)")
+    ap.add_argument("--profile-target", default=None, choices=["trace-mixed", "trace-fp64", "beams", "surrogate"],
+                    help="one untimed call of one leg at --size (an ncu target), then exit")
     args = ap.parse_args()
     if args.impl == "reference":
         run_reference(args)
@@ -591,6 +625,9 @@ def main():
         eng = Engine(local)
         print(json.dumps(train_leg(eng, abi, np, torch, dev, steps=args.train_steps)), flush=True)
         eng.close()
+        return
+    if args.profile_target:
+        profile_target(args.profile_target, args.size, Engine, abi, np)
         return
     if args.surrogate_only:
         eng = Engine(local)
@@ -687,7 +724,7 @@ def main():
             "gpu_launches": launches,
             "roofline": {"bound": "fp32_simt", "achieved": achieved, "peak": peak32, "unit": "TFLOP/s",
                          "frac": achieved / peak32, "traffic": TRAFFIC_BYTES_PER_RAY * total,
-                         "traffic_unit": "bytes per launch (ncu, 256^2 capture scaled by rays)",
+                         "traffic_unit": "bytes per launch (ncu, 512^2 capture scaled by rays)",
                          "peak_source": "measured FMA-chain microbenchmark (sirius_cuda_measure_fma_peak)",
                          "fp64_peak": peak64, "flops_per_accepted_step": acc_f, "flops_per_rhs": rhs_f,
                          "kernel": "trace_kernel<mixed>"},
@@ -727,6 +764,9 @@ def main():
         line["heterogeneous_batch"] = batch_leg(eng, abi)
         line["stress_symplectic"] = stress_leg(eng, abi)
         line.update(cpu_baseline_sample(res_mixed, img_mixed, spc_mixed))
+    if world > 1 and not args.no_extras:
+        # the heterogeneous batch split by whole frames (every rank takes part)
+        line["heterogeneous_batch"] = batch_leg(eng, abi, rank, world, dist, dev)
     if rank == 0:
         print(json.dumps(line), flush=True)
     eng.close()

@@ -1,15 +1,15 @@
-"""The reference-side adapter of INTEGRATION.md compiles against the reference's
-own IAccelerator header and links against the library.
+"""The reference-side adapter compiles against the reference's own IAccelerator
+header and links against the library.
 
-The adapter (CUDAAccelerator, the class a maintainer adds beside the reserved
-BackendType::CUDA slot, src/Sirius.Render/Acceleration/Backend/ACIB001A.h:27,148-189)
-is taken verbatim from INTEGRATION.md, built against the real ACIB001A.h of a
-reference checkout and linked against libsirius_b200.so. Without a GPU the
+The adapter (CUDAAccelerator in sirius_b200/host/reference_adapter/RDCA001A.h,
+the class a maintainer adds beside the reserved BackendType::CUDA slot,
+src/Sirius.Render/Acceleration/Backend/ACIB001A.h:27,148-189) is built as it
+stands against the real ACIB001A.h of a reference checkout and linked against
+libsirius_b200.so. Without a GPU the
 program checks that initialise() fails cleanly (no CUDA device) rather than
 crashing. Skipped where no reference checkout is present (the checkout is read at
 build and test time only)."""
 import os
-import re
 import shutil
 import subprocess
 
@@ -48,11 +48,8 @@ def reference_root():
 
 
 def adapter_source():
-    text = open(os.path.join(ROOT, "INTEGRATION.md")).read()
-    blocks = re.findall(r"```cpp\n(.*?)```", text, flags=re.S)
-    src = [b for b in blocks if "class CUDAAccelerator" in b]
-    assert len(src) == 1
-    return src[0]
+    with open(os.path.join(ROOT, "sirius_b200", "host", "reference_adapter", "RDCA001A.h")) as f:
+        return f.read()
 
 
 def test_adapter_compiles_against_the_reference_interface(tmp_path):
