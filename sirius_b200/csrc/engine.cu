@@ -751,9 +751,10 @@ CfgDev make_cfg(const sirius_trace_config& c) {
     d.npair = (d.nbins + 1) / 2;
     for (int b = 0; b < d.nbins; ++b) {
         const double nu = d.nbins == 1 ? c.nu_min : c.nu_min * std::pow(c.nu_max / c.nu_min, double(b) / (d.nbins - 1));
-        const float w = float(std::pow(nu, -c.vol_spectral_index));
-        if (b & 1) d.nu_pow2[b / 2].y = w;
-        else d.nu_pow2[b / 2] = make_float2(w, 0.f);
+        // dtau_b = dtau nu_b^-s, applied as 2^(-dtau_b / ln 2)
+        const float w = float(-std::pow(nu, -c.vol_spectral_index) / std::log(2.0));
+        if (b & 1) d.nu_l2[b / 2].y = w;
+        else d.nu_l2[b / 2] = make_float2(w, 0.f);
     }
     return d;
 }
