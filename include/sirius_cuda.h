@@ -392,7 +392,8 @@ typedef struct {
     int32_t coarse_rays;       /* MLP rows of the inner-disk gate's coarse pass */
 } sirius_surrogate_stats;
 
-/* features (n x 5 floats, device) and gate (n bytes, device, may be NULL) of the frames' pixels */
+/* features (n x 5 floats, device) and gate (n bytes, device, may be NULL) of the frames' pixels; the
+ * gate's inner-disk part needs loaded weights (its coarse MLP pass) and is left out without them */
 int sirius_cuda_surrogate_features(sirius_cuda_handle handle, const sirius_frame* frames, int32_t n_frames,
                                    const sirius_surrogate_config* config, float* d_features, uint8_t* d_gate,
                                    void* stream);

@@ -8,11 +8,13 @@ library's own definition of the network and loss (5 -> 256 -> 256 -> 256 ->
 256 -> 4, SiLU after the hidden layers, parameters in nn.Linear order W1 b1 ...
 W5 b5) in plain numpy float64.
 
-`rounded=True` applies the roundings the device arithmetic applies — BF16
-inputs, weights and hidden activations in the forward pass, BF16 dL/dY and dZ
-as operands of the backward products — with exact sums and an exact SiLU, so
-that the device gradient can be compared with the gradient of the same
-rounded network. `rounded=False` is the plain FP64 network.
+`rounded=True` applies the roundings the device arithmetic applies — each
+input feature as the sum of two BF16 terms (hi = bf16(x), lo = bf16(x - hi),
+the kernels' pack_input_row), BF16 weights and hidden activations in the
+forward pass, BF16 dL/dY and dZ as operands of the backward products — with
+exact sums and an exact SiLU, so that the device gradient can be compared with
+the gradient of the same rounded network. `rounded=False` is the plain FP64
+network.
 """
 import numpy as np
 
@@ -42,6 +44,14 @@ def bf16(x):
     return (r.astype(np.uint32) << 16).view(np.float32).astype(np.float64)
 
 
+def bf16_pair(x):
+    """The two-term BF16 form of FP32 inputs: bf16(x) + bf16(x - bf16(x))."""
+    f = np.asarray(x, dtype=np.float32)
+    hi = bf16(f)
+    lo = bf16((f.astype(np.float64) - hi).astype(np.float32))
+    return hi + lo
+
+
 def sigmoid(x):
     return 0.5 * (1.0 + np.tanh(0.5 * x))
 
@@ -64,7 +74,7 @@ def forward(params, X, rounded=False):
     (activations[0] is the input)."""
     layers = unpack(params)
     rnd = bf16 if rounded else _identity
-    h = rnd(X)
+    h = bf16_pair(X) if rounded else _identity(X)
     zs, hs = [], [h]
     for li, (W, b) in enumerate(layers):
         z = h @ rnd(W).T + b

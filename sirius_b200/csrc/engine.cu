@@ -1243,12 +1243,13 @@ void train_backward(const Handle* H, TrainState* T, int rows, cudaStream_t s) {
         g.e.z = T->z[l - 1]; g.e.ldz = kHid; g.e.h = nxt; g.e.ldh = kHid; g.e.grad = T->grad + kOffB[l - 1];
         gemm_launch<256, kEpiDHidden>(g, s);
     }
-    // dW1 = dZ1^T X0 (the 5 real input columns)
+    // dW1 = dZ1^T X0: the 2 x 5 input columns (high and low BF16 terms of each
+    // feature) folded onto the 5 weights they share
     g.a = Operand{T->dz[1], kHid, 0, kHid};
     g.b = Operand{T->x0, kInPad, 0, kInPad};
     g.M = kHid; g.N = kInPad; g.K = rows; g.k_per_cta = kpc;
     g.e = EpiArgs{};
-    g.e.grad = T->grad + kOffW[0]; g.e.ldg = kIn; g.e.ng = kIn;
+    g.e.grad = T->grad + kOffW[0]; g.e.ldg = kIn; g.e.ng = 2 * kIn; g.e.fold = kIn;
     gemm_launch<16, kEpiDWeight>(g, s);
 }
 
@@ -2088,7 +2089,7 @@ static int surrogate_gate_launch(Handle* H, const sirius_frame* frames, int n_fr
     const double inner = sc ? (sc->inner_gate == 0.f ? kInnerGateDefault : double(sc->inner_gate)) : kInnerGateDefault;
     const int stride = (sc && sc->coarse_stride > 0) ? sc->coarse_stride : kCoarseStrideDefault;
     long long n_coarse = 0;
-    if (inner > 0.0) {
+    if (inner > 0.0 && H->d_surrogate) {  // without weights (features only) there is no inner-disk gate
         for (int i = 0; i < n_frames; ++i) {
             const FrameDev F = make_frame(frames[i], H->cfg);
             const long long rows = F.n_rays / F.width;

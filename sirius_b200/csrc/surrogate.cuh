@@ -11,12 +11,14 @@
 //     + (k % 8) * 2, SBO = (K / 8) * 128.
 //   * The FP32 accumulator and the BF16 activations (the A operand of layers
 //     2-5) live in tensor memory; layer 1 reads its 16-wide padded input from
-//     shared memory. One thread issues tcgen05.mma (M = 128, N = 128 or 16,
+//     shared memory: each feature as two BF16 terms (hi, lo) against W1
+//     repeated in two column groups, so the inputs keep 16 significant bits
+//     (pack_input_row). One thread issues tcgen05.mma (M = 128, N = 128 or 16,
 //     K = 16 per instruction) and commits each N-half to its own mbarrier.
 //   * The 128 KB weight images of layers 2-4 stream from global memory by a
 //     bulk TMA copy (cp.async.bulk, no tensor map, no multicast) into one
 //     buffer, each issued as soon as the previous layer's MMAs have drained it,
-//     so the copy overlaps the epilogue. Layer 1 (K padded 5 -> 16) and layer 5
+//     so the copy overlaps the epilogue. Layer 1 (K 2 x 5 padded to 16) and layer 5
 //     (N padded 4 -> 16) weights and all biases stay resident.
 //   * Epilogue: 8 warps read the accumulator with tcgen05.ld, add the bias,
 //     apply SiLU x (1 + tanh(x / 2)) / 2 (one MUFU op), round to BF16 and write
@@ -148,15 +150,14 @@ __global__ void __launch_bounds__(kThreads, 1)
         const long long row0 = tile * kTileM;
         __syncthreads();  // every thread has read *next_s
         if (tid == 32) *next_s = (long long)atomicAdd(tile_counter, 1ull);
-        {  // input tile: 128 rows x 16 BF16 (features 0..4, zero padding)
+        {  // input tile: 128 rows x 16 BF16 (features 0..4 as two BF16 terms, zero padding)
             const int r = tid >> 1, chunk = tid & 1;
             uint4 w = make_uint4(0, 0, 0, 0);
             const long long gr = row0 + r;
-            if (chunk == 0 && gr < n) {
-                const float* f = feat + gr * kIn;
-                w.x = pack_bf16x2(f[0], f[1]);
-                w.y = pack_bf16x2(f[2], f[3]);
-                w.z = pack_bf16x2(f[4], 0.f);
+            if (gr < n) {
+                uint4 c0, c1;
+                pack_input_row(feat + gr * kIn, c0, c1);
+                w = chunk == 0 ? c0 : c1;
             }
             *reinterpret_cast<uint4*>(Xs + packed_offset(r, chunk * 8, kInPad)) = w;
         }
@@ -314,6 +315,11 @@ inline void pack_weights(const float* p, unsigned char* img) {
     put(kBigBytes, kHid, kHid, kHid, W3);
     put(2 * kBigBytes, kHid, kHid, kHid, W4);
     put(kOffW1, kHid, kInPad, kIn, W1);
+    for (int r = 0; r < kHid; ++r)  // columns kIn..2 kIn - 1 repeat W1 for the inputs' low BF16 terms
+        for (int k = 0; k < kIn; ++k) {
+            const uint16_t h = bf16(W1[r * kIn + k]);
+            __builtin_memcpy(img + kOffW1 + packed_offset(r, kIn + k, kInPad), &h, 2);
+        }
     put(kOffW5, kOut, kHid, kHid, W5);
     float* bias = reinterpret_cast<float*>(img + kOffBias);
     for (int i = 0; i < kHid; ++i) {

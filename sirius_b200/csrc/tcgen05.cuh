@@ -150,6 +150,24 @@ __device__ __forceinline__ uint32_t pack_bf16x2(float lo, float hi) {
     return *reinterpret_cast<const uint32_t*>(&p);
 }
 
+// A network input row as two BF16 terms per feature: columns 0..4 hold
+// hi_i = bf16(f_i), columns 5..9 lo_i = bf16(f_i - hi_i) (f_i - hi_i is exact in
+// FP32), columns 10..15 zero. With the first layer's weights repeated in columns
+// 0..4 and 5..9, the product W1 (hi + lo) carries 16 significant bits of each
+// feature instead of 8 (one BF16 step of alpha / 20 near 0.5 is 0.04 M, more
+// than a pixel of a 2048-wide frame). The two 8-column chunks of the row as uint4.
+__device__ __forceinline__ void pack_input_row(const float* f, uint4& c0, uint4& c1) {
+    float hi[5], lo[5];
+#pragma unroll
+    for (int i = 0; i < 5; ++i) {
+        hi[i] = __bfloat162float(__float2bfloat16_rn(f[i]));
+        lo[i] = f[i] - hi[i];
+    }
+    c0 = make_uint4(pack_bf16x2(hi[0], hi[1]), pack_bf16x2(hi[2], hi[3]), pack_bf16x2(hi[4], lo[0]),
+                    pack_bf16x2(lo[1], lo[2]));
+    c1 = make_uint4(pack_bf16x2(lo[3], lo[4]), 0u, 0u, 0u);
+}
+
 __device__ __forceinline__ void mma_bf16_ts(uint32_t tmem_d, uint32_t tmem_a, uint64_t bdesc, uint32_t idesc,
                                             uint32_t accumulate) {
     asm volatile(

@@ -5,7 +5,7 @@
 //
 //   gather      rows of the device-resident training set, picked by a keyed
 //               Feistel permutation of [0, n) per epoch, into a BF16 input
-//               tile X0 (B x 16, features 0..4, zero padding) and FP32
+//               tile X0 (B x 16, features 0..4 as two BF16 terms, zero padding) and FP32
 //               targets / weights; zeroes the loss sums
 //   forward     Z_l = H_{l-1} W_l^T + b_l, H_l = BF16(SiLU(Z_l)) for l = 1..4
 //               and Y = H_4 W_5^T + b_5 (tcgen05 GEMMs, epilogue fused)
@@ -93,6 +93,7 @@ struct EpiArgs {
     float* grad;            // DHidden: per-column sums; DWeight: grad[m * ldg + n]; DWeightT: grad[n * ldg + m]
     long long ldg;
     int ng;                 // DWeight / DWeightT: columns n < ng are accumulated
+    int fold;               // DWeight with BN 16: > 0 adds column n into column n % fold
 };
 
 struct GemmArgs {
@@ -236,7 +237,9 @@ __device__ __forceinline__ void gemm_epilogue(const GemmArgs& g, uint32_t tmem, 
             if constexpr (E == kEpiOutput) {
                 if (j < g.e.ny) g.e.y[row * g.e.ldy + j] = v[j] + g.e.bias[j];
             } else if constexpr (E == kEpiDWeight) {
-                if (j < g.e.ng && n0 + j < g.N) atomicAdd(g.e.grad + row * g.e.ldg + n0 + j, v[j]);
+                // fold > 0: columns c and c + fold hold the same weight (W1's two input terms)
+                const int c = n0 + j, cf = g.e.fold > 0 ? c % g.e.fold : c;
+                if (j < g.e.ng && c < g.N) atomicAdd(g.e.grad + row * g.e.ldg + cf, v[j]);
             } else if constexpr (E == kEpiDWeightT) {
                 if (j < g.e.ng && n0 + j < g.N) atomicAdd(g.e.grad + (long long)(n0 + j) * g.e.ldg + row, v[j]);
             }
@@ -443,10 +446,8 @@ __global__ void gather_kernel(const float* __restrict__ feat, const float* __res
         const long long epoch = step / steps_per_epoch, pos = step % steps_per_epoch;
         idx = permute_row(pos * batch + b, n_rows, seed * 0x85EBCA6Bu + uint32_t(epoch) * 0xC2B2AE35u + 1u);
     }
-    const float* f = feat + idx * kIn;
     uint4* xr = reinterpret_cast<uint4*>(x0 + (long long)b * kInPad);
-    xr[0] = make_uint4(pack_bf16x2(f[0], f[1]), pack_bf16x2(f[2], f[3]), pack_bf16x2(f[4], 0.f), 0u);
-    xr[1] = make_uint4(0, 0, 0, 0);
+    pack_input_row(feat + idx * kIn, xr[0], xr[1]);  // the inference kernel's two-term inputs
     reinterpret_cast<float4*>(t)[b] = reinterpret_cast<const float4*>(targets)[idx];
     w[b] = weights[idx];
 }
@@ -568,6 +569,7 @@ __global__ void adam_kernel(float* __restrict__ params, float* __restrict__ grad
         grad[i] = 0.f;
         const long long k = bf16_slot(i);
         if (k >= 0) wbf[k] = __float2bfloat16_rn(p);
+        if (i < kHid * kIn) wbf[k + kIn] = __float2bfloat16_rn(p);  // W1 again, for the inputs' low terms
     }
     __threadfence();
     __syncthreads();
@@ -585,6 +587,7 @@ __global__ void weights_to_bf16_kernel(const float* __restrict__ params, __nv_bf
          i += (long long)gridDim.x * blockDim.x) {
         const long long k = bf16_slot(i);
         if (k >= 0) wbf[k] = __float2bfloat16_rn(params[i]);
+        if (i < kHid * kIn) wbf[k + kIn] = __float2bfloat16_rn(params[i]);
     }
 }
 #endif  // __CUDACC__

@@ -1,6 +1,7 @@
 """The surrogate MLP on the tensor cores (tcgen05, BF16 operands, FP32
 accumulation) against a plain PyTorch FP32 reference of the same network with
-the same BF16 roundings of weights and activations.
+the same BF16 roundings of weights and activations (each input feature as two
+BF16 terms, bf16(x) + bf16(x - bf16(x))).
 
 Tolerance: the device rounds each hidden activation to BF16 (2^-8 relative)
 after an FP32 sum whose order differs from the reference's, and evaluates the
@@ -33,7 +34,8 @@ def mlp_reference(params, x):
     import torch
     bf = lambda t: t.to(torch.bfloat16).to(torch.float32)  # noqa: E731
     sizes = [(256, 5), (256, 256), (256, 256), (256, 256), (4, 256)]
-    h = bf(torch.from_numpy(x))
+    xt = torch.from_numpy(x)
+    h = bf(xt) + bf(xt - bf(xt))
     off = 0
     for i, (out, inp) in enumerate(sizes):
         W = torch.from_numpy(params[off:off + out * inp].reshape(out, inp)); off += out * inp
