@@ -522,6 +522,15 @@ def beam_leg(eng, abi, side=256):
 
 
 TRAIN_FLOP_PER_ROW = 3 * 2 * 198912 - 2 * 5 * 256  # forward, dW and dH (no dH for the input layer)
+# Algorithmic HBM bytes per training row of one step, from the kernels' operands:
+# gather 92 (features, targets, weight in; the BF16 input row, targets, weight
+# out); forward 8,240 (layer 1: input 32, Z 1024 FP32, H 512 BF16; layers 2-4:
+# H in 512, Z 1024 and H 512 out; output layer: H 512 in, y 16 out); loss 68;
+# backward 11,872 (dW5: H4 512 + dY 32; dH4: dY 32, Z4 1024 in, dZ 512 out;
+# layers 4..2: dW 512 + 512, dH 512 + Z 1024 in and dZ 512 out; dW1: 512 + 32);
+# Adam 5.6 MB of parameters and moments per step over the batch (171 B/row at
+# 32768 rows). Weights are re-read from L2 and not counted.
+TRAIN_BYTES_PER_ROW = 92 + 8240 + 68 + 11872 + 171
 
 
 def train_leg(eng, abi, np, torch, dev, rows=1 << 21, batch=32768, steps=64):
@@ -546,12 +555,17 @@ def train_leg(eng, abi, np, torch, dev, rows=1 << 21, batch=32768, steps=64):
         with open(MEASURED_PEAKS) as f:
             peaks = json.load(f)
     bf16_peak = float(peaks.get("bf16_tflops", 1590.0))
+    hbm_peak = float(peaks.get("hbm_gbs", 6650.0))
     tflops = rows_per_s * TRAIN_FLOP_PER_ROW / 1e12
+    gbs = rows_per_s * TRAIN_BYTES_PER_ROW / 1e9
+    # the step moves 20 KB of activations and gradients per row for 1.19 MFLOP:
+    # at the measured peaks the bytes take ~4x the tensor-core time, so HBM is the bound
     return {"workload": f"surrogate_mlp_training_batch{batch}", "steps": steps, "ms_per_step": ms / steps,
-            "rows_per_s": rows_per_s, "flop_per_row": TRAIN_FLOP_PER_ROW,
-            "roofline": {"bound": "tensor", "achieved": tflops, "peak": bf16_peak, "unit": "TFLOP/s",
-                         "frac": tflops / bf16_peak, "peak_source": "MEASURED_PEAKS.json bf16_tflops (burst)"
-                         if "bf16_tflops" in peaks else "fallback 1590 TFLOP/s"},
+            "rows_per_s": rows_per_s, "flop_per_row": TRAIN_FLOP_PER_ROW, "bytes_per_row": TRAIN_BYTES_PER_ROW,
+            "roofline": {"bound": "hbm", "achieved": gbs, "peak": hbm_peak, "unit": "GB/s", "frac": gbs / hbm_peak,
+                         "peak_source": "MEASURED_PEAKS.json hbm_gbs" if "hbm_gbs" in peaks else "fallback 6650 GB/s",
+                         "tensor": {"achieved": tflops, "peak": bf16_peak, "unit": "TFLOP/s",
+                                    "frac": tflops / bf16_peak}},
             "data": "synthetic rows (seeded), the surrogate's feature ranges"}
 
 

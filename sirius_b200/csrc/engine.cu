@@ -883,6 +883,11 @@ int launch_trace(Handle* H, int n_frames, long long total, sirius_ray_result* d_
     if (shmem_launch > 48 * 1024)
         CK(cudaFuncSetAttribute((const void*)launch_fn[0], cudaFuncAttributeMaxDynamicSharedMemorySize,
                                 int(shmem_launch)));
+    // a one-frame launch of camera rays traces 16 x 8 pixel tiles per block
+    P.tiled = (n_frames == 1 && !d_list && !d_rays && !P.persistent && !pair && block == 128 &&
+               H->frame0.ray_offset == 0 && H->frame0.width > 0 && H->frame0.width % 16 == 0 &&
+               total == H->frame0.n_rays && total % H->frame0.width == 0 && (total / H->frame0.width) % 8 == 0)
+                  ? 1 : 0;
     int grid;
     if (P.persistent) {
         int per_sm = c.blocks_per_sm;

@@ -40,6 +40,9 @@ struct Params {
     int persistent;
     int refill_threshold;
     int family;                           // >= 0: trace only the rays of frames of this family
+    int tiled;                            // one-frame launch of 128-thread blocks over a frame whose width is a
+                                          // multiple of 16 and row count of 8: block b traces a 16 x 8 pixel
+                                          // tile, each warp an 8 x 4 quarter of it (tile_ray)
     unsigned long long* clock0;           // launch start on the device clock (first warp stamps it)
     unsigned long long watchdog_ns;       // globaltimer bound for the whole launch, per warp
     CfgDev c;
@@ -783,6 +786,19 @@ __device__ __forceinline__ int advance_post(const Params& P, Ray<MIXED>& s, bool
     return -1;
 }
 
+// The ray (pixel of the frame's row window) of this thread in a tiled launch:
+// block b covers the 16 x 8 pixel tile b of the window (row-major over tiles),
+// warp w its 8 x 4 quarter (w % 2, w / 2), lane l pixel (l % 8, l / 8) of that.
+// A warp's rays then lie within 8 x 4 pixels instead of 32 x 1, so fewer warps
+// straddle an edge of the image (the disk's rim, the photon ring) where
+// neighbouring geodesics take different branches.
+__device__ __forceinline__ long long tile_ray(int width) {
+    const int bpr = width / 16, b = int(blockIdx.x), w = int(threadIdx.x >> 5), l = int(threadIdx.x & 31);
+    const int x = (b % bpr) * 16 + (w & 1) * 8 + (l & 7);
+    const int y = (b / bpr) * 8 + (w >> 1) * 4 + (l >> 3);
+    return (long long)y * width + x;
+}
+
 // Persistent tracer. Dynamic shared memory: 2 * npair float2 per thread (volumetric bin pairs).
 template <bool MIXED, int FAM, bool UNI, int INT>
 __device__ __forceinline__ void trace_body(const Params& P) {
@@ -806,7 +822,7 @@ __device__ __forceinline__ void trace_body(const Params& P) {
     t_start = __shfl_sync(kFull, t_start, 0);
 
     if (!P.persistent) {
-        const long long gid = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+        const long long gid = UNI && P.tiled ? tile_ray(P.f0.width) : (long long)blockIdx.x * blockDim.x + threadIdx.x;
         const unsigned entry = (P.list && gid < P.total) ? P.list[gid] : 0u;
         if (gid < P.total && entry != kListSkip) {
             const long long idx = P.list ? (long long)entry : gid;
