@@ -883,10 +883,12 @@ int launch_trace(Handle* H, int n_frames, long long total, sirius_ray_result* d_
     if (shmem_launch > 48 * 1024)
         CK(cudaFuncSetAttribute((const void*)launch_fn[0], cudaFuncAttributeMaxDynamicSharedMemorySize,
                                 int(shmem_launch)));
-    // a one-frame launch of camera rays traces 16 x 8 pixel tiles per block
-    P.tiled = (n_frames == 1 && !d_list && !d_rays && !P.persistent && !pair && block == 128 &&
-               H->frame0.ray_offset == 0 && H->frame0.width > 0 && H->frame0.width % 16 == 0 &&
-               total == H->frame0.n_rays && total % H->frame0.width == 0 && (total / H->frame0.width) % 8 == 0)
+    // a one-frame launch of camera rays traces 8 x 4 pixel tiles per warp (tile_ray:
+    // blocks of 32, 64 and 128 threads cover 8 x 4, 16 x 4 and 16 x 8 pixels)
+    const int tile_x = block >= 64 ? 16 : 8, tile_y = block == 128 ? 8 : 4;
+    P.tiled = (n_frames == 1 && !d_list && !d_rays && !P.persistent && !pair && H->frame0.ray_offset == 0 &&
+               H->frame0.width > 0 && H->frame0.width % tile_x == 0 && total == H->frame0.n_rays &&
+               total % H->frame0.width == 0 && (total / H->frame0.width) % tile_y == 0)
                   ? 1 : 0;
     int grid;
     if (P.persistent) {

@@ -40,9 +40,9 @@ struct Params {
     int persistent;
     int refill_threshold;
     int family;                           // >= 0: trace only the rays of frames of this family
-    int tiled;                            // one-frame launch of 128-thread blocks over a frame whose width is a
-                                          // multiple of 16 and row count of 8: block b traces a 16 x 8 pixel
-                                          // tile, each warp an 8 x 4 quarter of it (tile_ray)
+    int tiled;                            // one-frame launch over a frame whose width and row count are
+                                          // multiples of the block's pixel tile: each warp traces an 8 x 4
+                                          // pixel tile (tile_ray)
     unsigned long long* clock0;           // launch start on the device clock (first warp stamps it)
     unsigned long long watchdog_ns;       // globaltimer bound for the whole launch, per warp
     CfgDev c;
@@ -786,16 +786,19 @@ __device__ __forceinline__ int advance_post(const Params& P, Ray<MIXED>& s, bool
     return -1;
 }
 
-// The ray (pixel of the frame's row window) of this thread in a tiled launch:
-// block b covers the 16 x 8 pixel tile b of the window (row-major over tiles),
-// warp w its 8 x 4 quarter (w % 2, w / 2), lane l pixel (l % 8, l / 8) of that.
-// A warp's rays then lie within 8 x 4 pixels instead of 32 x 1, so fewer warps
-// straddle an edge of the image (the disk's rim, the photon ring) where
-// neighbouring geodesics take different branches.
+// The ray (pixel of the frame's row window) of this thread in a tiled launch.
+// Each warp traces an 8 x 4 pixel tile (lane l: pixel (l % 8, l / 8) of it);
+// a block's warps sit side by side in pairs (block of 32 threads: 8 x 4 pixels,
+// 64: 16 x 4, 128: 16 x 8), and blocks cover the window row-major. A warp's rays
+// then lie within 8 x 4 pixels instead of 32 x 1, so fewer warps straddle an
+// edge of the image (the disk's rim, the photon ring) where neighbouring
+// geodesics take different branches, and a block's warps, close together, end
+// at about the same time (a block holds its SM slot until its last warp ends).
 __device__ __forceinline__ long long tile_ray(int width) {
-    const int bpr = width / 16, b = int(blockIdx.x), w = int(threadIdx.x >> 5), l = int(threadIdx.x & 31);
-    const int x = (b % bpr) * 16 + (w & 1) * 8 + (l & 7);
-    const int y = (b / bpr) * 8 + (w >> 1) * 4 + (l >> 3);
+    const int nw = int(blockDim.x >> 5), across = nw >= 2 ? 2 : 1, bx = 8 * across, by = 4 * (nw / across);
+    const int bpr = width / bx, b = int(blockIdx.x), w = int(threadIdx.x >> 5), l = int(threadIdx.x & 31);
+    const int x = (b % bpr) * bx + (w % across) * 8 + (l & 7);
+    const int y = (b / bpr) * by + (w / across) * 4 + (l >> 3);
     return (long long)y * width + x;
 }
 
