@@ -211,8 +211,9 @@ typedef struct sirius_trace_config {
                                     statistics count the last pass. At most 4096. */
     int32_t max_registers;       /* one-thread-per-ray launch: the register cap of the trace kernel,
                                     255 (8 warps per SM), 168 (12) or 128 (16; these two spill).
-                                    0 = measured default: 128 for mixed DP45, else 255 (FP64,
-                                    symplectic). The budgets' FP32 roundings differ, so mixed
+                                    0 = measured default: 128 for mixed DP45, 168 for FP64 DP45,
+                                    255 for the symplectic integrator. The budgets' FP32
+                                    roundings differ, so mixed
                                     images at different caps agree to ~1e-5 of the peak, not
                                     bit for bit. The persistent launch takes its budget from
                                     blocks_per_sm. */

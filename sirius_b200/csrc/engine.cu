@@ -72,6 +72,7 @@ __global__ void __launch_bounds__(kFluxN) flux_table_kernel(const FrameDev* fram
 
 constexpr int kDefaultMinBlocks = 2;       // up to 255 registers
 constexpr int kDefaultMinBlocksMixed = 4;  // 128 registers: mixed DP45
+constexpr int kDefaultMinBlocksFp64 = 3;   // 168 registers: FP64 DP45
 constexpr int kDefaultRaysPerThread = 1;   // rays per thread of mixed DP45 over Kerr-Schild frames
 
 // A kernel specialised for one metric family carries only that family's
@@ -197,10 +198,24 @@ __global__ void sur_features_kernel(const FrameDev* frames, const SurFrameDev* s
 // 0 = the MLP's pixel; and the rays to integrate counted per block and class
 // (sur_scan_kernel and sur_scatter_kernel list every gated ray before every
 // audit ray, each class in pixel order)
+// The pixel of this thread in the gate and scatter kernels: in pixel order, or,
+// for one frame whose width and row count are multiples of 16 (tile_w = its
+// width), in 16 x 16 tiles of 256-thread blocks with 8 x 4 pixels per warp, so
+// that the compacted list of gated rays, which follows this order, hands the
+// integrator warps of neighbouring pixels (as the tiled one-frame launch does).
+__device__ __forceinline__ long long sur_pixel(int tile_w) {
+    if (tile_w <= 0) return (long long)blockIdx.x * blockDim.x + threadIdx.x;
+    const int bpr = tile_w / 16, b = int(blockIdx.x), w = int(threadIdx.x >> 5), l = int(threadIdx.x & 31);
+    const int x = (b % bpr) * 16 + (w & 1) * 8 + (l & 7);
+    const int y = (b / bpr) * 16 + (w >> 1) * 4 + (l >> 3);
+    return (long long)y * tile_w + x;
+}
+
 __global__ void sur_gate_kernel(const FrameDev* frames, const SurFrameDev* sf, int n_frames, long long total,
                                 float band, unsigned audit_threshold, unsigned seed, const float* feat,
-                                int stride, const float* cout, unsigned char* gate, unsigned* block_counts) {
-    const long long idx = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+                                int stride, const float* cout, unsigned char* gate, unsigned* block_counts,
+                                int tile_w) {
+    const long long idx = sur_pixel(tile_w);
     unsigned char g = 0;
     if (idx < total) {
         const int f = n_frames > 1 ? find_frame(frames, n_frames, idx) : 0;
@@ -283,9 +298,9 @@ __global__ void sur_scan_kernel(unsigned* block_counts, int n_blocks) {
 // the audit rays in pixel order (so each audit run of 32 pixels fills one warp).
 // block_offsets: class-1 offsets of the blocks, then their class-2 offsets.
 __global__ void sur_scatter_kernel(const unsigned char* gate, long long total, const unsigned* block_offsets,
-                                   unsigned* list) {
+                                   unsigned* list, int tile_w) {
     __shared__ unsigned warp_base[2][32];
-    const long long idx = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+    const long long idx = sur_pixel(tile_w);
     const unsigned char g = idx < total ? gate[idx] : 0;
     const unsigned m1 = __ballot_sync(kFull, g == 1), m2 = __ballot_sync(kFull, g == 2);
     const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
@@ -830,10 +845,11 @@ int launch_trace(Handle* H, int n_frames, long long total, sirius_ray_result* d_
     const size_t shmem = size_t(2) * P.c.npair * block * sizeof(float2);
     // register budget: the kernel compiled for blocks_per_sm resident 128-thread
     // blocks per SM (persistent), or for max_registers (one thread per ray);
-    // fewer registers, possibly spills. The default was measured: the mixed DP45
-    // kernel runs fastest at 128 registers (16 warps per SM; 1024^2 bench frame
-    // 38.9 ms against 41.5 ms at 255); FP64 (63.0 ms against 78.0 ms at 128) and
-    // the symplectic integrator keep 255. The choice depends on the configuration
+    // fewer registers, possibly spills. The default was measured on the 1024^2
+    // bench frame in the tiled layout: mixed DP45 runs fastest at 128 registers
+    // (16 warps per SM; 22.8 ms against 23.6 at 168 and 25.2 at 255), FP64 DP45 at
+    // 168 (41.3 ms against 44.2 at 255 and 52.4 at 128); the symplectic
+    // integrator keeps 255. The choice depends on the configuration
     // only, never on the launch's size or contents: the budgets' FP32 roundings
     // differ, and a ray's result must not depend on what else shares its launch.
     const bool symp = c.integrator == SIRIUS_INTEGRATOR_SYMPLECTIC;
@@ -843,6 +859,7 @@ int launch_trace(Handle* H, int n_frames, long long total, sirius_ray_result* d_
                      : c.max_registers == 168 ? 3
                      : c.max_registers == 255 ? 2
                      : mixed_dp45             ? kDefaultMinBlocksMixed
+                     : !mixed && !symp        ? kDefaultMinBlocksFp64
                                               : kDefaultMinBlocks;
     // the families present: one family -> its specialised kernel; several ->
     // one launch per family (each thread skips the rays of other families), so
@@ -2118,12 +2135,18 @@ static int surrogate_gate_launch(Handle* H, const sirius_frame* frames, int n_fr
         if ((rc = surrogate_launch(H, H->d_coarse_feat, n_coarse, H->d_coarse_out, st)) != SIRIUS_OK) return rc;
     }
     H->last_coarse = n_coarse;
+    // one frame in 16 x 16 pixel tiles: the list of gated rays in tile order
+    int tile_w = 0;
+    if (n_frames == 1) {
+        const FrameDev F = make_frame(frames[0], H->cfg);
+        if (F.width % 16 == 0 && F.n_rays == total && (total / F.width) % 16 == 0) tile_w = F.width;
+    }
     sur_gate_kernel<<<n_blocks, block, 0, st>>>(H->d_frames, H->d_sur_frames, n_frames, total, float(band), thr, seed,
-                                                H->d_feat, stride, H->d_coarse_out, d_gate, H->d_block_counts);
+                                                H->d_feat, stride, H->d_coarse_out, d_gate, H->d_block_counts, tile_w);
     CK(cudaGetLastError());
     sur_scan_kernel<<<1, 1024, 0, st>>>(H->d_block_counts, 2 * n_blocks);
     CK(cudaGetLastError());
-    sur_scatter_kernel<<<n_blocks, block, 0, st>>>(d_gate, total, H->d_block_counts, H->d_list);
+    sur_scatter_kernel<<<n_blocks, block, 0, st>>>(d_gate, total, H->d_block_counts, H->d_list, tile_w);
     CK(cudaGetLastError());
     CK(cudaMemcpyAsync(H->h_list_len, H->d_block_counts + n_blocks, sizeof(unsigned), cudaMemcpyDeviceToHost, st));
     CK(cudaMemcpyAsync(H->h_list_len + 1, H->d_block_counts + 2 * size_t(n_blocks), sizeof(unsigned),
