@@ -116,6 +116,7 @@ struct GemmSmem {
     static constexpr uint32_t Cols = BN < 32 ? 32 : BN;
 };
 static_assert(GemmSmem<256>::Stage % 1024 == 0 && GemmSmem<16>::Stage % 1024 == 0, "stage alignment");
+static_assert(GemmSmem<256>::Bar >= (kGemmThreads / 32) * 32 * 33 * 4, "the epilogue's transposition tiles fit the stages");
 static_assert(GemmSmem<256>::Bytes <= 113 * 1024, "two 256-wide GEMM CTAs fit one SM (and its 512 TMEM columns)");
 
 #ifdef __CUDACC__
@@ -221,8 +222,73 @@ __device__ __forceinline__ float transpose_sum32(float v[32]) {
     return v[0];
 }
 
+// A warp's 32 x 32 block of FP32 values (block row r held by lane r) to global
+// memory through the warp's shared tile (32 x 33 floats, conflict-free): each
+// store instruction then writes four 128-byte row segments, where a lane per
+// row would write 32 scattered 16-byte pieces. Rows at or beyond rows_end are
+// left alone.
+__device__ __forceinline__ void warp_rows_f32_out(float* t, const float v[32], float* dst, long long ld,
+                                                  long long row0, long long rows_end) {
+    const int lane = threadIdx.x & 31;
+#pragma unroll
+    for (int j = 0; j < 32; ++j) t[lane * 33 + j] = v[j];
+    __syncwarp();
+#pragma unroll
+    for (int i = 0; i < 8; ++i) {
+        const int r = 4 * i + (lane >> 3), c = (lane & 7) * 4;
+        if (row0 + r < rows_end) {
+            const float* q = t + r * 33 + c;
+            *reinterpret_cast<float4*>(dst + (row0 + r) * ld + c) = make_float4(q[0], q[1], q[2], q[3]);
+        }
+    }
+    __syncwarp();
+}
+
+// The same for BF16 values (eight 64-byte row segments per store instruction).
+__device__ __forceinline__ void warp_rows_bf16_out(float* t, const float v[32], __nv_bfloat16* dst, long long ld,
+                                                   long long row0, long long rows_end) {
+    const int lane = threadIdx.x & 31;
+#pragma unroll
+    for (int j = 0; j < 32; ++j) t[lane * 33 + j] = v[j];
+    __syncwarp();
+#pragma unroll
+    for (int i = 0; i < 4; ++i) {
+        const int r = 8 * i + (lane >> 2), c = (lane & 3) * 8;
+        if (row0 + r < rows_end) {
+            const float* q = t + r * 33 + c;
+            *reinterpret_cast<uint4*>(dst + (row0 + r) * ld + c) =
+                make_uint4(pack_bf16x2(q[0], q[1]), pack_bf16x2(q[2], q[3]), pack_bf16x2(q[4], q[5]),
+                           pack_bf16x2(q[6], q[7]));
+        }
+    }
+    __syncwarp();
+}
+
+// A warp's 32 x 32 FP32 block from global memory (coalesced, as above); lane r
+// returns block row r (zeros for rows at or beyond rows_end).
+__device__ __forceinline__ void warp_rows_f32_in(float* t, float v[32], const float* src, long long ld,
+                                                 long long row0, long long rows_end) {
+    const int lane = threadIdx.x & 31;
+#pragma unroll
+    for (int i = 0; i < 8; ++i) {
+        const int r = 4 * i + (lane >> 3), c = (lane & 7) * 4;
+        const float4 z = row0 + r < rows_end ? *reinterpret_cast<const float4*>(src + (row0 + r) * ld + c)
+                                             : make_float4(0.f, 0.f, 0.f, 0.f);
+        float* q = t + r * 33 + c;
+        q[0] = z.x;
+        q[1] = z.y;
+        q[2] = z.z;
+        q[3] = z.w;
+    }
+    __syncwarp();
+#pragma unroll
+    for (int j = 0; j < 32; ++j) v[j] = t[lane * 33 + j];
+    __syncwarp();
+}
+
+// tile: shared memory for the warps' 32 x 33 transposition tiles (the drained stages)
 template <int BN, int E>
-__device__ __forceinline__ void gemm_epilogue(const GemmArgs& g, uint32_t tmem, int m0, int n0) {
+__device__ __forceinline__ void gemm_epilogue(const GemmArgs& g, uint32_t tmem, int m0, int n0, float* tile) {
     const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
     const uint32_t tl = tmem + (uint32_t(warp * 32) << 16);
     const long long row = (long long)m0 + warp * 32 + lane;
@@ -250,42 +316,23 @@ __device__ __forceinline__ void gemm_epilogue(const GemmArgs& g, uint32_t tmem, 
             float v[32];
             tmem_ld32(tl + uint32_t(c0), v);
             const int n = n0 + c0;
+            float* t = tile + warp * (32 * 33);
+            const long long row0 = (long long)m0 + warp * 32;
             if constexpr (E == kEpiHidden) {
-                if (live) {
-                    float4* zr = reinterpret_cast<float4*>(g.e.z + row * g.e.ldz + n);
-                    uint4* hr = reinterpret_cast<uint4*>(g.e.h + row * g.e.ldh + n);
+                // Z = acc + bias (FP32, kept for the backward pass), H = SiLU(Z) (BF16)
 #pragma unroll
-                    for (int i = 0; i < 32; ++i) v[i] += g.e.bias[n + i];
+                for (int i = 0; i < 32; ++i) v[i] += g.e.bias[n + i];
+                warp_rows_f32_out(t, v, g.e.z + n, g.e.ldz, row0, g.M);
 #pragma unroll
-                    for (int i = 0; i < 8; ++i) zr[i] = make_float4(v[4 * i], v[4 * i + 1], v[4 * i + 2], v[4 * i + 3]);
-#pragma unroll
-                    for (int i = 0; i < 4; ++i)
-                        hr[i] = make_uint4(pack_bf16x2(silu(v[8 * i]), silu(v[8 * i + 1])),
-                                           pack_bf16x2(silu(v[8 * i + 2]), silu(v[8 * i + 3])),
-                                           pack_bf16x2(silu(v[8 * i + 4]), silu(v[8 * i + 5])),
-                                           pack_bf16x2(silu(v[8 * i + 6]), silu(v[8 * i + 7])));
-                }
+                for (int i = 0; i < 32; ++i) v[i] = silu(v[i]);
+                warp_rows_bf16_out(t, v, g.e.h + n, g.e.ldh, row0, g.M);
             } else if constexpr (E == kEpiDHidden) {
-                if (live) {
-                    const float4* zr = reinterpret_cast<const float4*>(g.e.z + row * g.e.ldz + n);
+                // dZ = dH SiLU'(Z) (BF16) and the bias gradient (column sums)
+                float z[32];
+                warp_rows_f32_in(t, z, g.e.z + n, g.e.ldz, row0, g.M);
 #pragma unroll
-                    for (int i = 0; i < 8; ++i) {
-                        const float4 z = zr[i];
-                        v[4 * i] *= dsilu(z.x);
-                        v[4 * i + 1] *= dsilu(z.y);
-                        v[4 * i + 2] *= dsilu(z.z);
-                        v[4 * i + 3] *= dsilu(z.w);
-                    }
-                    uint4* hr = reinterpret_cast<uint4*>(g.e.h + row * g.e.ldh + n);
-#pragma unroll
-                    for (int i = 0; i < 4; ++i)
-                        hr[i] = make_uint4(pack_bf16x2(v[8 * i], v[8 * i + 1]), pack_bf16x2(v[8 * i + 2], v[8 * i + 3]),
-                                           pack_bf16x2(v[8 * i + 4], v[8 * i + 5]),
-                                           pack_bf16x2(v[8 * i + 6], v[8 * i + 7]));
-                } else {
-#pragma unroll
-                    for (int i = 0; i < 32; ++i) v[i] = 0.f;
-                }
+                for (int i = 0; i < 32; ++i) v[i] = live ? v[i] * dsilu(z[i]) : 0.f;
+                warp_rows_bf16_out(t, v, g.e.h + n, g.e.ldh, row0, g.M);
                 const float s = transpose_sum32(v);
                 atomicAdd(g.e.grad + n + lane, s);
             } else if constexpr (E == kEpiDWeight) {
@@ -375,7 +422,7 @@ __global__ void __launch_bounds__(kGemmThreads) gemm_kernel(const __grid_constan
     ok = __syncthreads_and(ok && drained);
     tc_fence_after();
     if (ok && chunk > 0) {
-        gemm_epilogue<BN, E>(g, tmem, m0, n0);
+        gemm_epilogue<BN, E>(g, tmem, m0, n0, reinterpret_cast<float*>(sm));
     } else if (!ok && tid == 0) {
         atomicOr(g.err, 4);
     }
