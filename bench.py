@@ -388,8 +388,10 @@ def surrogate_config(abi, precision):
 def surrogate_leg(eng, abi, np, torch, dev, stream, side=SURROGATE_SIDE, reps=3, inner_gate=0.0):
     """Surrogate-gated rendering of the Kerr a = 0.9 frame at side^2 (gate +-0.3 M
     around the critical curve, the inner-disk gate r_1 < 2.5 r_in from a coarse
-    MLP pass on 8 x 8 pixel cells, 1 % audit rays) against the plain FP64
-    integrator on the same frame; CUDA events on the launch stream around whole calls."""
+    MLP pass on 8 x 8 pixel cells, 1 % audit rays; pixels whose coarse
+    neighbourhood predicts no disk crossing take 0 without the per-pixel MLP)
+    against the plain FP64 integrator on the same frame; CUDA events on the launch
+    stream around whole calls."""
     params = np.load(SURROGATE_WEIGHTS)
     eng.surrogate_load(params)
     frame = workload_frame(abi, side, side)
@@ -447,6 +449,7 @@ def surrogate_leg(eng, abi, np, torch, dev, stream, side=SURROGATE_SIDE, reps=3,
             "coarse_stride": 8, "coarse_mlp_rows": int(stats.coarse_rays),
             "audit_fraction": 0.01, "gated_fraction": float(np.mean(gate == 1)),
             "audit_fraction_measured": float(np.mean(gate == 2)), "integrated_rays": int(stats.integrated),
+            "empty_fraction": float(np.mean(gate == 3)),
             "stage_ms": {"features_gate": stats.ms_features, "mlp_end": stats.ms_mlp, "shade": stats.ms_shade,
                          "integrate_gated_and_audit": stats.ms_trace,
                          "note": "after the list is built, the gated trace and the MLP run side by side; mlp_end and "

@@ -362,7 +362,10 @@ int sirius_cuda_surrogate_infer(sirius_cuda_handle handle, const float* d_featur
  * chosen by a hash seeded with audit_seed), and
  * every ray of a frame that is not charge- and Lambda-free Kerr are integrated
  * instead (the configured integrator, compacted into one launch) and overwrite
- * their pixels. gate (optional): per pixel 0 = MLP, 1 = gated, 2 = audit.
+ * their pixels. gate (optional): per pixel 0 = MLP, 1 = gated, 2 = audit, 3 = empty
+ * (no disk crossing predicted around it: intensity 0, no MLP; see empty_skip). A ray
+ * that never crosses the disk plane inside the disk carries no light (thin disk only),
+ * so the coarse pass's confident no-hit cells need no per-pixel network.
  * The inner-disk gate: the MLP first runs on a coarse grid (every
  * coarse_stride-th pixel in each direction, the cell centres); every pixel whose
  * coarse cell or a neighbouring one predicts a disk hit at r_1 < inner_gate *
@@ -378,7 +381,12 @@ typedef struct {
     float inner_gate;          /* r_1 bound of the inner-disk gate in units of r_in: 0 = 2.5, < 0 = off */
     int32_t coarse_stride;     /* pixels per coarse cell side of the inner-disk gate: 0 = 8 */
     float audit_budget;        /* 0: the audit only reports */
-    int32_t reserved[2];
+    int32_t empty_skip;        /* 0 = on, < 0 = off: pixels whose coarse cell and its eight
+                                  neighbours all predict no disk crossing (hit logit below -4)
+                                  take intensity 0 without the per-pixel MLP (gate 3); the MLP
+                                  runs only on the pixels it shades and the audit pixels. Off
+                                  when d_image_mlp is requested (it needs every pixel). */
+    int32_t reserved;
 } sirius_surrogate_config;
 
 typedef struct {

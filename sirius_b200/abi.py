@@ -122,7 +122,7 @@ class LaunchStats(C.Structure):
 class SurrogateConfig(C.Structure):
     _fields_ = [("gate_band", C.c_double), ("audit_fraction", C.c_double), ("audit_seed", C.c_uint32),
                 ("inner_gate", C.c_float), ("coarse_stride", C.c_int32), ("audit_budget", C.c_float),
-                ("reserved", C.c_int32 * 2)]
+                ("empty_skip", C.c_int32), ("reserved", C.c_int32)]
 
 
 class SurrogateStats(C.Structure):
@@ -133,9 +133,10 @@ class SurrogateStats(C.Structure):
 
 
 def surrogate_config(gate_band=0.3, audit_fraction=0.01, audit_seed=0, inner_gate=0.0, coarse_stride=0,
-                     audit_budget=0.0):
-    """sirius_surrogate_config (inner_gate 0: 2.5 r_in, < 0: off; coarse_stride 0: 8; audit_budget 0: report only)."""
-    return SurrogateConfig(gate_band, audit_fraction, audit_seed, inner_gate, coarse_stride, audit_budget)
+                     audit_budget=0.0, empty_skip=0):
+    """sirius_surrogate_config (inner_gate 0: 2.5 r_in, < 0: off; coarse_stride 0: 8; audit_budget 0: report
+    only; empty_skip 0: on, < 0: off)."""
+    return SurrogateConfig(gate_band, audit_fraction, audit_seed, inner_gate, coarse_stride, audit_budget, empty_skip)
 
 
 class BeamResult(C.Structure):

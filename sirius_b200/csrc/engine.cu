@@ -95,6 +95,7 @@ constexpr double kInnerGateDefault = 2.5;  // inner-disk gate: r_1 < 2.5 r_in
 constexpr int kCoarseStrideDefault = 8;    // inner-disk gate: 8 x 8 pixels per coarse cell
 constexpr float kSurRScale = 15.f;   // MLP output 1: r_1 = 15 (1 + o_1)
 constexpr float kSurHigher = 1e-3f;  // MLP output 3: higher-order intensity / 1e-3
+constexpr float kEmptyLogit = -4.f;  // empty pixels: every neighbouring coarse cell's hit logit below this
 
 struct SurFrameDev {
     double sin_o, theta_deg;      // camera Boyer-Lindquist polar angle
@@ -214,7 +215,7 @@ __device__ __forceinline__ long long sur_pixel(int tile_w) {
 __global__ void sur_gate_kernel(const FrameDev* frames, const SurFrameDev* sf, int n_frames, long long total,
                                 float band, unsigned audit_threshold, unsigned seed, const float* feat,
                                 int stride, const float* cout, unsigned char* gate, unsigned* block_counts,
-                                int tile_w) {
+                                int tile_w, int empty_skip) {
     const long long idx = sur_pixel(tile_w);
     unsigned char g = 0;
     if (idx < total) {
@@ -250,17 +251,34 @@ __global__ void sur_gate_kernel(const FrameDev* frames, const SurFrameDev* sf, i
         }
         // audit rays come in runs of 32 consecutive pixels, so that they integrate as coherent warps
         if (!g && audit_hash((unsigned long long)idx >> 5, seed) < audit_threshold) g = 2;
+        // empty: the pixel's coarse cell and its eight neighbours all predict no
+        // disk crossing (a ray that never crosses the disk carries no light)
+        if (!g && empty_skip && S.kerr && S.cw > 0) {
+            const FrameDev& F = frames[f];
+            const long long pix = idx - F.ray_offset;
+            const int cx = int(pix % F.width) / stride, cy = int(pix / F.width / stride);
+            bool empty = true;
+            for (int dy = -1; dy <= 1 && empty; ++dy)
+                for (int dx2 = -1; dx2 <= 1; ++dx2) {
+                    const int ux = min(max(cx + dx2, 0), S.cw - 1), uy = min(max(cy + dy, 0), S.ch - 1);
+                    if (cout[(S.coarse_offset + (long long)uy * S.cw + ux) * 4] > kEmptyLogit) { empty = false; break; }
+                }
+            if (empty) g = 3;
+        }
         gate[idx] = g;
     }
-    __shared__ unsigned warp_counts[2][32];
+    // per block: gated, audit and MLP-row counts (class k at block_counts[k * gridDim.x + block])
+    __shared__ unsigned warp_counts[3][32];
     const unsigned m1 = __ballot_sync(kFull, g == 1);
     const unsigned m2 = __ballot_sync(kFull, g == 2);
+    const unsigned m3 = __ballot_sync(kFull, idx < total && (g == 0 || g == 2));
     if ((threadIdx.x & 31) == 0) {
         warp_counts[0][threadIdx.x >> 5] = __popc(m1);
         warp_counts[1][threadIdx.x >> 5] = __popc(m2);
+        warp_counts[2][threadIdx.x >> 5] = __popc(m3);
     }
     __syncthreads();
-    if (threadIdx.x < 2) {
+    if (threadIdx.x < 3) {
         unsigned c = 0;
         for (int w = 0; w < int(blockDim.x >> 5); ++w) c += warp_counts[threadIdx.x][w];
         block_counts[threadIdx.x * gridDim.x + blockIdx.x] = c;
@@ -298,21 +316,25 @@ __global__ void sur_scan_kernel(unsigned* block_counts, int n_blocks) {
 // the audit rays in pixel order (so each audit run of 32 pixels fills one warp).
 // block_offsets: class-1 offsets of the blocks, then their class-2 offsets.
 __global__ void sur_scatter_kernel(const unsigned char* gate, long long total, const unsigned* block_offsets,
-                                   unsigned* list, int tile_w) {
-    __shared__ unsigned warp_base[2][32];
+                                   unsigned* list, int tile_w, unsigned* mlp_rows) {
+    __shared__ unsigned warp_base[3][32];
     const long long idx = sur_pixel(tile_w);
     const unsigned char g = idx < total ? gate[idx] : 0;
     const unsigned m1 = __ballot_sync(kFull, g == 1), m2 = __ballot_sync(kFull, g == 2);
+    const unsigned m3 = __ballot_sync(kFull, idx < total && (g == 0 || g == 2));
     const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
     if (lane == 0) {
         warp_base[0][warp] = __popc(m1);
         warp_base[1][warp] = __popc(m2);
+        warp_base[2][warp] = __popc(m3);
     }
     __syncthreads();
     const unsigned n1 = block_offsets[gridDim.x], pad = (32u - (n1 & 31u)) & 31u;
+    const unsigned n12 = block_offsets[2 * gridDim.x];  // the MLP rows' offsets start here
     if (blockIdx.x == 0 && threadIdx.x < pad) list[n1 + threadIdx.x] = kListSkip;
-    if (threadIdx.x < 2) {
-        unsigned run = block_offsets[threadIdx.x * gridDim.x + blockIdx.x] + (threadIdx.x == 1 ? pad : 0u);
+    if (threadIdx.x < 3) {
+        unsigned run = block_offsets[threadIdx.x * gridDim.x + blockIdx.x] + (threadIdx.x == 1 ? pad : 0u) -
+                       (threadIdx.x == 2 ? n12 : 0u);
         for (int w = 0; w < int(blockDim.x >> 5); ++w) {
             const unsigned c = warp_base[threadIdx.x][w];
             warp_base[threadIdx.x][w] = run;
@@ -323,6 +345,7 @@ __global__ void sur_scatter_kernel(const unsigned char* gate, long long total, c
     const unsigned below = (1u << lane) - 1u;
     if (g == 1) list[warp_base[0][warp] + __popc(m1 & below)] = unsigned(idx);
     if (g == 2) list[warp_base[1][warp] + __popc(m2 & below)] = unsigned(idx);
+    if (mlp_rows && idx < total && (g == 0 || g == 2)) mlp_rows[warp_base[2][warp] + __popc(m3 & below)] = unsigned(idx);
 }
 
 // pixel intensity from the MLP outputs: hit logit, r_1, g_1, higher orders
@@ -332,6 +355,13 @@ __global__ void sur_shade_kernel(const FrameDev* frames, int n_frames, long long
                                  const unsigned char* gate, const float* flux, float* image, float* image_mlp) {
     const long long idx = (long long)blockIdx.x * blockDim.x + threadIdx.x;
     if (idx >= total) return;
+    const unsigned char g = gate[idx];
+    if (g == 3) {  // empty: no disk crossing predicted around it, and no MLP outputs
+        image[idx] = 0.f;
+        if (image_mlp) image_mlp[idx] = 0.f;
+        return;
+    }
+    if (g == 1 && !image_mlp) return;  // the integrator writes it
     const int f = n_frames > 1 ? find_frame(frames, n_frames, idx) : 0;
     const FrameDev& F = frames[f];
     const float4 o = reinterpret_cast<const float4*>(out)[idx];
@@ -342,7 +372,6 @@ __global__ void sur_shade_kernel(const FrameDev* frames, int n_frames, long long
         I = g1 * g1 * g1 * g1 * flux_lookup(flux + size_t(F.flux_slot) * kFluxTable, F, r1);
     }
     I += fmax(double(o.w), 0.0) * double(kSurHigher);
-    const unsigned char g = gate[idx];
     if (g == 0) image[idx] = float(I);
     if (g == 2) out[idx * 4] = float(I);  // kept for the audit (the outputs are consumed)
     if (image_mlp) image_mlp[idx] = float(I);
@@ -524,7 +553,7 @@ struct Handle {
     SurFrameDev* d_sur_frames = nullptr;
     SurFrameDev* h_sur_frames = nullptr;  // pinned staging: per-frame basics, then with the curves
     size_t h_sur_frames_cap = 0;
-    unsigned* h_list_len = nullptr;       // pinned: gated count, gated + audit count
+    unsigned* h_list_len = nullptr;       // pinned: gated count, gated + audit count, + MLP rows
     size_t sur_frames_cap = 0;
     float* d_feat = nullptr;
     size_t feat_cap = 0;
@@ -539,7 +568,10 @@ struct Handle {
     long long last_coarse = 0;
     unsigned char* d_gate = nullptr;
     size_t gate_cap = 0;
-    unsigned* d_block_counts = nullptr;  // per-block gated and audit counts, then offsets; [2 n_blocks] = list length
+    unsigned* d_block_counts = nullptr;  // per-block gated, audit and MLP-row counts, then offsets
+    unsigned* d_mlp_rows = nullptr;      // pixels the per-pixel MLP evaluates (when empty pixels are skipped)
+    size_t mlp_rows_cap = 0;
+    bool last_empty_skip = false;        // the last gate launch listed MLP rows (empty pixels skipped)
     size_t block_counts_cap = 0;
     cudaEvent_t sev[5] = {};
     // surrogate rendering: the gated trace (high priority) and the MLP (low priority)
@@ -1358,6 +1390,7 @@ int sirius_cuda_destroy(sirius_cuda_handle h) {
     cudaFree(H->d_sur_frames); cudaFree(H->d_feat); cudaFree(H->d_mlp_out); cudaFree(H->d_list); cudaFree(H->d_gate);
     cudaFree(H->d_coarse_feat); cudaFree(H->d_coarse_out);
     cudaFree(H->d_block_counts);
+    cudaFree(H->d_mlp_rows);
     cudaFree(H->d_pass_image); cudaFree(H->d_pass_spectra); cudaFree(H->d_pass_frames); cudaFree(H->d_prep);
     if (H->h_sur_frames) cudaFreeHost(H->h_sur_frames);
     if (H->h_list_len) cudaFreeHost(H->h_list_len);
@@ -1791,7 +1824,8 @@ int sirius_cuda_surrogate_load(sirius_cuda_handle h, const float* params, int64_
 }
 
 // launches the MLP on n feature rows (device buffers) on stream st
-static int surrogate_launch(Handle* H, const float* d_features, long long n, float* d_out, cudaStream_t st) {
+static int surrogate_launch(Handle* H, const float* d_features, long long n, float* d_out, cudaStream_t st,
+                            const unsigned* rows = nullptr) {
     if (!H->d_surrogate) return fail(H, SIRIUS_ERR_NOT_CONFIGURED, "no surrogate weights loaded");
     if (n <= 0) return SIRIUS_OK;
     const long long tiles = (n + surrogate::kTileM - 1) / surrogate::kTileM;
@@ -1801,7 +1835,7 @@ static int surrogate_launch(Handle* H, const float* d_features, long long n, flo
     unsigned long long* counter = reinterpret_cast<unsigned long long*>(H->d_sur_err + 2);
     CK(cudaMemsetAsync(counter, 0, sizeof(unsigned long long), st));
     surrogate::mlp_kernel_ts<<<grid, surrogate::kThreads, surrogate::kTsSmBytes, st>>>(
-        H->d_surrogate, d_features, n, d_out, H->d_sur_err, counter, limit);
+        H->d_surrogate, d_features, n, d_out, H->d_sur_err, counter, limit, rows);
     CK(cudaGetLastError());
     return SIRIUS_OK;
 }
@@ -2091,36 +2125,41 @@ static int surrogate_features_launch(Handle* H, const sirius_frame* frames, int 
 // list counts are copied into pinned memory (read them once the stream has
 // passed this point).
 static int surrogate_gate_launch(Handle* H, const sirius_frame* frames, int n_frames, long long total,
-                                 const sirius_surrogate_config* sc, unsigned char* d_gate, cudaStream_t st) {
+                                 const sirius_surrogate_config* sc, unsigned char* d_gate, cudaStream_t st,
+                                 bool allow_empty = false) {
     int rc;
     SurFrameDev* full = H->h_sur_frames + n_frames;
     for (int i = 0; i < n_frames; ++i) full[i] = make_sur_frame(frames[i], make_frame(frames[i], H->cfg));
     if ((rc = ensure(H, H->d_list, H->list_cap, size_t(total) + 32)) != SIRIUS_OK) return rc;
     const int block = 256;
     const int n_blocks = int((total + block - 1) / block);
-    // per block: gated count, then audit count; [2 n_blocks] = gated + audit total
-    if ((rc = ensure(H, H->d_block_counts, H->block_counts_cap, 2 * size_t(n_blocks) + 1)) != SIRIUS_OK) return rc;
+    // per block: gated, audit and MLP-row counts; after the scan, offsets, with
+    // [n_blocks] = gated total, [2 n_blocks] = gated + audit, [3 n_blocks] = + MLP rows
+    if ((rc = ensure(H, H->d_block_counts, H->block_counts_cap, 3 * size_t(n_blocks) + 1)) != SIRIUS_OK) return rc;
     if (!d_gate) {
         if ((rc = ensure(H, H->d_gate, H->gate_cap, size_t(total))) != SIRIUS_OK) return rc;
         d_gate = H->d_gate;
     }
-    if (!H->h_list_len) CK(cudaMallocHost((void**)&H->h_list_len, 2 * sizeof(unsigned)));
+    if (!H->h_list_len) CK(cudaMallocHost((void**)&H->h_list_len, 3 * sizeof(unsigned)));
     const double band = sc ? sc->gate_band : 0.3;
     const double audit = sc ? std::clamp(sc->audit_fraction, 0.0, 1.0) : 0.01;
     const unsigned thr = unsigned(std::min(audit * 4294967296.0, 4294967295.0));
     const unsigned seed = sc ? sc->audit_seed : 0u;
-    // the inner-disk gate's coarse MLP pass (after the descriptors above reach the device)
+    // the coarse MLP pass of the inner-disk gate and of the empty pixels (after the
+    // descriptors above reach the device)
     const double inner = sc ? (sc->inner_gate == 0.f ? kInnerGateDefault : double(sc->inner_gate)) : kInnerGateDefault;
+    const bool empty = allow_empty && H->d_surrogate && !(sc && sc->empty_skip < 0);
+    H->last_empty_skip = empty;
     const int stride = (sc && sc->coarse_stride > 0) ? sc->coarse_stride : kCoarseStrideDefault;
     long long n_coarse = 0;
-    if (inner > 0.0 && H->d_surrogate) {  // without weights (features only) there is no inner-disk gate
+    if ((inner > 0.0 || empty) && H->d_surrogate) {  // without weights (features only) there is no coarse pass
         for (int i = 0; i < n_frames; ++i) {
             const FrameDev F = make_frame(frames[i], H->cfg);
             const long long rows = F.n_rays / F.width;
             full[i].coarse_offset = n_coarse;
             full[i].cw = (F.width + stride - 1) / stride;
             full[i].ch = int((rows + stride - 1) / stride);
-            full[i].r1_max = full[i].kerr ? float(inner * F.disk_in) : 0.f;
+            full[i].r1_max = full[i].kerr && inner > 0.0 ? float(inner * F.disk_in) : 0.f;
             n_coarse += (long long)full[i].cw * full[i].ch;
         }
     }
@@ -2142,14 +2181,23 @@ static int surrogate_gate_launch(Handle* H, const sirius_frame* frames, int n_fr
         if (F.width % 16 == 0 && F.n_rays == total && (total / F.width) % 16 == 0) tile_w = F.width;
     }
     sur_gate_kernel<<<n_blocks, block, 0, st>>>(H->d_frames, H->d_sur_frames, n_frames, total, float(band), thr, seed,
-                                                H->d_feat, stride, H->d_coarse_out, d_gate, H->d_block_counts, tile_w);
+                                                H->d_feat, stride, H->d_coarse_out, d_gate, H->d_block_counts, tile_w,
+                                                n_coarse > 0 && empty ? 1 : 0);
     CK(cudaGetLastError());
-    sur_scan_kernel<<<1, 1024, 0, st>>>(H->d_block_counts, 2 * n_blocks);
+    sur_scan_kernel<<<1, 1024, 0, st>>>(H->d_block_counts, 3 * n_blocks);
     CK(cudaGetLastError());
-    sur_scatter_kernel<<<n_blocks, block, 0, st>>>(d_gate, total, H->d_block_counts, H->d_list, tile_w);
+    unsigned* rows = nullptr;
+    if (empty && n_coarse > 0) {
+        if ((rc = ensure(H, H->d_mlp_rows, H->mlp_rows_cap, size_t(total))) != SIRIUS_OK) return rc;
+        rows = H->d_mlp_rows;
+    }
+    H->last_empty_skip = rows != nullptr;
+    sur_scatter_kernel<<<n_blocks, block, 0, st>>>(d_gate, total, H->d_block_counts, H->d_list, tile_w, rows);
     CK(cudaGetLastError());
     CK(cudaMemcpyAsync(H->h_list_len, H->d_block_counts + n_blocks, sizeof(unsigned), cudaMemcpyDeviceToHost, st));
     CK(cudaMemcpyAsync(H->h_list_len + 1, H->d_block_counts + 2 * size_t(n_blocks), sizeof(unsigned),
+                       cudaMemcpyDeviceToHost, st));
+    CK(cudaMemcpyAsync(H->h_list_len + 2, H->d_block_counts + 3 * size_t(n_blocks), sizeof(unsigned),
                        cudaMemcpyDeviceToHost, st));
     return SIRIUS_OK;
 }
@@ -2177,7 +2225,8 @@ static int render_surrogate_pass(Handle* H, const sirius_frame* frames, int n_fr
     CK(cudaMemsetAsync(H->d_sur_err, 0, sizeof(int), st));
     CK(cudaEventRecord(H->sev[0], st));
     if ((rc = surrogate_features_launch(H, frames, n_frames, total, st)) != SIRIUS_OK) return rc;
-    if ((rc = surrogate_gate_launch(H, frames, n_frames, total, sc, d_gate, st)) != SIRIUS_OK) return rc;
+    if ((rc = surrogate_gate_launch(H, frames, n_frames, total, sc, d_gate, st, d_image_mlp == nullptr)) != SIRIUS_OK)
+        return rc;
     // 2. the integrator on the compacted list of gated and audit rays, beside
     // 3. the MLP on every pixel and the shading of the ungated ones. The trace
     // goes first, from a high-priority stream, so its blocks take every free
@@ -2200,6 +2249,7 @@ static int render_surrogate_pass(Handle* H, const sirius_frame* frames, int n_fr
     CK(cudaStreamWaitEvent(s_mlp, H->sev[1], 0));
     CK(cudaEventSynchronize(H->sev[1]));
     const unsigned n_gated = H->h_list_len[0], n_int = H->h_list_len[1];
+    const long long n_mlp = H->last_empty_skip ? (long long)(H->h_list_len[2] - H->h_list_len[1]) : total;
     const long long n_list = (long long)n_int + ((32 - (n_gated & 31u)) & 31u);
     if (n_int > 0) {
         rc = launch_trace(H, n_frames, n_list, nullptr, d_image, nullptr, nullptr, s_trace, false, nullptr, H->d_list,
@@ -2207,7 +2257,9 @@ static int render_surrogate_pass(Handle* H, const sirius_frame* frames, int n_fr
         if (rc != SIRIUS_OK) return rc;
     }
     CK(cudaEventRecord(H->fev[0], s_trace));
-    if ((rc = surrogate_launch(H, H->d_feat, total, H->d_mlp_out, s_mlp)) != SIRIUS_OK) return rc;
+    if ((rc = surrogate_launch(H, H->d_feat, n_mlp, H->d_mlp_out, s_mlp,
+                               H->last_empty_skip ? H->d_mlp_rows : nullptr)) != SIRIUS_OK)
+        return rc;
     CK(cudaEventRecord(H->fev[1], s_mlp));
     sur_shade_kernel<<<int((total + 255) / 256), 256, 0, s_mlp>>>(H->d_frames, n_frames, total, H->d_mlp_out, d_gate,
                                                                   H->d_flux, d_image, d_image_mlp);

@@ -97,7 +97,7 @@ __device__ __forceinline__ void epilogue_half_ts(uint32_t tmem, int H, const flo
 __global__ void __launch_bounds__(kThreads, 1)
     mlp_kernel_ts(const unsigned char* __restrict__ wimg, const float* __restrict__ feat, long long n,
                   float* __restrict__ out, int* err, unsigned long long* tile_counter,
-                  unsigned long long wait_limit_ns) {
+                  unsigned long long wait_limit_ns, const unsigned* __restrict__ rows) {
     extern __shared__ __align__(1024) unsigned char sm[];
     unsigned char* Wbuf = sm + kTsSmWbuf;
     unsigned char* W1s = sm + kTsSmW1;
@@ -156,7 +156,7 @@ __global__ void __launch_bounds__(kThreads, 1)
             const long long gr = row0 + r;
             if (gr < n) {
                 uint4 c0, c1;
-                pack_input_row(feat + gr * kIn, c0, c1);
+                pack_input_row(feat + (rows ? (long long)rows[gr] : gr) * kIn, c0, c1);
                 w = chunk == 0 ? c0 : c1;
             }
             *reinterpret_cast<uint4*>(Xs + packed_offset(r, chunk * 8, kInPad)) = w;
@@ -258,7 +258,7 @@ __global__ void __launch_bounds__(kThreads, 1)
             const long long gr = row0 + warp * 32 + lane;
             if (gr < n) {
                 const float* b5 = bias + 4 * kHid;
-                *reinterpret_cast<float4*>(out + gr * kOut) =
+                *reinterpret_cast<float4*>(out + (rows ? (long long)rows[gr] : gr) * kOut) =
                     make_float4(v[0] + b5[0], v[1] + b5[1], v[2] + b5[2], v[3] + b5[3]);
             }
         }

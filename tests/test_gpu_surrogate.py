@@ -121,6 +121,28 @@ def test_surrogate_render_against_the_integrator(engine):
     np.testing.assert_allclose(st.audit_rel_max, d.max() / img[a].max(), rtol=1e-6)
 
 
+def test_empty_pixels_skip_the_network(engine):
+    """Pixels whose coarse cell and its eight neighbours all predict no disk
+    crossing (gate 3) take intensity 0 without the per-pixel MLP, which runs only
+    on the pixels it shades and the audit pixels. Every other pixel equals the
+    render without the skip bit for bit (the network evaluates each row on its
+    own), and the integrator finds no light at the empty pixels (thin disk: a
+    ray that never crosses it carries none)."""
+    engine.surrogate_load(np.load(WEIGHTS))
+    fr = kerr_frame(512)
+    engine.configure(render_config(abi.PRECISION_MIXED))
+    _, full, _ = engine.trace_frames([fr], results=False)
+    img, _, gate, st = engine.render_surrogate([fr])
+    ref, _, gate_ref, _ = engine.render_surrogate([fr], config=abi.surrogate_config(empty_skip=-1))
+    empty = gate == 3
+    assert 0.2 < empty.mean() < 0.8, empty.mean()
+    assert not np.any(gate_ref == 3)
+    np.testing.assert_array_equal(gate[~empty], gate_ref[~empty])
+    np.testing.assert_array_equal(img[~empty], ref[~empty])
+    assert np.all(img[empty] == 0.0)
+    assert np.abs(full[empty]).max() <= 1e-3 * full.max(), np.abs(full[empty]).max() / full.max()
+
+
 def test_surrogate_integrates_frames_it_does_not_cover(engine):
     """A Morris-Thorne frame (outside the MLP's training set) is integrated in full."""
     engine.surrogate_load(np.load(WEIGHTS))
