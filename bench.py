@@ -387,7 +387,7 @@ def surrogate_config(abi, precision):
 
 def surrogate_leg(eng, abi, np, torch, dev, stream, side=SURROGATE_SIDE, reps=3, inner_gate=0.0):
     """Surrogate-gated rendering of the Kerr a = 0.9 frame at side^2 (gate +-0.3 M
-    around the critical curve, the inner-disk gate r_1 < 2.5 r_in from a coarse
+    around the critical curve, the inner-disk gate r_1 < 2.75 r_in from a coarse
     MLP pass on 8 x 8 pixel cells, 1 % audit rays; pixels whose coarse
     neighbourhood predicts no disk crossing take 0 without the per-pixel MLP)
     against the plain FP64 integrator on the same frame; CUDA events on the launch
@@ -445,7 +445,7 @@ def surrogate_leg(eng, abi, np, torch, dev, stream, side=SURROGATE_SIDE, reps=3,
     bf16_peak = float(peaks.get("bf16_tflops", 1590.0))
     return {"workload": f"kerr_a0.9_{side}x{side}_nt_disk_surrogate_gated", "mrays_per_s": n / (ms * 1e-3) / 1e6,
             "ms_per_frame": ms, "fp64_plain_ms": t64, "speedup_vs_fp64_plain": t64 / ms,
-            "gate_band_m": 0.3, "inner_gate_r_in": 2.5 if inner_gate == 0.0 else (None if inner_gate < 0 else inner_gate),
+            "gate_band_m": 0.3, "inner_gate_r_in": 2.75 if inner_gate == 0.0 else (None if inner_gate < 0 else inner_gate),
             "coarse_stride": 8, "coarse_mlp_rows": int(stats.coarse_rays),
             "audit_fraction": 0.01, "gated_fraction": float(np.mean(gate == 1)),
             "audit_fraction_measured": float(np.mean(gate == 2)), "integrated_rays": int(stats.integrated),

@@ -378,7 +378,7 @@ typedef struct {
     double gate_band;          /* half width of the gate around the critical curve, M (0.3) */
     double audit_fraction;     /* fraction of ungated rays also integrated (0.01) */
     uint32_t audit_seed;
-    float inner_gate;          /* r_1 bound of the inner-disk gate in units of r_in: 0 = 2.5, < 0 = off */
+    float inner_gate;          /* r_1 bound of the inner-disk gate in units of r_in: 0 = 2.75, < 0 = off */
     int32_t coarse_stride;     /* pixels per coarse cell side of the inner-disk gate: 0 = 8 */
     float audit_budget;        /* 0: the audit only reports */
     int32_t empty_skip;        /* 0 = on, < 0 = off: pixels whose coarse cell and its eight

@@ -134,7 +134,7 @@ class SurrogateStats(C.Structure):
 
 def surrogate_config(gate_band=0.3, audit_fraction=0.01, audit_seed=0, inner_gate=0.0, coarse_stride=0,
                      audit_budget=0.0, empty_skip=0):
-    """sirius_surrogate_config (inner_gate 0: 2.5 r_in, < 0: off; coarse_stride 0: 8; audit_budget 0: report
+    """sirius_surrogate_config (inner_gate 0: 2.75 r_in, < 0: off; coarse_stride 0: 8; audit_budget 0: report
     only; empty_skip 0: on, < 0: off)."""
     return SurrogateConfig(gate_band, audit_fraction, audit_seed, inner_gate, coarse_stride, audit_budget, empty_skip)
 
