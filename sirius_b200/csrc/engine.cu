@@ -1202,23 +1202,76 @@ unsigned long long train_wait_limit(const Handle* H) {
 }
 
 template <int BN, int E>
-void gemm_launch(const train::GemmArgs& g, cudaStream_t s) {
+void gemm_launch(const train::GemmArgs& g0, cudaStream_t s) {
+    train::GemmArgs g = g0;
+    // a TMA operand moves whole 64-wide K boxes: other K splits take the register path
+    if (g.K % train::kBK != 0 || g.k_per_cta % train::kBK != 0) g.tma_a = g.tma_b = 0;
     const dim3 grid((g.M + train::kBM - 1) / train::kBM, (g.N + BN - 1) / BN, (g.K + g.k_per_cta - 1) / g.k_per_cta);
-    train::gemm_kernel<BN, E><<<grid, train::kGemmThreads, train::GemmSmem<BN>::Bytes, s>>>(g);
+    if (g.tma_a || g.tma_b)
+        train::gemm_kernel<BN, E, true><<<grid, train::kGemmThreads, train::GemmSmem<BN>::Bytes, s>>>(g);
+    else
+        train::gemm_kernel<BN, E, false><<<grid, train::kGemmThreads, train::GemmSmem<BN>::Bytes, s>>>(g);
 }
 
 int train_set_attributes(Handle* H) {
     using namespace train;
-    CK(cudaFuncSetAttribute(gemm_kernel<256, kEpiHidden>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+    CK(cudaFuncSetAttribute(gemm_kernel<256, kEpiHidden, false>, cudaFuncAttributeMaxDynamicSharedMemorySize,
                             GemmSmem<256>::Bytes));
-    CK(cudaFuncSetAttribute(gemm_kernel<256, kEpiDHidden>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+    CK(cudaFuncSetAttribute(gemm_kernel<256, kEpiHidden, true>, cudaFuncAttributeMaxDynamicSharedMemorySize,
                             GemmSmem<256>::Bytes));
-    CK(cudaFuncSetAttribute(gemm_kernel<256, kEpiDWeight>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+    CK(cudaFuncSetAttribute(gemm_kernel<256, kEpiDHidden, false>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                            GemmSmem<256>::Bytes));
+    CK(cudaFuncSetAttribute(gemm_kernel<256, kEpiDHidden, true>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                            GemmSmem<256>::Bytes));
+    CK(cudaFuncSetAttribute(gemm_kernel<256, kEpiDWeight, false>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                            GemmSmem<256>::Bytes));
+    CK(cudaFuncSetAttribute(gemm_kernel<256, kEpiDWeight, true>, cudaFuncAttributeMaxDynamicSharedMemorySize,
                             GemmSmem<256>::Bytes));
     return SIRIUS_OK;
 }
 
 constexpr long long kTrainBf[4] = {train::kBfW1, train::kBfW2, train::kBfW3, train::kBfW4};
+
+// cuTensorMapEncodeTiled from the driver, through the runtime's entry-point query
+// (the library links no driver library)
+using EncodeTiledFn = CUresult (*)(CUtensorMap*, CUtensorMapDataType, cuuint32_t, void*, const cuuint64_t*,
+                                   const cuuint64_t*, const cuuint32_t*, const cuuint32_t*, CUtensorMapInterleave,
+                                   CUtensorMapSwizzle, CUtensorMapL2promotion, CUtensorMapFloatOOBfill);
+EncodeTiledFn encode_tiled() {
+    static EncodeTiledFn fn = [] {
+        void* p = nullptr;
+        cudaDriverEntryPointQueryResult q{};
+        if (cudaGetDriverEntryPoint("cuTensorMapEncodeTiled", &p, cudaEnableDefault, &q) != cudaSuccess ||
+            q != cudaDriverEntryPointSuccess)
+            return EncodeTiledFn(nullptr);
+        return reinterpret_cast<EncodeTiledFn>(p);
+    }();
+    return fn;
+}
+
+// A K-major BF16 operand (rows x K, row stride ld elements) as a TMA map of
+// 64 x box_rows boxes with the 128-byte swizzle (rows beyond `rows` read as
+// zeros). False when the driver has no encoder or refuses the map; the operand
+// then goes through registers.
+bool kmajor_map(CUtensorMap* m, const __nv_bfloat16* p, long long rows, long long K, long long ld, int box_rows) {
+    const EncodeTiledFn fn = encode_tiled();
+    if (!fn || K % 64 != 0 || (ld * 2) % 16 != 0 || (reinterpret_cast<uintptr_t>(p) & 15) != 0) return false;
+    const cuuint64_t dims[2] = {cuuint64_t(K), cuuint64_t(rows)};
+    const cuuint64_t strides[1] = {cuuint64_t(ld) * 2};
+    const cuuint32_t box[2] = {64u, cuuint32_t(box_rows)};
+    const cuuint32_t es[2] = {1u, 1u};
+    return fn(m, CU_TENSOR_MAP_DATA_TYPE_BFLOAT16, 2, const_cast<__nv_bfloat16*>(p), dims, strides, box, es,
+              CU_TENSOR_MAP_INTERLEAVE_NONE, CU_TENSOR_MAP_SWIZZLE_128B, CU_TENSOR_MAP_L2_PROMOTION_L2_128B,
+              CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE) == CUDA_SUCCESS;
+}
+
+// TMA for the K-major operands of K = 256 (the hidden and output layers' A and B,
+// the backward dH products' A); the 16-wide input layer and the M-major operands
+// stay on the register path
+void use_tma(train::GemmArgs& g, int bn, bool a, bool b) {
+    g.tma_a = a && g.a.kmajor && g.K % 64 == 0 && kmajor_map(&g.ta, g.a.p, g.a.rows, g.K, g.a.ld, train::kBM);
+    g.tma_b = b && g.b.kmajor && g.K % 64 == 0 && kmajor_map(&g.tb, g.b.p, g.b.rows, g.K, g.b.ld, bn);
+}
 
 // forward over the first `rows` gathered rows: Z_l, H_l (l = 1..4) and Y
 void train_forward(const Handle* H, TrainState* T, int rows, cudaStream_t s) {
@@ -1239,6 +1292,7 @@ void train_forward(const Handle* H, TrainState* T, int rows, cudaStream_t s) {
         g.e.ldz = kHid;
         g.e.h = T->h[l];
         g.e.ldh = kHid;
+        use_tma(g, 256, l > 0, l > 0);
         gemm_launch<256, kEpiHidden>(g, s);
     }
     g.a = Operand{T->h[3], kHid, 1, rows};
@@ -1250,6 +1304,7 @@ void train_forward(const Handle* H, TrainState* T, int rows, cudaStream_t s) {
     g.e.y = T->y;
     g.e.ldy = kOut;
     g.e.ny = kOut;
+    use_tma(g, 16, true, true);
     gemm_launch<16, kEpiOutput>(g, s);
 }
 
@@ -1273,6 +1328,7 @@ void train_backward(const Handle* H, TrainState* T, int rows, cudaStream_t s) {
     g.M = kHid; g.N = kOutPad; g.K = rows; g.k_per_cta = kpc;
     g.e = EpiArgs{};
     g.e.grad = T->grad + kOffW[4]; g.e.ldg = kHid; g.e.ng = kOut;
+    use_tma(g, 16, true, true);
     gemm_launch<16, kEpiDWeightT>(g, s);
     // dH4 = dY W5 -> dZ4 (and the b4 gradient)
     g.a = Operand{T->dy, kOutPad, 1, rows};
@@ -1280,6 +1336,7 @@ void train_backward(const Handle* H, TrainState* T, int rows, cudaStream_t s) {
     g.M = rows; g.N = kHid; g.K = g.k_per_cta = kOutPad;
     g.e = EpiArgs{};
     g.e.z = T->z[3]; g.e.ldz = kHid; g.e.h = T->dz[0]; g.e.ldh = kHid; g.e.grad = T->grad + kOffB[3];
+    use_tma(g, 256, true, true);
     gemm_launch<256, kEpiDHidden>(g, s);
     for (int l = 3; l >= 1; --l) {  // layers 4, 3, 2
         __nv_bfloat16* cur = T->dz[(3 - l) % 2];
@@ -1290,6 +1347,7 @@ void train_backward(const Handle* H, TrainState* T, int rows, cudaStream_t s) {
         g.M = kHid; g.N = kHid; g.K = rows; g.k_per_cta = kpc;
         g.e = EpiArgs{};
         g.e.grad = T->grad + kOffW[l]; g.e.ldg = kHid; g.e.ng = kHid;
+        use_tma(g, 256, true, true);
         gemm_launch<256, kEpiDWeight>(g, s);
         // dH_{l-1} = dZ_l W_l -> dZ_{l-1} (and the b_{l-1} gradient)
         g.a = Operand{cur, kHid, 1, rows};
@@ -1297,6 +1355,7 @@ void train_backward(const Handle* H, TrainState* T, int rows, cudaStream_t s) {
         g.M = rows; g.N = kHid; g.K = g.k_per_cta = kHid;
         g.e = EpiArgs{};
         g.e.z = T->z[l - 1]; g.e.ldz = kHid; g.e.h = nxt; g.e.ldh = kHid; g.e.grad = T->grad + kOffB[l - 1];
+        use_tma(g, 256, true, true);
         gemm_launch<256, kEpiDHidden>(g, s);
     }
     // dW1 = dZ1^T X0: the 2 x 5 input columns (high and low BF16 terms of each
@@ -1306,6 +1365,7 @@ void train_backward(const Handle* H, TrainState* T, int rows, cudaStream_t s) {
     g.M = kHid; g.N = kInPad; g.K = rows; g.k_per_cta = kpc;
     g.e = EpiArgs{};
     g.e.grad = T->grad + kOffW[0]; g.e.ldg = kIn; g.e.ng = 2 * kIn; g.e.fold = kIn;
+    use_tma(g, 16, true, true);
     gemm_launch<16, kEpiDWeight>(g, s);
 }
 

@@ -89,6 +89,32 @@ __device__ __forceinline__ void bulk_load(uint32_t dst, const void* src, uint32_
                  : "memory");
 }
 
+// 2-D tiled tensor copy (TMA) from global to this CTA's shared memory, no
+// multicast; tmap is the address of a CUtensorMap in kernel-parameter or global
+// memory, (x, y) the box's first element (x the innermost, in elements). The
+// copy's bytes complete on bar, which must expect them.
+__device__ __forceinline__ void tma_load_2d(uint32_t dst, const void* tmap, int x, int y, uint32_t bar) {
+    asm volatile(
+        "cp.async.bulk.tensor.2d.shared::cluster.global.mbarrier::complete_tx::bytes [%0], [%1, {%2, %3}], [%4];" ::"r"(
+            dst),
+        "l"(tmap), "r"(x), "r"(y), "r"(bar)
+        : "memory");
+}
+
+__device__ __forceinline__ void mbar_expect_tx(uint32_t bar, uint32_t bytes) {
+    asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;" ::"r"(bar), "r"(bytes) : "memory");
+}
+
+// UMMA shared-memory descriptor, K-major with the 128-byte swizzle that a TMA box
+// of 128-byte rows writes: rows of 128 B with their 16-byte pieces XOR-permuted by
+// row % 8, 8-row groups 1024 B apart (SBO), LBO 16 B, layout type 2 (bits 61-63),
+// version 1. The box starts 1024-byte aligned; a K step of 16 elements advances
+// the start address by 32 B.
+__device__ __forceinline__ uint64_t smem_desc_sw128(uint32_t addr) {
+    return uint64_t((addr & 0x3FFFF) >> 4) | (uint64_t(1) << 16) | (uint64_t(1024 >> 4) << 32) | (uint64_t(1) << 46) |
+           (uint64_t(2) << 61);
+}
+
 __device__ __forceinline__ void fence_async_smem() { asm volatile("fence.proxy.async.shared::cta;" ::: "memory"); }
 __device__ __forceinline__ void tc_fence_before() { asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory"); }
 __device__ __forceinline__ void tc_fence_after() { asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory"); }

@@ -41,6 +41,7 @@
 // rounded to BF16 as GEMM operands, the bias gradients are FP32 sums.
 #pragma once
 
+#include <cuda.h>  // CUtensorMap (a plain 128-byte descriptor type; nothing from the driver library is linked)
 #include <cuda_bf16.h>
 #include <cstdint>
 
@@ -103,6 +104,11 @@ struct GemmArgs {
     EpiArgs e;
     int* err;
     unsigned long long wait_limit_ns;
+    // K-major operands whose K is a multiple of 64 may come by TMA: ta (kBM x 64
+    // boxes) and tb (BN x 64 boxes) with the 128-byte swizzle; the others are staged
+    // through registers into the no-swizzle core-matrix layout
+    int tma_a, tma_b;
+    CUtensorMap ta, tb;
 };
 
 template <int BN>
@@ -111,7 +117,7 @@ struct GemmSmem {
     static constexpr int B = BN * kBK * 2;
     static constexpr int Stage = A + B;
     static constexpr int Bar = kStages * Stage;
-    static constexpr int Slot = Bar + 8 * (kStages + 1);
+    static constexpr int Slot = Bar + 8 * (2 * kStages + 1);  // per stage: MMAs done; TMA landed; accumulator
     static constexpr int Bytes = Slot + 16;
     static constexpr uint32_t Cols = BN < 32 ? 32 : BN;
 };
@@ -354,7 +360,9 @@ __device__ __forceinline__ void gemm_epilogue(const GemmArgs& g, uint32_t tmem, 
     }
 }
 
-template <int BN, int E>
+// TMA: compiled with the TMA operand path (the launch has an operand in g.ta or
+// g.tb); without it the register path alone, as compact as before.
+template <int BN, int E, bool TMA>
 __global__ void __launch_bounds__(kGemmThreads) gemm_kernel(const __grid_constant__ GemmArgs g) {
     using S = GemmSmem<BN>;
     extern __shared__ __align__(1024) unsigned char sm[];
@@ -362,9 +370,9 @@ __global__ void __launch_bounds__(kGemmThreads) gemm_kernel(const __grid_constan
     const int m0 = blockIdx.x * kBM, n0 = blockIdx.y * BN;
     const int kbeg = blockIdx.z * g.k_per_cta, kend = min(g.K, kbeg + g.k_per_cta);
     uint32_t* slot = reinterpret_cast<uint32_t*>(sm + S::Slot);
-    const uint32_t bar0 = smem_u32(sm + S::Bar), bar_acc = bar0 + 8 * kStages;
+    const uint32_t bar0 = smem_u32(sm + S::Bar), bar_acc = bar0 + 8 * kStages, bar_full0 = bar0 + 8 * (kStages + 1);
     if (tid == 0) {
-        for (int s = 0; s <= kStages; ++s) mbar_init(bar0 + 8 * s, 1);
+        for (int s = 0; s < 2 * kStages + 1; ++s) mbar_init(bar0 + 8 * s, 1);
         asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
     }
     if (warp == 0) {
@@ -377,14 +385,17 @@ __global__ void __launch_bounds__(kGemmThreads) gemm_kernel(const __grid_constan
     tc_fence_after();
     const uint32_t tmem = *slot;
     const uint32_t idesc = instr_desc(BN);
-    uint32_t ph = 0, pending = 0;  // per stage: wait parity, a commit not yet waited for
+    const bool ta = TMA && g.tma_a != 0, tb = TMA && g.tma_b != 0;
+    const uint32_t tx_bytes = (ta ? uint32_t(S::A) : 0u) + (tb ? uint32_t(S::B) : 0u);
+    uint32_t ph = 0, pending = 0;   // per stage: MMA-barrier wait parity, a commit not yet waited for
+    uint32_t ph_full = 0, in_flight = 0;  // per stage: TMA-barrier wait parity, a copy not yet waited for (thread 0)
     bool ok = true;
     int chunk = 0;
     constexpr int NA = 8, NB = BN >= 256 ? 16 : 8;  // this thread's share of a chunk (uint4)
     uint4 ra[NA], rb[NB];
     if (kbeg < kend) {
-        fetch_operand(ra, g.a, m0, kBM, kbeg, min(kBK, kend - kbeg));
-        fetch_operand(rb, g.b, n0, BN, kbeg, min(kBK, kend - kbeg));
+        if (!ta) fetch_operand(ra, g.a, m0, kBM, kbeg, min(kBK, kend - kbeg));
+        if (!tb) fetch_operand(rb, g.b, n0, BN, kbeg, min(kBK, kend - kbeg));
     }
     for (int k0 = kbeg; k0 < kend; k0 += kBK, ++chunk) {
         const int s = chunk % kStages;
@@ -398,20 +409,41 @@ __global__ void __launch_bounds__(kGemmThreads) gemm_kernel(const __grid_constan
         }
         unsigned char* As = sm + s * S::Stage;
         unsigned char* Bs = As + S::A;
-        stash_operand(As, ra, g.a, kBM, kw);
-        stash_operand(Bs, rb, g.b, BN, kw);
-        if (k0 + kBK < kend) {  // the next chunk's loads fly while this one multiplies
-            fetch_operand(ra, g.a, m0, kBM, k0 + kBK, min(kBK, kend - k0 - kBK));
-            fetch_operand(rb, g.b, n0, BN, k0 + kBK, min(kBK, kend - k0 - kBK));
+        if (tx_bytes && tid == 0) {  // this chunk's TMA operands
+            mbar_expect_tx(bar_full0 + 8 * s, tx_bytes);
+            if (ta) tma_load_2d(smem_u32(As), &g.ta, k0, m0, bar_full0 + 8 * s);
+            if (tb) tma_load_2d(smem_u32(Bs), &g.tb, k0, n0, bar_full0 + 8 * s);
+        }
+        if (tx_bytes) in_flight |= 1u << s;
+        if (!ta) stash_operand(As, ra, g.a, kBM, kw);
+        if (!tb) stash_operand(Bs, rb, g.b, BN, kw);
+        if (k0 + kBK < kend) {  // the next chunk's register loads fly while this one multiplies
+            if (!ta) fetch_operand(ra, g.a, m0, kBM, k0 + kBK, min(kBK, kend - k0 - kBK));
+            if (!tb) fetch_operand(rb, g.b, n0, BN, k0 + kBK, min(kBK, kend - k0 - kBK));
         }
         fence_async_smem();
         __syncthreads();
         if (tid == 0) {
-            tc_fence_after();
-            for (int t = 0; t < kw / 16; ++t)
-                mma_bf16(tmem, smem_desc(smem_u32(As) + t * 256, 1024), smem_desc(smem_u32(Bs) + t * 256, 1024), idesc,
-                         (chunk > 0 || t > 0) ? 1u : 0u);
-            mma_commit(bar0 + 8 * s);
+            if (tx_bytes) {
+                ok = mbar_wait(bar_full0 + 8 * s, (ph_full >> s) & 1u, g.wait_limit_ns);
+                ph_full ^= 1u << s;
+                in_flight &= ~(1u << s);
+            }
+            if (ok) {
+                tc_fence_after();
+                for (int t = 0; t < kw / 16; ++t) {
+                    const uint64_t ad = ta ? smem_desc_sw128(smem_u32(As) + t * 32)
+                                           : smem_desc(smem_u32(As) + t * 256, 1024);
+                    const uint64_t bd = tb ? smem_desc_sw128(smem_u32(Bs) + t * 32)
+                                           : smem_desc(smem_u32(Bs) + t * 256, 1024);
+                    mma_bf16(tmem, ad, bd, idesc, (chunk > 0 || t > 0) ? 1u : 0u);
+                }
+                mma_commit(bar0 + 8 * s);
+            }
+        }
+        if (tx_bytes) {  // thread 0's wait for the copies may have run out
+            ok = __syncthreads_and(ok);
+            if (!ok) break;
         }
         pending |= 1u << s;
     }
@@ -419,6 +451,9 @@ __global__ void __launch_bounds__(kGemmThreads) gemm_kernel(const __grid_constan
     bool drained = mbar_wait(bar_acc, 0, g.wait_limit_ns);
     for (int s = 0; s < kStages; ++s)  // and the stage barriers' last arrivals have landed
         if (pending & (1u << s)) drained = mbar_wait(bar0 + 8 * s, (ph >> s) & 1u, g.wait_limit_ns) && drained;
+    if (tid == 0)  // no copy may land after the CTA has left
+        for (int s = 0; s < kStages; ++s)
+            if (in_flight & (1u << s)) drained = mbar_wait(bar_full0 + 8 * s, (ph_full >> s) & 1u, g.wait_limit_ns) && drained;
     ok = __syncthreads_and(ok && drained);
     tc_fence_after();
     if (ok && chunk > 0) {
