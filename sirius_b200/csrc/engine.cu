@@ -1265,12 +1265,35 @@ bool kmajor_map(CUtensorMap* m, const __nv_bfloat16* p, long long rows, long lon
               CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE) == CUDA_SUCCESS;
 }
 
-// TMA for the K-major operands of K = 256 (the hidden and output layers' A and B,
-// the backward dH products' A); the 16-wide input layer and the M-major operands
-// stay on the register path
+// An MN-major BF16 operand (element (row, k) at p[k * ld + row]: K rows of ld
+// elements, `rows` of them used) as a TMA map of 64 (MN) x 64 (K) boxes with the
+// 128-byte swizzle.
+bool mnmajor_map(CUtensorMap* m, const __nv_bfloat16* p, long long rows, long long K, long long ld) {
+    const EncodeTiledFn fn = encode_tiled();
+    if (!fn || K % 64 != 0 || (ld * 2) % 16 != 0 || (reinterpret_cast<uintptr_t>(p) & 15) != 0) return false;
+    const cuuint64_t dims[2] = {cuuint64_t(rows), cuuint64_t(K)};
+    const cuuint64_t strides[1] = {cuuint64_t(ld) * 2};
+    const cuuint32_t box[2] = {64u, 64u};
+    const cuuint32_t es[2] = {1u, 1u};
+    return fn(m, CU_TENSOR_MAP_DATA_TYPE_BFLOAT16, 2, const_cast<__nv_bfloat16*>(p), dims, strides, box, es,
+              CU_TENSOR_MAP_INTERLEAVE_NONE, CU_TENSOR_MAP_SWIZZLE_128B, CU_TENSOR_MAP_L2_PROMOTION_L2_128B,
+              CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE) == CUDA_SUCCESS;
+}
+
+// TMA for the operands whose K is a multiple of 64: K-major ones as rows x 64
+// boxes, MN-major ones (the weight-gradient products' dZ^T and H, the dH products'
+// W) as 64 x 64 boxes when their tile extent (kBM, or BN) is a multiple of 64; the
+// 16-wide input layer and the 16-wide MN-major operands stay on the register path
+int tma_mode(const train::Operand& op, int tile_rows, long long K, CUtensorMap* m) {
+    if (K % 64 != 0) return 0;
+    if (op.kmajor) return kmajor_map(m, op.p, op.rows, K, op.ld, tile_rows) ? 1 : 0;
+    if (tile_rows % 64 != 0) return 0;
+    return mnmajor_map(m, op.p, op.rows, K, op.ld) ? 2 : 0;
+}
+
 void use_tma(train::GemmArgs& g, int bn, bool a, bool b) {
-    g.tma_a = a && g.a.kmajor && g.K % 64 == 0 && kmajor_map(&g.ta, g.a.p, g.a.rows, g.K, g.a.ld, train::kBM);
-    g.tma_b = b && g.b.kmajor && g.K % 64 == 0 && kmajor_map(&g.tb, g.b.p, g.b.rows, g.K, g.b.ld, bn);
+    g.tma_a = a ? tma_mode(g.a, train::kBM, g.K, &g.ta) : 0;
+    g.tma_b = b ? tma_mode(g.b, bn, g.K, &g.tb) : 0;
 }
 
 // forward over the first `rows` gathered rows: Z_l, H_l (l = 1..4) and Y

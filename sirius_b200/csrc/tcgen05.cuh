@@ -115,6 +115,15 @@ __device__ __forceinline__ uint64_t smem_desc_sw128(uint32_t addr) {
            (uint64_t(2) << 61);
 }
 
+// The same swizzle for an MN-major operand: each TMA box holds 64 K rows of 64
+// MN elements (128 B per K row, 8 KB per box), the operand's MN extent in boxes
+// 8 KB apart (LBO), 8-row K groups 1024 B apart (SBO); a K step of 16 advances the
+// start by two groups (2048 B).
+__device__ __forceinline__ uint64_t smem_desc_sw128_mn(uint32_t addr) {
+    return uint64_t((addr & 0x3FFFF) >> 4) | (uint64_t(8192 >> 4) << 16) | (uint64_t(1024 >> 4) << 32) |
+           (uint64_t(1) << 46) | (uint64_t(2) << 61);
+}
+
 __device__ __forceinline__ void fence_async_smem() { asm volatile("fence.proxy.async.shared::cta;" ::: "memory"); }
 __device__ __forceinline__ void tc_fence_before() { asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory"); }
 __device__ __forceinline__ void tc_fence_after() { asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory"); }

@@ -104,9 +104,10 @@ struct GemmArgs {
     EpiArgs e;
     int* err;
     unsigned long long wait_limit_ns;
-    // K-major operands whose K is a multiple of 64 may come by TMA: ta (kBM x 64
-    // boxes) and tb (BN x 64 boxes) with the 128-byte swizzle; the others are staged
-    // through registers into the no-swizzle core-matrix layout
+    // Operands may come by TMA with the 128-byte swizzle (tma_a / tma_b: 0 = staged
+    // through registers into the no-swizzle K-major core-matrix layout; 1 = K-major,
+    // one box of rows x 64 K per chunk; 2 = MN-major, rows / 64 boxes of 64 MN x 64 K
+    // per chunk, read by the tensor core as MN-major without a transpose)
     int tma_a, tma_b;
     CUtensorMap ta, tb;
 };
@@ -386,6 +387,8 @@ __global__ void __launch_bounds__(kGemmThreads) gemm_kernel(const __grid_constan
     const uint32_t tmem = *slot;
     const uint32_t idesc = instr_desc(BN);
     const bool ta = TMA && g.tma_a != 0, tb = TMA && g.tma_b != 0;
+    const bool ta_mn = ta && g.tma_a == 2, tb_mn = tb && g.tma_b == 2;
+    const uint32_t idesc_t = idesc | (ta_mn ? 1u << 15 : 0u) | (tb_mn ? 1u << 16 : 0u);
     const uint32_t tx_bytes = (ta ? uint32_t(S::A) : 0u) + (tb ? uint32_t(S::B) : 0u);
     uint32_t ph = 0, pending = 0;   // per stage: MMA-barrier wait parity, a commit not yet waited for
     uint32_t ph_full = 0, in_flight = 0;  // per stage: TMA-barrier wait parity, a copy not yet waited for (thread 0)
@@ -411,8 +414,18 @@ __global__ void __launch_bounds__(kGemmThreads) gemm_kernel(const __grid_constan
         unsigned char* Bs = As + S::A;
         if (tx_bytes && tid == 0) {  // this chunk's TMA operands
             mbar_expect_tx(bar_full0 + 8 * s, tx_bytes);
-            if (ta) tma_load_2d(smem_u32(As), &g.ta, k0, m0, bar_full0 + 8 * s);
-            if (tb) tma_load_2d(smem_u32(Bs), &g.tb, k0, n0, bar_full0 + 8 * s);
+            if (ta) {
+                if (ta_mn)
+                    for (int j = 0; j < kBM / 64; ++j) tma_load_2d(smem_u32(As) + j * 8192, &g.ta, m0 + 64 * j, k0, bar_full0 + 8 * s);
+                else
+                    tma_load_2d(smem_u32(As), &g.ta, k0, m0, bar_full0 + 8 * s);
+            }
+            if (tb) {
+                if (tb_mn)
+                    for (int j = 0; j < BN / 64; ++j) tma_load_2d(smem_u32(Bs) + j * 8192, &g.tb, n0 + 64 * j, k0, bar_full0 + 8 * s);
+                else
+                    tma_load_2d(smem_u32(Bs), &g.tb, k0, n0, bar_full0 + 8 * s);
+            }
         }
         if (tx_bytes) in_flight |= 1u << s;
         if (!ta) stash_operand(As, ra, g.a, kBM, kw);
@@ -432,11 +445,13 @@ __global__ void __launch_bounds__(kGemmThreads) gemm_kernel(const __grid_constan
             if (ok) {
                 tc_fence_after();
                 for (int t = 0; t < kw / 16; ++t) {
-                    const uint64_t ad = ta ? smem_desc_sw128(smem_u32(As) + t * 32)
-                                           : smem_desc(smem_u32(As) + t * 256, 1024);
-                    const uint64_t bd = tb ? smem_desc_sw128(smem_u32(Bs) + t * 32)
-                                           : smem_desc(smem_u32(Bs) + t * 256, 1024);
-                    mma_bf16(tmem, ad, bd, idesc, (chunk > 0 || t > 0) ? 1u : 0u);
+                    const uint64_t ad = ta_mn ? smem_desc_sw128_mn(smem_u32(As) + t * 2048)
+                                        : ta  ? smem_desc_sw128(smem_u32(As) + t * 32)
+                                              : smem_desc(smem_u32(As) + t * 256, 1024);
+                    const uint64_t bd = tb_mn ? smem_desc_sw128_mn(smem_u32(Bs) + t * 2048)
+                                        : tb  ? smem_desc_sw128(smem_u32(Bs) + t * 32)
+                                              : smem_desc(smem_u32(Bs) + t * 256, 1024);
+                    mma_bf16(tmem, ad, bd, idesc_t, (chunk > 0 || t > 0) ? 1u : 0u);
                 }
                 mma_commit(bar0 + 8 * s);
             }
