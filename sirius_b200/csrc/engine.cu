@@ -796,6 +796,7 @@ CfgDev make_cfg(const sirius_trace_config& c) {
     d.fshrink = float(d.shrink); d.fvol_j0 = float(d.vol_j0); d.fvol_aoj = float(d.vol_aoj);
     d.fvol_hz = float(d.vol_hz); d.fvol_s = float(d.vol_s);
     d.npair = (d.nbins + 1) / 2;
+    d.nu_desc = c.vol_spectral_index >= 0.0 ? 1 : 0;
     for (int b = 0; b < d.nbins; ++b) {
         const double nu = d.nbins == 1 ? c.nu_min : c.nu_min * std::pow(c.nu_max / c.nu_min, double(b) / (d.nbins - 1));
         // dtau_b = dtau nu_b^-s, applied as 2^(-dtau_b / ln 2)

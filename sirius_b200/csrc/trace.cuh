@@ -60,6 +60,7 @@ struct CfgDev {
     float fatol, frtol, fsafety, fgrow, fshrink, fvol_j0, fvol_aoj, fvol_hz, fvol_s;
     int npair;                       // bin pairs, (nbins + 1) / 2
     float2 nu_l2[SIRIUS_MAX_BINS / 2];  // -nu^-s / ln 2 of bins (2j, 2j + 1); 0 pads an odd last pair
+    int nu_desc;                        // 1: |nu_l2| falls along the bins (spectral index >= 0)
 };
 
 // ---------------------------------------------------------------------------

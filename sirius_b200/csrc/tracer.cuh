@@ -270,6 +270,10 @@ __device__ __forceinline__ void hermite_xyz_f(const float x0[3], const float dx[
     zs = x0[2] + (h10 * k0[3] + h01 * dx[2] + h11 * k1[3]);
 }
 
+// |b| (base-2 exponent of a bin's optical depth) below which the series alone
+// is the bin's 1 - e^-x: x = |b| ln 2 < 0.04
+constexpr float kSeriesOnlyB = 0.04f / 0.693147180559945309f;
+
 // Volumetric transfer over the accepted segment x0 -> x1 (affine length h):
 // Gauss-Legendre points on the step's cubic Hermite interpolant (the reference
 // marches the chord with midpoints, GTRC001A.cpp:943-958) over the part of the
@@ -335,11 +339,14 @@ __device__ __forceinline__ void volumetric_segment(const Params& P, const FrameD
     // of 2^-20 e^-x that covers the rounding of the hardware 2^b, so the series
     // wins wherever x^4/24 is below that bias, x < 0.06). The result lies in
     // (0, 1], with a relative error below 2e-5 at every x.
-    auto one_minus_exp = [&](float2 b) {
-        constexpr float L = 0.693147180559945309f, L2h = 0.240226506959100712f,  // ln 2, ln^2 2 / 2
-            L3s = 0.0555041086648215800f;                                          // ln^3 2 / 6
+    constexpr float L = 0.693147180559945309f, L2h = 0.240226506959100712f,  // ln 2, ln^2 2 / 2
+        L3s = 0.0555041086648215800f;                                          // ln^3 2 / 6
+    auto series = [&](float2 b) {
         const float2 u = fma2(b, p2(-L3s), p2(-L2h));
-        const float2 ser = mul2(b, fma2(b, u, p2(-L)));
+        return mul2(b, fma2(b, u, p2(-L)));
+    };
+    auto one_minus_exp = [&](float2 b) {
+        const float2 ser = series(b);
         const float2 e = fma2(make_float2(ex2_approx(b.x), ex2_approx(b.y)), p2(-(1.f - 0x1p-20f)), p2(1.f));
         return make_float2(fminf(ser.x, e.x), fminf(ser.y, e.y));
     };
@@ -369,11 +376,25 @@ __device__ __forceinline__ void volumetric_segment(const Params& P, const FrameD
         point_at(s, dts, Ss);
         if (dts == 0.f) continue;
         const float2 dt0 = p2(dts), S = p2(Ss);
+        // bins in order of falling optical depth (c.nu_desc): once a pair's deeper
+        // bin is below x = 0.04, where the minimum above is the series, every
+        // later pair takes the series alone (the same values, no exponentials)
+        int j = 0;
 #pragma unroll 1
-        for (int j = 0; j < c.npair; ++j) {
+        for (; j < c.npair; ++j) {
+            const float2 b = mul2(dt0, c.nu_l2[j]);
+            if (c.nu_desc && b.x > -kSeriesOnlyB) break;
             const float2 I = vol[j * bd];
             const float2 T = vol[(c.npair + j) * bd];  // transmittance e^-tau to the camera
-            const float2 om = one_minus_exp(mul2(dt0, c.nu_l2[j]));
+            const float2 om = one_minus_exp(b);
+            vol[j * bd] = fma2(mul2(T, S), om, I);
+            vol[(c.npair + j) * bd] = fma2(neg2(T), om, T);
+        }
+#pragma unroll 1
+        for (; j < c.npair; ++j) {
+            const float2 I = vol[j * bd];
+            const float2 T = vol[(c.npair + j) * bd];
+            const float2 om = series(mul2(dt0, c.nu_l2[j]));
             vol[j * bd] = fma2(mul2(T, S), om, I);
             vol[(c.npair + j) * bd] = fma2(neg2(T), om, T);
         }
