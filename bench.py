@@ -593,6 +593,9 @@ def profile_target(target, side, Engine, abi, np):
                                          max_steps=20000, precision=abi.PRECISION_FP64, enable_disk=0))
         b = eng.trace_beams([frame])
         print(target, side, b.size, float(b["magnification"].mean()))
+    elif target == "stress":
+        out = stress_leg(eng, abi, stride=max(4096 // side, 1))
+        print(target, out["workload"], f"rays={out['rays']}", f"steps_per_ray={out['steps_per_ray']:.1f}")
     else:
         eng.surrogate_load(np.load(SURROGATE_WEIGHTS))
         eng.configure(surrogate_config(abi, abi.PRECISION_MIXED))
@@ -618,8 +621,10 @@ def main():
                     help="register cap of the mixed trace kernel (0: the library default, 128)")
     ap.add_argument("--size", type=int, default=WIDTH,
                     help="frame side (default 1024, the workload; smaller sides are profiling cases)")
-    ap.add_argument("--profile-target", default=None, choices=["trace-mixed", "trace-fp64", "beams", "surrogate"],
-                    help="one untimed call of one leg at --size (an ncu target), then exit")
+    ap.add_argument("--profile-target", default=None,
+                    choices=["trace-mixed", "trace-fp64", "beams", "surrogate", "stress"],
+                    help="one untimed call of one leg at --size (an ncu target; for stress, --size is the sky "
+                         "map's width), then exit")
     args = ap.parse_args()
     if args.impl == "reference":
         run_reference(args)
