@@ -570,6 +570,8 @@ struct Handle {
     size_t gate_cap = 0;
     unsigned* d_block_counts = nullptr;  // per-block gated, audit and MLP-row counts, then offsets
     unsigned* d_mlp_rows = nullptr;      // pixels the per-pixel MLP evaluates (when empty pixels are skipped)
+    int2* d_blocks = nullptr;            // a batch launch's per-frame block table
+    size_t blocks_cap = 0;
     size_t mlp_rows_cap = 0;
     bool last_empty_skip = false;        // the last gate launch listed MLP rows (empty pixels skipped)
     size_t block_counts_cap = 0;
@@ -954,6 +956,32 @@ int launch_trace(Handle* H, int n_frames, long long total, sirius_ray_result* d_
     } else {
         grid = int((total + rays_per_block - 1) / rays_per_block);
     }
+    // a batch of frames launched one thread per ray: each block traces one pixel
+    // tile of one frame (edge tiles cut by the frame), and a launch for one family
+    // covers only that family's frames. Per launch i: frame entries [tab_off[i], tab_off[i+1])
+    // of the table (x: first block, y: frame), grid tab_grid[i].
+    std::vector<int2> tab;
+    int tab_off[4] = {0, 0, 0, 0}, tab_grid[3] = {grid, grid, grid};
+    const bool use_table = n_frames > 1 && !P.persistent && !d_list && !d_rays && !pair && !scratch &&
+                           int(H->frames_host.size()) == n_frames;
+    if (use_table) {
+        for (int i = 0; i < n_launches; ++i) {
+            tab_off[i] = int(tab.size());
+            int b0 = 0;
+            for (int f = 0; f < n_frames; ++f) {
+                const FrameDev& F = H->frames_host[size_t(f)];
+                if (launch_family[i] >= 0 && F.m.family != launch_family[i]) continue;
+                tab.push_back(make_int2(b0, f));
+                const long long rows = F.n_rays / F.width;
+                b0 += int(((F.width + tile_x - 1) / tile_x) * ((rows + tile_y - 1) / tile_y));
+            }
+            tab_grid[i] = b0;
+        }
+        tab_off[n_launches] = int(tab.size());
+        int rc = ensure(H, H->d_blocks, H->blocks_cap, tab.size());
+        if (rc != SIRIUS_OK) return rc;
+        CK(cudaMemcpyAsync(H->d_blocks, tab.data(), tab.size() * sizeof(int2), cudaMemcpyHostToDevice, st));
+    }
     // [0] queue cursor, [1..3] counters, [4] launch start: all start at zero
     CK(cudaMemsetAsync(S.queue, 0, 5 * sizeof(unsigned long long), st));
     CK(cudaMemsetAsync(S.status, 0, sizeof(int), st));
@@ -973,7 +1001,14 @@ int launch_trace(Handle* H, int n_frames, long long total, sirius_ray_result* d_
     }
     for (int i = 0; i < n_launches; ++i) {
         P.family = launch_family[i];
-        launch_fn[i]<<<grid, block, shmem_launch, st>>>(P);
+        int g = grid;
+        if (use_table) {
+            P.blocks = H->d_blocks + tab_off[i];
+            P.n_block_frames = tab_off[i + 1] - tab_off[i];
+            g = tab_grid[i];
+            if (g == 0) continue;
+        }
+        launch_fn[i]<<<g, block, shmem_launch, st>>>(P);
         CK(cudaGetLastError());
     }
     if (timed) CK(cudaEventRecord(H->ev[2], st));
@@ -1475,6 +1510,7 @@ int sirius_cuda_destroy(sirius_cuda_handle h) {
     cudaFree(H->d_coarse_feat); cudaFree(H->d_coarse_out);
     cudaFree(H->d_block_counts);
     cudaFree(H->d_mlp_rows);
+    cudaFree(H->d_blocks);
     cudaFree(H->d_pass_image); cudaFree(H->d_pass_spectra); cudaFree(H->d_pass_frames); cudaFree(H->d_prep);
     if (H->h_sur_frames) cudaFreeHost(H->h_sur_frames);
     if (H->h_list_len) cudaFreeHost(H->h_list_len);

@@ -40,6 +40,9 @@ struct Params {
     int persistent;
     int refill_threshold;
     int family;                           // >= 0: trace only the rays of frames of this family
+    const int2* blocks;                   // multi-frame launch: per frame of the launch, x: its first block,
+    int n_block_frames;                   // y: its index; a block traces one pixel tile of one frame
+                                          // (tile_ray's layout, edge tiles cut by the frame)
     int tiled;                            // one-frame launch over a frame whose width and row count are
                                           // multiples of the block's pixel tile: each warp traces an 8 x 4
                                           // pixel tile (tile_ray)
@@ -815,9 +818,9 @@ __device__ __forceinline__ int advance_post(const Params& P, Ray<MIXED>& s, bool
 // edge of the image (the disk's rim, the photon ring) where neighbouring
 // geodesics take different branches, and a block's warps, close together, end
 // at about the same time (a block holds its SM slot until its last warp ends).
-__device__ __forceinline__ long long tile_ray(int width) {
+__device__ __forceinline__ long long tile_ray(int width, int b) {
     const int nw = int(blockDim.x >> 5), across = nw >= 2 ? 2 : 1, bx = 8 * across, by = 4 * (nw / across);
-    const int bpr = width / bx, b = int(blockIdx.x), w = int(threadIdx.x >> 5), l = int(threadIdx.x & 31);
+    const int bpr = width / bx, w = int(threadIdx.x >> 5), l = int(threadIdx.x & 31);
     const int x = (b % bpr) * bx + (w % across) * 8 + (l & 7);
     const int y = (b / bpr) * by + (w / across) * 4 + (l >> 3);
     return (long long)y * width + x;
@@ -846,14 +849,38 @@ __device__ __forceinline__ void trace_body(const Params& P) {
     t_start = __shfl_sync(kFull, t_start, 0);
 
     if (!P.persistent) {
-        const long long gid = UNI && P.tiled ? tile_ray(P.f0.width) : (long long)blockIdx.x * blockDim.x + threadIdx.x;
-        const unsigned entry = (P.list && gid < P.total) ? P.list[gid] : 0u;
-        if (gid < P.total && entry != kListSkip) {
-            const long long idx = P.list ? (long long)entry : gid;
-            const int frame = P.n_frames > 1 ? find_frame(P.frames, P.n_frames, idx) : 0;
-            if (P.family < 0 || P.frames[frame].m.family == P.family) {
-                begin_ray<MIXED, FAM, UNI>(P, s, idx, frame, vol);
+        if (!UNI && P.blocks) {
+            // this block's frame (the last entry whose first block is at or below it)
+            int lo = 0, hi = P.n_block_frames - 1;
+            while (lo < hi) {
+                const int mid = (lo + hi + 1) >> 1;
+                if (P.blocks[mid].x <= int(blockIdx.x)) lo = mid;
+                else hi = mid - 1;
+            }
+            const int frame = P.blocks[lo].y, lb = int(blockIdx.x) - P.blocks[lo].x;
+            const FrameDev& F = P.frames[frame];
+            // the frame's pixels in tiles (tile_ray's layout), the last tile column
+            // and row cut by the frame's edges
+            const int rows = int(F.n_rays / F.width);
+            const int nw = int(blockDim.x >> 5), across = nw >= 2 ? 2 : 1, bx = 8 * across, by = 4 * (nw / across);
+            const int bpr = (F.width + bx - 1) / bx, w = int(threadIdx.x >> 5), l = int(threadIdx.x & 31);
+            const int x = (lb % bpr) * bx + (w % across) * 8 + (l & 7);
+            const int y = (lb / bpr) * by + (w / across) * 4 + (l >> 3);
+            if (x < F.width && y < rows && (P.family < 0 || F.m.family == P.family)) {
+                begin_ray<MIXED, FAM, UNI>(P, s, F.ray_offset + (long long)y * F.width + x, frame, vol);
                 alive = true;
+            }
+        } else {
+            const long long gid = UNI && P.tiled ? tile_ray(P.f0.width, int(blockIdx.x))
+                                                 : (long long)blockIdx.x * blockDim.x + threadIdx.x;
+            const unsigned entry = (P.list && gid < P.total) ? P.list[gid] : 0u;
+            if (gid < P.total && entry != kListSkip) {
+                const long long idx = P.list ? (long long)entry : gid;
+                const int frame = P.n_frames > 1 ? find_frame(P.frames, P.n_frames, idx) : 0;
+                if (P.family < 0 || P.frames[frame].m.family == P.family) {
+                    begin_ray<MIXED, FAM, UNI>(P, s, idx, frame, vol);
+                    alive = true;
+                }
             }
         }
         exhausted = true;
