@@ -936,12 +936,14 @@ int launch_trace(Handle* H, int n_frames, long long total, sirius_ray_result* d_
         CK(cudaFuncSetAttribute((const void*)launch_fn[0], cudaFuncAttributeMaxDynamicSharedMemorySize,
                                 int(shmem_launch)));
     // a one-frame launch of camera rays traces 8 x 4 pixel tiles per warp (tile_ray:
-    // blocks of 32, 64 and 128 threads cover 8 x 4, 16 x 4 and 16 x 8 pixels)
+    // blocks of 32, 64 and 128 threads cover 8 x 4, 16 x 4 and 16 x 8 pixels; tiles
+    // at the right and bottom edges are cut by the frame)
     const int tile_x = block >= 64 ? 16 : 8, tile_y = block == 128 ? 8 : 4;
     P.tiled = (n_frames == 1 && !d_list && !d_rays && !P.persistent && !pair && H->frame0.ray_offset == 0 &&
-               H->frame0.width > 0 && H->frame0.width % tile_x == 0 && total == H->frame0.n_rays &&
-               total % H->frame0.width == 0 && (total / H->frame0.width) % tile_y == 0)
+               H->frame0.width > 0 && total == H->frame0.n_rays && total % H->frame0.width == 0)
                   ? 1 : 0;
+    const long long tiled_blocks =
+        P.tiled ? ((H->frame0.width + tile_x - 1) / tile_x) * ((total / H->frame0.width + tile_y - 1) / tile_y) : 0;
     int grid;
     if (P.persistent) {
         int per_sm = c.blocks_per_sm;
@@ -954,7 +956,7 @@ int launch_trace(Handle* H, int n_frames, long long total, sirius_ray_result* d_
         const long long need = (total + block - 1) / block;
         if (grid > need) grid = int(std::max<long long>(need, 1));
     } else {
-        grid = int((total + rays_per_block - 1) / rays_per_block);
+        grid = P.tiled ? int(tiled_blocks) : int((total + rays_per_block - 1) / rays_per_block);
     }
     // a batch of frames launched one thread per ray: each block traces one pixel
     // tile of one frame (edge tiles cut by the frame), and a launch for one family

@@ -43,9 +43,8 @@ struct Params {
     const int2* blocks;                   // multi-frame launch: per frame of the launch, x: its first block,
     int n_block_frames;                   // y: its index; a block traces one pixel tile of one frame
                                           // (tile_ray's layout, edge tiles cut by the frame)
-    int tiled;                            // one-frame launch over a frame whose width and row count are
-                                          // multiples of the block's pixel tile: each warp traces an 8 x 4
-                                          // pixel tile (tile_ray)
+    int tiled;                            // one-frame launch in pixel tiles: each warp traces an 8 x 4
+                                          // pixel tile (tile_ray), edge tiles cut by the frame
     unsigned long long* clock0;           // launch start on the device clock (first warp stamps it)
     unsigned long long watchdog_ns;       // globaltimer bound for the whole launch, per warp
     CfgDev c;
@@ -818,12 +817,14 @@ __device__ __forceinline__ int advance_post(const Params& P, Ray<MIXED>& s, bool
 // edge of the image (the disk's rim, the photon ring) where neighbouring
 // geodesics take different branches, and a block's warps, close together, end
 // at about the same time (a block holds its SM slot until its last warp ends).
-__device__ __forceinline__ long long tile_ray(int width, int b) {
+// Tiles at the frame's right and bottom edges are cut by it: their pixels beyond
+// the edge return -1 (no ray).
+__device__ __forceinline__ long long tile_ray(int width, int rows, int b) {
     const int nw = int(blockDim.x >> 5), across = nw >= 2 ? 2 : 1, bx = 8 * across, by = 4 * (nw / across);
-    const int bpr = width / bx, w = int(threadIdx.x >> 5), l = int(threadIdx.x & 31);
+    const int bpr = (width + bx - 1) / bx, w = int(threadIdx.x >> 5), l = int(threadIdx.x & 31);
     const int x = (b % bpr) * bx + (w % across) * 8 + (l & 7);
     const int y = (b / bpr) * by + (w / across) * 4 + (l >> 3);
-    return (long long)y * width + x;
+    return x < width && y < rows ? (long long)y * width + x : -1;
 }
 
 // Persistent tracer. Dynamic shared memory: 2 * npair float2 per thread (volumetric bin pairs).
@@ -859,22 +860,16 @@ __device__ __forceinline__ void trace_body(const Params& P) {
             }
             const int frame = P.blocks[lo].y, lb = int(blockIdx.x) - P.blocks[lo].x;
             const FrameDev& F = P.frames[frame];
-            // the frame's pixels in tiles (tile_ray's layout), the last tile column
-            // and row cut by the frame's edges
-            const int rows = int(F.n_rays / F.width);
-            const int nw = int(blockDim.x >> 5), across = nw >= 2 ? 2 : 1, bx = 8 * across, by = 4 * (nw / across);
-            const int bpr = (F.width + bx - 1) / bx, w = int(threadIdx.x >> 5), l = int(threadIdx.x & 31);
-            const int x = (lb % bpr) * bx + (w % across) * 8 + (l & 7);
-            const int y = (lb / bpr) * by + (w / across) * 4 + (l >> 3);
-            if (x < F.width && y < rows && (P.family < 0 || F.m.family == P.family)) {
-                begin_ray<MIXED, FAM, UNI>(P, s, F.ray_offset + (long long)y * F.width + x, frame, vol);
+            const long long pix = tile_ray(F.width, int(F.n_rays / F.width), lb);
+            if (pix >= 0 && (P.family < 0 || F.m.family == P.family)) {
+                begin_ray<MIXED, FAM, UNI>(P, s, F.ray_offset + pix, frame, vol);
                 alive = true;
             }
         } else {
-            const long long gid = UNI && P.tiled ? tile_ray(P.f0.width, int(blockIdx.x))
+            const long long gid = UNI && P.tiled ? tile_ray(P.f0.width, int(P.f0.n_rays / P.f0.width), int(blockIdx.x))
                                                  : (long long)blockIdx.x * blockDim.x + threadIdx.x;
-            const unsigned entry = (P.list && gid < P.total) ? P.list[gid] : 0u;
-            if (gid < P.total && entry != kListSkip) {
+            const unsigned entry = (P.list && gid >= 0 && gid < P.total) ? P.list[gid] : 0u;
+            if (gid >= 0 && gid < P.total && entry != kListSkip) {
                 const long long idx = P.list ? (long long)entry : gid;
                 const int frame = P.n_frames > 1 ? find_frame(P.frames, P.n_frames, idx) : 0;
                 if (P.family < 0 || P.frames[frame].m.family == P.family) {
