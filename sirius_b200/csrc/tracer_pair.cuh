@@ -136,29 +136,6 @@ __device__ __forceinline__ void ks_rhs_pair(const MetricPair& m, const float2 xs
     }
 }
 
-// Dormand-Prince tableau as lane pairs (a, a), read with one 64-bit constant
-// load: the sliding-window form of DPTable (trace.cuh).
-struct DPTablePair {
-    float2 A[6][6];
-    float2 E[7];
-};
-#define SIRIUS_P2(v) {float(v), float(v)}
-static __constant__ DPTablePair kDPpair = {
-    {{SIRIUS_P2(1.0 / 5.0), SIRIUS_P2(3.0 / 40.0), SIRIUS_P2(44.0 / 45.0), SIRIUS_P2(19372.0 / 6561.0),
-      SIRIUS_P2(9017.0 / 3168.0), SIRIUS_P2(35.0 / 384.0)},
-     {SIRIUS_P2(9.0 / 40.0), SIRIUS_P2(-56.0 / 15.0), SIRIUS_P2(-25360.0 / 2187.0), SIRIUS_P2(-355.0 / 33.0),
-      SIRIUS_P2(0), SIRIUS_P2(0)},
-     {SIRIUS_P2(32.0 / 9.0), SIRIUS_P2(64448.0 / 6561.0), SIRIUS_P2(46732.0 / 5247.0), SIRIUS_P2(500.0 / 1113.0),
-      SIRIUS_P2(0), SIRIUS_P2(0)},
-     {SIRIUS_P2(-212.0 / 729.0), SIRIUS_P2(49.0 / 176.0), SIRIUS_P2(125.0 / 192.0), SIRIUS_P2(0), SIRIUS_P2(0),
-      SIRIUS_P2(0)},
-     {SIRIUS_P2(-5103.0 / 18656.0), SIRIUS_P2(-2187.0 / 6784.0), SIRIUS_P2(0), SIRIUS_P2(0), SIRIUS_P2(0),
-      SIRIUS_P2(0)},
-     {SIRIUS_P2(11.0 / 84.0), SIRIUS_P2(0), SIRIUS_P2(0), SIRIUS_P2(0), SIRIUS_P2(0), SIRIUS_P2(0)}},
-    {SIRIUS_P2(35.0 / 384.0 - 5179.0 / 57600.0), SIRIUS_P2(0), SIRIUS_P2(500.0 / 1113.0 - 7571.0 / 16695.0),
-     SIRIUS_P2(125.0 / 192.0 - 393.0 / 640.0), SIRIUS_P2(-2187.0 / 6784.0 + 92097.0 / 339200.0),
-     SIRIUS_P2(11.0 / 84.0 - 187.0 / 2100.0), SIRIUS_P2(-1.0 / 40.0)}};
-#undef SIRIUS_P2
 
 // The two rays' DP45 attempts (dp45_attempt<float> for a pair): stage inputs
 // x + h acc in packed FP32 with acc = sum_j a_sj k_j in a sliding window, the
