@@ -37,8 +37,8 @@ N_BINS = 16
 MEASURED_PEAKS = os.path.join(ROOT, "MEASURED_PEAKS.json")
 # DRAM bytes (read + write) per ray of the trace kernel, from one ncu capture of
 # the 512^2 case of this workload (profiles/trace_kernel_mixed_kerr512_full.md):
-# (3.64 + 1.33) MB / 262,144 rays; traffic grows with the ray count.
-TRAFFIC_BYTES_PER_RAY = 19.0
+# (4.01 + 1.49) MB / 262,144 rays; traffic grows with the ray count.
+TRAFFIC_BYTES_PER_RAY = 21.0
 
 
 def inclination_deg(seed=SEED):
