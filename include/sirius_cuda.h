@@ -298,7 +298,12 @@ int sirius_cuda_configure(sirius_cuda_handle handle, const sirius_trace_config* 
  * frame.ray_offset + y * width + x. Any output pointer may be NULL.
  *   image:   one float per pixel (bolometric intensity)
  *   spectra: n_bins floats per pixel (volumetric transfer), pixel-major
- * Host variant: host buffers, synchronous. */
+ * Host variant: host buffers, synchronous. When every output given is
+ * page-locked (cudaHostAlloc / cudaHostRegister) and one frame of at least
+ * 2048 pixel tiles (16 x 8) is traced with samples_per_pixel <= 1, the trace
+ * runs as up to 8 launches of consecutive tile rows on their own streams, and
+ * each piece's outputs are copied to the host while the later pieces trace;
+ * the outputs are bit for bit those of one launch. */
 int sirius_cuda_trace_frames(sirius_cuda_handle handle,
                              const sirius_frame* frames, int32_t n_frames,
                              sirius_ray_result* results, float* image, float* spectra);

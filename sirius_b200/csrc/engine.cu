@@ -74,6 +74,11 @@ constexpr int kDefaultMinBlocks = 2;       // up to 255 registers
 constexpr int kDefaultMinBlocksMixed = 4;  // 128 registers: mixed DP45
 constexpr int kDefaultMinBlocksFp64 = 3;   // 168 registers: FP64 DP45
 constexpr int kDefaultRaysPerThread = 1;   // rays per thread of mixed DP45 over Kerr-Schild frames
+// a one-frame trace into host memory of at least kPieceMinBlocks tiles runs as
+// up to kMaxPieces launches of tile rows, each piece's rays copied to the host
+// while the next pieces trace
+constexpr int kMaxPieces = 8;
+constexpr long long kPieceMinBlocks = 2048;
 
 // A kernel specialised for one metric family carries only that family's
 // right-hand side (a smaller loop body and register set); kAnyFamily
@@ -580,7 +585,24 @@ struct Handle {
     cudaStream_t sur_stream[2] = {};
     cudaEvent_t fev[4] = {};  // trace done, MLP done, shade done, join
     TrainState* train = nullptr;  // surrogate training state (sirius_cuda_train_init)
+    // a one-frame trace into host memory in row pieces: the trace streams of
+    // pieces 1.. (piece 0 runs on the caller's stream), then the copy stream;
+    // events: fork, one per piece, copies done
+    cudaStream_t piece_stream[kMaxPieces] = {};
+    cudaEvent_t piece_ev[kMaxPieces + 2] = {};
 };
+
+// Outputs of a one-frame trace in host memory (the host entry point); done: the
+// launch copied them itself, piece by piece, and `copied` completes with the copies.
+struct HostOut {
+    sirius_ray_result* results;
+    float* image;
+    float* spectra;
+    int nb;
+    bool done;
+    cudaEvent_t copied;
+};
+
 
 int fail(Handle* h, int code, const std::string& msg) {
     if (h) h->last_error = msg;
@@ -842,9 +864,17 @@ int validate_config(Handle* H, const sirius_trace_config& c) {
 // Launch the tracer over [0, total) of already-uploaded frames.
 
 
+int ensure_piece_streams(Handle* H) {
+    if (H->piece_stream[kMaxPieces - 1]) return SIRIUS_OK;
+    for (auto& q : H->piece_stream) CK(cudaStreamCreateWithFlags(&q, cudaStreamNonBlocking));
+    for (auto& e : H->piece_ev) CK(cudaEventCreateWithFlags(&e, cudaEventDisableTiming));
+    return SIRIUS_OK;
+}
+
 int launch_trace(Handle* H, int n_frames, long long total, sirius_ray_result* d_results, float* d_image,
                  float* d_spectra, const sirius_camera_ray* d_rays, cudaStream_t st, bool timed,
-                 const LaunchScratch* scratch = nullptr, const unsigned* d_list = nullptr, bool flux_ready = false) {
+                 const LaunchScratch* scratch = nullptr, const unsigned* d_list = nullptr, bool flux_ready = false,
+                 HostOut* host = nullptr) {
     const sirius_trace_config& c = H->cfg;
     if (!scratch && (c.precision == SIRIUS_PRECISION_MIXED)) {
         const int rc = ensure(H, H->d_flux, H->flux_cap, size_t(n_frames) * kFluxTable);
@@ -1001,6 +1031,53 @@ int launch_trace(Handle* H, int n_frames, long long total, sirius_ray_result* d_
         }
         P.flux = S.flux;
     }
+    // A one-frame tiled launch whose outputs go to host memory traces its tile
+    // rows in pieces, each on its own stream (all queued at once, so the next
+    // piece's blocks fill the SMs as the previous piece drains, as in one launch),
+    // and copies each piece's rays (whole pixel rows, contiguous in every output)
+    // to the host on a copy stream while the next pieces trace. The kernel and
+    // each ray's result are those of the single launch.
+    const int tiles_x = P.tiled ? (H->frame0.width + tile_x - 1) / tile_x : 1;
+    const int tile_rows = P.tiled ? int(tiled_blocks / tiles_x) : 0;
+    const int n_pieces = (host && P.tiled && n_launches == 1 && tiled_blocks >= kPieceMinBlocks)
+                             ? std::min(kMaxPieces, tile_rows) : 0;
+    if (n_pieces > 1) {
+        const int rc = ensure_piece_streams(H);
+        if (rc != SIRIUS_OK) return rc;
+        cudaStream_t cs = H->piece_stream[kMaxPieces - 1];
+        cudaEvent_t* E = H->piece_ev;
+        CK(cudaEventRecord(E[0], st));
+        for (int k = 1; k < n_pieces; ++k) CK(cudaStreamWaitEvent(H->piece_stream[k - 1], E[0], 0));
+        const long long width = H->frame0.width, rows = total / width;
+        const size_t nb = size_t(host->nb);
+        P.family = launch_family[0];
+        for (int k = 0; k < n_pieces; ++k) {
+            const int t0 = int((long long)tile_rows * k / n_pieces), t1 = int((long long)tile_rows * (k + 1) / n_pieces);
+            cudaStream_t sk = k == 0 ? st : H->piece_stream[k - 1];
+            P.block0 = t0 * tiles_x;
+            launch_fn[0]<<<(t1 - t0) * tiles_x, block, shmem_launch, sk>>>(P);
+            CK(cudaGetLastError());
+            CK(cudaEventRecord(E[1 + k], sk));
+            CK(cudaStreamWaitEvent(cs, E[1 + k], 0));
+            const long long r0 = (long long)t0 * tile_y * width;
+            const long long r1 = std::min<long long>((long long)t1 * tile_y, rows) * width;
+            const size_t n = size_t(r1 - r0);
+            if (host->results)
+                CK(cudaMemcpyAsync(host->results + r0, d_results + r0, n * sizeof(sirius_ray_result),
+                                   cudaMemcpyDeviceToHost, cs));
+            if (host->image)
+                CK(cudaMemcpyAsync(host->image + r0, d_image + r0, n * sizeof(float), cudaMemcpyDeviceToHost, cs));
+            if (host->spectra && nb)
+                CK(cudaMemcpyAsync(host->spectra + size_t(r0) * nb, d_spectra + size_t(r0) * nb, n * nb * sizeof(float),
+                                   cudaMemcpyDeviceToHost, cs));
+        }
+        P.block0 = 0;
+        for (int k = 1; k < n_pieces; ++k) CK(cudaStreamWaitEvent(st, E[1 + k], 0));
+        CK(cudaEventRecord(E[n_pieces + 1], cs));
+        host->copied = E[n_pieces + 1];
+        host->done = true;
+        n_launches = 0;  // the pieces were the launch
+    }
     for (int i = 0; i < n_launches; ++i) {
         P.family = launch_family[i];
         int g = grid;
@@ -1016,7 +1093,7 @@ int launch_trace(Handle* H, int n_frames, long long total, sirius_ray_result* d_
     if (timed) CK(cudaEventRecord(H->ev[2], st));
     H->stats.grid_blocks = grid;
     H->stats.block_size = block;
-    H->stats.kernel_launches = n_launches + extra_launches;
+    H->stats.kernel_launches = (n_pieces > 1 ? n_pieces : n_launches) + extra_launches;
     return SIRIUS_OK;
 }
 
@@ -1064,9 +1141,11 @@ int prepare_passes(Handle* H, long long total, cudaStream_t st) {
 // 1/g^2. prepared: the pass descriptors are already on the device
 // (sirius_cuda_prepare_frames), so only stream work is issued.
 int launch_frames(Handle* H, int n_frames, long long total, sirius_ray_result* d_results, float* d_image,
-                  float* d_spectra, cudaStream_t st, bool timed, bool prepared = false) {
+                  float* d_spectra, cudaStream_t st, bool timed, bool prepared = false, HostOut* host = nullptr) {
     const int g = samples_grid(H->cfg);
-    if (g == 1) return launch_trace(H, n_frames, total, d_results, d_image, d_spectra, nullptr, st, timed);
+    if (g == 1)
+        return launch_trace(H, n_frames, total, d_results, d_image, d_spectra, nullptr, st, timed, nullptr, nullptr,
+                            false, host);
     if (d_results) return fail(H, SIRIUS_ERR_INVALID_ARGUMENT, "per-ray results need samples_per_pixel <= 1");
     if (!d_image && !d_spectra) return SIRIUS_OK;
     const int nb = H->cfg.enable_volumetric ? std::min(H->cfg.n_bins, SIRIUS_MAX_BINS) : 0;
@@ -1520,6 +1599,8 @@ int sirius_cuda_destroy(sirius_cuda_handle h) {
     for (auto& e : H->sev) if (e) cudaEventDestroy(e);
     for (auto& e : H->fev) if (e) cudaEventDestroy(e);
     for (auto& q : H->sur_stream) if (q) cudaStreamDestroy(q);
+    for (auto& e : H->piece_ev) if (e) cudaEventDestroy(e);
+    for (auto& q : H->piece_stream) if (q) cudaStreamDestroy(q);
     for (auto& e : H->ev) if (e) cudaEventDestroy(e);
     if (H->stream) cudaStreamDestroy(H->stream);
     delete H;
@@ -1579,12 +1660,29 @@ int sirius_cuda_trace_frames(sirius_cuda_handle h, const sirius_frame* frames, i
     if (results && (rc = ensure(H, H->d_results, H->results_cap, size_t(total))) != SIRIUS_OK) return rc;
     if (image && (rc = ensure(H, H->d_image, H->image_cap, size_t(total))) != SIRIUS_OK) return rc;
     if (spectra && nb && (rc = ensure(H, H->d_spectra, H->spectra_cap, size_t(total) * nb)) != SIRIUS_OK) return rc;
+    // copies overlap the trace only into page-locked memory (a copy into pageable
+    // memory returns once it is done, which would hold back the next piece's launch)
+    auto page_locked = [](const void* p) {
+        cudaPointerAttributes a{};
+        if (cudaPointerGetAttributes(&a, p) != cudaSuccess) {
+            cudaGetLastError();
+            return false;
+        }
+        return a.type == cudaMemoryTypeHost;
+    };
+    const bool overlap = (!results || page_locked(results)) && (!image || page_locked(image)) &&
+                         (!(spectra && nb) || page_locked(spectra));
+    HostOut host{results, image, (spectra && nb) ? spectra : nullptr, nb, false, nullptr};
     rc = launch_frames(H, n_frames, total, results ? H->d_results : nullptr, image ? H->d_image : nullptr,
-                       (spectra && nb) ? H->d_spectra : nullptr, st, true);
+                       (spectra && nb) ? H->d_spectra : nullptr, st, true, false, overlap ? &host : nullptr);
     if (rc != SIRIUS_OK) return rc;
-    if (results) CK(cudaMemcpyAsync(results, H->d_results, size_t(total) * sizeof(sirius_ray_result), cudaMemcpyDeviceToHost, st));
-    if (image) CK(cudaMemcpyAsync(image, H->d_image, size_t(total) * sizeof(float), cudaMemcpyDeviceToHost, st));
-    if (spectra && nb) CK(cudaMemcpyAsync(spectra, H->d_spectra, size_t(total) * nb * sizeof(float), cudaMemcpyDeviceToHost, st));
+    if (host.done) {  // copied piece by piece during the trace
+        CK(cudaStreamWaitEvent(st, host.copied, 0));
+    } else {
+        if (results) CK(cudaMemcpyAsync(results, H->d_results, size_t(total) * sizeof(sirius_ray_result), cudaMemcpyDeviceToHost, st));
+        if (image) CK(cudaMemcpyAsync(image, H->d_image, size_t(total) * sizeof(float), cudaMemcpyDeviceToHost, st));
+        if (spectra && nb) CK(cudaMemcpyAsync(spectra, H->d_spectra, size_t(total) * nb * sizeof(float), cudaMemcpyDeviceToHost, st));
+    }
     CK(cudaEventRecord(H->ev[3], st));
     return finish_stats(H, st, total, true);
 }

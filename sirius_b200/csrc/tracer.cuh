@@ -45,6 +45,7 @@ struct Params {
                                           // (tile_ray's layout, edge tiles cut by the frame)
     int tiled;                            // one-frame launch in pixel tiles: each warp traces an 8 x 4
                                           // pixel tile (tile_ray), edge tiles cut by the frame
+    int block0;                           // tiled launch: the tile of block 0 (a launch of a run of tile rows)
     unsigned long long* clock0;           // launch start on the device clock (first warp stamps it)
     unsigned long long watchdog_ns;       // globaltimer bound for the whole launch, per warp
     CfgDev c;
@@ -866,7 +867,7 @@ __device__ __forceinline__ void trace_body(const Params& P) {
                 alive = true;
             }
         } else {
-            const long long gid = UNI && P.tiled ? tile_ray(P.f0.width, int(P.f0.n_rays / P.f0.width), int(blockIdx.x))
+            const long long gid = UNI && P.tiled ? tile_ray(P.f0.width, int(P.f0.n_rays / P.f0.width), int(blockIdx.x) + P.block0)
                                                  : (long long)blockIdx.x * blockDim.x + threadIdx.x;
             const unsigned entry = (P.list && gid >= 0 && gid < P.total) ? P.list[gid] : 0u;
             if (gid >= 0 && gid < P.total && entry != kListSkip) {
