@@ -142,6 +142,19 @@ __global__ void __launch_bounds__(kThreads, 1)
     uint32_t ph_a = 0, ph_b = 0, ph_tma = 0;
     bool tma_pending = false, ok = true;
     long long tile = *next_s;
+    // this thread's input row (tid / 2) of the tile to come, gathered a tile ahead
+    // so that the gather's latency (row index, then the row) overlaps the current
+    // tile's layers; rows past n read as zeros, which pack to zero operands
+    const int in_r = tid >> 1, in_chunk = tid & 1;
+    float xin[kIn];
+    auto fetch_row = [&](long long t) {
+        const long long gr = t * kTileM + in_r;
+        const bool live = t < ntiles && gr < n;
+        const float* f = feat + (live ? (rows ? (long long)rows[gr] : gr) : 0LL) * kIn;
+#pragma unroll
+        for (int k = 0; k < kIn; ++k) xin[k] = live ? f[k] : 0.f;
+    };
+    fetch_row(tile);
     if (tid == 0 && tile < ntiles) bulk_load(smem_u32(Wbuf), wimg, kBigBytes, bar_tma);
     tma_pending = tile < ntiles;
     const uint32_t idesc128 = instr_desc(128), idesc16 = instr_desc(kOutPad);
@@ -151,19 +164,14 @@ __global__ void __launch_bounds__(kThreads, 1)
         __syncthreads();  // every thread has read *next_s
         if (tid == 32) *next_s = (long long)atomicAdd(tile_counter, 1ull);
         {  // input tile: 128 rows x 16 BF16 (features 0..4 as two BF16 terms, zero padding)
-            const int r = tid >> 1, chunk = tid & 1;
-            uint4 w = make_uint4(0, 0, 0, 0);
-            const long long gr = row0 + r;
-            if (gr < n) {
-                uint4 c0, c1;
-                pack_input_row(feat + (rows ? (long long)rows[gr] : gr) * kIn, c0, c1);
-                w = chunk == 0 ? c0 : c1;
-            }
-            *reinterpret_cast<uint4*>(Xs + packed_offset(r, chunk * 8, kInPad)) = w;
+            uint4 c0, c1;
+            pack_input_row(xin, c0, c1);
+            *reinterpret_cast<uint4*>(Xs + packed_offset(in_r, in_chunk * 8, kInPad)) = in_chunk == 0 ? c0 : c1;
         }
         fence_async_smem();
         __syncthreads();
         const long long next = *next_s;
+        fetch_row(next);  // in flight during this tile's layers
         // layer 1 (A from shared memory, K = 16): two N-halves
         if (tid == 0) {
             tc_fence_after();
