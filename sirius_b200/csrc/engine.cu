@@ -585,22 +585,22 @@ struct Handle {
     cudaStream_t sur_stream[2] = {};
     cudaEvent_t fev[4] = {};  // trace done, MLP done, shade done, join
     TrainState* train = nullptr;  // surrogate training state (sirius_cuda_train_init)
-    // a one-frame trace into host memory in row pieces: the trace streams of
-    // pieces 1.. (piece 0 runs on the caller's stream), then the copy stream;
-    // events: fork, one per piece, copies done
-    cudaStream_t piece_stream[kMaxPieces] = {};
-    cudaEvent_t piece_ev[kMaxPieces + 2] = {};
+    // a one-frame trace into host memory in row pieces: the streams of pieces
+    // 1.. (piece 0 runs on the caller's stream); events: [0] fork, [1 + k] piece k
+    // traced, [1 + kMaxPieces + k] piece k copied to the host
+    cudaStream_t piece_stream[kMaxPieces - 1] = {};
+    cudaEvent_t piece_ev[2 * kMaxPieces + 1] = {};
 };
 
 // Outputs of a one-frame trace in host memory (the host entry point); done: the
-// launch copied them itself, piece by piece, and `copied` completes with the copies.
+// launch copied them itself, piece by piece, and the stream it was given is
+// ordered after the copies.
 struct HostOut {
     sirius_ray_result* results;
     float* image;
     float* spectra;
     int nb;
     bool done;
-    cudaEvent_t copied;
 };
 
 
@@ -865,7 +865,7 @@ int validate_config(Handle* H, const sirius_trace_config& c) {
 
 
 int ensure_piece_streams(Handle* H) {
-    if (H->piece_stream[kMaxPieces - 1]) return SIRIUS_OK;
+    if (H->piece_stream[kMaxPieces - 2]) return SIRIUS_OK;
     for (auto& q : H->piece_stream) CK(cudaStreamCreateWithFlags(&q, cudaStreamNonBlocking));
     for (auto& e : H->piece_ev) CK(cudaEventCreateWithFlags(&e, cudaEventDisableTiming));
     return SIRIUS_OK;
@@ -1035,8 +1035,9 @@ int launch_trace(Handle* H, int n_frames, long long total, sirius_ray_result* d_
     // rows in pieces, each on its own stream (all queued at once, so the next
     // piece's blocks fill the SMs as the previous piece drains, as in one launch),
     // and copies each piece's rays (whole pixel rows, contiguous in every output)
-    // to the host on a copy stream while the next pieces trace. The kernel and
-    // each ray's result are those of the single launch.
+    // to the host on the piece's stream as soon as it is traced, while the other
+    // pieces trace (pieces end out of order: the rows of the shadow and the disk
+    // cost most). The kernel and each ray's result are those of the single launch.
     const int tiles_x = P.tiled ? (H->frame0.width + tile_x - 1) / tile_x : 1;
     const int tile_rows = P.tiled ? int(tiled_blocks / tiles_x) : 0;
     const int n_pieces = (host && P.tiled && n_launches == 1 && tiled_blocks >= kPieceMinBlocks)
@@ -1044,7 +1045,6 @@ int launch_trace(Handle* H, int n_frames, long long total, sirius_ray_result* d_
     if (n_pieces > 1) {
         const int rc = ensure_piece_streams(H);
         if (rc != SIRIUS_OK) return rc;
-        cudaStream_t cs = H->piece_stream[kMaxPieces - 1];
         cudaEvent_t* E = H->piece_ev;
         CK(cudaEventRecord(E[0], st));
         for (int k = 1; k < n_pieces; ++k) CK(cudaStreamWaitEvent(H->piece_stream[k - 1], E[0], 0));
@@ -1058,23 +1058,21 @@ int launch_trace(Handle* H, int n_frames, long long total, sirius_ray_result* d_
             launch_fn[0]<<<(t1 - t0) * tiles_x, block, shmem_launch, sk>>>(P);
             CK(cudaGetLastError());
             CK(cudaEventRecord(E[1 + k], sk));
-            CK(cudaStreamWaitEvent(cs, E[1 + k], 0));
             const long long r0 = (long long)t0 * tile_y * width;
             const long long r1 = std::min<long long>((long long)t1 * tile_y, rows) * width;
             const size_t n = size_t(r1 - r0);
             if (host->results)
                 CK(cudaMemcpyAsync(host->results + r0, d_results + r0, n * sizeof(sirius_ray_result),
-                                   cudaMemcpyDeviceToHost, cs));
+                                   cudaMemcpyDeviceToHost, sk));
             if (host->image)
-                CK(cudaMemcpyAsync(host->image + r0, d_image + r0, n * sizeof(float), cudaMemcpyDeviceToHost, cs));
+                CK(cudaMemcpyAsync(host->image + r0, d_image + r0, n * sizeof(float), cudaMemcpyDeviceToHost, sk));
             if (host->spectra && nb)
                 CK(cudaMemcpyAsync(host->spectra + size_t(r0) * nb, d_spectra + size_t(r0) * nb, n * nb * sizeof(float),
-                                   cudaMemcpyDeviceToHost, cs));
+                                   cudaMemcpyDeviceToHost, sk));
+            CK(cudaEventRecord(E[1 + kMaxPieces + k], sk));
         }
         P.block0 = 0;
         for (int k = 1; k < n_pieces; ++k) CK(cudaStreamWaitEvent(st, E[1 + k], 0));
-        CK(cudaEventRecord(E[n_pieces + 1], cs));
-        host->copied = E[n_pieces + 1];
         host->done = true;
         n_launches = 0;  // the pieces were the launch
     }
@@ -1091,6 +1089,8 @@ int launch_trace(Handle* H, int n_frames, long long total, sirius_ray_result* d_
         CK(cudaGetLastError());
     }
     if (timed) CK(cudaEventRecord(H->ev[2], st));
+    // the pieces' copies: after the end event, which times the kernels alone
+    for (int k = 1; k < n_pieces; ++k) CK(cudaStreamWaitEvent(st, H->piece_ev[1 + kMaxPieces + k], 0));
     H->stats.grid_blocks = grid;
     H->stats.block_size = block;
     H->stats.kernel_launches = (n_pieces > 1 ? n_pieces : n_launches) + extra_launches;
@@ -1672,13 +1672,11 @@ int sirius_cuda_trace_frames(sirius_cuda_handle h, const sirius_frame* frames, i
     };
     const bool overlap = (!results || page_locked(results)) && (!image || page_locked(image)) &&
                          (!(spectra && nb) || page_locked(spectra));
-    HostOut host{results, image, (spectra && nb) ? spectra : nullptr, nb, false, nullptr};
+    HostOut host{results, image, (spectra && nb) ? spectra : nullptr, nb, false};
     rc = launch_frames(H, n_frames, total, results ? H->d_results : nullptr, image ? H->d_image : nullptr,
                        (spectra && nb) ? H->d_spectra : nullptr, st, true, false, overlap ? &host : nullptr);
     if (rc != SIRIUS_OK) return rc;
-    if (host.done) {  // copied piece by piece during the trace
-        CK(cudaStreamWaitEvent(st, host.copied, 0));
-    } else {
+    if (!host.done) {  // else copied piece by piece during the trace
         if (results) CK(cudaMemcpyAsync(results, H->d_results, size_t(total) * sizeof(sirius_ray_result), cudaMemcpyDeviceToHost, st));
         if (image) CK(cudaMemcpyAsync(image, H->d_image, size_t(total) * sizeof(float), cudaMemcpyDeviceToHost, st));
         if (spectra && nb) CK(cudaMemcpyAsync(spectra, H->d_spectra, size_t(total) * nb * sizeof(float), cudaMemcpyDeviceToHost, st));
